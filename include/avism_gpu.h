@@ -1,0 +1,186 @@
+/*
+ * avism_gpu.h -- C-ABI of the B200 (sm_100a) AVISM void-finding library.
+ *
+ * The Fortran driver of AVISM (src/avism.f90) keeps reading config/voids.dat and
+ * the particle files and keeps writing the catalogue; it calls these entry points
+ * through an ISO_C_BINDING interface module in place of the Fortran routines named
+ * in each comment.  All functions return an int status (AVISM_OK == 0) and never
+ * exit or throw.  avism_gpu_last_error() returns the message of the last failure.
+ *
+ * Conventions (match the reference's arrays one to one):
+ *   - 3D grids are Fortran column-major, x fastest.  "inner" grids are NX^3
+ *     (indices 1..NX); "ext" grids cover LOW1..LOW2 per axis (periodic ghost
+ *     shell of NPLUS cells, src/avism.f90:780-812), NE = LOW2-LOW1+1 per side.
+ *   - index outputs keep the reference's values: 1-based particle/cube ids,
+ *     grid indices in LOW1..LOW2.
+ *   - every array argument may be a host pointer or a CUDA device pointer of the
+ *     context's device; the library detects which and copies host arrays.
+ *   - a context is bound to one GPU, is not re-entrant, and retains no caller
+ *     pointer after a call returns.
+ */
+#ifndef AVISM_GPU_H
+#define AVISM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+enum {
+    AVISM_OK = 0,
+    AVISM_ERR_ARG = 1,          /* invalid argument (size, null, range)          */
+    AVISM_ERR_CUDA = 2,         /* CUDA runtime error                            */
+    AVISM_ERR_OOM = 3,          /* device or host allocation failed             */
+    AVISM_ERR_NVOID_MAX = 4,    /* 'NVOID > NVOID_MAX!! Increase NVOID_MAX'      */
+    AVISM_ERR_OUT_OF_BOX = 5,   /* 'Particles outside the bounding box! Check L0!' */
+    AVISM_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up            */
+    AVISM_ERR_NO_DEVICE = 7,    /* no CUDA device / wrong architecture           */
+    AVISM_ERR_UNSUPPORTED = 8,  /* option not implemented by this library        */
+    AVISM_ERR_INTERNAL = 9      /* internal consistency check failed             */
+};
+
+/* ---- parameters: POD mirror of config/voids.dat (src/avism.f90:173-254) -- */
+typedef struct avism_params {
+    int32_t nx;                 /* NCOX=NCOY=NCOZ: cells per side of this level   */
+    int32_t periodic;           /* FLAG_PERIOD (0/1)                              */
+    float   lado0;              /* LADO0, box side [cMpc]                         */
+    float   ache;               /* h                                              */
+    float   omega0;             /* Omega_m                                        */
+    float   zeta;               /* redshift of the snapshot (ZETA)                */
+    int32_t nvoid_max;          /* NVOID_MAX                                      */
+    float   dens_thre;          /* DENS_THRE  (centres)                           */
+    float   dens_thre2;         /* DENS_THRE2 (edges)                             */
+    float   grad_thre;          /* GRAD_THRE                                      */
+    float   div_thre;           /* DIV_THRE                                       */
+    float   rmin;               /* RMIN [cMpc]                                    */
+    float   rmin_sub;           /* RMIN_SUB [cMpc]                                */
+    int32_t kneighbours;        /* KNEIGHBOURS                                    */
+    int32_t flag_vel_interp;    /* 0 TSC, 1 SPH                                   */
+    int32_t flag_dens_interp;   /* 0 TSC, 1 SPH                                   */
+    int32_t level;              /* IR                                             */
+    int32_t levmin;             /* LEVMIN                                         */
+    int32_t learned;            /* 0: plain search, 1: learned proposals          */
+    int32_t reserved[7];
+} avism_params;
+
+/* ---- level geometry (MALLA + PBC extension, src/avism.f90:780-865) ------ */
+typedef struct avism_grid {
+    int32_t nx, nplus, low1, low2, ne;   /* ne = low2-low1+1                       */
+    int32_t rad_lo, rad_hi;              /* index range held by the RADX array     */
+    float   dx;                          /* DX = RADX(2)-RADX(1)                   */
+    float   rx1;                         /* RADX(1)                                */
+    float   lado;                        /* LADO = LADO0-LADO0/NX                  */
+    float   lado0plus;                   /* LADO0PLUS (periodic extended box)      */
+    float   rete, rote, hte;             /* scale factor, background density, H(z) */
+} avism_grid;
+
+/* ---- VOIDFIND outputs: the cube arrays of module COMMONDATA ------------- */
+/* Each array holds at least nvoid_max entries; entry i is cube i+1.         */
+typedef struct avism_cubes {
+    int32_t *inicio_x, *final_x, *inicio_y, *final_y, *inicio_z, *final_z;
+    int32_t *icx, *icy, *icz;
+    int32_t *father;
+    float   *vol;
+    float   *rini_x, *rfin_x, *rini_y, *rfin_y, *rini_z, *rfin_z;
+} avism_cubes;
+
+/* ---- MERGE_VOID + post-processing outputs (src/avism.f90:1738-1973) ------ */
+/* Arrays hold nvoid entries (one per cube, entry i is cube id i+1); marca is  */
+/* the ext grid (NE^3 int32) and may be NULL.                                 */
+typedef struct avism_voids {
+    int32_t *indice;            /* cube ids by volume, largest first (INDICE)    */
+    int32_t *uvoid;             /* -1 main void, 0 removed, >0 owner id          */
+    int32_t *ncellv;            /* cells of each main void (inner grid)          */
+    float   *volnew, *req;      /* volume [cMpc^3], equivalent radius            */
+    float   *xc, *yc, *zc;      /* centre = cell of max divergence               */
+    float   *gxc, *gyc, *gzc;   /* volume-weighted geometrical centre            */
+    float   *eps, *ip;          /* ellipticity, inverse porosity                 */
+    float   *umean, *mtot;      /* mean rho/rho_mean, mass [Msun]                */
+    int32_t *marca;             /* ext grid of void ids (nullable)               */
+    int32_t nvoid2;             /* voids after merging                           */
+    int32_t nvoidt;             /* voids after post-processing (NVOIDT)          */
+    double  volt_clean;         /* total comoving volume in voids                */
+} avism_voids;
+
+typedef struct avism_gpu_ctx avism_gpu_ctx;
+
+/* ---- context ------------------------------------------------------------- */
+int avism_gpu_create(avism_gpu_ctx **out, int device);
+int avism_gpu_destroy(avism_gpu_ctx *ctx);
+const char *avism_gpu_last_error(const avism_gpu_ctx *ctx);
+/* Device-side time of the last call's stages (ms); n = number of entries. */
+int avism_gpu_stage_times(const avism_gpu_ctx *ctx, double *ms, int n);
+
+/* ---- a1: level grid, replaces MALLA (src/grid.f90:3-76) and the PBC block
+ *      src/avism.f90:780-865.  radx receives RADX(rad_lo..rad_hi); pass NULL
+ *      to query the geometry only.  Host only, no GPU needed.                 */
+int avism_gpu_grid_setup(const avism_params *p, avism_grid *g, float *radx);
+
+/* ---- a3/a4: k nearest neighbours, replaces knn_search (src/kdtree.f90:504-540)
+ *      Neighbours of each query sorted by (squared distance, particle index);
+ *      idx is 1-based, dist = sqrt(squared distance).  box_l > 0 selects the
+ *      periodic minimum-image distance of src/kdtree.f90:1441-1465.           */
+int avism_gpu_knn(avism_gpu_ctx *ctx, int64_t n, const float *x, const float *y,
+                  const float *z, float box_l, int64_t nq, const float *qx,
+                  const float *qy, const float *qz, int32_t k, int64_t *idx,
+                  float *dist);
+
+/* ---- a5-a10: particles to grid.  Replaces PPART_DENS, VVEL_INTERP_SPH_VW,
+ *      FILL_H_ZEROS, H_DISTANCE, DDENS_INTERP_SPH (src/particles.f90:276-929)
+ *      and DENS_INTERP_TSC / VEL_INTERP_TSC (src/particles.f90:16-271), called
+ *      at src/avism.f90:1159-1245.  Inputs in the units READ_BINARY_PART_1
+ *      leaves (src/reader.f90:441-457).  u_mass: mass per inner cell (the
+ *      U1DMCO of DDENS/TSC before normalisation); u2..u4: velocity grids;
+ *      hpart / part_dens: per particle, nullable.  smask: inner NX^3, nullable
+ *      (all ones).                                                              */
+int avism_gpu_particles_to_grid(avism_gpu_ctx *ctx, const avism_params *p, int64_t n,
+                                const float *x, const float *y, const float *z,
+                                const float *vx, const float *vy, const float *vz,
+                                const float *m, const int8_t *smask,
+                                float *u_mass, float *u2, float *u3, float *u4,
+                                float *hpart, float *part_dens);
+
+/* ---- a11-a13: density normalisation (src/avism.f90:1249-1250, 1384-1411),
+ *      DIVER_UNIFORM (src/divergence.f90:2-50) and REAL_MAKE_PERIODIC
+ *      (src/num.f90:89-133).  Outputs the ext grids U1CO and DIVERCO and the
+ *      mean density MEANDENS [Msun/Mpc^3].                                      */
+int avism_gpu_fields(avism_gpu_ctx *ctx, const avism_params *p, const float *u_mass,
+                     const float *u2, const float *u3, const float *u4,
+                     float *u1co_ext, float *diverco_ext, float *meandens);
+
+/* ---- a14-a17: MARK_ALL + VOIDFIND (src/voidfinding.f90:13-713).  Inputs are
+ *      the ext grids; smask_ext / marcap_ext are nullable (all ones / all -1,
+ *      i.e. the first level of a particle run); reqp has one entry per parent
+ *      void (nullable when marcap_ext is NULL).  Fills cubes[0..nvoid-1].       */
+int avism_gpu_voidfind(avism_gpu_ctx *ctx, const avism_params *p, const float *u1co_ext,
+                       const float *diverco_ext, const int8_t *smask_ext,
+                       const int32_t *marcap_ext, const float *reqp,
+                       avism_cubes *cubes, int32_t *nvoid);
+
+/* ---- a18: INDEXX (src/num.f90:2-84): the Numerical Recipes index sort,
+ *      reproducing its exact permutation of equal keys.  indx is 1-based.      */
+int avism_gpu_indexx(avism_gpu_ctx *ctx, int32_t n, const float *arr, int32_t *indx);
+
+/* ---- a18-a24: volume ordering, MERGE_VOID (src/voidfinding.f90:718-999) and
+ *      the post-processing of src/avism.f90:1797-1973 (NCELL_MIN and RMIN
+ *      filters, VOID_SHAPE, SIMPLE_CONNECTION_FAST, VOID_PERIODIC, global
+ *      properties).  u1co_ext: the U1CO grid; meandens from avism_gpu_fields.   */
+int avism_gpu_merge_post(avism_gpu_ctx *ctx, const avism_params *p, int32_t nvoid,
+                         const avism_cubes *cubes, const float *u1co_ext,
+                         float meandens, avism_voids *out);
+
+/* ---- whole level on the device: particles in, catalogue out (a5-a24).
+ *      Intermediate grids stay in HBM; only the catalogue arrays come back.    */
+int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n,
+                        const float *x, const float *y, const float *z,
+                        const float *vx, const float *vy, const float *vz,
+                        const float *m, avism_cubes *cubes, int32_t *nvoid,
+                        avism_voids *voids, float *meandens);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AVISM_GPU_H */

@@ -1,0 +1,176 @@
+"""ctypes wrapper of the C oracle (oracle/liboracle.so) -- test infrastructure.
+
+Every function restates a reference routine; see the C sources for the
+file:line each follows.  Arrays are numpy, grids Fortran column-major and
+flattened (x fastest), index outputs keep the reference's values.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from avism_b200._abi import (AVISM_OK, AvismGrid, AvismParams, Cubes, Params, Voids,
+                             STATUS_NAMES, ptr)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the committed Makefile."""
+    if force or not os.path.exists(_LIB):
+        subprocess.run(["make", "-C", _HERE, "-B" if force else "liboracle.so"],
+                       check=True, capture_output=True)
+    return _LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(_LIB)
+    return _lib
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def _chk(st):
+    if st != AVISM_OK:
+        raise OracleError(f"oracle status {st} ({STATUS_NAMES.get(st, '?')})")
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def grid_setup(p: Params):
+    g = AvismGrid()
+    pc = p.to_c()
+    _chk(lib().orc_grid_setup(C.byref(pc), C.byref(g), None))
+    rad = np.zeros(g.rad_hi - g.rad_lo + 1, np.float32)
+    _chk(lib().orc_grid_setup(C.byref(pc), C.byref(g), ptr(rad, C.c_float)))
+    return g, rad
+
+
+def knn(x, y, z, qx, qy, qz, k, box_l=0.0):
+    x, y, z, qx, qy, qz = map(_f32, (x, y, z, qx, qy, qz))
+    nq = len(qx)
+    idx = np.zeros(nq * k, np.int64)
+    dist = np.zeros(nq * k, np.float32)
+    f = lib().orc_knn
+    f.argtypes = [C.c_int64] + [C.POINTER(C.c_float)] * 3 + [C.c_float, C.c_int64] + \
+        [C.POINTER(C.c_float)] * 3 + [C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_float)]
+    _chk(f(len(x), ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float), box_l, nq,
+           ptr(qx, C.c_float), ptr(qy, C.c_float), ptr(qz, C.c_float), k,
+           ptr(idx, C.c_int64), ptr(dist, C.c_float)))
+    return idx.reshape(nq, k), dist.reshape(nq, k)
+
+
+def particles_to_grid(p: Params, x, y, z, vx, vy, vz, m, smask=None):
+    x, y, z, vx, vy, vz, m = map(_f32, (x, y, z, vx, vy, vz, m))
+    n = len(x)
+    nc = p.nx ** 3
+    out = [np.zeros(nc, np.float32) for _ in range(4)]
+    h = np.zeros(n, np.float32)
+    pd = np.zeros(n, np.float32)
+    f = lib().orc_particles_to_grid
+    f.argtypes = [C.c_void_p, C.c_int64] + [C.POINTER(C.c_float)] * 7 + \
+        [C.c_void_p] + [C.POINTER(C.c_float)] * 6
+    pc = p.to_c()
+    sm = None if smask is None else np.ascontiguousarray(smask, np.int8)
+    _chk(f(C.byref(pc), n, *(ptr(a, C.c_float) for a in (x, y, z, vx, vy, vz, m)),
+           None if sm is None else sm.ctypes.data, *(ptr(a, C.c_float) for a in out),
+           ptr(h, C.c_float), ptr(pd, C.c_float)))
+    return dict(u_mass=out[0], u2=out[1], u3=out[2], u4=out[3], hpart=h, part_dens=pd)
+
+
+def fields(p: Params, u_mass, u2, u3, u4):
+    g, _ = grid_setup(p)
+    ne3 = g.ne ** 3
+    u1 = np.zeros(ne3, np.float32)
+    dv = np.zeros(ne3, np.float32)
+    md = C.c_float()
+    f = lib().orc_fields
+    f.argtypes = [C.c_void_p] + [C.POINTER(C.c_float)] * 6 + [C.POINTER(C.c_float)]
+    pc = p.to_c()
+    _chk(f(C.byref(pc), *(ptr(_f32(a), C.c_float) for a in (u_mass, u2, u3, u4)),
+           ptr(u1, C.c_float), ptr(dv, C.c_float), C.byref(md)))
+    return u1, dv, md.value
+
+
+def diver_uniform(nx, dx, v2, v3, v4, periodic):
+    out = np.zeros(nx ** 3, np.float32)
+    f = lib().orc_diver_uniform
+    f.argtypes = [C.c_int, C.c_float] + [C.POINTER(C.c_float)] * 3 + [C.c_int, C.POINTER(C.c_float)]
+    _chk(f(nx, dx, *(ptr(_f32(a), C.c_float) for a in (v2, v3, v4)), periodic,
+           ptr(out, C.c_float)))
+    return out
+
+
+def voidfind(p: Params, u1co_ext, diverco_ext, smask_ext=None, marcap_ext=None, reqp=None):
+    g, _ = grid_setup(p)
+    ne3 = g.ne ** 3
+    u1 = _f32(u1co_ext)
+    dv = _f32(diverco_ext)
+    flags = np.zeros(ne3, np.uint8)
+    cap = int(min(p.nvoid_max, max(ne3 // 8, 1024)))
+    cubes = Cubes(cap)
+    nvoid = C.c_int32()
+    nc = C.c_int32()
+    order = np.zeros(ne3, np.int32)
+    f = lib().orc_voidfind
+    f.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_void_p,
+                  C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.c_void_p,
+                  C.POINTER(C.c_int32), C.c_void_p]
+    pc = p.to_c()
+    sm = None if smask_ext is None else np.ascontiguousarray(smask_ext, np.int8)
+    mp = None if marcap_ext is None else np.ascontiguousarray(marcap_ext, np.int32)
+    rq = None if reqp is None else _f32(reqp)
+    # capacity guard: the oracle writes at most nvoid_max cubes
+    pc.nvoid_max = min(p.nvoid_max, cap)
+    st = f(C.byref(pc), ptr(u1, C.c_float), ptr(dv, C.c_float),
+           None if sm is None else sm.ctypes.data, None if mp is None else mp.ctypes.data,
+           None if rq is None else rq.ctypes.data, C.byref(cubes.c), C.byref(nvoid),
+           flags.ctypes.data, C.byref(nc), order.ctypes.data)
+    if st == 4 and cap < p.nvoid_max:
+        raise OracleError("oracle cube buffer too small for this test grid")
+    _chk(st)
+    return dict(cubes=cubes.view(nvoid.value), nvoid=nvoid.value, flags=flags,
+                ncand=nc.value, order=order[:nc.value].copy())
+
+
+def indexx(arr):
+    arr = _f32(arr)
+    out = np.zeros(len(arr), np.int32)
+    f = lib().orc_indexx
+    f.argtypes = [C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_int32)]
+    _chk(f(len(arr), ptr(arr, C.c_float), ptr(out, C.c_int32)))
+    return out
+
+
+def merge_post(p: Params, nvoid, cubes: dict, u1co_ext, meandens):
+    g, _ = grid_setup(p)
+    cb = Cubes.from_dict(cubes, nvoid)
+    vo = Voids(nvoid, g.ne)
+    f = lib().orc_merge_post
+    f.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_float), C.c_float, C.c_void_p]
+    pc = p.to_c()
+    _chk(f(C.byref(pc), nvoid, C.byref(cb.c), ptr(_f32(u1co_ext), C.c_float),
+           C.c_float(meandens), C.byref(vo.c)))
+    return vo.view(nvoid)
+
+
+def run_level(p: Params, parts: dict):
+    """particles -> catalogue on the CPU (a5-a24)."""
+    g, _ = grid_setup(p)
+    pg = particles_to_grid(p, *(parts[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")))
+    u1, dv, md = fields(p, pg["u_mass"], pg["u2"], pg["u3"], pg["u4"])
+    vf = voidfind(p, u1, dv)
+    cat = merge_post(p, vf["nvoid"], vf["cubes"], u1, md)
+    return dict(grid=pg, u1co=u1, diverco=dv, meandens=md, vf=vf, cat=cat)
