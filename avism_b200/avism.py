@@ -1,0 +1,189 @@
+"""Host-side mirror of the reference's routines for the AVISM hot path.
+
+Each method keeps the name of the Fortran routine it replaces and calls the
+C-ABI of libavism_gpu.so (include/avism_gpu.h); arrays are numpy (host) or any
+object exposing a CUDA device pointer through ``data_ptr()`` (torch tensors).
+Errors raise AvismError carrying the status code and, where the reference
+stops, its STOP text.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._abi import (AVISM_OK, STATUS_NAMES, STOP_TEXT, AvismGrid, Cubes, Params, Voids, ptr)
+
+
+class AvismError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        self.code = code
+        text = STOP_TEXT.get(code, "")
+        super().__init__(f"avism status {code} ({STATUS_NAMES.get(code, '?')}): {msg}"
+                         + (f" [{text}]" if text and text not in msg else ""))
+
+
+def _vp(a):
+    """void* of a numpy array (host) or a tensor-like with data_ptr() (device)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    if isinstance(a, np.ndarray):
+        assert a.flags.c_contiguous
+        return C.c_void_p(a.ctypes.data)
+    raise TypeError(type(a))
+
+
+def _f32(a):
+    if hasattr(a, "data_ptr"):
+        return a
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def grid_setup(p: Params):
+    """MALLA (src/grid.f90:3-76) + the PBC extension (src/avism.f90:780-865)."""
+    lib = _lib.load()
+    g = AvismGrid()
+    pc = p.to_c()
+    st = lib.avism_gpu_grid_setup(C.byref(pc), C.byref(g), None)
+    if st != AVISM_OK:
+        raise AvismError(st, "grid setup")
+    rad = np.zeros(g.rad_hi - g.rad_lo + 1, np.float32)
+    lib.avism_gpu_grid_setup(C.byref(pc), C.byref(g), _vp(rad))
+    return g, rad
+
+
+class AvismGPU:
+    """One context on one GPU (avism_gpu_create)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        st = self.lib.avism_gpu_create(C.byref(h), device)
+        if st != AVISM_OK:
+            raise AvismError(st, f"cannot open CUDA device {device} (sm_100 required)")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.avism_gpu_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _chk(self, st):
+        if st != AVISM_OK:
+            msg = self.lib.avism_gpu_last_error(self.h)
+            raise AvismError(st, msg.decode() if msg else "")
+
+    def stage_times(self):
+        buf = (C.c_double * 16)()
+        n = self.lib.avism_gpu_stage_times(self.h, buf, 16)
+        return [buf[i] for i in range(min(n, 16))]
+
+    # ---- kNN (knn_search, src/kdtree.f90:504-540) ----------------------------
+    def knn_search(self, x, y, z, qx, qy, qz, k, box_l=0.0):
+        x, y, z, qx, qy, qz = map(_f32, (x, y, z, qx, qy, qz))
+        nq = len(qx)
+        idx = np.zeros(nq * k, np.int64)
+        dist = np.zeros(nq * k, np.float32)
+        self._chk(self.lib.avism_gpu_knn(self.h, len(x), _vp(x), _vp(y), _vp(z), box_l, nq,
+                                         _vp(qx), _vp(qy), _vp(qz), k, _vp(idx), _vp(dist)))
+        return idx.reshape(nq, k), dist.reshape(nq, k)
+
+    # ---- PPART_DENS / VVEL_INTERP_SPH_VW / FILL_H_ZEROS / DDENS_INTERP_SPH / TSC
+    def particles_to_grid(self, p: Params, parts: dict, smask=None):
+        a = {k: _f32(parts[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        n = len(a["x"])
+        nc = p.nx ** 3
+        out = [np.zeros(nc, np.float32) for _ in range(4)]
+        h = np.zeros(n, np.float32)
+        pd = np.zeros(n, np.float32)
+        sm = None if smask is None else np.ascontiguousarray(smask, np.int8)
+        pc = p.to_c()
+        self._chk(self.lib.avism_gpu_particles_to_grid(
+            self.h, C.byref(pc), n, *(_vp(a[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")),
+            _vp(sm), *(_vp(o) for o in out), _vp(h), _vp(pd)))
+        return dict(u_mass=out[0], u2=out[1], u3=out[2], u4=out[3], hpart=h, part_dens=pd)
+
+    # ---- normalisation, DIVER_UNIFORM, REAL_MAKE_PERIODIC ---------------------
+    def fields(self, p: Params, u_mass, u2, u3, u4):
+        g, _ = grid_setup(p)
+        ne3 = g.ne ** 3
+        u1 = np.zeros(ne3, np.float32)
+        dv = np.zeros(ne3, np.float32)
+        md = C.c_float()
+        pc = p.to_c()
+        self._chk(self.lib.avism_gpu_fields(self.h, C.byref(pc), *(_vp(_f32(v)) for v in (u_mass, u2, u3, u4)),
+                                            _vp(u1), _vp(dv), C.byref(md)))
+        return u1, dv, md.value
+
+    # ---- MARK_ALL + VOIDFIND --------------------------------------------------
+    def voidfind(self, p: Params, u1co_ext, diverco_ext, smask_ext=None, marcap_ext=None, reqp=None,
+                 capacity=None):
+        g, _ = grid_setup(p)
+        cap = int(capacity or min(p.nvoid_max, max(g.ne ** 3 // 8, 1024)))
+        cubes = Cubes(cap)
+        nv = C.c_int32()
+        pc = p.to_c()
+        pc.nvoid_max = min(p.nvoid_max, cap)
+        sm = None if smask_ext is None else np.ascontiguousarray(smask_ext, np.int8)
+        mp = None if marcap_ext is None else np.ascontiguousarray(marcap_ext, np.int32)
+        rq = None if reqp is None else _f32(reqp)
+        self._chk(self.lib.avism_gpu_voidfind(self.h, C.byref(pc), _vp(_f32(u1co_ext)), _vp(_f32(diverco_ext)),
+                                              _vp(sm), _vp(mp), _vp(rq), C.byref(cubes.c), C.byref(nv)))
+        return cubes.view(nv.value), nv.value
+
+    def mark_all(self, p: Params, u1co_ext, diverco_ext, smask_ext=None, marcap_ext=None):
+        """MARK_ALL + the directional flag grids, one packed byte per ext cell."""
+        g, _ = grid_setup(p)
+        fl = np.zeros(g.ne ** 3, np.uint8)
+        sm = None if smask_ext is None else np.ascontiguousarray(smask_ext, np.int8)
+        mp = None if marcap_ext is None else np.ascontiguousarray(marcap_ext, np.int32)
+        pc = p.to_c()
+        self._chk(self.lib.avism_gpu_flags(self.h, C.byref(pc), _vp(_f32(u1co_ext)), _vp(_f32(diverco_ext)),
+                                           _vp(sm), _vp(mp), _vp(fl)))
+        return fl
+
+    # ---- INDEXX (src/num.f90:2-84) --------------------------------------------
+    def indexx(self, arr):
+        arr = _f32(arr)
+        out = np.zeros(len(arr), np.int32)
+        self._chk(self.lib.avism_gpu_indexx(self.h, len(arr), _vp(arr), _vp(out)))
+        return out
+
+    # ---- MERGE_VOID + post-processing -----------------------------------------
+    def merge_post(self, p: Params, nvoid, cubes: dict, u1co_ext, meandens, want_marca=True):
+        g, _ = grid_setup(p)
+        cb = Cubes.from_dict(cubes, nvoid)
+        vo = Voids(nvoid, g.ne if want_marca else None)
+        pc = p.to_c()
+        self._chk(self.lib.avism_gpu_merge_post(self.h, C.byref(pc), nvoid, C.byref(cb.c),
+                                                _vp(_f32(u1co_ext)), meandens, C.byref(vo.c)))
+        return vo.view(nvoid)
+
+    # ---- whole level ------------------------------------------------------------
+    def run_level(self, p: Params, parts: dict, want_marca=False, want_cubes=True, capacity=None):
+        g, _ = grid_setup(p)
+        cap = int(capacity or p.nvoid_max)
+        a = {k: _f32(parts[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        n = len(a["x"])
+        cubes = Cubes(cap) if want_cubes else None
+        vo = Voids(cap, g.ne if want_marca else None)
+        nv = C.c_int32()
+        md = C.c_float()
+        pc = p.to_c()
+        pc.nvoid_max = min(p.nvoid_max, cap)
+        self._chk(self.lib.avism_gpu_run_level(
+            self.h, C.byref(pc), n, *(_vp(a[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")),
+            C.byref(cubes.c) if cubes else None, C.byref(nv), C.byref(vo.c), C.byref(md)))
+        return dict(cubes=cubes.view(nv.value) if cubes else None, nvoid=nv.value,
+                    cat=vo.view(nv.value), meandens=md.value)

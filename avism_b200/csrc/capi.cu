@@ -1,0 +1,417 @@
+// capi.cu -- the extern "C" entry points declared in include/avism_gpu.h.
+#include <cstring>
+#include <exception>
+#include <vector>
+
+#include "common.cuh"
+
+struct avism_gpu_ctx {
+    avism::Ctx c;
+};
+
+using namespace avism;
+
+namespace {
+
+int fail(avism_gpu_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->c.last_error = msg;
+    return code;
+}
+
+template <class F>
+int guarded(avism_gpu_ctx *ctx, F &&f) {
+    if (!ctx) return AVISM_ERR_ARG;
+    try {
+        AV_CUDA(cudaSetDevice(ctx->c.device));
+        f(ctx->c);
+        ctx->c.last_error.clear();
+        return AVISM_OK;
+    } catch (const Error &e) {
+        cudaGetLastError();
+        return fail(ctx, e.code, e.msg);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, AVISM_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(ctx, AVISM_ERR_INTERNAL, e.what());
+    }
+}
+
+struct Timer {
+    Ctx &c;
+    cudaEvent_t a, b;
+    explicit Timer(Ctx &cc) : c(cc) {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, c.stream);
+    }
+    void lap() {
+        cudaEventRecord(b, c.stream);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        c.stage_ms.push_back(ms);
+        std::swap(a, b);
+    }
+    ~Timer() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+};
+
+// copies packed device cube arrays into the caller's avism_cubes
+void cubes_out(Ctx &c, const CubesDev &d, int32_t nvoid, avism_cubes *o) {
+    int32_t *ints[10] = {o->inicio_x, o->final_x, o->inicio_y, o->final_y, o->inicio_z, o->final_z,
+                         o->icx, o->icy, o->icz, o->father};
+    float *flts[7] = {o->vol, o->rini_x, o->rfin_x, o->rini_y, o->rfin_y, o->rini_z, o->rfin_z};
+    for (int k = 0; k < 10; k++) from_device(c, ints[k], d.i32 + (size_t)k * d.cap, sizeof(int32_t) * (size_t)nvoid);
+    for (int k = 0; k < 7; k++) from_device(c, flts[k], d.f32 + (size_t)k * d.cap, sizeof(float) * (size_t)nvoid);
+    c.sync();
+}
+
+// host copy of caller cube arrays (host or device memory)
+struct HostCubes {
+    std::vector<int32_t> i[10];
+    std::vector<float> f[7];
+    avism_cubes v;
+    HostCubes(Ctx &c, const avism_cubes *in, int32_t n) {
+        const int32_t *ints[10] = {in->inicio_x, in->final_x, in->inicio_y, in->final_y, in->inicio_z,
+                                   in->final_z, in->icx, in->icy, in->icz, in->father};
+        const float *flts[7] = {in->vol, in->rini_x, in->rfin_x, in->rini_y, in->rfin_y, in->rini_z, in->rfin_z};
+        for (int k = 0; k < 10; k++) {
+            AV_CHECK(ints[k] != nullptr || n == 0, AVISM_ERR_ARG, "null cube array");
+            i[k].resize(std::max(n, 1));
+            if (n) AV_CUDA(cudaMemcpyAsync(i[k].data(), ints[k], sizeof(int32_t) * n, cudaMemcpyDefault, c.stream));
+        }
+        for (int k = 0; k < 7; k++) {
+            AV_CHECK(flts[k] != nullptr || n == 0, AVISM_ERR_ARG, "null cube array");
+            f[k].resize(std::max(n, 1));
+            if (n) AV_CUDA(cudaMemcpyAsync(f[k].data(), flts[k], sizeof(float) * n, cudaMemcpyDefault, c.stream));
+        }
+        c.sync();
+        int32_t **vi[10] = {&v.inicio_x, &v.final_x, &v.inicio_y, &v.final_y, &v.inicio_z, &v.final_z,
+                            &v.icx, &v.icy, &v.icz, &v.father};
+        float **vf[7] = {&v.vol, &v.rini_x, &v.rfin_x, &v.rini_y, &v.rfin_y, &v.rini_z, &v.rfin_z};
+        for (int k = 0; k < 10; k++) *vi[k] = i[k].data();
+        for (int k = 0; k < 7; k++) *vf[k] = f[k].data();
+    }
+    HostCubes(Ctx &c, const CubesDev &d, int32_t n) {
+        for (int k = 0; k < 10; k++) {
+            i[k].resize(std::max(n, 1));
+            if (n) AV_CUDA(cudaMemcpyAsync(i[k].data(), d.i32 + (size_t)k * d.cap, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c.stream));
+        }
+        for (int k = 0; k < 7; k++) {
+            f[k].resize(std::max(n, 1));
+            if (n) AV_CUDA(cudaMemcpyAsync(f[k].data(), d.f32 + (size_t)k * d.cap, sizeof(float) * n, cudaMemcpyDeviceToHost, c.stream));
+        }
+        c.sync();
+        int32_t **vi[10] = {&v.inicio_x, &v.final_x, &v.inicio_y, &v.final_y, &v.inicio_z, &v.final_z,
+                            &v.icx, &v.icy, &v.icz, &v.father};
+        float **vf[7] = {&v.vol, &v.rini_x, &v.rfin_x, &v.rini_y, &v.rfin_y, &v.rini_z, &v.rfin_z};
+        for (int k = 0; k < 10; k++) *vi[k] = i[k].data();
+        for (int k = 0; k < 7; k++) *vf[k] = f[k].data();
+    }
+};
+
+__global__ void k_inner_from_ext(int nx, int low1, int ne, const float *ext, float *inner) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int64_t)nx * nx * nx) return;
+    const int i = (int)(c % nx) + 1, j = (int)((c / nx) % nx) + 1, k = (int)(c / ((int64_t)nx * nx)) + 1;
+    inner[c] = ext[(int64_t)(i - low1) + (int64_t)ne * ((int64_t)(j - low1) + (int64_t)ne * (k - low1))];
+}
+
+P2G p2g_args(Ctx &c, const avism_params *p, const Level &L, int64_t n, const float *x, const float *y,
+             const float *z, const float *vx, const float *vy, const float *vz, const float *m,
+             const int8_t *smask) {
+    const size_t nb = sizeof(float) * (size_t)std::max<int64_t>(n, 1);
+    const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
+    P2G a;
+    a.n = n;
+    a.x = (const float *)to_device(c, B_PX, x, nb);
+    a.y = (const float *)to_device(c, B_PY, y, nb);
+    a.z = (const float *)to_device(c, B_PZ, z, nb);
+    a.vx = (const float *)to_device(c, B_PVX, vx, nb);
+    a.vy = (const float *)to_device(c, B_PVY, vy, nb);
+    a.vz = (const float *)to_device(c, B_PVZ, vz, nb);
+    a.m = (const float *)to_device(c, B_PM, m, nb);
+    a.smask = (const int8_t *)to_device(c, B_SMASK, smask, (size_t)nc);
+    a.u_mass = c.get_t<float>(B_UMASS, nc);
+    a.u2 = c.get_t<float>(B_U2, nc);
+    a.u3 = c.get_t<float>(B_U3, nc);
+    a.u4 = c.get_t<float>(B_U4, nc);
+    a.hpart = c.get_t<float>(B_HPART, std::max<int64_t>(n, 1));
+    a.part_dens = c.get_t<float>(B_PDENS, std::max<int64_t>(n, 1));
+    AV_CHECK(x && y && z && m && vx && vy && vz, AVISM_ERR_ARG, "null particle array");
+    return a;
+}
+
+void check_params(const avism_params *p) {
+    AV_CHECK(p != nullptr, AVISM_ERR_ARG, "null params");
+    AV_CHECK(p->nx >= 4 && p->lado0 > 0.0f, AVISM_ERR_ARG, "nx >= 4 and lado0 > 0 required");
+    AV_CHECK(p->periodic == 0 || p->periodic == 1, AVISM_ERR_ARG, "FLAG_PERIOD must be 0 or 1");
+    AV_CHECK(p->flag_vel_interp == 0 || p->flag_vel_interp == 1, AVISM_ERR_ARG, "FLAG_VEL_INTERP must be 0 or 1");
+    AV_CHECK(p->flag_dens_interp == 0 || p->flag_dens_interp == 1, AVISM_ERR_ARG, "FLAG_DENS_INTERP must be 0 or 1");
+    AV_CHECK(p->nvoid_max >= 1, AVISM_ERR_ARG, "NVOID_MAX must be positive");
+}
+
+}  // namespace
+
+extern "C" {
+
+int avism_gpu_create(avism_gpu_ctx **out, int device) {
+    if (!out) return AVISM_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) {
+        cudaGetLastError();
+        return AVISM_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+        cudaGetLastError();
+        return AVISM_ERR_NO_DEVICE;          // this library carries sm_100a code only
+    }
+    avism_gpu_ctx *ctx = new (std::nothrow) avism_gpu_ctx();
+    if (!ctx) return AVISM_ERR_OOM;
+    ctx->c.device = device;
+    ctx->c.num_sms = prop.multiProcessorCount;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return AVISM_ERR_CUDA;
+    }
+    *out = ctx;
+    return AVISM_OK;
+}
+
+int avism_gpu_destroy(avism_gpu_ctx *ctx) {
+    if (!ctx) return AVISM_OK;
+    cudaSetDevice(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    for (int i = 0; i < B_NUM; i++)
+        if (ctx->c.buf[i]) cudaFree(ctx->c.buf[i]);
+    if (ctx->c.hpin) cudaFreeHost(ctx->c.hpin);
+    cudaStreamDestroy(ctx->c.stream);
+    delete ctx;
+    return AVISM_OK;
+}
+
+const char *avism_gpu_last_error(const avism_gpu_ctx *ctx) {
+    return ctx ? ctx->c.last_error.c_str() : "null context";
+}
+
+int avism_gpu_stage_times(const avism_gpu_ctx *ctx, double *ms, int n) {
+    if (!ctx) return AVISM_ERR_ARG;
+    const int m = (int)ctx->c.stage_ms.size();
+    for (int i = 0; i < n && i < m; i++) ms[i] = ctx->c.stage_ms[i];
+    return m;
+}
+
+int avism_gpu_grid_setup(const avism_params *p, avism_grid *g, float *radx) {
+    return grid_setup_host(p, g, radx);
+}
+
+int avism_gpu_knn(avism_gpu_ctx *ctx, int64_t n, const float *x, const float *y, const float *z, float box_l,
+                  int64_t nq, const float *qx, const float *qy, const float *qz, int32_t k, int64_t *idx,
+                  float *dist) {
+    return guarded(ctx, [&](Ctx &c) {
+        AV_CHECK(n >= 1 && nq >= 0 && k >= 1 && k <= 256 && x && y && z && idx && dist, AVISM_ERR_ARG,
+                 "knn: bad arguments");
+        c.stage_ms.clear();
+        const size_t nb = sizeof(float) * (size_t)n, qb = sizeof(float) * (size_t)std::max<int64_t>(nq, 1);
+        const float *dx = (const float *)to_device(c, B_PX, x, nb);
+        const float *dy = (const float *)to_device(c, B_PY, y, nb);
+        const float *dz = (const float *)to_device(c, B_PZ, z, nb);
+        const float *dqx = (const float *)to_device(c, B_PVX, qx, qb);
+        const float *dqy = (const float *)to_device(c, B_PVY, qy, qb);
+        const float *dqz = (const float *)to_device(c, B_PVZ, qz, qb);
+        float box = box_l;
+        int periodic = box_l > 0.0f;
+        if (!periodic) {
+            // bounding cube of the points and the queries, centred at 0
+            float lim = 0.0f;
+            std::vector<float> hv;
+            for (const float *a : {dx, dy, dz, dqx, dqy, dqz}) {
+                const int64_t cnt = (a == dqx || a == dqy || a == dqz) ? nq : n;
+                if (cnt == 0) continue;
+                float *d = c.get_t<float>(B_RED0, 2);
+                size_t tmp = 0;
+                AV_CUDA(cub::DeviceReduce::Max(nullptr, tmp, a, d, (int)cnt, c.stream));
+                void *t = c.get(B_CUB_TMP, tmp);
+                AV_CUDA(cub::DeviceReduce::Max(t, tmp, a, d, (int)cnt, c.stream));
+                AV_CUDA(cub::DeviceReduce::Min(t, tmp, a, d + 1, (int)cnt, c.stream));
+                float h2[2];
+                AV_CUDA(cudaMemcpyAsync(h2, d, 8, cudaMemcpyDeviceToHost, c.stream));
+                c.sync();
+                lim = std::max(lim, std::max(std::fabs(h2[0]), std::fabs(h2[1])));
+            }
+            box = 2.0f * lim * 1.0001f + 1e-6f;
+        }
+        BinnedParticles bp = bin_particles(c, n, dx, dy, dz, box, periodic, 4.0f);
+        int64_t *di = (int64_t *)(is_device_ptr(idx) ? (void *)idx : c.get(B_LIST_A, sizeof(int64_t) * (size_t)std::max<int64_t>(nq * k, 1)));
+        float *dd = (float *)(is_device_ptr(dist) ? (void *)dist : c.get(B_LIST_B, sizeof(float) * (size_t)std::max<int64_t>(nq * k, 1)));
+        knn_batch(c, bp, nq, dqx, dqy, dqz, k, di, dd);
+        from_device(c, idx, di, sizeof(int64_t) * (size_t)(nq * k));
+        from_device(c, dist, dd, sizeof(float) * (size_t)(nq * k));
+        c.sync();
+    });
+}
+
+int avism_gpu_particles_to_grid(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x,
+                                const float *y, const float *z, const float *vx, const float *vy,
+                                const float *vz, const float *m, const int8_t *smask, float *u_mass,
+                                float *u2, float *u3, float *u4, float *hpart, float *part_dens) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        c.stage_ms.clear();
+        Level L = make_level(p);
+        P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, smask);
+        particles_to_grid(c, p, L, a);
+        const size_t gb = sizeof(float) * (size_t)L.g.nx * L.g.nx * L.g.nx;
+        from_device(c, u_mass, a.u_mass, gb);
+        from_device(c, u2, a.u2, gb);
+        from_device(c, u3, a.u3, gb);
+        from_device(c, u4, a.u4, gb);
+        from_device(c, hpart, a.hpart, sizeof(float) * (size_t)n);
+        from_device(c, part_dens, a.part_dens, sizeof(float) * (size_t)n);
+        c.sync();
+    });
+}
+
+int avism_gpu_fields(avism_gpu_ctx *ctx, const avism_params *p, const float *u_mass, const float *u2,
+                     const float *u3, const float *u4, float *u1co_ext, float *diverco_ext, float *meandens) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        c.stage_ms.clear();
+        Level L = make_level(p);
+        const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
+        const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
+        const size_t gb = sizeof(float) * (size_t)nc;
+        const float *dm = (const float *)to_device(c, B_UMASS, u_mass, gb);
+        const float *d2 = (const float *)to_device(c, B_U2, u2, gb);
+        const float *d3 = (const float *)to_device(c, B_U3, u3, gb);
+        const float *d4 = (const float *)to_device(c, B_U4, u4, gb);
+        float *u1 = c.get_t<float>(B_U1CO, nc), *dv = c.get_t<float>(B_DIVER, nc);
+        FieldsOut fo = fields_inner(c, p, L, dm, d2, d3, d4, u1, dv);
+        float *e1 = is_device_ptr(u1co_ext) ? u1co_ext : c.get_t<float>(B_U1EXT, ne3);
+        float *e2 = is_device_ptr(diverco_ext) ? diverco_ext : c.get_t<float>(B_DVEXT, ne3);
+        if (u1co_ext) { ext_copy(c, L, u1, e1); from_device(c, u1co_ext, e1, sizeof(float) * (size_t)ne3); }
+        if (diverco_ext) { ext_copy(c, L, dv, e2); from_device(c, diverco_ext, e2, sizeof(float) * (size_t)ne3); }
+        c.sync();
+        if (meandens) *meandens = fo.meandens;
+    });
+}
+
+int avism_gpu_voidfind(avism_gpu_ctx *ctx, const avism_params *p, const float *u1co_ext,
+                       const float *diverco_ext, const int8_t *smask_ext, const int32_t *marcap_ext,
+                       const float *reqp, avism_cubes *cubes, int32_t *nvoid) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        AV_CHECK(u1co_ext && diverco_ext && cubes && nvoid, AVISM_ERR_ARG, "voidfind: null argument");
+        c.stage_ms.clear();
+        Level L = make_level(p);
+        const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
+        const float *u1 = (const float *)to_device(c, B_U1EXT, u1co_ext, sizeof(float) * (size_t)ne3);
+        const float *dv = (const float *)to_device(c, B_DVEXT, diverco_ext, sizeof(float) * (size_t)ne3);
+        const int8_t *sm = (const int8_t *)to_device(c, B_SMASK, smask_ext, (size_t)ne3);
+        const int32_t *mp = (const int32_t *)to_device(c, B_MARCAP, marcap_ext, sizeof(int32_t) * (size_t)ne3);
+        // parent radii: one per parent id, as many as the largest id in marcap
+        int32_t nreqp = 0;
+        const float *rq = nullptr;
+        if (mp && reqp) {
+            int32_t *d = c.get_t<int32_t>(B_RED0, 1);
+            size_t tmp = 0;
+            AV_CUDA(cub::DeviceReduce::Max(nullptr, tmp, mp, d, (int)ne3, c.stream));
+            void *t = c.get(B_CUB_TMP, tmp);
+            AV_CUDA(cub::DeviceReduce::Max(t, tmp, mp, d, (int)ne3, c.stream));
+            AV_CUDA(cudaMemcpyAsync(&nreqp, d, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+            c.sync();
+            nreqp = std::max(nreqp, 0);
+            rq = (const float *)to_device(c, B_REQP, reqp, sizeof(float) * (size_t)std::max(nreqp, 1));
+        }
+        CubesDev cd{};
+        const int32_t nv = voidfind_device(c, p, L, u1, dv, 1, sm, mp, rq, nreqp, cd);
+        cubes_out(c, cd, nv, cubes);
+        *nvoid = nv;
+    });
+}
+
+int avism_gpu_flags(avism_gpu_ctx *ctx, const avism_params *p, const float *u1co_ext, const float *diverco_ext,
+                    const int8_t *smask_ext, const int32_t *marcap_ext, uint8_t *flags_ext) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        AV_CHECK(u1co_ext && diverco_ext && flags_ext, AVISM_ERR_ARG, "flags: null argument");
+        c.stage_ms.clear();
+        Level L = make_level(p);
+        const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
+        const float *u1 = (const float *)to_device(c, B_U1EXT, u1co_ext, sizeof(float) * (size_t)ne3);
+        const float *dv = (const float *)to_device(c, B_DVEXT, diverco_ext, sizeof(float) * (size_t)ne3);
+        const int8_t *sm = (const int8_t *)to_device(c, B_SMASK, smask_ext, (size_t)ne3);
+        const int32_t *mp = (const int32_t *)to_device(c, B_MARCAP, marcap_ext, sizeof(int32_t) * (size_t)ne3);
+        uint8_t *fl = is_device_ptr(flags_ext) ? flags_ext : c.get_t<uint8_t>(B_FLAGS, ne3);
+        make_flags(c, p, L, u1, dv, 1, sm, mp, fl);
+        from_device(c, flags_ext, fl, (size_t)ne3);
+        c.sync();
+    });
+}
+
+int avism_gpu_indexx(avism_gpu_ctx *ctx, int32_t n, const float *arr, int32_t *indx) {
+    return guarded(ctx, [&](Ctx &c) {
+        AV_CHECK(n >= 0 && (n == 0 || (arr && indx)), AVISM_ERR_ARG, "indexx: bad arguments");
+        if (n == 0) return;
+        c.stage_ms.clear();
+        const float *k = (const float *)to_device(c, B_CAND_KEY, arr, sizeof(float) * (size_t)n);
+        int32_t *o = is_device_ptr(indx) ? indx : c.get_t<int32_t>(B_CAND_POS, n);
+        indexx_device(c, n, k, o);
+        from_device(c, indx, o, sizeof(int32_t) * (size_t)n);
+        c.sync();
+    });
+}
+
+int avism_gpu_merge_post(avism_gpu_ctx *ctx, const avism_params *p, int32_t nvoid, const avism_cubes *cubes,
+                         const float *u1co_ext, float meandens, avism_voids *out) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        AV_CHECK(nvoid >= 0 && cubes && u1co_ext && out, AVISM_ERR_ARG, "merge_post: null argument");
+        c.stage_ms.clear();
+        Level L = make_level(p);
+        const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
+        const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
+        const float *e1 = (const float *)to_device(c, B_U1EXT, u1co_ext, sizeof(float) * (size_t)ne3);
+        float *u1 = c.get_t<float>(B_U1CO, nc);
+        k_inner_from_ext<<<grid_for(nc, 256), 256, 0, c.stream>>>(L.g.nx, L.g.low1, L.g.ne, e1, u1);
+        HostCubes hc(c, cubes, nvoid);
+        merge_post(c, p, L, nvoid, &hc.v, u1, meandens, out, out->marca);
+    });
+}
+
+int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x, const float *y,
+                        const float *z, const float *vx, const float *vy, const float *vz, const float *m,
+                        avism_cubes *cubes, int32_t *nvoid, avism_voids *voids, float *meandens) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        AV_CHECK(nvoid && voids, AVISM_ERR_ARG, "run_level: null argument");
+        c.stage_ms.clear();
+        Timer tm(c);
+        Level L = make_level(p);
+        const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
+        P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, nullptr);
+        tm.lap();                                       // 0: inputs to device
+        particles_to_grid(c, p, L, a);
+        tm.lap();                                       // 1: particles -> grid
+        float *u1 = c.get_t<float>(B_U1CO, nc), *dv = c.get_t<float>(B_DIVER, nc);
+        FieldsOut fo = fields_inner(c, p, L, a.u_mass, a.u2, a.u3, a.u4, u1, dv);
+        tm.lap();                                       // 2: fields
+        CubesDev cd{};
+        const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, nullptr, nullptr, 0, cd);
+        tm.lap();                                       // 3: voidfind
+        HostCubes hc(c, cd, nv);
+        if (cubes) cubes_out(c, cd, nv, cubes);
+        merge_post(c, p, L, nv, &hc.v, u1, fo.meandens, voids, voids->marca);
+        tm.lap();                                       // 4: merge + post
+        *nvoid = nv;
+        if (meandens) *meandens = fo.meandens;
+    });
+}
+
+}  // extern "C"

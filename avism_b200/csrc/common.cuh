@@ -1,0 +1,186 @@
+// common.cuh -- shared definitions of the AVISM B200 library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/avism_gpu.h"
+
+namespace avism {
+
+// ---- status plumbing ------------------------------------------------------
+struct Error {
+    int code;
+    std::string msg;
+};
+
+#define AV_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            throw ::avism::Error{AVISM_ERR_CUDA, std::string(#call) + ": " +           \
+                                                     cudaGetErrorString(e_)};           \
+    } while (0)
+
+#define AV_CHECK(cond, code, text)                                                      \
+    do {                                                                                \
+        if (!(cond)) throw ::avism::Error{(code), (text)};                              \
+    } while (0)
+
+// ---- device buffer pool: named, grow-only --------------------------------
+enum BufId : int {
+    B_SP = 0,        // float4 binned particles (x, y, z, orig index)
+    B_BIN_START,     // int64 bin offsets
+    B_KEYS_A, B_KEYS_B, B_VALS_A, B_VALS_B,
+    B_CUB_TMP,
+    B_PX, B_PY, B_PZ, B_PVX, B_PVY, B_PVZ, B_PM,   // particle inputs (device copies)
+    B_HPART, B_PDENS, B_NORM,
+    B_UMASS, B_U2, B_U3, B_U4,                     // inner grids
+    B_FIX0, B_FIX1, B_FIX2, B_FIX3,                // int64 fixed-point accumulators
+    B_U1CO, B_DIVER,                               // inner normalised density / divergence
+    B_U1EXT, B_DVEXT,                              // ext grids (ABI outputs)
+    B_FLAGS, B_SMASK, B_MARCAP,                    // ext byte flags, ext mask, ext parent ids
+    B_REQP,
+    B_CAND_POS, B_CAND_KEY, B_SORT_KEY, B_SORT_IDX, B_SEG_A, B_SEG_B, B_GE, B_LE, B_SCAN_A, B_SCAN_B,
+    B_CUBE_W, B_CUBE_ST, B_COVER, B_UMIN, B_LIST_A, B_LIST_B, B_COUNTERS,
+    B_CUBES,                                       // packed cube arrays
+    B_MARCA, B_PAINT, B_LABMAP, B_LABEL_AUX, B_CCL,
+    B_RED0, B_RED1, B_RED2,
+    B_QUERY, B_RAD, B_BALL, B_SCAL,
+    B_NUM
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    void *buf[B_NUM] = {};
+    size_t cap[B_NUM] = {};
+    std::string last_error;
+    std::vector<double> stage_ms;
+    int num_sms = 148;
+    // scratch pinned host memory for small readbacks
+    void *hpin = nullptr;
+    size_t hpin_cap = 0;
+
+    void *get(BufId id, size_t bytes) {
+        if (bytes == 0) bytes = 16;
+        if (cap[id] < bytes) {
+            if (buf[id]) AV_CUDA(cudaFree(buf[id]));
+            buf[id] = nullptr;
+            cap[id] = 0;
+            size_t want = bytes + bytes / 8;
+            cudaError_t e = cudaMalloc(&buf[id], want);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                e = cudaMalloc(&buf[id], bytes);
+                want = bytes;
+            }
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                throw Error{AVISM_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed"};
+            }
+            cap[id] = want;
+        }
+        return buf[id];
+    }
+    template <class T> T *get_t(BufId id, size_t n) { return (T *)get(id, n * sizeof(T)); }
+
+    void *host_pinned(size_t bytes) {
+        if (hpin_cap < bytes) {
+            if (hpin) cudaFreeHost(hpin);
+            hpin = nullptr;
+            AV_CUDA(cudaMallocHost(&hpin, bytes));
+            hpin_cap = bytes;
+        }
+        return hpin;
+    }
+    void sync() { AV_CUDA(cudaStreamSynchronize(stream)); }
+};
+
+// pointer classification: true if p is device (or managed) memory
+bool is_device_ptr(const void *p);
+
+// copies a caller array into a device buffer (no copy if it is already device memory)
+const void *to_device(Ctx &c, BufId id, const void *src, size_t bytes);
+// copies a device result to the caller's array (device-to-device if it is device memory)
+void from_device(Ctx &c, void *dst, const void *src_dev, size_t bytes);
+
+// ---- level geometry (host) -------------------------------------------------
+struct Level {
+    avism_grid g;
+    std::vector<float> rad;          // RADX(rad_lo..rad_hi)
+    float rad_at(int i) const { return rad[(size_t)(i - g.rad_lo)]; }
+};
+int grid_setup_host(const avism_params *p, avism_grid *g, float *radx);
+Level make_level(const avism_params *p);
+
+// ---- launch helpers ----------------------------------------------------------
+inline unsigned grid_for(int64_t n, int block) {
+    int64_t g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > 0x7fffffffLL) g = 0x7fffffffLL;
+    return (unsigned)g;
+}
+
+// ---- stage entry points (implemented across the .cu files) -----------------
+struct BinnedParticles {
+    int64_t n = 0;
+    int nb = 1;                      // bins per axis
+    float box = 0.f, bw = 0.f, inv_bw = 0.f, origin = 0.f;
+    int periodic = 0;
+    const float4 *sp = nullptr;      // binned particles (x, y, z, orig idx bits)
+    const int64_t *start = nullptr;  // nb^3 + 1 offsets
+};
+
+BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y, const float *z,
+                              float box, int periodic, float occupancy);
+
+void knn_batch(Ctx &c, const BinnedParticles &bp, int64_t nq, const float *qx, const float *qy,
+               const float *qz, int k, int64_t *idx_out, float *dist_out);
+
+// particles -> grid (SPH/TSC).  All pointers are device pointers.
+struct P2G {
+    int64_t n;
+    const float *x, *y, *z, *vx, *vy, *vz, *m;
+    float *u_mass, *u2, *u3, *u4;    // inner NX^3
+    float *hpart, *part_dens;        // per particle
+    const int8_t *smask;             // inner NX^3 or null
+};
+void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G &a);
+
+// normalisation + divergence (inner grids) and ext copies.
+struct FieldsOut {
+    float meandens;
+};
+FieldsOut fields_inner(Ctx &c, const avism_params *p, const Level &L, const float *u_mass,
+                       const float *u2, const float *u3, const float *u4, float *u1co_in,
+                       float *diver_in);
+void ext_copy(Ctx &c, const Level &L, const float *inner, float *ext);
+
+// flags on the ext grid from inner (wrapped) fields, or from given ext fields.
+void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, const float *dv,
+                int fields_are_ext, const int8_t *smask_ext, const int32_t *marcap_ext,
+                uint8_t *flags);
+
+// exact Numerical Recipes INDEXX on device arrays (key f32, idx i32 1-based out)
+void indexx_device(Ctx &c, int32_t n, const float *key_in, int32_t *indx_out);
+
+// candidates + growth + acceptance; fills device cube arrays (packed), returns nvoid
+struct CubesDev {
+    int32_t *i32;   // 10 arrays of cap entries: inicio_x..final_z, icx, icy, icz, father
+    float *f32;     // 7 arrays: vol, rini_x..rfin_z
+    int32_t cap;
+};
+int32_t voidfind_device(Ctx &c, const avism_params *p, const Level &L, const float *u1,
+                        const float *dv, int fields_are_ext, const int8_t *smask_ext,
+                        const int32_t *marcap_ext, const float *reqp, int32_t nreqp,
+                        CubesDev &cubes);
+
+// merge + post-processing; cubes in host memory (copied), outputs host arrays
+void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nvoid,
+                const avism_cubes *cubes_host, const float *u1co_inner_dev, float meandens,
+                avism_voids *out, int32_t *marca_ext_out);
+
+}  // namespace avism

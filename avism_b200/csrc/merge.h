@@ -1,0 +1,31 @@
+// merge.h -- host-side MERGE_VOID on cube records and the small host helpers
+// of the post-processing.
+#pragma once
+
+#include <stdint.h>
+#include <vector>
+
+namespace avism {
+
+struct MergeIn {
+    int32_t nvoid;
+    int low1, low2, periodic;
+    float dx, rx1, lado0plus;
+    const int32_t *x0, *x1, *y0, *y1, *z0, *z1, *icx, *icy, *icz, *father;
+    const float *rix, *rfx, *riy, *rfy, *riz, *rfz;
+    const int32_t *indice;          // cube ids by volume, largest first
+};
+
+struct MergeOut {
+    std::vector<int32_t> uvoid;     // -1 main void, >0 owner id
+    std::vector<float> gxc, gyc, gzc, volnew;
+    std::vector<int32_t> paint_time;   // order in which each cube painted its box
+    std::vector<int32_t> paint_owner;  // void id painted by that cube
+    int32_t nvoid2 = 0;
+};
+
+void merge_cubes_host(const MergeIn &in, MergeOut &out);
+void jacobi3_ref(float a[3][3], float d[3]);
+void sort_desc3_ref(float d[3]);
+
+}  // namespace avism

@@ -1,0 +1,641 @@
+// post.cu -- volume ordering, MERGE_VOID painting and the post-processing of
+// src/avism.f90:1738-1973 on the device.
+//
+//  * INDEXX on VOL (exact permutation), MERGE_VOID on cube records (merge.cpp);
+//  * MARCA painting: every cell takes the owner of the earliest-painted cube
+//    containing it (atomicMin of the paint time), which is the reference's
+//    first-writer-wins "IF(MARCA.EQ.0) MARCA=IND0";
+//  * NCELLV, the NCELL_MIN / RMIN removals (decided per void on the host,
+//    applied by one relabel pass instead of a WHERE per void);
+//  * VOID_SHAPE inertia sums, JACOBI / SORT on the host (src/shape.f90);
+//  * SIMPLE_CONNECTION_FAST as union-find connected components of the non-void
+//    cells: everything not connected to the LOW1 corner is a hole, filled with
+//    the id of the first void cell in +x;
+//  * VOID_PERIODIC: overlap counts of every outer-centred void computed in one
+//    pass, then validated in catalogue order on the host; a void whose inputs
+//    an earlier merge could have changed is recounted on the device;
+//  * global properties on the inner cells, FP64 sums.
+#include <cub/cub.cuh>
+#include <algorithm>
+#include <array>
+#include <climits>
+#include <functional>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "merge.h"
+
+namespace avism {
+
+struct PostGrid {
+    int low1, low2, ne, nx;
+};
+
+__device__ __forceinline__ int64_t pidx(const PostGrid &G, int i, int j, int k) {
+    return (int64_t)(i - G.low1) + (int64_t)G.ne * ((int64_t)(j - G.low1) + (int64_t)G.ne * (k - G.low1));
+}
+
+// cube boxes: 6 int arrays of cap entries (x0,x1,y0,y1,z0,z1)
+__global__ void k_paint_time(PostGrid G, const int32_t *box, int32_t cap, const int32_t *ptime, int32_t nv,
+                             int32_t *tgrid) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wi = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wi >= nv) return;
+    const int32_t x0 = box[0 * cap + wi], x1 = box[1 * cap + wi], y0 = box[2 * cap + wi];
+    const int32_t y1 = box[3 * cap + wi], z0 = box[4 * cap + wi], z1 = box[5 * cap + wi];
+    const int sx = x1 - x0 + 1, sy = y1 - y0 + 1, sz = z1 - z0 + 1;
+    const int64_t vol = (int64_t)sx * sy * sz;
+    const int32_t t = ptime[wi];
+    for (int64_t q = lane; q < vol; q += 32) {
+        const int a = (int)(q % sx), b = (int)((q / sx) % sy), d = (int)(q / ((int64_t)sx * sy));
+        atomicMin(&tgrid[pidx(G, x0 + a, y0 + b, z0 + d)], t);
+    }
+}
+
+__global__ void k_fill_i32(int64_t n, int32_t *a, int32_t v) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) a[e] = v;
+}
+
+__global__ void k_time_to_label(int64_t ne3, const int32_t *tgrid, const int32_t *owner_by_time, int32_t *marca) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne3) return;
+    const int32_t t = tgrid[e];
+    marca[e] = t == INT_MAX ? 0 : owner_by_time[t];
+}
+
+__global__ void k_relabel(int64_t ne3, int32_t *marca, const int32_t *map) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne3) return;
+    const int32_t m = marca[e];
+    if (m > 0) marca[e] = map[m];
+}
+
+// warp-aggregated count per main-void label (uvoid == -1) over the ext grid
+__global__ void k_ncellv(int64_t ne3, const int32_t *marca, const int32_t *uvoid, int32_t *ncell) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t m = 0;
+    if (e < ne3) {
+        m = marca[e];
+        if (m > 0 && uvoid[m - 1] != -1) m = 0;
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, m);
+    const int lane = threadIdx.x & 31;
+    if (m > 0 && lane == __ffs(grp) - 1) atomicAdd(&ncell[m - 1], __popc(grp));
+}
+
+// ---- VOID_SHAPE inertia: per cell terms in REAL*4 (src/shape.f90:176-196) ----
+__global__ void k_inertia(PostGrid G, const int32_t *marca, const float *rad, int rad_lo, const float *gxc,
+                          const float *gyc, const float *gzc, double *inert /* 6 per label */) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t ne3 = (int64_t)G.ne * G.ne * G.ne;
+    int32_t m = 0;
+    float t[6] = {0, 0, 0, 0, 0, 0};
+    if (e < ne3) {
+        m = marca[e];
+        if (m > 0) {
+            const int i = (int)(e % G.ne) + G.low1, j = (int)((e / G.ne) % G.ne) + G.low1;
+            const int k = (int)(e / ((int64_t)G.ne * G.ne)) + G.low1;
+            const float r0 = __fsub_rn(rad[i - rad_lo], gxc[m - 1]);
+            const float r1 = __fsub_rn(rad[j - rad_lo], gyc[m - 1]);
+            const float r2 = __fsub_rn(rad[k - rad_lo], gzc[m - 1]);
+            const float rr = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(r0, r0), __fmul_rn(r1, r1)), __fmul_rn(r2, r2)));
+            const float rr2 = __fmul_rn(rr, rr);
+            t[0] = __fsub_rn(rr2, __fmul_rn(r0, r0));
+            t[1] = __fsub_rn(rr2, __fmul_rn(r1, r1));
+            t[2] = __fsub_rn(rr2, __fmul_rn(r2, r2));
+            t[3] = -__fmul_rn(r0, r1);
+            t[4] = -__fmul_rn(r0, r2);
+            t[5] = -__fmul_rn(r1, r2);
+        }
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, m);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(grp) - 1;
+    for (int q = 0; q < 6; q++) {
+        // sum in lane order inside the group
+        double s = 0.0;
+        for (int src = 0; src < 32; src++) {
+            const float v = __shfl_sync(0xffffffffu, t[q], src);
+            if ((grp >> src) & 1) s += (double)v;
+        }
+        if (m > 0 && lane == leader) atomicAdd(&inert[(size_t)(m - 1) * 6 + q], s);
+    }
+}
+
+// ---- SIMPLE_CONNECTION_FAST: union-find of non-void cells --------------------
+__device__ __forceinline__ int32_t uf_find(int32_t *P, int32_t x) {
+    while (true) {
+        const int32_t px = P[x];
+        if (px == x) return x;
+        const int32_t ppx = P[px];
+        if (ppx != px) P[x] = ppx;
+        x = px;
+    }
+}
+__device__ __forceinline__ void uf_union(int32_t *P, int32_t a, int32_t b) {
+    while (true) {
+        a = uf_find(P, a);
+        b = uf_find(P, b);
+        if (a == b) return;
+        if (a < b) { const int32_t t = a; a = b; b = t; }
+        const int32_t old = atomicCAS(&P[a], a, b);
+        if (old == a) return;
+        a = old;
+    }
+}
+__global__ void k_ccl_init(int64_t ne3, const int32_t *marca, int32_t *P) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < ne3) P[e] = marca[e] > 0 ? -1 : (int32_t)e;
+}
+__global__ void k_ccl_union(PostGrid G, int32_t *P) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int ne = G.ne;
+    const int64_t ne3 = (int64_t)ne * ne * ne;
+    if (e >= ne3 || P[e] < 0) return;
+    const int i = (int)(e % ne), j = (int)((e / ne) % ne), k = (int)(e / ((int64_t)ne * ne));
+    if (i > 0 && P[e - 1] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - 1));
+    if (j > 0 && P[e - ne] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - ne));
+    if (k > 0 && P[e - (int64_t)ne * ne] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - (int64_t)ne * ne));
+}
+__global__ void k_ccl_flatten(int64_t ne3, int32_t *P) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < ne3 && P[e] >= 0) P[e] = uf_find(P, (int32_t)e);
+}
+// a hole takes the id of the first non-hole cell in +x (src/voidfinding.f90:1142-1158)
+__global__ void k_fill_holes(PostGrid G, const int32_t *P, const int32_t *marca_in, int32_t *marca_out) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int ne = G.ne;
+    const int64_t ne3 = (int64_t)ne * ne * ne;
+    if (e >= ne3) return;
+    const int32_t root = P[0];
+    auto hole = [&](int64_t f) { const int32_t r = P[f]; return r >= 0 && r != root; };
+    if (!hole(e)) {
+        marca_out[e] = marca_in[e];
+        return;
+    }
+    const int64_t rowend = e - (e % ne) + ne;
+    int64_t f = e;
+    while (f < rowend && hole(f)) f++;
+    marca_out[e] = f < rowend ? marca_in[f] : 0;
+}
+
+// ---- VOID_PERIODIC helpers ----------------------------------------------------
+__global__ void k_inner_presence(PostGrid G, const int32_t *marca, int32_t *has) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = G.nx;
+    if (c >= (int64_t)nx * nx * nx) return;
+    const int i = (int)(c % nx) + 1, j = (int)((c / nx) % nx) + 1, k = (int)(c / ((int64_t)nx * nx)) + 1;
+    const int32_t m = marca[pidx(G, i, j, k)];
+    if (m > 0) has[m - 1] = 1;
+}
+__global__ void k_bbox(PostGrid G, const int32_t *marca, int32_t *bb /* 6 per label: min xyz, max xyz */) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int ne = G.ne;
+    if (e >= (int64_t)ne * ne * ne) return;
+    const int32_t m = marca[e];
+    if (m <= 0) return;
+    const int c[3] = {(int)(e % ne) + G.low1, (int)((e / ne) % ne) + G.low1, (int)(e / ((int64_t)ne * ne)) + G.low1};
+    for (int a = 0; a < 3; a++) {
+        atomicMin(&bb[(size_t)(m - 1) * 6 + a], c[a]);
+        atomicMax(&bb[(size_t)(m - 1) * 6 + 3 + a], c[a]);
+    }
+}
+// shifted-cell overlap counts of every outer-centred void against its IND2;
+// labmap maps stored labels to the current ones (identity for the first pass);
+// only_label > 0 restricts the pass to one (current) label
+__global__ void k_periodic_counts(PostGrid G, const int32_t *marca, const int32_t *labmap, const int8_t *shift,
+                                  const int32_t *ind2, int32_t only_label, int32_t *cnt /* 2 per label */) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int ne = G.ne;
+    if (e >= (int64_t)ne * ne * ne) return;
+    int32_t m = marca[e];
+    if (m <= 0) return;
+    m = labmap[m];
+    if (only_label > 0 && m != only_label) return;
+    const int8_t *s = shift + (size_t)(m - 1) * 3;
+    if (s[0] == 0 && s[1] == 0 && s[2] == 0) return;
+    const int i = (int)(e % ne) + G.low1 + s[0] * G.nx;
+    const int j = (int)((e / ne) % ne) + G.low1 + s[1] * G.nx;
+    const int k = (int)(e / ((int64_t)ne * ne)) + G.low1 + s[2] * G.nx;
+    if (i < G.low1 || i > G.low2 || j < G.low1 || j > G.low2 || k < G.low1 || k > G.low2) return;
+    atomicAdd(&cnt[(size_t)(m - 1) * 2 + 1], 1);
+    int32_t lab = marca[pidx(G, i, j, k)];
+    if (lab > 0) lab = labmap[lab];
+    if (lab == ind2[m - 1]) atomicAdd(&cnt[(size_t)(m - 1) * 2], 1);
+}
+
+// ---- global properties on the inner cells (src/avism.f90:1917-1933) ------------
+__global__ void k_final_props(PostGrid G, const int32_t *marca, const int32_t *uvoid, const float *u1co,
+                              float meandens, float dx, float rete3, int32_t *ncell, double *sums /* 2 per label */) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = G.nx;
+    int32_t m = 0;
+    float u = 0.0f, mt = 0.0f;
+    if (c < (int64_t)nx * nx * nx) {
+        const int i = (int)(c % nx) + 1, j = (int)((c / nx) % nx) + 1, k = (int)(c / ((int64_t)nx * nx)) + 1;
+        m = marca[pidx(G, i, j, k)];
+        if (m > 0 && uvoid[m - 1] != -1) m = 0;
+        if (m > 0) {
+            u = u1co[c];
+            mt = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(u, meandens), dx), dx), dx), rete3);
+        }
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, m);
+    const int lane = threadIdx.x & 31;
+    double su = 0.0, sm = 0.0;
+    for (int src = 0; src < 32; src++) {
+        const float a = __shfl_sync(0xffffffffu, u, src), b = __shfl_sync(0xffffffffu, mt, src);
+        if ((grp >> src) & 1) { su += (double)a; sm += (double)b; }
+    }
+    if (m > 0 && lane == __ffs(grp) - 1) {
+        atomicAdd(&ncell[m - 1], __popc(grp));
+        atomicAdd(&sums[(size_t)(m - 1) * 2], su);
+        atomicAdd(&sums[(size_t)(m - 1) * 2 + 1], sm);
+    }
+}
+
+template <class T>
+static T *dev_upload(Ctx &c, BufId id, const T *h, size_t n) {
+    T *d = c.get_t<T>(id, std::max<size_t>(n, 1));
+    if (n) AV_CUDA(cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+    return d;
+}
+template <class T>
+static void dev_download(Ctx &c, T *h, const T *d, size_t n) {
+    if (n) AV_CUDA(cudaMemcpyAsync(h, d, n * sizeof(T), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+}
+
+void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const avism_cubes *cb,
+                const float *u1co_inner, float meandens, avism_voids *out, int32_t *marca_ext_out) {
+    const avism_grid &g = L.g;
+    const int ne = g.ne, nx = g.nx;
+    const int64_t ne3 = (int64_t)ne * ne * ne;
+    const float dx = g.dx;
+    const double pi = 3.141592653589793;
+    PostGrid PG{g.low1, g.low2, ne, nx};
+    const int32_t nvs = std::max(nv, 1);
+
+    // ---- INDEXX on VOL, reversed (avism.f90:1738-1745)
+    std::vector<int32_t> indice(nvs);
+    {
+        float *vol_d = dev_upload<float>(c, B_RED2, cb->vol, nv);
+        int32_t *ind_d = c.get_t<int32_t>(B_QUERY, nvs);
+        indexx_device(c, nv, vol_d, ind_d);
+        std::vector<int32_t> asc(nvs);
+        dev_download(c, asc.data(), ind_d, nv);
+        for (int32_t i = 0; i < nv; i++) indice[i] = asc[nv - 1 - i];
+    }
+    // ---- MERGE_VOID
+    MergeIn mi;
+    mi.nvoid = nv; mi.low1 = g.low1; mi.low2 = g.low2; mi.periodic = p->periodic;
+    mi.dx = dx; mi.rx1 = L.rad_at(1); mi.lado0plus = g.lado0plus;
+    mi.x0 = cb->inicio_x; mi.x1 = cb->final_x; mi.y0 = cb->inicio_y; mi.y1 = cb->final_y;
+    mi.z0 = cb->inicio_z; mi.z1 = cb->final_z; mi.icx = cb->icx; mi.icy = cb->icy; mi.icz = cb->icz;
+    mi.father = cb->father; mi.rix = cb->rini_x; mi.rfx = cb->rfin_x; mi.riy = cb->rini_y;
+    mi.rfy = cb->rfin_y; mi.riz = cb->rini_z; mi.rfz = cb->rfin_z; mi.indice = indice.data();
+    MergeOut mo;
+    merge_cubes_host(mi, mo);
+    std::vector<int32_t> &uvoid = mo.uvoid;
+    std::vector<float> &volnew = mo.volnew;
+
+    // ---- paint MARCA
+    int32_t *marca = c.get_t<int32_t>(B_MARCA, ne3);
+    {
+        std::vector<int32_t> boxes((size_t)nvs * 6);
+        const int32_t *src[6] = {cb->inicio_x, cb->final_x, cb->inicio_y, cb->final_y, cb->inicio_z, cb->final_z};
+        for (int a = 0; a < 6; a++) std::memcpy(&boxes[(size_t)a * nvs], src[a], sizeof(int32_t) * (size_t)nv);
+        int32_t *box_d = dev_upload<int32_t>(c, B_RED0, boxes.data(), boxes.size());
+        int32_t *pt_d = dev_upload<int32_t>(c, B_RED1, mo.paint_time.data(), nv);
+        std::vector<int32_t> owner_by_time(nvs, 0);
+        for (int32_t i = 0; i < nv; i++) {
+            AV_CHECK(mo.paint_time[i] >= 0 && mo.paint_time[i] < nv, AVISM_ERR_INTERNAL, "merge: cube never painted");
+            owner_by_time[mo.paint_time[i]] = mo.paint_owner[i];
+        }
+        int32_t *obt_d = dev_upload<int32_t>(c, B_LABMAP, owner_by_time.data(), nv);
+        int32_t *tgrid = c.get_t<int32_t>(B_CCL, ne3);
+        k_fill_i32<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, tgrid, INT_MAX);
+        if (nv > 0) k_paint_time<<<grid_for((int64_t)nv * 32, 256), 256, 0, c.stream>>>(PG, box_d, nvs, pt_d, nv, tgrid);
+        k_time_to_label<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, tgrid, obt_d, marca);
+        AV_CUDA(cudaGetLastError());
+    }
+    std::vector<char> rm(nvs + 1, 0);
+    std::vector<int32_t> ncellv(nvs, 0);
+    int32_t *map_d = c.get_t<int32_t>(B_LABEL_AUX, nvs + 1);
+    int32_t *uv_d = c.get_t<int32_t>(B_RED1, nvs);
+    auto push_uvoid = [&]() { AV_CUDA(cudaMemcpyAsync(uv_d, uvoid.data(), sizeof(int32_t) * (size_t)nv, cudaMemcpyHostToDevice, c.stream)); };
+    // removal of main voids: cells to 0, owners of absorbed cubes to 0
+    auto apply_removals = [&]() {
+        bool any = false;
+        for (int32_t i = 1; i <= nv; i++) any |= rm[i] != 0;
+        if (!any) return;
+        std::vector<int32_t> map(nvs + 1);
+        for (int32_t i = 0; i <= nv; i++) map[i] = rm[i] ? 0 : i;
+        AV_CUDA(cudaMemcpyAsync(map_d, map.data(), sizeof(int32_t) * (size_t)(nv + 1), cudaMemcpyHostToDevice, c.stream));
+        k_relabel<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, map_d);
+        for (int32_t i = 0; i < nv; i++)
+            if (uvoid[i] > 0 && rm[uvoid[i]]) uvoid[i] = 0;
+        for (int32_t i = 1; i <= nv; i++)
+            if (rm[i]) { uvoid[i - 1] = 0; volnew[i - 1] = 0.0f; ncellv[i - 1] = 0; rm[i] = 0; }
+        c.sync();
+    };
+    auto count_cells = [&]() {
+        int32_t *nc_d = c.get_t<int32_t>(B_RED2, nvs);
+        AV_CUDA(cudaMemsetAsync(nc_d, 0, sizeof(int32_t) * (size_t)nvs, c.stream));
+        push_uvoid();
+        k_ncellv<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, uv_d, nc_d);
+        dev_download(c, ncellv.data(), nc_d, nv);
+    };
+    count_cells();
+    for (int32_t I = 0; I < nv; I++) {                        // NCELL_MIN = 10
+        const int32_t ind = indice[I];
+        if (uvoid[ind - 1] >= 0) continue;
+        if (ncellv[ind - 1] < 10) rm[ind] = 1;
+    }
+    apply_removals();
+
+    // ---- VOID_SHAPE
+    std::vector<float> eps(nvs, 0.0f), ipv(nvs, 0.0f);
+    {
+        float *rad_d = dev_upload<float>(c, B_RAD, L.rad.data(), L.rad.size());
+        float *gc_d = c.get_t<float>(B_RED0, (size_t)nvs * 3);
+        AV_CUDA(cudaMemcpyAsync(gc_d, mo.gxc.data(), sizeof(float) * nv, cudaMemcpyHostToDevice, c.stream));
+        AV_CUDA(cudaMemcpyAsync(gc_d + nvs, mo.gyc.data(), sizeof(float) * nv, cudaMemcpyHostToDevice, c.stream));
+        AV_CUDA(cudaMemcpyAsync(gc_d + 2 * nvs, mo.gzc.data(), sizeof(float) * nv, cudaMemcpyHostToDevice, c.stream));
+        double *in_d = c.get_t<double>(B_SCAN_A, (size_t)nvs * 6);
+        AV_CUDA(cudaMemsetAsync(in_d, 0, sizeof(double) * 6 * (size_t)nvs, c.stream));
+        k_inertia<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, rad_d, g.rad_lo, gc_d, gc_d + nvs, gc_d + 2 * nvs, in_d);
+        std::vector<double> inert((size_t)nvs * 6);
+        dev_download(c, inert.data(), in_d, (size_t)nv * 6);
+        for (int32_t I = 0; I < nv; I++) {
+            const int32_t ind = indice[I];
+            if (uvoid[ind - 1] != -1) continue;
+            const double *s = &inert[(size_t)(ind - 1) * 6];
+            const float n = (float)ncellv[ind - 1];
+            float a[3][3];
+            a[0][0] = (float)s[0] / n; a[1][1] = (float)s[1] / n; a[2][2] = (float)s[2] / n;
+            a[0][1] = a[1][0] = (float)s[3] / n;
+            a[0][2] = a[2][0] = (float)s[4] / n;
+            a[1][2] = a[2][1] = (float)s[5] / n;
+            float ev[3] = {0.0f, 0.0f, 0.0f}, ax[3];
+            jacobi3_ref(a, ev);
+            ax[0] = std::sqrt(2.5f * std::fabs((ev[1] + ev[2]) - ev[0]));
+            ax[1] = std::sqrt(2.5f * std::fabs((ev[2] + ev[0]) - ev[1]));
+            ax[2] = std::sqrt(2.5f * std::fabs((ev[0] + ev[1]) - ev[2]));
+            sort_desc3_ref(ax);
+            float e = 1.0f - ax[2] / ax[0];
+            const float volm = (((float)ncellv[ind - 1] * dx) * dx) * dx;
+            const float vell = (float)(((((double)(4.0f / 3.0f) * pi) * (double)ax[0]) * (double)ax[1]) * (double)ax[2]);
+            float ip = volm / vell;
+            if (ip > 1.0f) { ip = -99.0f; e = -99.0f; }
+            eps[ind - 1] = e;
+            ipv[ind - 1] = ip;
+        }
+    }
+    const float cellv = (dx * dx) * dx;
+    const double vmin = ((double)(4.0f / 3.0f) * pi) * (double)((p->rmin * p->rmin) * p->rmin);
+    auto redefine_volnew = [&]() {
+        for (int32_t i = 0; i < nv; i++) volnew[i] = 0.0f;
+        for (int32_t I = 0; I < nv; I++) {
+            const int32_t ind = indice[I];
+            if (uvoid[ind - 1] >= 0) continue;
+            volnew[ind - 1] = (float)((double)ncellv[ind - 1] * (double)cellv);
+        }
+    };
+    auto rmin_filter = [&]() {
+        for (int32_t I = 0; I < nv; I++) {
+            const int32_t ind = indice[I];
+            if (uvoid[ind - 1] >= 0) continue;
+            if ((double)volnew[ind - 1] < vmin) rm[ind] = 1;
+        }
+        apply_removals();
+    };
+    redefine_volnew();
+    rmin_filter();
+    std::vector<float> xc(nvs, 0.0f), yc(nvs, 0.0f), zc(nvs, 0.0f);
+    for (int32_t I = 0; I < nv; I++) {
+        const int32_t ind = indice[I];
+        if (uvoid[ind - 1] >= 0) continue;
+        xc[ind - 1] = L.rad_at(1) + (float)(cb->icx[ind - 1] - 1) * dx;
+        yc[ind - 1] = L.rad_at(1) + (float)(cb->icy[ind - 1] - 1) * dx;
+        zc[ind - 1] = L.rad_at(1) + (float)(cb->icz[ind - 1] - 1) * dx;
+    }
+
+    // ---- SIMPLE_CONNECTION_FAST
+    {
+        int32_t *P = c.get_t<int32_t>(B_CCL, ne3);
+        int32_t *m2 = c.get_t<int32_t>(B_PAINT, ne3);
+        k_ccl_init<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, P);
+        k_ccl_union<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, P);
+        k_ccl_flatten<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, P);
+        k_fill_holes<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, P, marca, m2);
+        AV_CUDA(cudaMemcpyAsync(marca, m2, (size_t)ne3 * 4, cudaMemcpyDeviceToDevice, c.stream));
+        AV_CUDA(cudaGetLastError());
+    }
+
+    // ---- VOID_PERIODIC
+    if (p->periodic) {
+        std::vector<int32_t> has(nvs, 0);
+        {
+            int32_t *has_d = c.get_t<int32_t>(B_RED2, nvs);
+            AV_CUDA(cudaMemsetAsync(has_d, 0, sizeof(int32_t) * (size_t)nvs, c.stream));
+            k_inner_presence<<<grid_for((int64_t)nx * nx * nx, 256), 256, 0, c.stream>>>(PG, marca, has_d);
+            dev_download(c, has.data(), has_d, nv);
+        }
+        std::vector<int32_t> kept;
+        for (int32_t I = 0; I < nv; I++) {
+            const int32_t ind = indice[I];
+            if (uvoid[ind - 1] >= 0) continue;
+            if (!has[ind - 1]) rm[ind] = 1; else kept.push_back(ind);
+        }
+        apply_removals();
+        const float half = p->lado0 / 2.0f;
+        std::vector<int8_t> shift((size_t)nvs * 3, 0);
+        std::vector<int32_t> ind2spec(nvs, 0);
+        std::vector<int32_t> outer;
+        std::vector<int64_t> centre_cell(nvs, -1);
+        for (int32_t ind : kept) {
+            const float x = mo.gxc[ind - 1], y = mo.gyc[ind - 1], z = mo.gzc[ind - 1];
+            int s[3] = {0, 0, 0};
+            if (x < -half) s[0] = 1; if (x > half) s[0] = -1;
+            if (y < -half) s[1] = 1; if (y > half) s[1] = -1;
+            if (z < -half) s[2] = 1; if (z > half) s[2] = -1;
+            if (!s[0] && !s[1] && !s[2]) continue;
+            const int ig[3] = {(int)((x - L.rad_at(1)) / dx) + 1, (int)((y - L.rad_at(1)) / dx) + 1,
+                               (int)((z - L.rad_at(1)) / dx) + 1};
+            int cc[3];
+            bool ok = true;
+            for (int a = 0; a < 3; a++) {
+                cc[a] = ig[a] + s[a] * nx;
+                if (cc[a] < g.low1 || cc[a] > g.low2) ok = false;
+            }
+            if (!ok) continue;
+            for (int a = 0; a < 3; a++) shift[(size_t)(ind - 1) * 3 + a] = (int8_t)s[a];
+            centre_cell[ind - 1] = (int64_t)(cc[0] - g.low1) + (int64_t)ne * ((int64_t)(cc[1] - g.low1) + (int64_t)ne * (cc[2] - g.low1));
+            outer.push_back(ind);
+        }
+        if (!outer.empty()) {
+            // labels at the shifted centres, initial state
+            std::vector<int32_t> m0(outer.size());
+            for (size_t q = 0; q < outer.size(); q++) {
+                AV_CUDA(cudaMemcpyAsync(&m0[q], marca + centre_cell[outer[q] - 1], sizeof(int32_t),
+                                        cudaMemcpyDeviceToHost, c.stream));
+            }
+            c.sync();
+            for (size_t q = 0; q < outer.size(); q++) ind2spec[outer[q] - 1] = m0[q];
+            std::vector<int32_t> labmap(nvs + 1);
+            for (int32_t i = 0; i <= nv; i++) labmap[i] = i;
+            int32_t *lm_d = dev_upload<int32_t>(c, B_LABMAP, labmap.data(), nv + 1);
+            int8_t *sh_d = dev_upload<int8_t>(c, B_RED0, shift.data(), (size_t)nvs * 3);
+            int32_t *i2_d = dev_upload<int32_t>(c, B_RED1, ind2spec.data(), nvs);
+            int32_t *cnt_d = c.get_t<int32_t>(B_RED2, (size_t)nvs * 2);
+            AV_CUDA(cudaMemsetAsync(cnt_d, 0, sizeof(int32_t) * 2 * (size_t)nvs, c.stream));
+            k_periodic_counts<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, lm_d, sh_d, i2_d, 0, cnt_d);
+            std::vector<int32_t> cnt((size_t)nvs * 2);
+            dev_download(c, cnt.data(), cnt_d, (size_t)nv * 2);
+            std::vector<int32_t> bb((size_t)nvs * 6);
+            {
+                int32_t *bb_d = c.get_t<int32_t>(B_SCAN_B, (size_t)nvs * 6);
+                std::vector<int32_t> init((size_t)nvs * 6);
+                for (int32_t i = 0; i < nvs; i++)
+                    for (int a = 0; a < 3; a++) { init[(size_t)i * 6 + a] = INT_MAX; init[(size_t)i * 6 + 3 + a] = INT_MIN; }
+                AV_CUDA(cudaMemcpyAsync(bb_d, init.data(), sizeof(int32_t) * init.size(), cudaMemcpyHostToDevice, c.stream));
+                k_bbox<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, bb_d);
+                dev_download(c, bb.data(), bb_d, (size_t)nv * 6);
+            }
+            // union-find over labels for CHANGE_BELONG
+            std::vector<int32_t> parent(nvs + 1);
+            for (int32_t i = 0; i <= nv; i++) parent[i] = i;
+            std::function<int32_t(int32_t)> find = [&](int32_t x) {
+                while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; }
+                return x;
+            };
+            std::vector<std::vector<int32_t>> members(nvs + 1);
+            std::vector<std::array<int32_t, 6>> curbb(nvs + 1);
+            for (int32_t i = 1; i <= nv; i++) {
+                for (int a = 0; a < 6; a++) curbb[i][a] = bb[(size_t)(i - 1) * 6 + a];
+            }
+            std::vector<std::array<int32_t, 6>> changed_bb;
+            bool lm_dirty = false;
+            for (int32_t ind : outer) {
+                const int8_t *s = &shift[(size_t)(ind - 1) * 3];
+                int32_t i2 = ind2spec[ind - 1];
+                if (i2 > 0) i2 = find(i2);
+                if (i2 == 0) continue;
+                // could an earlier CHANGE_BELONG have touched this void's counts?
+                bool affected = !members[ind].empty() || i2 != ind2spec[ind - 1];
+                const auto &b = curbb[ind];
+                if (!affected && b[0] <= b[3]) {
+                    for (const auto &cbx : changed_bb) {
+                        bool inter = true;
+                        for (int a = 0; a < 3; a++) {
+                            const int lo = b[a] + s[a] * nx, hi = b[3 + a] + s[a] * nx;
+                            if (hi < cbx[a] || lo > cbx[3 + a]) inter = false;
+                        }
+                        if (inter) { affected = true; break; }
+                    }
+                }
+                int64_t counter = cnt[(size_t)(ind - 1) * 2], counter2 = cnt[(size_t)(ind - 1) * 2 + 1];
+                if (affected) {
+                    if (lm_dirty) {
+                        std::vector<int32_t> flat(nvs + 1);
+                        for (int32_t i = 0; i <= nv; i++) flat[i] = i == 0 ? 0 : find(i);
+                        AV_CUDA(cudaMemcpyAsync(lm_d, flat.data(), sizeof(int32_t) * (size_t)(nv + 1), cudaMemcpyHostToDevice, c.stream));
+                        lm_dirty = false;
+                    }
+                    std::vector<int32_t> i2v(nvs, 0);
+                    i2v[ind - 1] = i2;
+                    int32_t *i2d = dev_upload<int32_t>(c, B_RED1, i2v.data(), nvs);
+                    int32_t *one = c.get_t<int32_t>(B_RED2, (size_t)nvs * 2);
+                    AV_CUDA(cudaMemsetAsync(one + (size_t)(ind - 1) * 2, 0, 8, c.stream));
+                    k_periodic_counts<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, lm_d, sh_d, i2d, ind, one);
+                    int32_t r2[2];
+                    dev_download(c, r2, one + (size_t)(ind - 1) * 2, 2);
+                    counter = r2[0];
+                    counter2 = r2[1];
+                }
+                const float inter = counter2 == 0 ? 0.0f : (float)counter / (float)counter2;
+                if (inter > 0.4f) {                                  // CHANGE_BELONG(IND2, IND)
+                    uvoid[ind - 1] = i2;
+                    for (int32_t i = 0; i < nv; i++) if (uvoid[i] == ind) uvoid[i] = i2;
+                    if (i2 != ind) {
+                        parent[ind] = i2;
+                        members[i2].push_back(ind);
+                        for (int32_t mm : members[ind]) members[i2].push_back(mm);
+                        auto &tb = curbb[i2];
+                        for (int a = 0; a < 3; a++) {
+                            tb[a] = std::min(tb[a], b[a]);
+                            tb[3 + a] = std::max(tb[3 + a], b[3 + a]);
+                        }
+                        changed_bb.push_back(b);
+                        lm_dirty = true;
+                    }
+                    volnew[ind - 1] = 0.0f;
+                }
+            }
+            // apply the label changes to MARCA
+            std::vector<int32_t> flat(nvs + 1);
+            for (int32_t i = 0; i <= nv; i++) flat[i] = i == 0 ? 0 : find(i);
+            AV_CUDA(cudaMemcpyAsync(map_d, flat.data(), sizeof(int32_t) * (size_t)(nv + 1), cudaMemcpyHostToDevice, c.stream));
+            k_relabel<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, map_d);
+            c.sync();
+        }
+    }
+
+    // ---- global properties (inner cells), VOLNEW, RMIN, NVOIDT
+    std::vector<float> umean(nvs, 0.0f), mtot(nvs, 0.0f);
+    double volt = 0.0;
+    {
+        int32_t *nc_d = c.get_t<int32_t>(B_RED2, nvs);
+        double *sum_d = c.get_t<double>(B_SCAN_A, (size_t)nvs * 2);
+        AV_CUDA(cudaMemsetAsync(nc_d, 0, sizeof(int32_t) * (size_t)nvs, c.stream));
+        AV_CUDA(cudaMemsetAsync(sum_d, 0, sizeof(double) * 2 * (size_t)nvs, c.stream));
+        push_uvoid();
+        const float rete3 = (g.rete * g.rete) * g.rete;
+        k_final_props<<<grid_for((int64_t)nx * nx * nx, 256), 256, 0, c.stream>>>(PG, marca, uv_d, u1co_inner,
+                                                                                  meandens, dx, rete3, nc_d, sum_d);
+        std::vector<double> sums((size_t)nvs * 2);
+        dev_download(c, ncellv.data(), nc_d, nv);
+        dev_download(c, sums.data(), sum_d, (size_t)nv * 2);
+        int64_t ncount = 0;
+        for (int32_t i = 0; i < nv; i++) {
+            umean[i] = (float)sums[(size_t)i * 2];
+            mtot[i] = (float)sums[(size_t)i * 2 + 1];
+            ncount += ncellv[i];
+            if (ncellv[i] > 0) umean[i] = umean[i] / (float)ncellv[i];
+        }
+        volt = (double)ncount * (double)cellv;
+    }
+    redefine_volnew();
+    rmin_filter();
+    int32_t nvoidt = 0;
+    std::vector<float> req(nvs, 0.0f);
+    for (int32_t i = 0; i < nv; i++) {
+        if (uvoid[i] != -1) continue;
+        nvoidt++;
+        req[i] = (float)std::pow((3.0 * (double)volnew[i]) / (4.0 * pi), (double)(1.0f / 3.0f));
+    }
+
+    // ---- outputs
+    auto put_i = [&](int32_t *dst, const std::vector<int32_t> &v) { if (dst) from_device(c, dst, v.data(), sizeof(int32_t) * (size_t)nv); };
+    auto put_f = [&](float *dst, const std::vector<float> &v) { if (dst) from_device(c, dst, v.data(), sizeof(float) * (size_t)nv); };
+    put_i(out->indice, indice);
+    put_i(out->uvoid, uvoid);
+    put_i(out->ncellv, ncellv);
+    put_f(out->volnew, volnew);
+    put_f(out->req, req);
+    put_f(out->xc, xc); put_f(out->yc, yc); put_f(out->zc, zc);
+    put_f(out->gxc, mo.gxc); put_f(out->gyc, mo.gyc); put_f(out->gzc, mo.gzc);
+    put_f(out->eps, eps); put_f(out->ip, ipv);
+    put_f(out->umean, umean); put_f(out->mtot, mtot);
+    out->nvoid2 = mo.nvoid2;
+    out->nvoidt = nvoidt;
+    out->volt_clean = volt;
+    if (marca_ext_out) from_device(c, marca_ext_out, marca, (size_t)ne3 * 4);
+    c.sync();
+}
+
+}  // namespace avism

@@ -1,0 +1,520 @@
+// sph.cu -- SPH particle-to-grid interpolation on the exact kNN engine.
+//
+// Replaces src/particles.f90: PPART_DENS (742-801), VVEL_INTERP_SPH_VW
+// (806-929) with KERNEL_FUNC (935-963), H_DISTANCE (276-350), FILL_H_ZEROS
+// (398-430) and DDENS_INTERP_SPH (434-617).  Every REAL*4 expression is
+// evaluated in the reference's order (the library is built with --fmad=false);
+// the reference's REAL*8 accumulators stay REAL*8.  DDENS's FP64 atomic
+// scatter becomes a 128-bit fixed-point scatter, which is exact and order
+// independent, so the grid does not depend on thread timing.
+#include <cub/cub.cuh>
+#include <cfloat>
+
+#include "common.cuh"
+#include "knn_core.cuh"
+
+namespace avism {
+
+__device__ __forceinline__ float kernel_m4(float h, float dist) {
+    // KERNEL_FUNC, M4 branch: Q = DIST/(H/2)
+    const float q = __fdiv_rn(dist, __fdiv_rn(h, 2.0f));
+    if (q <= 1.0f) return __fsub_rn(1.0f, __fmul_rn(__fmul_rn(1.5f, __fmul_rn(q, q)), __fsub_rn(1.0f, __fmul_rn(0.5f, q))));
+    if (q <= 2.0f) {
+        const float t = __fsub_rn(2.0f, q);
+        return __fmul_rn(0.25f, __fmul_rn(__fmul_rn(t, t), t));
+    }
+    return 0.0f;
+}
+
+// HPART(j) = MAX(HPART(j), d): non-negative floats order as their int bits
+__device__ __forceinline__ void atomic_max_pos(float *a, float v) {
+    atomicMax((int *)a, __float_as_int(v));
+}
+
+// cell (ix, jy, kz), 1-based, of thread t in a tiled traversal of the NX^3 grid
+__device__ __forceinline__ bool tile_cell(int nx, int tx, int ty, int tz, int &ix, int &jy, int &kz) {
+    const int ntx = (nx + tx - 1) / tx, nty = (nx + ty - 1) / ty;
+    const int64_t b = blockIdx.x;
+    const int bx = (int)(b % ntx), by = (int)((b / ntx) % nty), bz = (int)(b / ((int64_t)ntx * nty));
+    const int t = threadIdx.x;
+    ix = bx * tx + (t % tx) + 1;
+    jy = by * ty + ((t / tx) % ty) + 1;
+    kz = bz * tz + t / (tx * ty) + 1;
+    return ix <= nx && jy <= nx && kz <= nx;
+}
+
+template <int T> struct TileDims;
+template <> struct TileDims<256> { static constexpr int x = 8, y = 8, z = 4; };
+template <> struct TileDims<128> { static constexpr int x = 8, y = 4, z = 4; };
+template <> struct TileDims<64> { static constexpr int x = 4, y = 4, z = 4; };
+template <> struct TileDims<32> { static constexpr int x = 4, y = 4, z = 2; };
+
+// ---- PPART_DENS: rho_p = sum_k m / ((4/3) pi h_k^3) ------------------------------
+template <int KCAP>
+__global__ void __launch_bounds__(KNN_THREADS(KCAP))
+k_ppart_dens(KnnGrid G, int64_t n, int K, const float *__restrict__ m, float *__restrict__ part_dens) {
+    extern __shared__ unsigned long long knn_smem[];
+    const int S = blockDim.x;
+    unsigned long long *col = knn_smem + threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = G.sp[i];
+    const int cnt = knn_query<KCAP>(G, p.x, p.y, p.z, K, col, S);
+    double bas8 = 0.0;
+    for (int j = 0; j < cnt; j++) bas8 = bas8 + (double)m[key_idx(col[(size_t)j * S])];
+    const float hk = sqrtf(key_d2(col[(size_t)(K - 1) * S]));
+    const double pi = 3.141592653589793;     // DACOS(-1.D0)
+    part_dens[__float_as_int(p.w)] = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(hk, hk), hk)));
+}
+
+// ---- FILL_H_ZEROS: h = k-th neighbour distance where h is still 0 -----------
+template <int KCAP>
+__global__ void __launch_bounds__(KNN_THREADS(KCAP))
+k_fill_h(KnnGrid G, int64_t n, int K, float *__restrict__ hpart) {
+    extern __shared__ unsigned long long knn_smem[];
+    const int S = blockDim.x;
+    unsigned long long *col = knn_smem + threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = G.sp[i];
+    const int o = __float_as_int(p.w);
+    if (hpart[o] > 0.0f) return;
+    knn_query<KCAP>(G, p.x, p.y, p.z, K, col, S);
+    hpart[o] = sqrtf(key_d2(col[(size_t)(K - 1) * S]));
+}
+
+struct CellArgs {
+    int nx, rad_lo, K;
+    float dx;
+    const float *rad;
+    const int8_t *smask;
+    const float *m, *vx, *vy, *vz, *part_dens;
+    float *hpart, *u2, *u3, *u4;
+    int do_vel;
+    int32_t *ball_list;
+    int32_t *ball_count;
+};
+
+// ---- VVEL_INTERP_SPH_VW / H_DISTANCE for cells whose k-th distance > DX ------
+template <int KCAP>
+__global__ void __launch_bounds__(KNN_THREADS(KCAP))
+k_cells_knn(KnnGrid G, CellArgs A) {
+    extern __shared__ unsigned long long knn_smem[];
+    constexpr int T = KNN_THREADS(KCAP);
+    const int S = blockDim.x;
+    unsigned long long *col = knn_smem + threadIdx.x;
+    int ix, jy, kz;
+    if (!tile_cell(A.nx, TileDims<T>::x, TileDims<T>::y, TileDims<T>::z, ix, jy, kz)) return;
+    const int64_t c = (int64_t)(ix - 1) + (int64_t)A.nx * ((int64_t)(jy - 1) + (int64_t)A.nx * (kz - 1));
+    if (A.smask && A.smask[c] == 0) return;
+    const float qx = A.rad[ix - A.rad_lo], qy = A.rad[jy - A.rad_lo], qz = A.rad[kz - A.rad_lo];
+    const int K = A.K;
+    const int cnt = knn_query<KCAP>(G, qx, qy, qz, K, col, S);
+    const float hk = sqrtf(key_d2(col[(size_t)(cnt - 1) * S]));
+    if (!(hk > A.dx)) {                       // ball_search(TREE, TAR, DX) branch
+        const int slot = atomicAdd(A.ball_count, 1);
+        A.ball_list[slot] = (int32_t)c;
+        return;
+    }
+    for (int i = 0; i < cnt; i++) {
+        const unsigned long long key = col[(size_t)i * S];
+        atomic_max_pos(&A.hpart[key_idx(key)], sqrtf(key_d2(key)));
+    }
+    if (!A.do_vel) return;
+    double b = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
+    for (int i = 0; i < cnt; i++) {
+        const unsigned long long key = col[(size_t)i * S];
+        const uint32_t j = key_idx(key);
+        float w = kernel_m4(hk, sqrtf(key_d2(key)));
+        w = __fmul_rn(w, __fdiv_rn(A.m[j], A.part_dens[j]));
+        const double w8 = (double)w;
+        b = b + w8;
+        bx = bx + w8 * (double)A.vx[j];
+        by = by + w8 * (double)A.vy[j];
+        bz = bz + w8 * (double)A.vz[j];
+    }
+    A.u2[c] = (float)(bx / b);
+    A.u3[c] = (float)(by / b);
+    A.u4[c] = (float)(bz / b);
+}
+
+// ---- cells in the ball branch: all particles within DX (src/particles.f90:868-878)
+__global__ void k_cells_ball(KnnGrid G, CellArgs A, int32_t nlist) {
+    const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (t >= nlist) return;
+    const int64_t c = A.ball_list[t];
+    const int nx = A.nx;
+    const int ix = (int)(c % nx) + 1, jy = (int)((c / nx) % nx) + 1, kz = (int)(c / ((int64_t)nx * nx)) + 1;
+    const float q[3] = {A.rad[ix - A.rad_lo], A.rad[jy - A.rad_lo], A.rad[kz - A.rad_lo]};
+    const float r2 = __fmul_rn(A.dx, A.dx);                   // radius**2 in REAL*4
+    const int b[3] = {bin_coord(q[0], G.origin, G.inv_bw, G.nb), bin_coord(q[1], G.origin, G.inv_bw, G.nb),
+                      bin_coord(q[2], G.origin, G.inv_bw, G.nb)};
+    const int sb = (int)ceilf(A.dx * G.inv_bw) + 1;
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; a++) axis_window(G, b[a], sb, lo[a], hi[a]);
+    float dmax2 = -1.0f;
+    for (int pass = 0; pass < (A.do_vel ? 2 : 1); pass++) {
+        const float hk = sqrtf(dmax2);
+        double bs = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
+        for (int dz = lo[2]; dz <= hi[2]; dz++) {
+            const int bz_ = G.periodic ? wrap_bin(b[2] + dz, G.nb) : b[2] + dz;
+            for (int dy = lo[1]; dy <= hi[1]; dy++) {
+                const int by_ = G.periodic ? wrap_bin(b[1] + dy, G.nb) : b[1] + dy;
+                for (int dx = lo[0]; dx <= hi[0]; dx++) {
+                    const int bx_ = G.periodic ? wrap_bin(b[0] + dx, G.nb) : b[0] + dx;
+                    const int bin = bx_ + G.nb * (by_ + G.nb * bz_);
+                    for (int64_t p = G.start[bin]; p < G.start[bin + 1]; p++) {
+                        const float4 v = G.sp[p];
+                        const float d2 = dist2_ref(v.x, v.y, v.z, q[0], q[1], q[2], G.box, G.periodic);
+                        if (!(d2 <= r2)) continue;
+                        const int j = __float_as_int(v.w);
+                        if (pass == 0) {
+                            dmax2 = fmaxf(dmax2, d2);
+                            atomic_max_pos(&A.hpart[j], sqrtf(d2));
+                        } else {
+                            float w = kernel_m4(hk, sqrtf(d2));
+                            w = __fmul_rn(w, __fdiv_rn(A.m[j], A.part_dens[j]));
+                            const double w8 = (double)w;
+                            bs = bs + w8;
+                            bx = bx + w8 * (double)A.vx[j];
+                            by = by + w8 * (double)A.vy[j];
+                            bz = bz + w8 * (double)A.vz[j];
+                        }
+                    }
+                }
+            }
+        }
+        if (pass == 1) {
+            A.u2[c] = (float)(bx / bs);
+            A.u3[c] = (float)(by / bs);
+            A.u4[c] = (float)(bz / bs);
+        }
+    }
+}
+
+// ---- DDENS_INTERP_SPH: per-particle NORM in the reference's loop order, then
+//      a 128-bit fixed-point scatter of m*w/NORM --------------------------------
+struct DdensArgs {
+    int nx, rad_lo;
+    float dx, rx1;
+    const float *rad, *hpart, *m;
+    unsigned long long *fix;      // 2 words per cell: low, high
+    double scale;
+};
+
+__device__ __forceinline__ void add128(unsigned long long *cell, unsigned long long v) {
+    const unsigned long long old = atomicAdd(cell, v);
+    if (old + v < old) atomicAdd(cell + 1, 1ULL);
+}
+
+__device__ __forceinline__ float m4_q(float d2, float inv_h) {
+    const float q = __fmul_rn(sqrtf(d2), inv_h);
+    if (q <= 1.0f) return __fsub_rn(1.0f, __fmul_rn(__fmul_rn(1.5f, __fmul_rn(q, q)), __fsub_rn(1.0f, __fmul_rn(0.5f, q))));
+    if (q <= 2.0f) {
+        const float t = __fsub_rn(2.0f, q);
+        return __fmul_rn(0.25f, __fmul_rn(__fmul_rn(t, t), t));
+    }
+    return 0.0f;
+}
+
+__global__ void k_ddens(KnnGrid G, int64_t n, DdensArgs A) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = G.sp[i];
+    const int o = __float_as_int(p.w);
+    const int nx = A.nx;
+    const float dx = A.dx;
+    const int ix = (int)__fdiv_rn(__fsub_rn(p.x, A.rx1), dx) + 1;
+    const int jy = (int)__fdiv_rn(__fsub_rn(p.y, A.rx1), dx) + 1;
+    const int kz = (int)__fdiv_rn(__fsub_rn(p.z, A.rx1), dx) + 1;
+    const float h = A.hpart[o];
+    const float inv_h = __fdiv_rn(2.0f, h);
+    const float h2max = __fmul_rn(__fmul_rn(4.0f, h), h);
+    const int inc = (int)__fadd_rn(__fdiv_rn(__fmul_rn(2.0f, h), dx), 0.5f);
+    // only cells with Q < 2 carry weight; rows and planes beyond h are skipped
+    const float hh = h * h * 1.00002f + 1e-30f;
+    const float *rad = A.rad - A.rad_lo;
+    const float m = A.m[o];
+    const int k_lo = max(kz - inc, 1), k_hi = min(kz + inc, nx);
+    const int j_lo = max(jy - inc, 1), j_hi = min(jy + inc, nx);
+    const int i_lo = max(ix - inc, 1), i_hi = min(ix + inc, nx);
+    float norm = 0.0f;
+    for (int pass = 0; pass < 2; pass++) {
+        for (int k2 = k_lo; k2 <= k_hi; k2++) {
+            const float tz = __fsub_rn(p.z, rad[k2]);
+            const float dz2 = __fmul_rn(tz, tz);
+            if (dz2 > hh) continue;
+            for (int j2 = j_lo; j2 <= j_hi; j2++) {
+                const float ty = __fsub_rn(p.y, rad[j2]);
+                const float dy2 = __fmul_rn(ty, ty);
+                const float rem = hh - dz2 - dy2;
+                if (rem < 0.0f) continue;
+                const float R = sqrtf(rem) * 1.00001f + 1e-6f * dx;
+                const int a = max(i_lo, (int)floorf((p.x - R - A.rx1) / dx) + 1 - 1);
+                const int e = min(i_hi, (int)ceilf((p.x + R - A.rx1) / dx) + 1 + 1);
+                for (int i2 = a; i2 <= e; i2++) {
+                    const float tx = __fsub_rn(p.x, rad[i2]);
+                    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), dy2), dz2);
+                    if (d2 > h2max) continue;
+                    const float w = m4_q(d2, inv_h);
+                    if (pass == 0) {
+                        norm = __fadd_rn(norm, w);
+                    } else if (w != 0.0f) {
+                        const float contrib = __fdiv_rn(__fmul_rn(w, m), norm);
+                        const unsigned long long v = (unsigned long long)llrint((double)contrib * A.scale);
+                        const int64_t cid = (int64_t)(i2 - 1) + (int64_t)nx * ((int64_t)(j2 - 1) + (int64_t)nx * (k2 - 1));
+                        add128(A.fix + 2 * cid, v);
+                    }
+                }
+            }
+        }
+        if (pass == 0 && norm == 0.0f) {
+            // the particle only contributes to its own cell
+            if (ix >= 1 && ix <= nx && jy >= 1 && jy <= nx && kz >= 1 && kz <= nx) {
+                const int64_t cid = (int64_t)(ix - 1) + (int64_t)nx * ((int64_t)(jy - 1) + (int64_t)nx * (kz - 1));
+                add128(A.fix + 2 * cid, (unsigned long long)llrint((double)m * A.scale));
+            }
+            break;
+        }
+    }
+}
+
+__global__ void k_fix128_to_f32(int64_t nc, const unsigned long long *__restrict__ fix, double inv_scale,
+                                float *__restrict__ out) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const unsigned long long lo = fix[2 * c], hi = fix[2 * c + 1];
+    const double v = ((double)hi * 18446744073709551616.0 + (double)lo) * inv_scale;
+    out[c] = (float)v;
+}
+
+// ---- TSC (DENS_INTERP_TSC / VEL_INTERP_TSC) as a gather over TSC cells -------
+// Particles are sorted by their TSC cell I (src/particles.f90:73-75); each grid
+// cell gathers from the 27 neighbouring TSC cells in a fixed order.
+struct TscArgs {
+    int nx, rad_lo, periodic;
+    float dx, r1, rn, leng;
+    const float *rad;
+};
+
+__device__ __forceinline__ void tsc_axis(const TscArgs &A, float xt, int &cell, float w[3]) {
+    const float *rad = A.rad - A.rad_lo;
+    if (A.periodic) {
+        if (xt < A.r1) xt = __fadd_rn(xt, A.leng);
+        if (xt >= A.rn) xt = __fsub_rn(xt, A.leng);
+    }
+    const int i = (int)__fadd_rn(__fdiv_rn(__fsub_rn(xt, rad[1]), A.dx), 0.49999f) + 1;
+    float bas = fabsf(__fsub_rn(rad[i - 1], xt));
+    float t = __fsub_rn(1.5f, __fdiv_rn(bas, A.dx));
+    w[0] = __fmul_rn(0.5f, __fmul_rn(t, t));
+    bas = fabsf(__fsub_rn(rad[i], xt));
+    t = __fdiv_rn(bas, A.dx);
+    w[1] = __fsub_rn(0.75f, __fmul_rn(t, t));
+    bas = fabsf(__fsub_rn(rad[i + 1], xt));
+    t = __fsub_rn(1.5f, __fdiv_rn(bas, A.dx));
+    w[2] = __fmul_rn(0.5f, __fmul_rn(t, t));
+    cell = i;
+}
+
+__global__ void k_tsc_keys(int64_t n, const float *__restrict__ x, const float *__restrict__ y,
+                           const float *__restrict__ z, TscArgs A, uint32_t *__restrict__ keys,
+                           int32_t *__restrict__ vals) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int ci, cj, ck;
+    float w[3];
+    tsc_axis(A, x[i], ci, w);
+    tsc_axis(A, y[i], cj, w);
+    tsc_axis(A, z[i], ck, w);
+    keys[i] = (uint32_t)(ci - 1) + (uint32_t)A.nx * ((uint32_t)(cj - 1) + (uint32_t)A.nx * (uint32_t)(ck - 1));
+    vals[i] = (int32_t)i;
+}
+
+__global__ void k_tsc_gather(int64_t nc, const int64_t *__restrict__ start, const int32_t *__restrict__ order,
+                             const float *__restrict__ x, const float *__restrict__ y,
+                             const float *__restrict__ z, const float *__restrict__ m,
+                             const float *__restrict__ vx, const float *__restrict__ vy,
+                             const float *__restrict__ vz, TscArgs A, float *__restrict__ u_mass,
+                             float *__restrict__ u2, float *__restrict__ u3, float *__restrict__ u4) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const int nx = A.nx;
+    const int ix = (int)(c % nx) + 1, jy = (int)((c / nx) % nx) + 1, kz = (int)(c / ((int64_t)nx * nx)) + 1;
+    double dm = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0, sw = 0.0;
+    for (int oz = -1; oz <= 1; oz++) {
+        int k = kz + oz;
+        if (A.periodic) { if (k < 1) k += nx; if (k > nx) k -= nx; } else if (k < 1 || k > nx) continue;
+        for (int oy = -1; oy <= 1; oy++) {
+            int j = jy + oy;
+            if (A.periodic) { if (j < 1) j += nx; if (j > nx) j -= nx; } else if (j < 1 || j > nx) continue;
+            for (int ox = -1; ox <= 1; ox++) {
+                int i = ix + ox;
+                if (A.periodic) { if (i < 1) i += nx; if (i > nx) i -= nx; } else if (i < 1 || i > nx) continue;
+                const int64_t b = (int64_t)(i - 1) + (int64_t)nx * ((int64_t)(j - 1) + (int64_t)nx * (k - 1));
+                for (int64_t q = start[b]; q < start[b + 1]; q++) {
+                    const int32_t pidx = order[q];
+                    int ci, cj, ck;
+                    float wx[3], wy[3], wz[3];
+                    tsc_axis(A, x[pidx], ci, wx);
+                    tsc_axis(A, y[pidx], cj, wy);
+                    tsc_axis(A, z[pidx], ck, wz);
+                    // offset of this grid cell from the particle's TSC cell is -ox etc.
+                    const float fx = wx[1 - ox], fy = wy[1 - oy], fz = wz[1 - oz];
+                    if (u_mass) dm += (double)__fmul_rn(__fmul_rn(__fmul_rn(m[pidx], fx), fy), fz);
+                    if (u2) {
+                        const float w = __fmul_rn(__fmul_rn(fx, fy), fz);
+                        s2 += (double)__fmul_rn(vx[pidx], w);
+                        s3 += (double)__fmul_rn(vy[pidx], w);
+                        s4 += (double)__fmul_rn(vz[pidx], w);
+                        sw += (double)w;
+                    }
+                }
+            }
+        }
+    }
+    if (u_mass) u_mass[c] = (float)dm;
+    if (u2) {
+        float wei = (float)sw;
+        if (wei == 0.0f) wei = 1.0f;
+        u2[c] = __fdiv_rn((float)s2, wei);
+        u3[c] = __fdiv_rn((float)s3, wei);
+        u4[c] = __fdiv_rn((float)s4, wei);
+    }
+}
+
+// ---- out-of-box check (src/avism.f90:560-589) ---------------------------------
+__global__ void k_box_check(int64_t n, const float *x, const float *y, const float *z, float half, int *bad) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (x[i] < -half || x[i] > half || y[i] < -half || y[i] > half || z[i] < -half || z[i] > half) atomicOr(bad, 1);
+}
+
+__global__ void k_zero_f32(int64_t n, float *a) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = 0.0f;
+}
+
+template <int KCAP>
+static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, const Level &L,
+                            const P2G &a, const float *rad_d, bool vel_sph, bool need_h_cells) {
+    const int T = KNN_THREADS(KCAP);
+    const size_t sm = (size_t)KCAP * T * sizeof(unsigned long long);
+    const int K = p->kneighbours;
+    const int nx = L.g.nx;
+    const int64_t nc = (int64_t)nx * nx * nx;
+    AV_CUDA(cudaFuncSetAttribute(k_ppart_dens<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    AV_CUDA(cudaFuncSetAttribute(k_cells_knn<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    AV_CUDA(cudaFuncSetAttribute(k_fill_h<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    if (vel_sph)
+        k_ppart_dens<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, a.m, a.part_dens);
+    if (vel_sph || need_h_cells) {
+        int32_t *ball_list = c.get_t<int32_t>(B_BALL, nc);
+        int32_t *cnt_d = c.get_t<int32_t>(B_SCAL, 4);
+        AV_CUDA(cudaMemsetAsync(cnt_d, 0, sizeof(int32_t), c.stream));
+        CellArgs A;
+        A.nx = nx; A.rad_lo = L.g.rad_lo; A.K = K; A.dx = L.g.dx; A.rad = rad_d; A.smask = a.smask;
+        A.m = a.m; A.vx = a.vx; A.vy = a.vy; A.vz = a.vz; A.part_dens = a.part_dens;
+        A.hpart = a.hpart; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
+        A.ball_list = ball_list; A.ball_count = cnt_d;
+        const int tx = TileDims<T>::x, ty = TileDims<T>::y, tz = TileDims<T>::z;
+        const int64_t nblk = (int64_t)((nx + tx - 1) / tx) * ((nx + ty - 1) / ty) * ((nx + tz - 1) / tz);
+        k_cells_knn<KCAP><<<(unsigned)nblk, T, sm, c.stream>>>(G, A);
+        AV_CUDA(cudaGetLastError());
+        int32_t nball = 0;
+        AV_CUDA(cudaMemcpyAsync(&nball, cnt_d, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+        if (nball > 0) k_cells_ball<<<grid_for(nball, 128), 128, 0, c.stream>>>(G, A, nball);
+        AV_CUDA(cudaGetLastError());
+        k_fill_h<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, a.hpart);
+    }
+    AV_CUDA(cudaGetLastError());
+}
+
+void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G &a) {
+    const int nx = L.g.nx;
+    const int64_t nc = (int64_t)nx * nx * nx;
+    const int K = p->kneighbours;
+    AV_CHECK(K >= 1 && K <= 256, AVISM_ERR_ARG, "kneighbours must be in 1..256");
+    AV_CHECK(a.n >= K || (p->flag_vel_interp == 0 && p->flag_dens_interp == 0), AVISM_ERR_ARG,
+             "fewer particles than kneighbours");
+    // particles must lie in [-L0/2, L0/2]
+    {
+        int *bad = c.get_t<int>(B_SCAL, 4);
+        AV_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), c.stream));
+        if (a.n > 0) k_box_check<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.x, a.y, a.z, p->lado0 / 2.0f, bad);
+        int hbad = 0;
+        AV_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+        AV_CHECK(hbad == 0, AVISM_ERR_OUT_OF_BOX,
+                 "Particles outside the bounding box! Check L0! (must be inside [-L0/2, L0/2])");
+    }
+    float *rad_d = c.get_t<float>(B_RAD, L.rad.size());
+    AV_CUDA(cudaMemcpyAsync(rad_d, L.rad.data(), L.rad.size() * sizeof(float), cudaMemcpyHostToDevice, c.stream));
+    for (float *g : {a.u_mass, a.u2, a.u3, a.u4}) k_zero_f32<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, g);
+    k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.hpart);
+    k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.part_dens);
+    const bool vel_sph = p->flag_vel_interp == 1, dens_sph = p->flag_dens_interp == 1;
+    TscArgs TA;
+    TA.nx = nx; TA.rad_lo = L.g.rad_lo; TA.periodic = p->periodic; TA.dx = L.g.dx; TA.rad = rad_d;
+    TA.r1 = L.rad_at(1) - 0.5f * L.g.dx;
+    TA.rn = L.rad_at(nx) + 0.5f * L.g.dx;
+    TA.leng = TA.rn - TA.r1;
+    if (vel_sph || dens_sph) {
+        BinnedParticles bp = bin_particles(c, a.n, a.x, a.y, a.z, p->lado0, p->periodic, 4.0f);
+        KnnGrid G = make_knn_grid(bp);
+        const bool need_h_cells = dens_sph && !vel_sph;
+        if (K <= 32) run_sph_kernels<32>(c, G, p, L, a, rad_d, vel_sph, need_h_cells);
+        else if (K <= 64) run_sph_kernels<64>(c, G, p, L, a, rad_d, vel_sph, need_h_cells);
+        else if (K <= 128) run_sph_kernels<128>(c, G, p, L, a, rad_d, vel_sph, need_h_cells);
+        else run_sph_kernels<256>(c, G, p, L, a, rad_d, vel_sph, need_h_cells);
+        if (dens_sph) {
+            // scale: the largest term m*w/NORM <= m_max stays below 2^62
+            float mmax = 0.0f;
+            {
+                float *d = c.get_t<float>(B_RED0, 1);
+                size_t tmp = 0;
+                AV_CUDA(cub::DeviceReduce::Max(nullptr, tmp, a.m, d, (int)a.n, c.stream));
+                void *t = c.get(B_CUB_TMP, tmp);
+                AV_CUDA(cub::DeviceReduce::Max(t, tmp, a.m, d, (int)a.n, c.stream));
+                AV_CUDA(cudaMemcpyAsync(&mmax, d, sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+                c.sync();
+            }
+            AV_CHECK(mmax > 0.0f && std::isfinite(mmax), AVISM_ERR_ARG, "particle masses must be positive");
+            int e2;
+            std::frexp((double)mmax, &e2);              // mmax < 2^e2
+            const double scale = std::ldexp(1.0, 62 - e2);
+            unsigned long long *fix = c.get_t<unsigned long long>(B_FIX0, 2 * nc);
+            AV_CUDA(cudaMemsetAsync(fix, 0, 2 * nc * sizeof(unsigned long long), c.stream));
+            DdensArgs D;
+            D.nx = nx; D.rad_lo = L.g.rad_lo; D.dx = L.g.dx; D.rx1 = L.rad_at(1); D.rad = rad_d;
+            D.hpart = a.hpart; D.m = a.m; D.fix = fix; D.scale = scale;
+            k_ddens<<<grid_for(a.n, 128), 128, 0, c.stream>>>(G, a.n, D);
+            AV_CUDA(cudaGetLastError());
+            k_fix128_to_f32<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, fix, 1.0 / scale, a.u_mass);
+        }
+    }
+    if (!vel_sph || !dens_sph) {
+        // TSC: sort particles by their TSC cell, then gather
+        uint32_t *ka = c.get_t<uint32_t>(B_KEYS_A, a.n), *kb = c.get_t<uint32_t>(B_KEYS_B, a.n);
+        int32_t *va = c.get_t<int32_t>(B_VALS_A, a.n), *vb = c.get_t<int32_t>(B_VALS_B, a.n);
+        k_tsc_keys<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.x, a.y, a.z, TA, ka, va);
+        cub::DoubleBuffer<uint32_t> dk(ka, kb);
+        cub::DoubleBuffer<int32_t> dv(va, vb);
+        int end_bit = 1;
+        while ((1LL << end_bit) < nc) end_bit++;
+        size_t tmp = 0;
+        AV_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, (int)a.n, 0, end_bit, c.stream));
+        void *t = c.get(B_CUB_TMP, tmp);
+        AV_CUDA(cub::DeviceRadixSort::SortPairs(t, tmp, dk, dv, (int)a.n, 0, end_bit, c.stream));
+        int64_t *start = c.get_t<int64_t>(B_BIN_START, nc + 1);
+        float4 *dummy = c.get_t<float4>(B_SP, std::max<int64_t>(a.n, 1));
+        k_bin_gather<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, dk.Current(), dv.Current(), a.x, a.y, a.z,
+                                                                dummy, start, nc);
+        k_tsc_gather<<<grid_for(nc, 128), 128, 0, c.stream>>>(
+            nc, start, dv.Current(), a.x, a.y, a.z, a.m, a.vx, a.vy, a.vz, TA,
+            dens_sph ? nullptr : a.u_mass, vel_sph ? nullptr : a.u2, a.u3, a.u4);
+        AV_CUDA(cudaGetLastError());
+    }
+}
+
+}  // namespace avism

@@ -159,6 +159,14 @@ int avism_gpu_voidfind(avism_gpu_ctx *ctx, const avism_params *p, const float *u
                        const int32_t *marcap_ext, const float *reqp,
                        avism_cubes *cubes, int32_t *nvoid);
 
+/* ---- a14/a16: MARK_ALL (src/voidfinding.f90:13-55) and the six directional
+ *      flag grids of VOIDFIND (src/voidfinding.f90:256-432) as one byte per ext
+ *      cell: bit0 FLAGV, bit1 X1, bit2 X2, bit3 Y1, bit4 Y2, bit5 Z1, bit6 Z2,
+ *      bit7 FLAG_SUB.  Inputs as avism_gpu_voidfind.                             */
+int avism_gpu_flags(avism_gpu_ctx *ctx, const avism_params *p, const float *u1co_ext,
+                    const float *diverco_ext, const int8_t *smask_ext,
+                    const int32_t *marcap_ext, uint8_t *flags_ext);
+
 /* ---- a18: INDEXX (src/num.f90:2-84): the Numerical Recipes index sort,
  *      reproducing its exact permutation of equal keys.  indx is 1-based.      */
 int avism_gpu_indexx(avism_gpu_ctx *ctx, int32_t n, const float *arr, int32_t *indx);

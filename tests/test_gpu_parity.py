@@ -1,0 +1,195 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the CPU oracle.
+
+Bit-exact: kNN lists, INDEXX permutations, the SPH fields, normalised density,
+divergence, flag grids, the grown cubes and all integer catalogue columns.
+Floating-point reductions whose order the reference itself leaves open (the
+REAL*4 inertia, mean-density and mass sums over a void) agree to the stated
+tolerances."""
+import numpy as np
+import pytest
+
+from avism_b200._abi import Params
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _pts(rng, n, lo, hi):
+    return [rng.uniform(lo, hi, n).astype(np.float32) for _ in range(3)]
+
+
+@pytest.mark.parametrize("periodic", [0, 1])
+@pytest.mark.parametrize("k", [1, 32, 48, 100])
+def test_knn_exact(gpu, periodic, k):
+    rng = np.random.default_rng(10 * k + periodic)
+    x, y, z = _pts(rng, 40000, -50, 50)
+    q = _pts(rng, 5000, -50, 50)
+    L = 100.0 if periodic else 0.0
+    i1, d1 = O.knn(x, y, z, *q, k, L)
+    i2, d2 = gpu.knn_search(x, y, z, *q, k, L)
+    assert np.array_equal(i1, i2)
+    assert np.array_equal(d1, d2)
+
+
+def test_knn_lattice_ties(gpu):
+    g = np.arange(-8, 8, dtype=np.float32) + 0.5
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    x, y, z = (a.ravel().copy() for a in (X, Y, Z))
+    for L in (16.0, 0.0):
+        i1, d1 = O.knn(x, y, z, x, y, z, 32, L)
+        i2, d2 = gpu.knn_search(x, y, z, x, y, z, 32, L)
+        assert np.array_equal(i1, i2) and np.array_equal(d1, d2)
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 8, 48, 49, 1000, 65537, 1_000_003])
+def test_indexx_exact(gpu, n):
+    rng = np.random.default_rng(n)
+    cases = [rng.integers(0, max(2, n // 20), n).astype(np.float32),
+             rng.standard_normal(n).astype(np.float32),
+             np.full(n, 3.0, np.float32),
+             np.arange(n, dtype=np.float32),
+             np.arange(n, dtype=np.float32)[::-1].copy()]
+    for a in cases:
+        assert np.array_equal(gpu.indexx(a), O.indexx(a))
+
+
+@pytest.fixture(scope="module")
+def p2g_pair(gpu, mock1):
+    res = {}
+    for vel, dens in ((1, 1), (0, 0), (0, 1), (1, 0)):
+        p = Params(nx=64, periodic=1, lado0=100.0, flag_vel_interp=vel, flag_dens_interp=dens)
+        o = O.particles_to_grid(p, *(mock1[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")))
+        g = gpu.particles_to_grid(p, mock1)
+        res[(vel, dens)] = (o, g)
+    return res
+
+
+def test_sph_fields_exact(p2g_pair):
+    o, g = p2g_pair[(1, 1)]
+    for k in ("part_dens", "hpart", "u2", "u3", "u4", "u_mass"):
+        assert np.array_equal(o[k], g[k]), k
+
+
+def _rel_close(a, b, tol):
+    a = a.astype(np.float64)
+    b = b.astype(np.float64)
+    scale = np.abs(a) + np.mean(np.abs(a))
+    return np.all(np.abs(a - b) <= tol * scale)
+
+
+@pytest.mark.parametrize("mode", [(0, 0), (0, 1), (1, 0)])
+def test_tsc_and_mixed_modes(p2g_pair, mode):
+    # FP32 atomics make the reference's TSC velocity order-dependent: 1e-5 relative
+    o, g = p2g_pair[mode]
+    for k in ("u_mass", "u2", "u3", "u4"):
+        assert _rel_close(o[k], g[k], 1e-5), k
+    if mode[1] == 1:
+        assert np.array_equal(o["hpart"], g["hpart"])
+
+
+@pytest.fixture(scope="module")
+def fields_pair(gpu, oracle_mock1):
+    res = {}
+    for per in (1, 0):
+        p = Params(nx=64, periodic=per, lado0=100.0)
+        grid = oracle_mock1[per]["grid"]
+        o = O.fields(p, grid["u_mass"], grid["u2"], grid["u3"], grid["u4"])
+        g = gpu.fields(p, grid["u_mass"], grid["u2"], grid["u3"], grid["u4"])
+        res[per] = (p, o, g)
+    return res
+
+
+def test_fields_exact(fields_pair):
+    for per, (p, o, g) in fields_pair.items():
+        assert np.array_equal(o[0], g[0]) and np.array_equal(o[1], g[1]) and o[2] == g[2]
+
+
+def test_flags_exact(gpu, fields_pair):
+    for per, (p, o, g) in fields_pair.items():
+        vo = O.voidfind(p, o[0], o[1])
+        fl = gpu.mark_all(p, o[0], o[1])
+        assert np.array_equal(vo["flags"], fl)
+
+
+def test_voidfind_exact(gpu, fields_pair):
+    for per, (p, o, g) in fields_pair.items():
+        vo = O.voidfind(p, o[0], o[1])
+        cubes, nv = gpu.voidfind(p, o[0], o[1])
+        assert nv == vo["nvoid"]
+        for k in cubes:
+            assert np.array_equal(cubes[k], vo["cubes"][k]), k
+
+
+def test_merge_post_parity(gpu, fields_pair):
+    for per, (p, o, g) in fields_pair.items():
+        vo = O.voidfind(p, o[0], o[1])
+        co = O.merge_post(p, vo["nvoid"], vo["cubes"], o[0], o[2])
+        cg = gpu.merge_post(p, vo["nvoid"], vo["cubes"], o[0], o[2])
+        for k in ("indice", "uvoid", "ncellv", "marca", "volnew", "req", "xc", "yc", "zc", "gxc", "gyc", "gzc"):
+            assert np.array_equal(co[k], cg[k]), k
+        assert (co["nvoid2"], co["nvoidt"], co["volt_clean"]) == (cg["nvoid2"], cg["nvoidt"], cg["volt_clean"])
+        main = co["uvoid"] == -1
+        # REAL*4 sums in K,J,I order (reference) vs FP64 sums (GPU)
+        n = np.maximum(co["ncellv"][main], 1).astype(np.float64)
+        tol = 2e-6 * np.sqrt(n) + 1e-6
+        for k in ("umean", "mtot"):
+            a, b = co[k][main].astype(np.float64), cg[k][main].astype(np.float64)
+            assert np.all(np.abs(a - b) <= tol * np.abs(a)), k
+        for k in ("eps", "ip"):
+            a, b = co[k][main].astype(np.float64), cg[k][main].astype(np.float64)
+            ok = (np.abs(a - b) <= 1e-4 * np.maximum(1.0, np.abs(a))) | (a == -99) | (b == -99)
+            assert np.all(ok), k
+
+
+def test_run_level_matches_oracle(gpu, mock1, oracle_mock1):
+    for per in (1, 0):
+        p = Params(nx=64, periodic=per, lado0=100.0)
+        r = gpu.run_level(p, mock1, capacity=100000, want_marca=True)
+        o = oracle_mock1[per]
+        assert r["nvoid"] == o["vf"]["nvoid"]
+        for k in r["cubes"]:
+            assert np.array_equal(r["cubes"][k], o["vf"]["cubes"][k]), k
+        assert r["meandens"] == o["meandens"]
+        for k in ("indice", "uvoid", "ncellv", "marca", "volnew", "req", "gxc", "gyc", "gzc"):
+            assert np.array_equal(r["cat"][k], o["cat"][k]), k
+        assert r["cat"]["nvoidt"] == o["cat"]["nvoidt"] and r["cat"]["nvoidt"] > 0
+
+
+def test_run_level_deterministic(gpu, mock1):
+    p = Params(nx=64, periodic=1, lado0=100.0)
+    a = gpu.run_level(p, mock1, capacity=100000)
+    b = gpu.run_level(p, mock1, capacity=100000)
+    for k in a["cat"]:
+        assert np.array_equal(np.asarray(a["cat"][k]), np.asarray(b["cat"][k])), k
+
+
+def test_out_of_box_is_an_error(gpu, mock_small):
+    from avism_b200.avism import AvismError
+    parts = {k: np.array(v, copy=True) for k, v in mock_small.items() if isinstance(v, np.ndarray)}
+    parts["x"][5] = 40.0                       # box is [-32, 32]
+    p = Params(nx=32, periodic=1, lado0=64.0)
+    with pytest.raises(AvismError) as e:
+        gpu.run_level(p, parts, capacity=10000)
+    assert e.value.code == 5
+
+
+def test_nvoid_max_matches_reference_stop(gpu, fields_pair):
+    """'NVOID > NVOID_MAX!! Increase NVOID_MAX' fires exactly when the oracle's does."""
+    from avism_b200.avism import AvismError
+    p0, o, _ = fields_pair[1]
+    nv = O.voidfind(p0, o[0], o[1])["nvoid"]
+    for cap in (nv - 1, nv, nv + 1):
+        p = Params(nx=64, periodic=1, lado0=100.0, nvoid_max=cap)
+        try:
+            O.voidfind(p, o[0], o[1])
+            ref_err = None
+        except O.OracleError as e:
+            ref_err = str(e)
+        if ref_err is None:
+            cubes, n = gpu.voidfind(p, o[0], o[1], capacity=cap)
+            assert n == nv
+        else:
+            assert "4" in ref_err
+            with pytest.raises(AvismError) as e:
+                gpu.voidfind(p, o[0], o[1], capacity=cap)
+            assert e.value.code == 4
