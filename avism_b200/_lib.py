@@ -18,6 +18,8 @@ SIGNATURES = {
     "avism_gpu_destroy": (C.c_int, [_c_void]),
     "avism_gpu_last_error": (C.c_char_p, [_c_void]),
     "avism_gpu_stage_times": (C.c_int, [_c_void, _c_void, C.c_int]),
+    "avism_gpu_stage_name": (C.c_char_p, [_c_void, C.c_int]),
+    "avism_gpu_launches": (C.c_int64, [_c_void]),
     "avism_gpu_grid_setup": (C.c_int, [_c_void, _c_void, _c_void]),
     "avism_gpu_knn": (C.c_int, [_c_void, _i64, _c_void, _c_void, _c_void, _f32, _i64,
                                 _c_void, _c_void, _c_void, _i32, _c_void, _c_void]),

@@ -85,9 +85,13 @@ class AvismGPU:
             raise AvismError(st, msg.decode() if msg else "")
 
     def stage_times(self):
-        buf = (C.c_double * 16)()
-        n = self.lib.avism_gpu_stage_times(self.h, buf, 16)
-        return [buf[i] for i in range(min(n, 16))]
+        """{stage name: device ms} of the last call."""
+        buf = (C.c_double * 64)()
+        n = min(self.lib.avism_gpu_stage_times(self.h, buf, 64), 64)
+        return {self.lib.avism_gpu_stage_name(self.h, i).decode() or f"s{i}": buf[i] for i in range(n)}
+
+    def launches(self) -> int:
+        return int(self.lib.avism_gpu_launches(self.h))
 
     # ---- kNN (knn_search, src/kdtree.f90:504-540) ----------------------------
     def knn_search(self, x, y, z, qx, qy, qz, k, box_l=0.0):

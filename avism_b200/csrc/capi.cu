@@ -23,11 +23,15 @@ int guarded(avism_gpu_ctx *ctx, F &&f) {
     if (!ctx) return AVISM_ERR_ARG;
     try {
         AV_CUDA(cudaSetDevice(ctx->c.device));
+        ctx->c.stage_open();
         f(ctx->c);
+        ctx->c.mark("end");
+        ctx->c.stage_close();
         ctx->c.last_error.clear();
         return AVISM_OK;
     } catch (const Error &e) {
         cudaGetLastError();
+        ctx->c.stage_close();
         return fail(ctx, e.code, e.msg);
     } catch (const std::bad_alloc &) {
         return fail(ctx, AVISM_ERR_OOM, "host allocation failed");
@@ -207,6 +211,13 @@ int avism_gpu_stage_times(const avism_gpu_ctx *ctx, double *ms, int n) {
     return m;
 }
 
+const char *avism_gpu_stage_name(const avism_gpu_ctx *ctx, int i) {
+    if (!ctx || i < 0 || i >= (int)ctx->c.stage_names.size()) return "";
+    return ctx->c.stage_names[(size_t)i].c_str();
+}
+
+int64_t avism_gpu_launches(const avism_gpu_ctx *ctx) { return ctx ? ctx->c.launches : -1; }
+
 int avism_gpu_grid_setup(const avism_params *p, avism_grid *g, float *radx) {
     return grid_setup_host(p, g, radx);
 }
@@ -217,7 +228,6 @@ int avism_gpu_knn(avism_gpu_ctx *ctx, int64_t n, const float *x, const float *y,
     return guarded(ctx, [&](Ctx &c) {
         AV_CHECK(n >= 1 && nq >= 0 && k >= 1 && k <= 256 && x && y && z && idx && dist, AVISM_ERR_ARG,
                  "knn: bad arguments");
-        c.stage_ms.clear();
         const size_t nb = sizeof(float) * (size_t)n, qb = sizeof(float) * (size_t)std::max<int64_t>(nq, 1);
         const float *dx = (const float *)to_device(c, B_PX, x, nb);
         const float *dy = (const float *)to_device(c, B_PY, y, nb);
@@ -263,7 +273,6 @@ int avism_gpu_particles_to_grid(avism_gpu_ctx *ctx, const avism_params *p, int64
                                 float *u2, float *u3, float *u4, float *hpart, float *part_dens) {
     return guarded(ctx, [&](Ctx &c) {
         check_params(p);
-        c.stage_ms.clear();
         Level L = make_level(p);
         P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, smask);
         particles_to_grid(c, p, L, a);
@@ -282,7 +291,6 @@ int avism_gpu_fields(avism_gpu_ctx *ctx, const avism_params *p, const float *u_m
                      const float *u3, const float *u4, float *u1co_ext, float *diverco_ext, float *meandens) {
     return guarded(ctx, [&](Ctx &c) {
         check_params(p);
-        c.stage_ms.clear();
         Level L = make_level(p);
         const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
         const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
@@ -308,7 +316,6 @@ int avism_gpu_voidfind(avism_gpu_ctx *ctx, const avism_params *p, const float *u
     return guarded(ctx, [&](Ctx &c) {
         check_params(p);
         AV_CHECK(u1co_ext && diverco_ext && cubes && nvoid, AVISM_ERR_ARG, "voidfind: null argument");
-        c.stage_ms.clear();
         Level L = make_level(p);
         const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
         const float *u1 = (const float *)to_device(c, B_U1EXT, u1co_ext, sizeof(float) * (size_t)ne3);
@@ -341,7 +348,6 @@ int avism_gpu_flags(avism_gpu_ctx *ctx, const avism_params *p, const float *u1co
     return guarded(ctx, [&](Ctx &c) {
         check_params(p);
         AV_CHECK(u1co_ext && diverco_ext && flags_ext, AVISM_ERR_ARG, "flags: null argument");
-        c.stage_ms.clear();
         Level L = make_level(p);
         const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
         const float *u1 = (const float *)to_device(c, B_U1EXT, u1co_ext, sizeof(float) * (size_t)ne3);
@@ -359,7 +365,6 @@ int avism_gpu_indexx(avism_gpu_ctx *ctx, int32_t n, const float *arr, int32_t *i
     return guarded(ctx, [&](Ctx &c) {
         AV_CHECK(n >= 0 && (n == 0 || (arr && indx)), AVISM_ERR_ARG, "indexx: bad arguments");
         if (n == 0) return;
-        c.stage_ms.clear();
         const float *k = (const float *)to_device(c, B_CAND_KEY, arr, sizeof(float) * (size_t)n);
         int32_t *o = is_device_ptr(indx) ? indx : c.get_t<int32_t>(B_CAND_POS, n);
         indexx_device(c, n, k, o);
@@ -373,13 +378,12 @@ int avism_gpu_merge_post(avism_gpu_ctx *ctx, const avism_params *p, int32_t nvoi
     return guarded(ctx, [&](Ctx &c) {
         check_params(p);
         AV_CHECK(nvoid >= 0 && cubes && u1co_ext && out, AVISM_ERR_ARG, "merge_post: null argument");
-        c.stage_ms.clear();
         Level L = make_level(p);
         const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
         const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
         const float *e1 = (const float *)to_device(c, B_U1EXT, u1co_ext, sizeof(float) * (size_t)ne3);
         float *u1 = c.get_t<float>(B_U1CO, nc);
-        k_inner_from_ext<<<grid_for(nc, 256), 256, 0, c.stream>>>(L.g.nx, L.g.low1, L.g.ne, e1, u1);
+        ++c.launches, k_inner_from_ext<<<grid_for(nc, 256), 256, 0, c.stream>>>(L.g.nx, L.g.low1, L.g.ne, e1, u1);
         HostCubes hc(c, cubes, nvoid);
         merge_post(c, p, L, nvoid, &hc.v, u1, meandens, out, out->marca);
     });
@@ -391,24 +395,21 @@ int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, co
     return guarded(ctx, [&](Ctx &c) {
         check_params(p);
         AV_CHECK(nvoid && voids, AVISM_ERR_ARG, "run_level: null argument");
-        c.stage_ms.clear();
-        Timer tm(c);
         Level L = make_level(p);
         const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
         P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, nullptr);
-        tm.lap();                                       // 0: inputs to device
+        c.mark("h2d");
         particles_to_grid(c, p, L, a);
-        tm.lap();                                       // 1: particles -> grid
         float *u1 = c.get_t<float>(B_U1CO, nc), *dv = c.get_t<float>(B_DIVER, nc);
         FieldsOut fo = fields_inner(c, p, L, a.u_mass, a.u2, a.u3, a.u4, u1, dv);
-        tm.lap();                                       // 2: fields
+        c.mark("fields");
         CubesDev cd{};
         const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, nullptr, nullptr, 0, cd);
-        tm.lap();                                       // 3: voidfind
         HostCubes hc(c, cd, nv);
         if (cubes) cubes_out(c, cd, nv, cubes);
+        c.mark("cubes_d2h");
         merge_post(c, p, L, nv, &hc.v, u1, fo.meandens, voids, voids->marca);
-        tm.lap();                                       // 4: merge + post
+        c.mark("catalogue_d2h");
         *nvoid = nv;
         if (meandens) *meandens = fo.meandens;
     });

@@ -63,6 +63,41 @@ struct Ctx {
     // scratch pinned host memory for small readbacks
     void *hpin = nullptr;
     size_t hpin_cap = 0;
+    // number of this library's kernels launched since the context was created
+    int64_t launches = 0;
+    // named stage marks: events recorded on the stream, resolved by stage_close()
+    std::vector<cudaEvent_t> marks;
+    std::vector<std::string> mark_names;
+    std::vector<std::string> stage_names;
+
+    void stage_open() {
+        for (cudaEvent_t e : marks) cudaEventDestroy(e);
+        marks.clear();
+        mark_names.clear();
+        stage_ms.clear();
+        stage_names.clear();
+        mark("start");
+    }
+    void mark(const char *name) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        cudaEventRecord(e, stream);
+        marks.push_back(e);
+        mark_names.push_back(name);
+    }
+    void stage_close() {
+        if (marks.empty()) return;
+        cudaEventSynchronize(marks.back());
+        for (size_t i = 1; i < marks.size(); i++) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, marks[i - 1], marks[i]);
+            stage_ms.push_back(ms);
+            stage_names.push_back(mark_names[i]);
+        }
+        for (cudaEvent_t e : marks) cudaEventDestroy(e);
+        marks.clear();
+        mark_names.clear();
+    }
 
     void *get(BufId id, size_t bytes) {
         if (bytes == 0) bytes = 16;

@@ -74,7 +74,7 @@ FieldsOut fields_inner(Ctx &c, const avism_params *p, const Level &L, const floa
     const int64_t nc = (int64_t)nx * nx * nx;
     const float dx = L.g.dx;
     const float vol = ((dx * dx) * dx) * ((L.g.rete * L.g.rete) * L.g.rete);
-    k_rho<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u_mass, vol, L.g.rote, u1co_in);
+    ++c.launches, k_rho<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u_mass, vol, L.g.rote, u1co_in);
     double *sum_d = c.get_t<double>(B_RED1, 1);
     cub::TransformInputIterator<double, ToDouble, const float *> it(u1co_in, ToDouble());
     size_t tmp = 0;
@@ -85,8 +85,8 @@ FieldsOut fields_inner(Ctx &c, const avism_params *p, const Level &L, const floa
     AV_CUDA(cudaMemcpyAsync(&sum, sum_d, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
     const float mean = (float)(sum / (double)nc);
-    k_div_scalar<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u1co_in, mean);
-    k_diver<<<grid_for(nc, 256), 256, 0, c.stream>>>(nx, dx, p->periodic, u2, u3, u4, diver_in);
+    ++c.launches, k_div_scalar<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u1co_in, mean);
+    ++c.launches, k_diver<<<grid_for(nc, 256), 256, 0, c.stream>>>(nx, dx, p->periodic, u2, u3, u4, diver_in);
     AV_CUDA(cudaGetLastError());
     FieldsOut o;
     const float ul3 = (UL_F * UL_F) * UL_F;
@@ -107,7 +107,7 @@ __global__ void k_ext_copy(int nx, int low1, int ne, const float *__restrict__ i
 
 void ext_copy(Ctx &c, const Level &L, const float *inner, float *ext) {
     const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
-    k_ext_copy<<<grid_for(ne3, 256), 256, 0, c.stream>>>(L.g.nx, L.g.low1, L.g.ne, inner, ext);
+    ++c.launches, k_ext_copy<<<grid_for(ne3, 256), 256, 0, c.stream>>>(L.g.nx, L.g.low1, L.g.ne, inner, ext);
     AV_CUDA(cudaGetLastError());
 }
 
@@ -223,7 +223,7 @@ void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, 
     A.div_thre = p->div_thre;
     A.gthr = grad_threshold(p->grad_thre, L.g.dx);
     const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
-    k_flags<<<grid_for(ne3, 256), 256, 0, c.stream>>>(A, flags);
+    ++c.launches, k_flags<<<grid_for(ne3, 256), 256, 0, c.stream>>>(A, flags);
     AV_CUDA(cudaGetLastError());
 }
 

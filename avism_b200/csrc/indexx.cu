@@ -248,7 +248,7 @@ void indexx_device(Ctx &c, int32_t n, const float *key_in, int32_t *indx_out) {
     if (n <= 0) return;
     float *K = c.get_t<float>(B_SORT_KEY, n);
     int32_t *I = c.get_t<int32_t>(B_SORT_IDX, n);
-    k_init_idx<<<grid_for(n, 256), 256, 0, c.stream>>>(n, key_in, K, I);
+    ++c.launches, k_init_idx<<<grid_for(n, 256), 256, 0, c.stream>>>(n, key_in, K, I);
     // segment lists: two ping-pong large lists and one small list
     const int32_t segcap = n / 2 + 8;
     Seg *large[2] = {(Seg *)c.get(B_SEG_A, sizeof(Seg) * (size_t)segcap * 2), nullptr};
@@ -280,16 +280,16 @@ void indexx_device(Ctx &c, int32_t n, const float *key_in, int32_t *indx_out) {
     while (nlarge > 0) {
         Seg *S = large[cur], *N = large[cur ^ 1];
         AV_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int32_t), c.stream));
-        k_med3<<<grid_for(nlarge, 128), 128, 0, c.stream>>>(S, nlarge, K, I);
+        ++c.launches, k_med3<<<grid_for(nlarge, 128), 128, 0, c.stream>>>(S, nlarge, K, I);
         AV_CUDA(cudaMemsetAsync(seg_of, 0xff, sizeof(int32_t) * (size_t)n, c.stream));
-        k_seg_of<<<nlarge, 256, 0, c.stream>>>(S, seg_of);
-        k_flags_ge_le<<<grid_for(n, 256), 256, 0, c.stream>>>(n, S, seg_of, K, ge, le);
+        ++c.launches, k_seg_of<<<nlarge, 256, 0, c.stream>>>(S, seg_of);
+        ++c.launches, k_flags_ge_le<<<grid_for(n, 256), 256, 0, c.stream>>>(n, S, seg_of, K, ge, le);
         AV_CUDA(cub::DeviceScan::ExclusiveSum(tbuf, tmp, ge, Pge, n, c.stream));
         AV_CUDA(cub::DeviceScan::ExclusiveSum(tbuf, tmp, le, Ple, n, c.stream));
-        k_lists<<<grid_for(n, 256), 256, 0, c.stream>>>(n, S, seg_of, ge, le, Pge, Ple, GE, LE);
-        k_cross<<<grid_for(nlarge, 128), 128, 0, c.stream>>>(S, nlarge, GE, LE, cnt + 2);
-        k_swap_pairs<<<grid_for(n, 256), 256, 0, c.stream>>>(n, S, seg_of, ge, Pge, LE, K, I);
-        k_finish<<<grid_for(nlarge, 128), 128, 0, c.stream>>>(S, nlarge, K, I, N, cnt, small, cnt + 1);
+        ++c.launches, k_lists<<<grid_for(n, 256), 256, 0, c.stream>>>(n, S, seg_of, ge, le, Pge, Ple, GE, LE);
+        ++c.launches, k_cross<<<grid_for(nlarge, 128), 128, 0, c.stream>>>(S, nlarge, GE, LE, cnt + 2);
+        ++c.launches, k_swap_pairs<<<grid_for(n, 256), 256, 0, c.stream>>>(n, S, seg_of, ge, Pge, LE, K, I);
+        ++c.launches, k_finish<<<grid_for(nlarge, 128), 128, 0, c.stream>>>(S, nlarge, K, I, N, cnt, small, cnt + 1);
         AV_CUDA(cudaGetLastError());
         AV_CUDA(cudaMemcpyAsync(hcnt, cnt, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
         c.sync();
@@ -301,8 +301,8 @@ void indexx_device(Ctx &c, int32_t n, const float *key_in, int32_t *indx_out) {
     c.sync();
     nsmall = tail[0];
     AV_CHECK(tail[1] == 0, AVISM_ERR_INTERNAL, "indexx: inconsistent partition");
-    if (nsmall > 0) k_small<<<grid_for(nsmall, 64), 64, 0, c.stream>>>(small, nsmall, K, I);
-    k_copy_out<<<grid_for(n, 256), 256, 0, c.stream>>>(n, I, indx_out);
+    if (nsmall > 0) ++c.launches, k_small<<<grid_for(nsmall, 64), 64, 0, c.stream>>>(small, nsmall, K, I);
+    ++c.launches, k_copy_out<<<grid_for(n, 256), 256, 0, c.stream>>>(n, I, indx_out);
     AV_CUDA(cudaGetLastError());
 }
 

@@ -67,13 +67,13 @@ BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y,
     bp.sp = sp;
     bp.start = start;
     if (n == 0) {
-        k_empty_start<<<grid_for(nbins + 1, 256), 256, 0, c.stream>>>(start, nbins);
+        ++c.launches, k_empty_start<<<grid_for(nbins + 1, 256), 256, 0, c.stream>>>(start, nbins);
         return bp;
     }
     AV_CHECK(n < (int64_t)INT32_MAX, AVISM_ERR_ARG, "more than 2^31-1 particles");
     uint32_t *ka = c.get_t<uint32_t>(B_KEYS_A, n), *kb = c.get_t<uint32_t>(B_KEYS_B, n);
     int32_t *va = c.get_t<int32_t>(B_VALS_A, n), *vb = c.get_t<int32_t>(B_VALS_B, n);
-    k_bin_keys<<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, y, z, bp.origin, bp.inv_bw, nb, ka, va);
+    ++c.launches, k_bin_keys<<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, y, z, bp.origin, bp.inv_bw, nb, ka, va);
     AV_CUDA(cudaGetLastError());
     cub::DoubleBuffer<uint32_t> dk(ka, kb);
     cub::DoubleBuffer<int32_t> dv(va, vb);
@@ -83,7 +83,7 @@ BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y,
     AV_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, (int)n, 0, end_bit, c.stream));
     void *t = c.get(B_CUB_TMP, tmp);
     AV_CUDA(cub::DeviceRadixSort::SortPairs(t, tmp, dk, dv, (int)n, 0, end_bit, c.stream));
-    k_bin_gather<<<grid_for(n, 256), 256, 0, c.stream>>>(n, dk.Current(), dv.Current(), x, y, z, sp,
+    ++c.launches, k_bin_gather<<<grid_for(n, 256), 256, 0, c.stream>>>(n, dk.Current(), dv.Current(), x, y, z, sp,
                                                            start, nbins);
     AV_CUDA(cudaGetLastError());
     return bp;
@@ -119,7 +119,7 @@ static void launch_knn_batch(Ctx &c, const KnnGrid &G, int64_t nq, const float *
     const int T = KNN_THREADS(KCAP);
     const size_t sm = (size_t)KCAP * T * sizeof(unsigned long long);
     AV_CUDA(cudaFuncSetAttribute(k_knn_batch<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_knn_batch<KCAP><<<grid_for(nq, T), T, sm, c.stream>>>(G, nq, qx, qy, qz, k, idx, dist);
+    ++c.launches, k_knn_batch<KCAP><<<grid_for(nq, T), T, sm, c.stream>>>(G, nq, qx, qy, qz, k, idx, dist);
     AV_CUDA(cudaGetLastError());
 }
 

@@ -289,6 +289,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         dev_download(c, asc.data(), ind_d, nv);
         for (int32_t i = 0; i < nv; i++) indice[i] = asc[nv - 1 - i];
     }
+    c.mark("indexx_vol");
     // ---- MERGE_VOID
     MergeIn mi;
     mi.nvoid = nv; mi.low1 = g.low1; mi.low2 = g.low2; mi.periodic = p->periodic;
@@ -299,6 +300,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
     mi.rfy = cb->rfin_y; mi.riz = cb->rini_z; mi.rfz = cb->rfin_z; mi.indice = indice.data();
     MergeOut mo;
     merge_cubes_host(mi, mo);
+    c.mark("merge_host");
     std::vector<int32_t> &uvoid = mo.uvoid;
     std::vector<float> &volnew = mo.volnew;
 
@@ -317,11 +319,12 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         }
         int32_t *obt_d = dev_upload<int32_t>(c, B_LABMAP, owner_by_time.data(), nv);
         int32_t *tgrid = c.get_t<int32_t>(B_CCL, ne3);
-        k_fill_i32<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, tgrid, INT_MAX);
-        if (nv > 0) k_paint_time<<<grid_for((int64_t)nv * 32, 256), 256, 0, c.stream>>>(PG, box_d, nvs, pt_d, nv, tgrid);
-        k_time_to_label<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, tgrid, obt_d, marca);
+        ++c.launches, k_fill_i32<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, tgrid, INT_MAX);
+        if (nv > 0) ++c.launches, k_paint_time<<<grid_for((int64_t)nv * 32, 256), 256, 0, c.stream>>>(PG, box_d, nvs, pt_d, nv, tgrid);
+        ++c.launches, k_time_to_label<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, tgrid, obt_d, marca);
         AV_CUDA(cudaGetLastError());
     }
+    c.mark("paint_marca");
     std::vector<char> rm(nvs + 1, 0);
     std::vector<int32_t> ncellv(nvs, 0);
     int32_t *map_d = c.get_t<int32_t>(B_LABEL_AUX, nvs + 1);
@@ -335,7 +338,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         std::vector<int32_t> map(nvs + 1);
         for (int32_t i = 0; i <= nv; i++) map[i] = rm[i] ? 0 : i;
         AV_CUDA(cudaMemcpyAsync(map_d, map.data(), sizeof(int32_t) * (size_t)(nv + 1), cudaMemcpyHostToDevice, c.stream));
-        k_relabel<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, map_d);
+        ++c.launches, k_relabel<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, map_d);
         for (int32_t i = 0; i < nv; i++)
             if (uvoid[i] > 0 && rm[uvoid[i]]) uvoid[i] = 0;
         for (int32_t i = 1; i <= nv; i++)
@@ -346,7 +349,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         int32_t *nc_d = c.get_t<int32_t>(B_RED2, nvs);
         AV_CUDA(cudaMemsetAsync(nc_d, 0, sizeof(int32_t) * (size_t)nvs, c.stream));
         push_uvoid();
-        k_ncellv<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, uv_d, nc_d);
+        ++c.launches, k_ncellv<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, uv_d, nc_d);
         dev_download(c, ncellv.data(), nc_d, nv);
     };
     count_cells();
@@ -356,6 +359,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         if (ncellv[ind - 1] < 10) rm[ind] = 1;
     }
     apply_removals();
+    c.mark("ncell_min");
 
     // ---- VOID_SHAPE
     std::vector<float> eps(nvs, 0.0f), ipv(nvs, 0.0f);
@@ -367,7 +371,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         AV_CUDA(cudaMemcpyAsync(gc_d + 2 * nvs, mo.gzc.data(), sizeof(float) * nv, cudaMemcpyHostToDevice, c.stream));
         double *in_d = c.get_t<double>(B_SCAN_A, (size_t)nvs * 6);
         AV_CUDA(cudaMemsetAsync(in_d, 0, sizeof(double) * 6 * (size_t)nvs, c.stream));
-        k_inertia<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, rad_d, g.rad_lo, gc_d, gc_d + nvs, gc_d + 2 * nvs, in_d);
+        ++c.launches, k_inertia<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, rad_d, g.rad_lo, gc_d, gc_d + nvs, gc_d + 2 * nvs, in_d);
         std::vector<double> inert((size_t)nvs * 6);
         dev_download(c, inert.data(), in_d, (size_t)nv * 6);
         for (int32_t I = 0; I < nv; I++) {
@@ -413,6 +417,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         }
         apply_removals();
     };
+    c.mark("void_shape");
     redefine_volnew();
     rmin_filter();
     std::vector<float> xc(nvs, 0.0f), yc(nvs, 0.0f), zc(nvs, 0.0f);
@@ -428,13 +433,14 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
     {
         int32_t *P = c.get_t<int32_t>(B_CCL, ne3);
         int32_t *m2 = c.get_t<int32_t>(B_PAINT, ne3);
-        k_ccl_init<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, P);
-        k_ccl_union<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, P);
-        k_ccl_flatten<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, P);
-        k_fill_holes<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, P, marca, m2);
+        ++c.launches, k_ccl_init<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, P);
+        ++c.launches, k_ccl_union<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, P);
+        ++c.launches, k_ccl_flatten<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, P);
+        ++c.launches, k_fill_holes<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, P, marca, m2);
         AV_CUDA(cudaMemcpyAsync(marca, m2, (size_t)ne3 * 4, cudaMemcpyDeviceToDevice, c.stream));
         AV_CUDA(cudaGetLastError());
     }
+    c.mark("simple_connection");
 
     // ---- VOID_PERIODIC
     if (p->periodic) {
@@ -442,7 +448,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         {
             int32_t *has_d = c.get_t<int32_t>(B_RED2, nvs);
             AV_CUDA(cudaMemsetAsync(has_d, 0, sizeof(int32_t) * (size_t)nvs, c.stream));
-            k_inner_presence<<<grid_for((int64_t)nx * nx * nx, 256), 256, 0, c.stream>>>(PG, marca, has_d);
+            ++c.launches, k_inner_presence<<<grid_for((int64_t)nx * nx * nx, 256), 256, 0, c.stream>>>(PG, marca, has_d);
             dev_download(c, has.data(), has_d, nv);
         }
         std::vector<int32_t> kept;
@@ -493,7 +499,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
             int32_t *i2_d = dev_upload<int32_t>(c, B_RED1, ind2spec.data(), nvs);
             int32_t *cnt_d = c.get_t<int32_t>(B_RED2, (size_t)nvs * 2);
             AV_CUDA(cudaMemsetAsync(cnt_d, 0, sizeof(int32_t) * 2 * (size_t)nvs, c.stream));
-            k_periodic_counts<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, lm_d, sh_d, i2_d, 0, cnt_d);
+            ++c.launches, k_periodic_counts<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, lm_d, sh_d, i2_d, 0, cnt_d);
             std::vector<int32_t> cnt((size_t)nvs * 2);
             dev_download(c, cnt.data(), cnt_d, (size_t)nv * 2);
             std::vector<int32_t> bb((size_t)nvs * 6);
@@ -503,7 +509,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
                 for (int32_t i = 0; i < nvs; i++)
                     for (int a = 0; a < 3; a++) { init[(size_t)i * 6 + a] = INT_MAX; init[(size_t)i * 6 + 3 + a] = INT_MIN; }
                 AV_CUDA(cudaMemcpyAsync(bb_d, init.data(), sizeof(int32_t) * init.size(), cudaMemcpyHostToDevice, c.stream));
-                k_bbox<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, bb_d);
+                ++c.launches, k_bbox<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, bb_d);
                 dev_download(c, bb.data(), bb_d, (size_t)nv * 6);
             }
             // union-find over labels for CHANGE_BELONG
@@ -551,7 +557,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
                     int32_t *i2d = dev_upload<int32_t>(c, B_RED1, i2v.data(), nvs);
                     int32_t *one = c.get_t<int32_t>(B_RED2, (size_t)nvs * 2);
                     AV_CUDA(cudaMemsetAsync(one + (size_t)(ind - 1) * 2, 0, 8, c.stream));
-                    k_periodic_counts<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, lm_d, sh_d, i2d, ind, one);
+                    ++c.launches, k_periodic_counts<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, lm_d, sh_d, i2d, ind, one);
                     int32_t r2[2];
                     dev_download(c, r2, one + (size_t)(ind - 1) * 2, 2);
                     counter = r2[0];
@@ -580,11 +586,12 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
             std::vector<int32_t> flat(nvs + 1);
             for (int32_t i = 0; i <= nv; i++) flat[i] = i == 0 ? 0 : find(i);
             AV_CUDA(cudaMemcpyAsync(map_d, flat.data(), sizeof(int32_t) * (size_t)(nv + 1), cudaMemcpyHostToDevice, c.stream));
-            k_relabel<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, map_d);
+            ++c.launches, k_relabel<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, map_d);
             c.sync();
         }
     }
 
+    c.mark("void_periodic");
     // ---- global properties (inner cells), VOLNEW, RMIN, NVOIDT
     std::vector<float> umean(nvs, 0.0f), mtot(nvs, 0.0f);
     double volt = 0.0;
@@ -595,7 +602,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         AV_CUDA(cudaMemsetAsync(sum_d, 0, sizeof(double) * 2 * (size_t)nvs, c.stream));
         push_uvoid();
         const float rete3 = (g.rete * g.rete) * g.rete;
-        k_final_props<<<grid_for((int64_t)nx * nx * nx, 256), 256, 0, c.stream>>>(PG, marca, uv_d, u1co_inner,
+        ++c.launches, k_final_props<<<grid_for((int64_t)nx * nx * nx, 256), 256, 0, c.stream>>>(PG, marca, uv_d, u1co_inner,
                                                                                   meandens, dx, rete3, nc_d, sum_d);
         std::vector<double> sums((size_t)nvs * 2);
         dev_download(c, ncellv.data(), nc_d, nv);

@@ -405,8 +405,10 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
     AV_CUDA(cudaFuncSetAttribute(k_ppart_dens<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     AV_CUDA(cudaFuncSetAttribute(k_cells_knn<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     AV_CUDA(cudaFuncSetAttribute(k_fill_h<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    if (vel_sph)
-        k_ppart_dens<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, a.m, a.part_dens);
+    if (vel_sph) {
+        ++c.launches, k_ppart_dens<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, a.m, a.part_dens);
+        c.mark("ppart_dens");
+    }
     if (vel_sph || need_h_cells) {
         int32_t *ball_list = c.get_t<int32_t>(B_BALL, nc);
         int32_t *cnt_d = c.get_t<int32_t>(B_SCAL, 4);
@@ -418,14 +420,17 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
         A.ball_list = ball_list; A.ball_count = cnt_d;
         const int tx = TileDims<T>::x, ty = TileDims<T>::y, tz = TileDims<T>::z;
         const int64_t nblk = (int64_t)((nx + tx - 1) / tx) * ((nx + ty - 1) / ty) * ((nx + tz - 1) / tz);
-        k_cells_knn<KCAP><<<(unsigned)nblk, T, sm, c.stream>>>(G, A);
+        ++c.launches, k_cells_knn<KCAP><<<(unsigned)nblk, T, sm, c.stream>>>(G, A);
         AV_CUDA(cudaGetLastError());
+        c.mark("cells_knn");
         int32_t nball = 0;
         AV_CUDA(cudaMemcpyAsync(&nball, cnt_d, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
         c.sync();
-        if (nball > 0) k_cells_ball<<<grid_for(nball, 128), 128, 0, c.stream>>>(G, A, nball);
+        if (nball > 0) ++c.launches, k_cells_ball<<<grid_for(nball, 128), 128, 0, c.stream>>>(G, A, nball);
         AV_CUDA(cudaGetLastError());
-        k_fill_h<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, a.hpart);
+        c.mark("cells_ball");
+        ++c.launches, k_fill_h<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, a.hpart);
+        c.mark("fill_h_zeros");
     }
     AV_CUDA(cudaGetLastError());
 }
@@ -441,7 +446,7 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
     {
         int *bad = c.get_t<int>(B_SCAL, 4);
         AV_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), c.stream));
-        if (a.n > 0) k_box_check<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.x, a.y, a.z, p->lado0 / 2.0f, bad);
+        if (a.n > 0) ++c.launches, k_box_check<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.x, a.y, a.z, p->lado0 / 2.0f, bad);
         int hbad = 0;
         AV_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
         c.sync();
@@ -450,9 +455,10 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
     }
     float *rad_d = c.get_t<float>(B_RAD, L.rad.size());
     AV_CUDA(cudaMemcpyAsync(rad_d, L.rad.data(), L.rad.size() * sizeof(float), cudaMemcpyHostToDevice, c.stream));
-    for (float *g : {a.u_mass, a.u2, a.u3, a.u4}) k_zero_f32<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, g);
-    k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.hpart);
-    k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.part_dens);
+    for (float *g : {a.u_mass, a.u2, a.u3, a.u4}) ++c.launches, k_zero_f32<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, g);
+    ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.hpart);
+    ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.part_dens);
+    c.mark("p2g_setup");
     const bool vel_sph = p->flag_vel_interp == 1, dens_sph = p->flag_dens_interp == 1;
     TscArgs TA;
     TA.nx = nx; TA.rad_lo = L.g.rad_lo; TA.periodic = p->periodic; TA.dx = L.g.dx; TA.rad = rad_d;
@@ -462,6 +468,7 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
     if (vel_sph || dens_sph) {
         BinnedParticles bp = bin_particles(c, a.n, a.x, a.y, a.z, p->lado0, p->periodic, 4.0f);
         KnnGrid G = make_knn_grid(bp);
+        c.mark("bin_particles");
         const bool need_h_cells = dens_sph && !vel_sph;
         if (K <= 32) run_sph_kernels<32>(c, G, p, L, a, rad_d, vel_sph, need_h_cells);
         else if (K <= 64) run_sph_kernels<64>(c, G, p, L, a, rad_d, vel_sph, need_h_cells);
@@ -488,16 +495,19 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
             DdensArgs D;
             D.nx = nx; D.rad_lo = L.g.rad_lo; D.dx = L.g.dx; D.rx1 = L.rad_at(1); D.rad = rad_d;
             D.hpart = a.hpart; D.m = a.m; D.fix = fix; D.scale = scale;
-            k_ddens<<<grid_for(a.n, 128), 128, 0, c.stream>>>(G, a.n, D);
+            c.mark("ddens_setup");
+            ++c.launches, k_ddens<<<grid_for(a.n, 128), 128, 0, c.stream>>>(G, a.n, D);
             AV_CUDA(cudaGetLastError());
-            k_fix128_to_f32<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, fix, 1.0 / scale, a.u_mass);
+            c.mark("ddens_scatter");
+            ++c.launches, k_fix128_to_f32<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, fix, 1.0 / scale, a.u_mass);
+            c.mark("ddens_convert");
         }
     }
     if (!vel_sph || !dens_sph) {
         // TSC: sort particles by their TSC cell, then gather
         uint32_t *ka = c.get_t<uint32_t>(B_KEYS_A, a.n), *kb = c.get_t<uint32_t>(B_KEYS_B, a.n);
         int32_t *va = c.get_t<int32_t>(B_VALS_A, a.n), *vb = c.get_t<int32_t>(B_VALS_B, a.n);
-        k_tsc_keys<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.x, a.y, a.z, TA, ka, va);
+        ++c.launches, k_tsc_keys<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.x, a.y, a.z, TA, ka, va);
         cub::DoubleBuffer<uint32_t> dk(ka, kb);
         cub::DoubleBuffer<int32_t> dv(va, vb);
         int end_bit = 1;
@@ -508,12 +518,13 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
         AV_CUDA(cub::DeviceRadixSort::SortPairs(t, tmp, dk, dv, (int)a.n, 0, end_bit, c.stream));
         int64_t *start = c.get_t<int64_t>(B_BIN_START, nc + 1);
         float4 *dummy = c.get_t<float4>(B_SP, std::max<int64_t>(a.n, 1));
-        k_bin_gather<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, dk.Current(), dv.Current(), a.x, a.y, a.z,
+        ++c.launches, k_bin_gather<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, dk.Current(), dv.Current(), a.x, a.y, a.z,
                                                                 dummy, start, nc);
-        k_tsc_gather<<<grid_for(nc, 128), 128, 0, c.stream>>>(
+        ++c.launches, k_tsc_gather<<<grid_for(nc, 128), 128, 0, c.stream>>>(
             nc, start, dv.Current(), a.x, a.y, a.z, a.m, a.vx, a.vy, a.vz, TA,
             dens_sph ? nullptr : a.u_mass, vel_sph ? nullptr : a.u2, a.u3, a.u4);
         AV_CUDA(cudaGetLastError());
+        c.mark("tsc");
     }
 }
 

@@ -275,6 +275,7 @@ int32_t voidfind_device(Ctx &c, const avism_params *p, const Level &L, const flo
     AV_CHECK(ne3 < (int64_t)INT32_MAX, AVISM_ERR_ARG, "ext grid larger than 2^31 cells");
     uint8_t *flags = c.get_t<uint8_t>(B_FLAGS, ne3);
     make_flags(c, p, L, u1, dv, fields_are_ext, smask_ext, marcap_ext, flags);
+    c.mark("flags");
 
     VfArgs A;
     A.low1 = L.g.low1; A.low2 = L.g.low2; A.ne = ne; A.nx = L.g.nx; A.ext = fields_are_ext;
@@ -298,10 +299,12 @@ int32_t voidfind_device(Ctx &c, const avism_params *p, const Level &L, const flo
     A.cand_pos = pos;
     if (ncand == 0) return 0;
     float *keys = c.get_t<float>(B_CAND_KEY, ncand);
-    k_cand_keys<<<grid_for(ncand, 256), 256, 0, c.stream>>>(A, dv, pos, ncand, keys);
+    ++c.launches, k_cand_keys<<<grid_for(ncand, 256), 256, 0, c.stream>>>(A, dv, pos, ncand, keys);
     int32_t *indx = c.get_t<int32_t>(B_QUERY, ncand);
+    c.mark("candidates");
     indexx_device(c, ncand, keys, indx);
     A.indx = indx;
+    c.mark("indexx_div");
 
     uint8_t *st = c.get_t<uint8_t>(B_CUBE_ST, ncand);
     int32_t *wv = c.get_t<int32_t>(B_CUBE_W, ncand);
@@ -323,7 +326,7 @@ int32_t voidfind_device(Ctx &c, const avism_params *p, const Level &L, const flo
         window++;
         AV_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int32_t), c.stream));
         const int64_t nthr = (int64_t)(r1 - r0) * 32;
-        k_phase1<<<grid_for(nthr, 256), 256, 0, c.stream>>>(A, r0, r1, open_a, cnt);
+        ++c.launches, k_phase1<<<grid_for(nthr, 256), 256, 0, c.stream>>>(A, r0, r1, open_a, cnt);
         AV_CUDA(cudaGetLastError());
         int32_t h[4];
         AV_CUDA(cudaMemcpyAsync(h, cnt, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
@@ -336,24 +339,25 @@ int32_t voidfind_device(Ctx &c, const avism_params *p, const Level &L, const flo
             epoch++;
             AV_CUDA(cudaMemsetAsync(cnt + 1, 0, sizeof(int32_t), c.stream));
             AV_CUDA(cudaMemcpyAsync(cnt + 2, &nacc_window, sizeof(int32_t), cudaMemcpyHostToDevice, c.stream));
-            k_paint_umin<<<grid_for((int64_t)nopen * 32, 256), 256, 0, c.stream>>>(A, cur, nopen, epoch);
-            k_decide<<<grid_for(nopen, 256), 256, 0, c.stream>>>(A, cur, nopen, epoch, window, nxt, cnt + 1, acc, cnt + 2);
+            ++c.launches, k_paint_umin<<<grid_for((int64_t)nopen * 32, 256), 256, 0, c.stream>>>(A, cur, nopen, epoch);
+            ++c.launches, k_decide<<<grid_for(nopen, 256), 256, 0, c.stream>>>(A, cur, nopen, epoch, window, nxt, cnt + 1, acc, cnt + 2);
             AV_CUDA(cudaMemcpyAsync(h, cnt, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
             c.sync();
             const int32_t newly = h[2] - nacc_window;
             if (newly > 0)
-                k_paint_amin<<<grid_for((int64_t)newly * 32, 256), 256, 0, c.stream>>>(A, acc + nacc_window, newly, window);
+                ++c.launches, k_paint_amin<<<grid_for((int64_t)newly * 32, 256), 256, 0, c.stream>>>(A, acc + nacc_window, newly, window);
             AV_CUDA(cudaGetLastError());
             nacc_window = h[2];
             nopen = h[1];
             std::swap(cur, nxt);
         }
         if (nacc_window > 0)
-            k_paint_cover<<<grid_for((int64_t)nacc_window * 32, 256), 256, 0, c.stream>>>(A, acc, nacc_window);
+            ++c.launches, k_paint_cover<<<grid_for((int64_t)nacc_window * 32, 256), 256, 0, c.stream>>>(A, acc, nacc_window);
         r0 = r1;
         if (survivors * 4 < B) B = std::min(B * 2, 1 << 22);
         else if (survivors * 2 > B) B = std::max(B / 2, 256);
     }
+    c.mark("grow_accept");
     // cube ids in rank order
     int32_t *ids = c.get_t<int32_t>(B_LE, ncand + 1);
     {
@@ -368,7 +372,7 @@ int32_t voidfind_device(Ctx &c, const avism_params *p, const Level &L, const flo
     AV_CUDA(cudaMemcpyAsync(&nvoid, ids + ncand, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
     int *err = (int *)(cnt + 4);
     AV_CUDA(cudaMemsetAsync(err, 0, sizeof(int), c.stream));
-    k_nvoid_check<<<grid_for(ncand, 256), 256, 0, c.stream>>>(st, ids, ncand, p->nvoid_max, err);
+    ++c.launches, k_nvoid_check<<<grid_for(ncand, 256), 256, 0, c.stream>>>(st, ids, ncand, p->nvoid_max, err);
     int herr = 0;
     AV_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
@@ -377,8 +381,9 @@ int32_t voidfind_device(Ctx &c, const avism_params *p, const Level &L, const flo
     cubes.cap = cap;
     cubes.i32 = (int32_t *)c.get(B_CUBES, (size_t)cap * 17 * 4);
     cubes.f32 = (float *)(cubes.i32 + (size_t)cap * 10);
-    k_write_cubes<<<grid_for(ncand, 256), 256, 0, c.stream>>>(A, ids, ncand, L.g.dx, L.rad_at(1), cubes.i32, cubes.f32, cap);
+    ++c.launches, k_write_cubes<<<grid_for(ncand, 256), 256, 0, c.stream>>>(A, ids, ncand, L.g.dx, L.rad_at(1), cubes.i32, cubes.f32, cap);
     AV_CUDA(cudaGetLastError());
+    c.mark("cube_arrays");
     return nvoid;
 }
 

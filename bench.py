@@ -1,0 +1,296 @@
+#!/usr/bin/env python
+"""bench.py -- grid cells/s of the AVISM hot path (particles -> void catalogue).
+
+Workload (the 512^3 configuration the metric is quoted on): 2^27 particles
+Poisson-sampled from a lognormal field (Gaussian random field with P(k) ~ k^-1.2,
+sigma_ln = 1) in a periodic L = 500 cMpc box, linear-theory velocities (350 km/s
+rms), equal masses; grid 512^3 (ext 640^3), k = 32, SPH density and velocity,
+README thresholds.  Synthetic, seeded (1004 + rank).
+
+A step is one pass of the whole level on the GPU: kNN / SPH particle-to-grid,
+normalisation, divergence, flags, candidate ordering, cube growth, merging and
+post-processing, ending with the catalogue on the host.
+  value  -- inputs already resident in HBM (device pointers through the C-ABI)
+  e2e    -- the same call with pinned host buffers: H2D of the particles and the
+            D2H of the catalogue inside the timed region
+Inputs (3.5 GB of particles, GBs of grids) exceed the 126 MB L2, so no flush is
+needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun each rank processes its own snapshot (iterations of the
+reference's FIRST..LAST loop are independent): replicas, weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid cells/s end-to-end at 512³, learned+batched vs plain GPU, exact catalogue"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=512)
+    ap.add_argument("--log2n", type=int, default=27)
+    ap.add_argument("--box", type=float, default=500.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--stages", action="store_true", help="print per-stage device times to stderr")
+    return ap.parse_args()
+
+
+# ---- clocks sampled during the timed region ----------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and s[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---- distributed plumbing -----------------------------------------------------
+def dist_setup(n_gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def workload_params(a):
+    from avism_b200._abi import Params
+    return Params(nx=a.nx, periodic=1, lado0=a.box, kneighbours=32, flag_vel_interp=1, flag_dens_interp=1,
+                  nvoid_max=4_000_000)
+
+
+def config_dict(a, world):
+    return {"workload": f"particles->void catalogue, {a.nx}^3 grid (ext {a.nx + 2 * (a.nx // 8)}^3), "
+                        f"2^{a.log2n} particles, L={a.box:g} cMpc periodic, k=32, SPH/SPH",
+            "grid": a.nx, "particles": 2 ** a.log2n, "box_cmpc": a.box, "kneighbours": 32,
+            "field": "lognormal GRF P(k)~k^-1.2 sigma_ln=1, linear-theory v 350 km/s rms",
+            "l2": "inputs > L2 (126 MB); no flush", "parallelism": f"replicas x{world} (one snapshot per rank)"}
+
+
+# ---- CPU baseline: the oracle on a bounded sample of the same workload -------
+def cpu_sample_run(steps: int, warmup: int, seed: int = 1004):
+    """The C oracle (restatement of the reference's algorithms: k-d tree kNN,
+    scatter SPH, serial growth and merge) on a 128^3 sub-box with the same cell
+    size and particle density (2^21 particles, L = 125 cMpc, periodic)."""
+    from avism_b200 import synth
+    from avism_b200._abi import Params
+    from oracle import oracle as O
+    nx, box, n = 128, 125.0, 2 ** 21
+    parts = synth.to_reader_units(synth.lognormal(n=n, ng=128, box=box, index=-1.2, sigma_ln=1.0,
+                                                  vrms=350.0, seed=seed))
+    p = Params(nx=nx, periodic=1, lado0=box, kneighbours=32, nvoid_max=4_000_000)
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        O.run_level(p, parts)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    t = statistics.mean(times)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return nx ** 3 / t, cores, t, f"oracle port, full level on a {nx}^3 sub-box (2^21 particles, L={box:g}, " \
+                                   f"ext {nx + 2 * 51}^3), same cell size and density; {t:.2f} s per level"
+
+
+def run_reference(a):
+    rank, world, _ = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    value, cores, t, sample = cpu_sample_run(max(1, min(a.steps, 3)), 1 if a.warmup > 0 else 0)
+    line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": config_dict(a, 1),
+            "cpu_baseline": {"value": value, "unit": "cells/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---- our arm ----------------------------------------------------------------
+# algorithmic bytes per unit of the dominant stages
+ALG_BYTES = {
+    # per cell query: the k neighbours' (x,y,z,m,vx,vy,vz,rho) are compulsory once per
+    # particle; per cell 3 velocity components written, per particle h read+written
+    "cells_knn": lambda n, nc: 36 * n + 8 * n + 12 * nc,
+    "ppart_dens": lambda n, nc: 20 * n + 4 * n,
+    "ddens_scatter": lambda n, nc: 24 * n + 16 * nc,
+    "fill_h_zeros": lambda n, nc: 20 * n,
+}
+
+
+def run_ours(a):
+    import numpy as np
+    import torch
+    from avism_b200 import synth
+    from avism_b200._abi import Cubes, Voids, ptr  # noqa: F401
+    from avism_b200.avism import AvismGPU
+
+    rank, world, local = dist_setup(a.gpus)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    p = workload_params(a)
+    n = 2 ** a.log2n
+    ncells = a.nx ** 3
+    with torch.no_grad():
+        parts = synth.lognormal_torch(n, min(a.nx, 512), a.box, -1.2, 1.0, 350.0, seed=1004 + rank, device=dev)
+        parts = synth.to_reader_units(parts)
+    dev_parts = {k: parts[k].contiguous() for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    host_parts = {k: v.cpu().pin_memory() for k, v in dev_parts.items()}
+    torch.cuda.synchronize()
+    ctx = AvismGPU(local)
+
+    def step(src):
+        return ctx.run_level(p, src, capacity=p.nvoid_max)
+
+    def timed(src, steps, warmup):
+        for _ in range(warmup):
+            step(src)
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.launches()
+        stages = []
+        e0.record()
+        for _ in range(steps):
+            r = step(src)
+            stages.append(ctx.stage_times())
+        e1.record()
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = e0.elapsed_time(e1) / steps
+        return ms, r, stages, ctx.launches() - l0
+
+    sampler = ClockSampler(local)
+    with sampler:
+        ms_dev, res, stages, launches = timed(dev_parts, a.steps, a.warmup)
+        ms_e2e, res_h, stages_h, _ = timed(host_parts, max(1, a.steps), 1)
+    ms_dev = max_over_ranks(ms_dev, world)
+    ms_e2e = max_over_ranks(ms_e2e, world)
+    # the catalogue of both paths must be the same
+    same = all(np.array_equal(res["cat"][k], res_h["cat"][k]) for k in ("indice", "uvoid", "ncellv", "volnew", "gxc"))
+    value = world * ncells / (ms_dev / 1e3)
+    e2e = world * ncells / (ms_e2e / 1e3)
+    # per-stage mean device time (events on the library's stream)
+    keys = stages[0].keys()
+    st = {k: statistics.mean(s.get(k, 0.0) for s in stages) for k in keys}
+    if a.stages and rank == 0:
+        print(json.dumps({"stages_ms": st, "nvoid": res["nvoid"], "nvoidt": res["cat"]["nvoidt"]}), file=sys.stderr)
+    dom = max((k for k in st if k in ALG_BYTES), key=lambda k: st[k])
+    peaks = json.load(open(PEAKS)) if os.path.exists(PEAKS) else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    alg = ALG_BYTES[dom](n, ncells)
+    achieved = alg / (st[dom] / 1e3) / 1e9
+    nvoid = res["nvoid"]
+    h2d = 7 * 4 * n
+    d2h = nvoid * (17 * 4) + nvoid * (15 * 4 + 3 * 4)
+    if rank == 0:
+        cpu = None
+        if not a.no_cpu_baseline:
+            v, cores, t, sample = cpu_sample_run(1, 0)
+            cpu = {"value": v, "unit": "cells/s", "cores": cores, "kind": "port", "sample": sample}
+        line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms_dev, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": config_dict(a, world),
+                "e2e": {"value": e2e, "unit": "cells/s", "ms_per_step": ms_e2e,
+                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                             "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                             "alg_bytes_per_launch": alg, "ms_per_launch": st[dom],
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback"},
+                "cpu_baseline": cpu,
+                "clocks": sampler.summary(),
+                "gpu_launches": launches,
+                "catalogue": {"cubes": nvoid, "voids": res["cat"]["nvoidt"], "host_vs_device_identical": same},
+                "stages_ms": {k: round(v, 3) for k, v in st.items()}}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

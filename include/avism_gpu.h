@@ -110,8 +110,12 @@ typedef struct avism_gpu_ctx avism_gpu_ctx;
 int avism_gpu_create(avism_gpu_ctx **out, int device);
 int avism_gpu_destroy(avism_gpu_ctx *ctx);
 const char *avism_gpu_last_error(const avism_gpu_ctx *ctx);
-/* Device-side time of the last call's stages (ms); n = number of entries. */
+/* Device-side time of the last call's stages (ms); returns the stage count and
+ * writes at most n entries.  avism_gpu_stage_name(i) names stage i.            */
 int avism_gpu_stage_times(const avism_gpu_ctx *ctx, double *ms, int n);
+const char *avism_gpu_stage_name(const avism_gpu_ctx *ctx, int i);
+/* Number of this library's kernels launched on the context so far.           */
+int64_t avism_gpu_launches(const avism_gpu_ctx *ctx);
 
 /* ---- a1: level grid, replaces MALLA (src/grid.f90:3-76) and the PBC block
  *      src/avism.f90:780-865.  radx receives RADX(rad_lo..rad_hi); pass NULL
