@@ -9,9 +9,12 @@
 //       integer box-overlap test.
 // (a) is answered from the painted boxes themselves: the closest cell of a
 // box to a point is the per-axis clamp, and the value painted on a cell is the
-// owner of the earliest-painted box containing it.  The merge therefore runs
-// on cube records only (O(cubes x neighbours)); the cell grid is painted
-// afterwards on the GPU from the recorded paint order.
+// owner of the earliest-painted box containing it.  Every cube that can touch
+// cube i -- through (a) or through absorption, which needs overlapping 1-cell
+// halo boxes -- is on i's neighbour list, built once on the GPU with the exact
+// ball-search distance.  The merge therefore runs on cube records only
+// (O(cubes x neighbours)); the cell grid is painted afterwards on the GPU from
+// the recorded paint order.
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -24,48 +27,8 @@ namespace avism {
 
 namespace {
 
-struct BoxHash {   // uniform buckets over the ext grid holding painted box ids
-    int low1, ne, bs, nbk;
-    std::vector<std::vector<int32_t>> bucket;
-    void init(int l1, int n, int b) {
-        low1 = l1; ne = n; bs = b;
-        nbk = (ne + bs - 1) / bs;
-        bucket.assign((size_t)nbk * nbk * nbk, {});
-    }
-    int bk(int v) const { return std::min(std::max((v - low1) / bs, 0), nbk - 1); }
-    void insert(int32_t id, const int lo[3], const int hi[3]) {
-        for (int z = bk(lo[2]); z <= bk(hi[2]); z++)
-            for (int y = bk(lo[1]); y <= bk(hi[1]); y++)
-                for (int x = bk(lo[0]); x <= bk(hi[0]); x++)
-                    bucket[(size_t)x + (size_t)nbk * ((size_t)y + (size_t)nbk * z)].push_back(id);
-    }
-};
-
-struct PointHash {  // static buckets of cube centres for the ball search
-    float origin, cell, L;
-    int nb, periodic;
-    std::vector<int32_t> start, items;
-    void build(const float *x, const float *y, const float *z, int32_t n, float org, float ext, float c,
-               float box, int per) {
-        origin = org; cell = c; L = box; periodic = per;
-        nb = std::max(1, (int)std::ceil(ext / c));
-        std::vector<int32_t> key(n);
-        start.assign((size_t)nb * nb * nb + 1, 0);
-        for (int32_t i = 0; i < n; i++) {
-            const int bx = co(x[i]), by = co(y[i]), bz = co(z[i]);
-            key[i] = bx + nb * (by + nb * bz);
-            start[key[i] + 1]++;
-        }
-        for (size_t b = 1; b < start.size(); b++) start[b] += start[b - 1];
-        items.resize(n);
-        std::vector<int32_t> fill(start.begin(), start.end() - 1);
-        for (int32_t i = 0; i < n; i++) items[fill[key[i]]++] = i;
-    }
-    int co(float v) const { return std::min(std::max((int)std::floor((v - origin) / cell), 0), nb - 1); }
-};
-
 // squared distance as distance() in src/kdtree.f90:1441-1465
-inline float dist2_ref(float px, float py, float pz, float qx, float qy, float qz, float L, int periodic) {
+[[maybe_unused]] inline float dist2_ref(float px, float py, float pz, float qx, float qy, float qz, float L, int periodic) {
     float dx = px - qx, dy = py - qy, dz = pz - qz;
     if (periodic) {
         float a = std::fabs(dx); dx = std::fmin(a, L - a);
@@ -79,6 +42,12 @@ inline float dist2_ref(float px, float py, float pz, float qx, float qy, float q
 }
 
 }  // namespace
+
+float merge_ball_r2(float vol, float dx) {
+    const float rthis = (std::sqrt(3.0f) / 2.0f) * std::pow(vol, 1.0f / 3.0f);
+    const float rr = 2.0f * rthis + ((2.1f * std::sqrt(3.0f)) * dx) * 1.0f;
+    return rr * rr;
+}
 
 void merge_cubes_host(const MergeIn &in, MergeOut &out) {
     const int32_t nv = in.nvoid;
@@ -97,29 +66,14 @@ void merge_cubes_host(const MergeIn &in, MergeOut &out) {
         gzc[i] = in.rx1 + (float)(in.icz[i] - 1) * dx;
         vol[i] = ((in.rfx[i] - in.rix[i]) * (in.rfy[i] - in.riy[i])) * (in.rfz[i] - in.riz[i]);
     }
-    // ball-search structure on the initial centres (the reference builds its
-    // k-d tree from them before any centre moves)
-    const float L = in.periodic ? in.lado0plus : 0.0f;
-    PointHash ph;
-    const float org = in.rx1 + (float)(low1 - 1) * dx - dx;
-    const float ext = (float)(low2 - low1 + 3) * dx;
-    ph.build(gxc.data(), gyc.data(), gzc.data(), nv, org, ext, 8.0f * dx, L, in.periodic);
-    const std::vector<float> cx0(gxc), cy0(gyc), cz0(gzc);
-
-    BoxHash bh;
-    bh.init(low1, low2 - low1 + 1, 8);
     std::vector<char> major(nv, 0);
-    std::vector<int32_t> stamp(nv, -1);
     int32_t ptime = 0;
     int32_t nvoid2 = nv;
-
-    auto paint = [&](int32_t cube, int32_t owner) {   // 1-based ids
+    auto paint = [&](int32_t cube, int32_t owner) {   // 1-based ids; each cube paints once
         const int c = cube - 1;
-        if (out.paint_time[c] >= 0) return;     // already painted (never repaint)
+        if (out.paint_time[c] >= 0) return;
         out.paint_time[c] = ptime++;
         out.paint_owner[c] = owner;
-        const int lo[3] = {X0[c], Y0[c], Z0[c]}, hi[3] = {X1[c], Y1[c], Z1[c]};
-        bh.insert(c, lo, hi);
     };
     auto absorb = [&](int32_t i0, int32_t i1) {       // src/voidfinding.f90:867-872
         const float v0 = vol[i0 - 1], v1 = vol[i1 - 1];
@@ -128,12 +82,13 @@ void merge_cubes_host(const MergeIn &in, MergeOut &out) {
         gzc[i0 - 1] = (gzc[i0 - 1] * v0 + gzc[i1 - 1] * v1) / (v0 + v1);
         vol[i0 - 1] = v0 + v1;
     };
-
     std::vector<std::pair<float, int32_t>> ball;
-    int32_t qstamp = 0;
+    const long long ne = low2 - low1 + 1;
     for (int32_t I = 0; I < nv; I++) {
         const int32_t ind1 = in.indice[I];
         const int c1 = ind1 - 1;
+        const int32_t *nb = in.nbr + in.nbr_start[c1];
+        const int32_t nnb = in.nbr_start[c1 + 1] - in.nbr_start[c1];
         int32_t ind0, indp;
         if (out.uvoid[c1] > 0) {
             ind0 = out.uvoid[c1];
@@ -141,44 +96,39 @@ void merge_cubes_host(const MergeIn &in, MergeOut &out) {
         } else {
             ind0 = ind1;
             indp = father[ind0 - 1];
-            // closest painted halo cell with the same father (src/voidfinding.f90:822-860)
+            // closest painted cell of the 1-cell halo box whose void has the same
+            // father (src/voidfinding.f90:822-860); ties: first in K,J,I order.
+            // Boxes of different fathers never overlap, so the painted boxes of
+            // this cube's own neighbour list are all that can hold such a cell.
             const int e0[3] = {std::max(X0[c1] - 1, low1), std::max(Y0[c1] - 1, low1), std::max(Z0[c1] - 1, low1)};
             const int e1[3] = {std::min(X1[c1] + 1, low2), std::min(Y1[c1] + 1, low2), std::min(Z1[c1] + 1, low2)};
             const int cc[3] = {in.icx[c1], in.icy[c1], in.icz[c1]};
             long long bestkey = LLONG_MAX;
             int best[3] = {0, 0, 0};
-            qstamp++;
-            std::vector<int32_t> cand;
-            for (int z = bh.bk(e0[2]); z <= bh.bk(e1[2]); z++)
-                for (int y = bh.bk(e0[1]); y <= bh.bk(e1[1]); y++)
-                    for (int x = bh.bk(e0[0]); x <= bh.bk(e1[0]); x++)
-                        for (int32_t j : bh.bucket[(size_t)x + (size_t)bh.nbk * ((size_t)y + (size_t)bh.nbk * z)]) {
-                            if (stamp[j] == qstamp) continue;
-                            stamp[j] = qstamp;
-                            const int lo[3] = {std::max(X0[j], e0[0]), std::max(Y0[j], e0[1]), std::max(Z0[j], e0[2])};
-                            const int hi[3] = {std::min(X1[j], e1[0]), std::min(Y1[j], e1[1]), std::min(Z1[j], e1[2])};
-                            if (lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]) continue;
-                            cand.push_back(j);
-                            if (father[j] != indp) continue;
-                            int q[3];
-                            long long d2 = 0;
-                            for (int a = 0; a < 3; a++) {
-                                q[a] = std::min(std::max(cc[a], lo[a]), hi[a]);
-                                d2 += (long long)(cc[a] - q[a]) * (cc[a] - q[a]);
-                            }
-                            // order: distance, then K, J, I of the cell (scan order)
-                            const long long ne = bh.ne;
-                            const long long key = d2 * ne * ne * ne +
-                                                  ((long long)(q[2] - low1) * ne + (q[1] - low1)) * ne + (q[0] - low1);
-                            if (key < bestkey) { bestkey = key; best[0] = q[0]; best[1] = q[1]; best[2] = q[2]; }
-                        }
+            for (int32_t t = 0; t < nnb; t++) {
+                const int32_t j = nb[t];
+                if (out.paint_time[j] < 0) continue;
+                const int lo[3] = {std::max(X0[j], e0[0]), std::max(Y0[j], e0[1]), std::max(Z0[j], e0[2])};
+                const int hi[3] = {std::min(X1[j], e1[0]), std::min(Y1[j], e1[1]), std::min(Z1[j], e1[2])};
+                if (lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]) continue;
+                int q[3];
+                long long d2 = 0;
+                for (int a = 0; a < 3; a++) {
+                    q[a] = std::min(std::max(cc[a], lo[a]), hi[a]);
+                    d2 += (long long)(cc[a] - q[a]) * (cc[a] - q[a]);
+                }
+                const long long key = d2 * ne * ne * ne + ((long long)(q[2] - low1) * ne + (q[1] - low1)) * ne + (q[0] - low1);
+                if (key < bestkey) { bestkey = key; best[0] = q[0]; best[1] = q[1]; best[2] = q[2]; }
+            }
             if (bestkey != LLONG_MAX) {
-                // value painted on that cell: owner of the earliest box containing it
+                // value painted on that cell: owner of the earliest painted box holding it
                 int32_t tmin = INT_MAX, own = 0;
-                for (int32_t j : cand) {
-                    if (best[0] < X0[j] || best[0] > X1[j] || best[1] < Y0[j] || best[1] > Y1[j] ||
+                for (int32_t t = 0; t < nnb; t++) {
+                    const int32_t j = nb[t];
+                    const int32_t pt = out.paint_time[j];
+                    if (pt < 0 || best[0] < X0[j] || best[0] > X1[j] || best[1] < Y0[j] || best[1] > Y1[j] ||
                         best[2] < Z0[j] || best[2] > Z1[j]) continue;
-                    if (out.paint_time[j] < tmin) { tmin = out.paint_time[j]; own = out.paint_owner[j]; }
+                    if (pt < tmin) { tmin = pt; own = out.paint_owner[j]; }
                 }
                 ind0 = own;
             }
@@ -192,62 +142,23 @@ void merge_cubes_host(const MergeIn &in, MergeOut &out) {
                 major[ind0 - 1] = 1;
             }
         }
-        // absorb overlapping unmerged cubes found by a ball search (918-987)
-        const int ix1 = X0[c1] - 1, ix2 = X1[c1] + 1, jy1 = Y0[c1] - 1, jy2 = Y1[c1] + 1;
-        const int kz1 = Z0[c1] - 1, kz2 = Z1[c1] + 1;
-        const float tx = gxc[c1], ty = gyc[c1], tz = gzc[c1];
-        const float rthis = (std::sqrt(3.0f) / 2.0f) * std::pow(vol[c1], 1.0f / 3.0f);
-        const float rr = 2.0f * rthis + ((2.1f * std::sqrt(3.0f)) * dx) * 1.0f;
-        const float r2 = rr * rr;
+        // absorb the cubes of the ball search (src/voidfinding.f90:904-987) in
+        // (distance, id) order; the overlap test on the 1-cell halo boxes is what
+        // put them on the neighbour list
         ball.clear();
-        {
-            // periodic: query the target and its images one box length away;
-            // the minimum-image distance decides membership, a stamp dedupes
-            const int span = (int)std::ceil(rr / ph.cell) + 1;
-            qstamp++;
-            for (int iz = -1; iz <= 1; iz++)
-                for (int iy = -1; iy <= 1; iy++)
-                    for (int ix = -1; ix <= 1; ix++) {
-                        if (!ph.periodic && (ix || iy || iz)) continue;
-                        const float qx = tx + (float)ix * L, qy = ty + (float)iy * L, qz = tz + (float)iz * L;
-                        const float lo_q[3] = {qx - rr, qy - rr, qz - rr}, hi_q[3] = {qx + rr, qy + rr, qz + rr};
-                        bool outside = false;
-                        for (int a = 0; a < 3; a++)
-                            if (hi_q[a] < ph.origin || lo_q[a] > ph.origin + ph.cell * (float)ph.nb) outside = true;
-                        if (outside) continue;
-                        const int b[3] = {ph.co(qx), ph.co(qy), ph.co(qz)};
-                        for (int z = std::max(b[2] - span, 0); z <= std::min(b[2] + span, ph.nb - 1); z++)
-                            for (int y = std::max(b[1] - span, 0); y <= std::min(b[1] + span, ph.nb - 1); y++)
-                                for (int x = std::max(b[0] - span, 0); x <= std::min(b[0] + span, ph.nb - 1); x++) {
-                                    const size_t bb = (size_t)x + (size_t)ph.nb * ((size_t)y + (size_t)ph.nb * z);
-                                    for (int32_t t = ph.start[bb]; t < ph.start[bb + 1]; t++) {
-                                        const int32_t j = ph.items[t];
-                                        if (stamp[j] == qstamp) continue;
-                                        const float d2 = dist2_ref(cx0[j], cy0[j], cz0[j], tx, ty, tz, L, ph.periodic);
-                                        if (d2 <= r2) {
-                                            stamp[j] = qstamp;
-                                            ball.push_back({d2, j});
-                                        }
-                                    }
-                                }
-                    }
-        }
+        for (int32_t t = 0; t < nnb; t++)
+            if (in.nbr_inball[in.nbr_start[c1] + t]) ball.push_back({in.nbr_d2[in.nbr_start[c1] + t], nb[t]});
         std::sort(ball.begin(), ball.end());
         for (const auto &bj : ball) {
             const int32_t j = bj.second;
             const int32_t ind2 = j + 1;
-            if (ind2 == ind1) continue;
             if (major[j]) continue;
             if (out.uvoid[j] >= 0) continue;
             if (indp != father[j]) continue;
-            const int ix3 = X0[j] - 1, ix4 = X1[j] + 1, jy3 = Y0[j] - 1, jy4 = Y1[j] + 1;
-            const int kz3 = Z0[j] - 1, kz4 = Z1[j] + 1;
-            if (ix1 <= ix4 && ix3 <= ix2 && jy1 <= jy4 && jy3 <= jy2 && kz1 <= kz4 && kz3 <= kz2) {
-                out.uvoid[j] = ind0;
-                absorb(ind0, ind2);
-                paint(ind2, ind0);
-                nvoid2--;
-            }
+            out.uvoid[j] = ind0;
+            absorb(ind0, ind2);
+            paint(ind2, ind0);
+            nvoid2--;
         }
     }
     out.nvoid2 = nvoid2;

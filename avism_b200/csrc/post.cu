@@ -257,6 +257,82 @@ __global__ void k_final_props(PostGrid G, const int32_t *marca, const int32_t *u
     }
 }
 
+
+// ---- neighbour lists of MERGE_VOID: cubes of the same father whose 1-cell
+//      halo boxes overlap; d2 is distance() of src/kdtree.f90:1441-1465 on the
+//      initial centres, inball tests it against the cube's ball radius ----------
+struct NbrArgs {
+    int32_t nv, cap, nbk, low1, bs;
+    const int32_t *box;          // x0,x1,y0,y1,z0,z1 arrays of cap entries
+    const int32_t *father;
+    const float *cx, *cy, *cz, *r2;
+    const int32_t *bstart, *bitems;
+    float L;
+    int periodic;
+};
+__device__ __forceinline__ int nbr_bucket(const NbrArgs &A, int v) {
+    const int b = (v - A.low1) / A.bs;
+    return b < 0 ? 0 : (b >= A.nbk ? A.nbk - 1 : b);
+}
+__global__ void k_cube_bucket_count(NbrArgs A, int32_t *cnt) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.nv) return;
+    const int bx = nbr_bucket(A, (A.box[0 * A.cap + i] + A.box[1 * A.cap + i]) / 2);
+    const int by = nbr_bucket(A, (A.box[2 * A.cap + i] + A.box[3 * A.cap + i]) / 2);
+    const int bz = nbr_bucket(A, (A.box[4 * A.cap + i] + A.box[5 * A.cap + i]) / 2);
+    atomicAdd(&cnt[bx + A.nbk * (by + A.nbk * bz)], 1);
+}
+__global__ void k_cube_bucket_fill(NbrArgs A, int32_t *cursor, int32_t *items) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.nv) return;
+    const int bx = nbr_bucket(A, (A.box[0 * A.cap + i] + A.box[1 * A.cap + i]) / 2);
+    const int by = nbr_bucket(A, (A.box[2 * A.cap + i] + A.box[3 * A.cap + i]) / 2);
+    const int bz = nbr_bucket(A, (A.box[4 * A.cap + i] + A.box[5 * A.cap + i]) / 2);
+    items[atomicAdd(&cursor[bx + A.nbk * (by + A.nbk * bz)], 1)] = i;
+}
+template <bool FILL>
+__global__ void k_cube_nbrs(NbrArgs A, int32_t *count, const int32_t *start, int32_t *nbr, float *d2out,
+                            uint8_t *inball) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.nv) return;
+    int lo[3], hi[3], bc[3];
+    for (int a = 0; a < 3; a++) {
+        lo[a] = A.box[(2 * a) * A.cap + i];
+        hi[a] = A.box[(2 * a + 1) * A.cap + i];
+        bc[a] = nbr_bucket(A, (lo[a] + hi[a]) / 2);
+    }
+    const int32_t f = A.father[i];
+    int32_t n = 0;
+    const int32_t base = FILL ? start[i] : 0;
+    for (int bz = max(bc[2] - 1, 0); bz <= min(bc[2] + 1, A.nbk - 1); bz++)
+        for (int by = max(bc[1] - 1, 0); by <= min(bc[1] + 1, A.nbk - 1); by++)
+            for (int bx = max(bc[0] - 1, 0); bx <= min(bc[0] + 1, A.nbk - 1); bx++) {
+                const int b = bx + A.nbk * (by + A.nbk * bz);
+                for (int32_t t = A.bstart[b]; t < A.bstart[b + 1]; t++) {
+                    const int32_t j = A.bitems[t];
+                    if (j == i || A.father[j] != f) continue;
+                    bool ov = true;
+                    for (int a = 0; a < 3; a++)
+                        if (lo[a] - 1 > A.box[(2 * a + 1) * A.cap + j] + 1 || A.box[(2 * a) * A.cap + j] - 1 > hi[a] + 1) ov = false;
+                    if (!ov) continue;
+                    if (FILL) {
+                        float dx = __fsub_rn(A.cx[j], A.cx[i]), dy = __fsub_rn(A.cy[j], A.cy[i]), dz = __fsub_rn(A.cz[j], A.cz[i]);
+                        if (A.periodic) {
+                            float q = fabsf(dx); dx = fminf(q, __fsub_rn(A.L, q));
+                            q = fabsf(dy); dy = fminf(q, __fsub_rn(A.L, q));
+                            q = fabsf(dz); dz = fminf(q, __fsub_rn(A.L, q));
+                        }
+                        const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+                        nbr[base + n] = j;
+                        d2out[base + n] = d2;
+                        inball[base + n] = d2 <= A.r2[i] ? 1 : 0;
+                    }
+                    n++;
+                }
+            }
+    if (!FILL) count[i] = n;
+}
+
 template <class T>
 static T *dev_upload(Ctx &c, BufId id, const T *h, size_t n) {
     T *d = c.get_t<T>(id, std::max<size_t>(n, 1));
@@ -290,6 +366,69 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         for (int32_t i = 0; i < nv; i++) indice[i] = asc[nv - 1 - i];
     }
     c.mark("indexx_vol");
+    // ---- neighbour lists for MERGE_VOID, built on the device
+    std::vector<int32_t> nbr_start(nvs + 1, 0), nbr;
+    std::vector<float> nbr_d2;
+    std::vector<uint8_t> nbr_inball;
+    int32_t *box_d = nullptr;
+    {
+        std::vector<int32_t> boxes((size_t)nvs * 6);
+        const int32_t *src[6] = {cb->inicio_x, cb->final_x, cb->inicio_y, cb->final_y, cb->inicio_z, cb->final_z};
+        int ext_max = 1;
+        for (int a = 0; a < 6; a++) std::memcpy(&boxes[(size_t)a * nvs], src[a], sizeof(int32_t) * (size_t)nv);
+        for (int32_t i = 0; i < nv; i++)
+            for (int a = 0; a < 3; a++) ext_max = std::max(ext_max, src[2 * a + 1][i] - src[2 * a][i] + 1);
+        box_d = dev_upload<int32_t>(c, B_RED0, boxes.data(), boxes.size());
+        std::vector<float> cen((size_t)nvs * 4);
+        for (int32_t i = 0; i < nv; i++) {
+            cen[i] = L.rad_at(1) + (float)(cb->icx[i] - 1) * dx;
+            cen[(size_t)nvs + i] = L.rad_at(1) + (float)(cb->icy[i] - 1) * dx;
+            cen[(size_t)2 * nvs + i] = L.rad_at(1) + (float)(cb->icz[i] - 1) * dx;
+            const float v = ((cb->rfin_x[i] - cb->rini_x[i]) * (cb->rfin_y[i] - cb->rini_y[i])) * (cb->rfin_z[i] - cb->rini_z[i]);
+            cen[(size_t)3 * nvs + i] = merge_ball_r2(v, dx);
+        }
+        float *cen_d = dev_upload<float>(c, B_RED1, cen.data(), cen.size());
+        int32_t *fa_d = dev_upload<int32_t>(c, B_LABMAP, cb->father, nv);
+        NbrArgs A;
+        A.nv = nv; A.cap = nvs; A.low1 = g.low1; A.bs = ext_max + 2;
+        A.nbk = std::max(1, (ne + A.bs - 1) / A.bs);
+        A.box = box_d; A.father = fa_d; A.cx = cen_d; A.cy = cen_d + nvs; A.cz = cen_d + 2 * (size_t)nvs;
+        A.r2 = cen_d + 3 * (size_t)nvs; A.L = p->periodic ? g.lado0plus : 0.0f; A.periodic = p->periodic;
+        const int64_t nb3 = (int64_t)A.nbk * A.nbk * A.nbk;
+        int32_t *bcnt = c.get_t<int32_t>(B_SCAN_A, nb3 + 1);
+        int32_t *bstart = c.get_t<int32_t>(B_SCAN_B, nb3 + 1);
+        int32_t *items = c.get_t<int32_t>(B_LIST_A, nvs);
+        AV_CUDA(cudaMemsetAsync(bcnt, 0, sizeof(int32_t) * (size_t)(nb3 + 1), c.stream));
+        if (nv > 0) ++c.launches, k_cube_bucket_count<<<grid_for(nv, 256), 256, 0, c.stream>>>(A, bcnt);
+        size_t tmp = 0;
+        AV_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, bcnt, bstart, (int)(nb3 + 1), c.stream));
+        void *t = c.get(B_CUB_TMP, tmp);
+        AV_CUDA(cub::DeviceScan::ExclusiveSum(t, tmp, bcnt, bstart, (int)(nb3 + 1), c.stream));
+        AV_CUDA(cudaMemcpyAsync(bcnt, bstart, sizeof(int32_t) * (size_t)(nb3 + 1), cudaMemcpyDeviceToDevice, c.stream));
+        if (nv > 0) ++c.launches, k_cube_bucket_fill<<<grid_for(nv, 256), 256, 0, c.stream>>>(A, bcnt, items);
+        A.bstart = bstart; A.bitems = items;
+        int32_t *ncount = c.get_t<int32_t>(B_LIST_B, nvs + 1);
+        int32_t *nstart = c.get_t<int32_t>(B_GE, nvs + 1);
+        AV_CUDA(cudaMemsetAsync(ncount, 0, sizeof(int32_t) * (size_t)(nvs + 1), c.stream));
+        if (nv > 0) ++c.launches, k_cube_nbrs<false><<<grid_for(nv, 128), 128, 0, c.stream>>>(A, ncount, nullptr, nullptr, nullptr, nullptr);
+        AV_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, ncount, nstart, nv + 1, c.stream));
+        t = c.get(B_CUB_TMP, tmp);
+        AV_CUDA(cub::DeviceScan::ExclusiveSum(t, tmp, ncount, nstart, nv + 1, c.stream));
+        dev_download(c, nbr_start.data(), nstart, (size_t)nv + 1);
+        const int32_t tot = nbr_start[nv];
+        int32_t *nbr_d = c.get_t<int32_t>(B_CAND_POS, std::max(tot, 1));
+        float *d2_d = c.get_t<float>(B_CAND_KEY, std::max(tot, 1));
+        uint8_t *ib_d = c.get_t<uint8_t>(B_COVER, std::max(tot, 1));
+        if (nv > 0) ++c.launches, k_cube_nbrs<true><<<grid_for(nv, 128), 128, 0, c.stream>>>(A, nullptr, nstart, nbr_d, d2_d, ib_d);
+        AV_CUDA(cudaGetLastError());
+        nbr.resize(std::max(tot, 1));
+        nbr_d2.resize(std::max(tot, 1));
+        nbr_inball.resize(std::max(tot, 1));
+        AV_CUDA(cudaMemcpyAsync(nbr.data(), nbr_d, sizeof(int32_t) * (size_t)tot, cudaMemcpyDeviceToHost, c.stream));
+        AV_CUDA(cudaMemcpyAsync(nbr_d2.data(), d2_d, sizeof(float) * (size_t)tot, cudaMemcpyDeviceToHost, c.stream));
+        dev_download(c, nbr_inball.data(), ib_d, (size_t)tot);
+    }
+    c.mark("merge_lists");
     // ---- MERGE_VOID
     MergeIn mi;
     mi.nvoid = nv; mi.low1 = g.low1; mi.low2 = g.low2; mi.periodic = p->periodic;
@@ -298,6 +437,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
     mi.z0 = cb->inicio_z; mi.z1 = cb->final_z; mi.icx = cb->icx; mi.icy = cb->icy; mi.icz = cb->icz;
     mi.father = cb->father; mi.rix = cb->rini_x; mi.rfx = cb->rfin_x; mi.riy = cb->rini_y;
     mi.rfy = cb->rfin_y; mi.riz = cb->rini_z; mi.rfz = cb->rfin_z; mi.indice = indice.data();
+    mi.nbr_start = nbr_start.data(); mi.nbr = nbr.data(); mi.nbr_d2 = nbr_d2.data(); mi.nbr_inball = nbr_inball.data();
     MergeOut mo;
     merge_cubes_host(mi, mo);
     c.mark("merge_host");
@@ -307,10 +447,6 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
     // ---- paint MARCA
     int32_t *marca = c.get_t<int32_t>(B_MARCA, ne3);
     {
-        std::vector<int32_t> boxes((size_t)nvs * 6);
-        const int32_t *src[6] = {cb->inicio_x, cb->final_x, cb->inicio_y, cb->final_y, cb->inicio_z, cb->final_z};
-        for (int a = 0; a < 6; a++) std::memcpy(&boxes[(size_t)a * nvs], src[a], sizeof(int32_t) * (size_t)nv);
-        int32_t *box_d = dev_upload<int32_t>(c, B_RED0, boxes.data(), boxes.size());
         int32_t *pt_d = dev_upload<int32_t>(c, B_RED1, mo.paint_time.data(), nv);
         std::vector<int32_t> owner_by_time(nvs, 0);
         for (int32_t i = 0; i < nv; i++) {
