@@ -20,6 +20,7 @@ struct KnnGrid {
     int nb;
     float origin, bw, inv_bw, box, margin;
     int periodic;
+    const float *r0;          // per-bin starting radius of the radius-guided search, or null
 };
 
 inline KnnGrid make_knn_grid(const BinnedParticles &bp) {
@@ -33,6 +34,7 @@ inline KnnGrid make_knn_grid(const BinnedParticles &bp) {
     G.box = bp.box;
     G.periodic = bp.periodic;
     G.margin = 2e-3f * bp.bw + 1e-6f * bp.box;
+    G.r0 = nullptr;
     return G;
 }
 
@@ -101,14 +103,56 @@ __device__ __forceinline__ void topk_insert(unsigned long long *col, int S, int 
     col[(size_t)i * S] = key;
 }
 
-__device__ __forceinline__ void scan_bin(const KnnGrid &G, int bin, float qx, float qy, float qz,
-                                         unsigned long long *col, int S, int K, int &cnt) {
-    const int64_t a = G.start[bin], e = G.start[bin + 1];
-    for (int64_t p = a; p < e; p++) {
+// candidates [a, e) of the binned array; tau = current K-th key (or ~0)
+__device__ __forceinline__ void scan_range(const KnnGrid &G, int64_t a, int64_t e, float qx, float qy, float qz,
+                                           unsigned long long *col, int S, int K, int &cnt,
+                                           unsigned long long &tau) {
+    int64_t p = a;
+    for (; p + 1 < e; p += 2) {                    // two independent loads in flight
+        const float4 v0 = G.sp[p], v1 = G.sp[p + 1];
+        const float d0 = dist2_ref(v0.x, v0.y, v0.z, qx, qy, qz, G.box, G.periodic);
+        const float d1 = dist2_ref(v1.x, v1.y, v1.z, qx, qy, qz, G.box, G.periodic);
+        const unsigned long long k0 = knn_key(d0, (uint32_t)__float_as_int(v0.w));
+        const unsigned long long k1 = knn_key(d1, (uint32_t)__float_as_int(v1.w));
+        if (k0 < tau) {
+            topk_insert<0>(col, S, K, cnt, k0);
+            if (cnt == K) tau = col[(size_t)(K - 1) * S];
+        }
+        if (k1 < tau) {
+            topk_insert<0>(col, S, K, cnt, k1);
+            if (cnt == K) tau = col[(size_t)(K - 1) * S];
+        }
+    }
+    if (p < e) {
         const float4 v = G.sp[p];
         const float d2 = dist2_ref(v.x, v.y, v.z, qx, qy, qz, G.box, G.periodic);
         const unsigned long long key = knn_key(d2, (uint32_t)__float_as_int(v.w));
-        if (cnt < K || key < col[(size_t)(K - 1) * S]) topk_insert<0>(col, S, K, cnt, key);
+        if (key < tau) {
+            topk_insert<0>(col, S, K, cnt, key);
+            if (cnt == K) tau = col[(size_t)(K - 1) * S];
+        }
+    }
+}
+
+__device__ __forceinline__ void scan_bin(const KnnGrid &G, int bin, float qx, float qy, float qz,
+                                         unsigned long long *col, int S, int K, int &cnt) {
+    unsigned long long tau = cnt == K ? col[(size_t)(K - 1) * S] : ~0ULL;
+    scan_range(G, G.start[bin], G.start[bin + 1], qx, qy, qz, col, S, K, cnt, tau);
+}
+
+// bins bx0..bx1 (unwrapped, at most nb of them) of one (by, bz) row
+__device__ __forceinline__ void scan_row(const KnnGrid &G, int row, int bx0, int bx1, float qx, float qy, float qz,
+                                         unsigned long long *col, int S, int K, int &cnt, unsigned long long &tau) {
+    if (!G.periodic) {
+        scan_range(G, G.start[row + bx0], G.start[row + bx1 + 1], qx, qy, qz, col, S, K, cnt, tau);
+        return;
+    }
+    const int w0 = wrap_bin(bx0, G.nb), n = bx1 - bx0 + 1;
+    if (w0 + n <= G.nb) {
+        scan_range(G, G.start[row + w0], G.start[row + w0 + n], qx, qy, qz, col, S, K, cnt, tau);
+    } else {                                       // the run wraps around x
+        scan_range(G, G.start[row + w0], G.start[row + G.nb], qx, qy, qz, col, S, K, cnt, tau);
+        scan_range(G, G.start[row], G.start[row + (w0 + n - G.nb)], qx, qy, qz, col, S, K, cnt, tau);
     }
 }
 
@@ -149,6 +193,7 @@ __device__ int knn_query(const KnnGrid &G, float qx, float qy, float qz, int K,
                       bin_coord(qz, G.origin, G.inv_bw, G.nb)};
     const float q[3] = {qx, qy, qz};
     int cnt = 0;
+    unsigned long long tau = ~0ULL;
     for (int s = 0;; s++) {
         int lz, hz, ly, hy, lx, hx;
         axis_window(G, b[2], s, lz, hz);
@@ -161,19 +206,10 @@ __device__ int knn_query(const KnnGrid &G, float qx, float qy, float qz, int K,
                 const bool face = (dz == s || dz == -s || dy == s || dy == -s);
                 const int row = G.nb * (by + G.nb * bz);
                 if (face) {
-                    for (int dx = lx; dx <= hx; dx++) {
-                        const int bx = G.periodic ? wrap_bin(b[0] + dx, G.nb) : b[0] + dx;
-                        scan_bin(G, row + bx, qx, qy, qz, col, S, K, cnt);
-                    }
+                    scan_row(G, row, b[0] + lx, b[0] + hx, qx, qy, qz, col, S, K, cnt, tau);
                 } else {
-                    if (lx == -s) {
-                        const int bx = G.periodic ? wrap_bin(b[0] - s, G.nb) : b[0] - s;
-                        scan_bin(G, row + bx, qx, qy, qz, col, S, K, cnt);
-                    }
-                    if (hx == s && s > 0) {
-                        const int bx = G.periodic ? wrap_bin(b[0] + s, G.nb) : b[0] + s;
-                        scan_bin(G, row + bx, qx, qy, qz, col, S, K, cnt);
-                    }
+                    if (lx == -s) scan_row(G, row, b[0] - s, b[0] - s, qx, qy, qz, col, S, K, cnt, tau);
+                    if (hx == s && s > 0) scan_row(G, row, b[0] + s, b[0] + s, qx, qy, qz, col, S, K, cnt, tau);
                 }
             }
         }
@@ -186,6 +222,88 @@ __device__ int knn_query(const KnnGrid &G, float qx, float qy, float qz, int K,
         }
     }
     return cnt;
+}
+
+
+// min distance from q to the bin with unwrapped coordinates (bx, by, bz)
+__device__ __forceinline__ float bin_mindist2(const KnnGrid &G, const float q[3], int bx, int by, int bz) {
+    const int b[3] = {bx, by, bz};
+    float d2 = 0.0f;
+    for (int a = 0; a < 3; a++) {
+        const float lo = G.origin + (float)b[a] * G.bw, hi = lo + G.bw;
+        const float g = fmaxf(fmaxf(lo - q[a], q[a] - hi), 0.0f);
+        d2 += g * g;
+    }
+    return d2;
+}
+
+// Exact K nearest of q, starting from the radius estimate r0: scan every bin
+// that meets the ball of radius r (bins met by the previous ball skipped),
+// stop once the K-th distance is <= r (every particle not scanned is farther
+// than r), else grow r by 1.5.  Same results as knn_query.
+template <int KCAP>
+__device__ int knn_query_radius(const KnnGrid &G, float qx, float qy, float qz, int K,
+                                unsigned long long *col, int S, float r0) {
+    const float q[3] = {qx, qy, qz};
+    const int bq[3] = {bin_coord(qx, G.origin, G.inv_bw, G.nb), bin_coord(qy, G.origin, G.inv_bw, G.nb),
+                       bin_coord(qz, G.origin, G.inv_bw, G.nb)};
+    int cnt = 0;
+    float r = fmaxf(r0, 0.5f * G.bw);
+    float rprev2 = -1.0f;                    // bins with mindist2 <= rprev2 were scanned
+    for (int it = 0;; it++) {
+        const float rm = r + G.margin;
+        const float rm2 = rm * rm;
+        int lo[3], hi[3];
+        bool wraps = false, full_all = true;
+        for (int a = 0; a < 3; a++) {
+            // one extra bin each side: the min-distance test decides, so the box
+            // only has to contain every bin that test can accept
+            lo[a] = (int)floorf((q[a] - rm - G.origin) * G.inv_bw) - 1;
+            hi[a] = (int)floorf((q[a] + rm - G.origin) * G.inv_bw) + 1;
+            if (G.periodic) {
+                if (hi[a] - lo[a] + 2 >= G.nb) wraps = true;
+            } else {
+                lo[a] = max(lo[a], 0);
+                hi[a] = min(hi[a], G.nb - 1);
+                if (lo[a] > 0 || hi[a] < G.nb - 1) full_all = false;
+            }
+        }
+        if (wraps) {
+            // the ball reaches around a periodic box: scan every bin once, exactly
+            cnt = 0;
+            const int64_t nbins = (int64_t)G.nb * G.nb * G.nb;
+            for (int64_t bb = 0; bb < nbins; bb++) scan_bin(G, (int)bb, qx, qy, qz, col, S, K, cnt);
+            break;
+        }
+        for (int bz = lo[2]; bz <= hi[2]; bz++)
+            for (int by = lo[1]; by <= hi[1]; by++)
+                for (int bx = lo[0]; bx <= hi[0]; bx++) {
+                    const float md = bin_mindist2(G, q, bx, by, bz);
+                    if (md > rm2 || md <= rprev2) continue;
+                    const int wx = G.periodic ? wrap_bin(bx, G.nb) : bx;
+                    const int wy = G.periodic ? wrap_bin(by, G.nb) : by;
+                    const int wz = G.periodic ? wrap_bin(bz, G.nb) : bz;
+                    scan_bin(G, wx + G.nb * (wy + G.nb * wz), qx, qy, qz, col, S, K, cnt);
+                }
+        if (!G.periodic && full_all) break;           // every bin scanned
+        if (cnt == K && key_d2(col[(size_t)(K - 1) * S]) <= __fmul_rn(r, r)) break;
+        rprev2 = rm2;
+        r *= 1.5f;
+    }
+    return cnt;
+}
+
+// exact kNN: shells of bins, or the radius-guided search when a starting
+// radius is available for q's bin
+template <int KCAP>
+__device__ __forceinline__ int knn_any(const KnnGrid &G, float qx, float qy, float qz, int K,
+                                       unsigned long long *col, int S) {
+    if (G.r0) {
+        const int b = bin_coord(qx, G.origin, G.inv_bw, G.nb) +
+                      G.nb * (bin_coord(qy, G.origin, G.inv_bw, G.nb) + G.nb * bin_coord(qz, G.origin, G.inv_bw, G.nb));
+        return knn_query_radius<KCAP>(G, qx, qy, qz, K, col, S, G.r0[b]);
+    }
+    return knn_query<KCAP>(G, qx, qy, qz, K, col, S);
 }
 
 }  // namespace avism

@@ -12,7 +12,6 @@
 
 #include "common.cuh"
 #include "knn_core.cuh"
-#include "knn_tiled.cuh"
 
 namespace avism {
 
@@ -50,6 +49,40 @@ template <> struct TileDims<128> { static constexpr int x = 8, y = 4, z = 4; };
 template <> struct TileDims<64> { static constexpr int x = 4, y = 4, z = 4; };
 template <> struct TileDims<32> { static constexpr int x = 4, y = 4, z = 2; };
 
+// ---- PPART_DENS: rho_p = sum_k m / ((4/3) pi h_k^3) ------------------------------
+template <int KCAP>
+__global__ void __launch_bounds__(KNN_THREADS(KCAP))
+k_ppart_dens(KnnGrid G, int64_t n, int K, const float *__restrict__ m, float *__restrict__ part_dens) {
+    extern __shared__ unsigned long long knn_smem[];
+    const int S = blockDim.x;
+    unsigned long long *col = knn_smem + threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = G.sp[i];
+    const int cnt = knn_any<KCAP>(G, p.x, p.y, p.z, K, col, S);
+    double bas8 = 0.0;
+    for (int j = 0; j < cnt; j++) bas8 = bas8 + (double)m[key_idx(col[(size_t)j * S])];
+    const float hk = sqrtf(key_d2(col[(size_t)(K - 1) * S]));
+    const double pi = 3.141592653589793;     // DACOS(-1.D0)
+    part_dens[__float_as_int(p.w)] = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(hk, hk), hk)));
+}
+
+// ---- FILL_H_ZEROS: h = k-th neighbour distance where h is still 0 -----------
+template <int KCAP>
+__global__ void __launch_bounds__(KNN_THREADS(KCAP))
+k_fill_h(KnnGrid G, int64_t n, int K, float *__restrict__ hpart) {
+    extern __shared__ unsigned long long knn_smem[];
+    const int S = blockDim.x;
+    unsigned long long *col = knn_smem + threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = G.sp[i];
+    const int o = __float_as_int(p.w);
+    if (hpart[o] > 0.0f) return;
+    knn_any<KCAP>(G, p.x, p.y, p.z, K, col, S);
+    hpart[o] = sqrtf(key_d2(col[(size_t)(K - 1) * S]));
+}
+
 struct CellArgs {
     int nx, rad_lo, K;
     float dx;
@@ -62,120 +95,47 @@ struct CellArgs {
     int32_t *ball_count;
 };
 
-// ---- tiled variants: VVEL / H_DISTANCE on 4x4x4 cell tiles ---------------------
+// ---- VVEL_INTERP_SPH_VW / H_DISTANCE for cells whose k-th distance > DX ------
 template <int KCAP>
-__global__ void __launch_bounds__(TK_THREADS)
-k_cells_tiled(KnnGrid G, CellArgs A) {
-    extern __shared__ __align__(16) unsigned char tk_raw[];
-    TkSmem<KCAP> &S = *reinterpret_cast<TkSmem<KCAP> *>(tk_raw);
-    const int tid = threadIdx.x;
-    const int nx = A.nx;
-    const int nt = (nx + 3) / 4;
-    const int64_t b = blockIdx.x;
-    const int tx = (int)(b % nt), ty = (int)((b / nt) % nt), tz = (int)(b / ((int64_t)nt * nt));
-    const int x0 = tx * 4 + 1, y0 = ty * 4 + 1, z0 = tz * 4 + 1;
-    const int x1 = min(x0 + 3, nx), y1 = min(y0 + 3, nx), z1 = min(z0 + 3, nx);
-    const int ix = x0 + (tid & 3), jy = y0 + ((tid >> 2) & 3), kz = z0 + (tid >> 4);
-    bool active = ix <= nx && jy <= nx && kz <= nx;
-    int64_t c = 0;
-    if (active) {
-        c = (int64_t)(ix - 1) + (int64_t)nx * ((int64_t)(jy - 1) + (int64_t)nx * (kz - 1));
-        if (A.smask && A.smask[c] == 0) active = false;
-    }
-    const float *rad = A.rad - A.rad_lo;
-    const float qx = active ? rad[ix] : 0.0f, qy = active ? rad[jy] : 0.0f, qz = active ? rad[kz] : 0.0f;
-    BinBlock blk;
-    blk.lo[0] = bin_coord(rad[x0], G.origin, G.inv_bw, G.nb); blk.hi[0] = bin_coord(rad[x1], G.origin, G.inv_bw, G.nb);
-    blk.lo[1] = bin_coord(rad[y0], G.origin, G.inv_bw, G.nb); blk.hi[1] = bin_coord(rad[y1], G.origin, G.inv_bw, G.nb);
-    blk.lo[2] = bin_coord(rad[z0], G.origin, G.inv_bw, G.nb); blk.hi[2] = bin_coord(rad[z1], G.origin, G.inv_bw, G.nb);
+__global__ void __launch_bounds__(KNN_THREADS(KCAP))
+k_cells_knn(KnnGrid G, CellArgs A) {
+    extern __shared__ unsigned long long knn_smem[];
+    constexpr int T = KNN_THREADS(KCAP);
+    const int S = blockDim.x;
+    unsigned long long *col = knn_smem + threadIdx.x;
+    int ix, jy, kz;
+    if (!tile_cell(A.nx, TileDims<T>::x, TileDims<T>::y, TileDims<T>::z, ix, jy, kz)) return;
+    const int64_t c = (int64_t)(ix - 1) + (int64_t)A.nx * ((int64_t)(jy - 1) + (int64_t)A.nx * (kz - 1));
+    if (A.smask && A.smask[c] == 0) return;
+    const float qx = A.rad[ix - A.rad_lo], qy = A.rad[jy - A.rad_lo], qz = A.rad[kz - A.rad_lo];
     const int K = A.K;
-    const int cnt = tk_query_tile<KCAP>(G, S, blk, active, qx, qy, qz, K);
-    if (!active) return;
-    const float hk = sqrtf(key_d2(S.list[cnt - 1][tid]));
+    const int cnt = knn_any<KCAP>(G, qx, qy, qz, K, col, S);
+    const float hk = sqrtf(key_d2(col[(size_t)(cnt - 1) * S]));
     if (!(hk > A.dx)) {                       // ball_search(TREE, TAR, DX) branch
         const int slot = atomicAdd(A.ball_count, 1);
         A.ball_list[slot] = (int32_t)c;
         return;
     }
     for (int i = 0; i < cnt; i++) {
-        const unsigned long long key = S.list[i][tid];
+        const unsigned long long key = col[(size_t)i * S];
         atomic_max_pos(&A.hpart[key_idx(key)], sqrtf(key_d2(key)));
     }
     if (!A.do_vel) return;
-    double bs = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
+    double b = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
     for (int i = 0; i < cnt; i++) {
-        const unsigned long long key = S.list[i][tid];
+        const unsigned long long key = col[(size_t)i * S];
         const uint32_t j = key_idx(key);
         float w = kernel_m4(hk, sqrtf(key_d2(key)));
         w = __fmul_rn(w, __fdiv_rn(A.m[j], A.part_dens[j]));
         const double w8 = (double)w;
-        bs = bs + w8;
+        b = b + w8;
         bx = bx + w8 * (double)A.vx[j];
         by = by + w8 * (double)A.vy[j];
         bz = bz + w8 * (double)A.vz[j];
     }
-    A.u2[c] = (float)(bx / bs);
-    A.u3[c] = (float)(by / bs);
-    A.u4[c] = (float)(bz / bs);
-}
-
-// ---- tiled variants: PPART_DENS (mode 0) / FILL_H_ZEROS (mode 1) on bin tiles --
-template <int KCAP>
-__global__ void __launch_bounds__(TK_THREADS)
-k_parts_tiled(KnnGrid G, int K, int mode, int tb, const float *__restrict__ m, float *__restrict__ part_dens,
-              float *__restrict__ hpart) {
-    extern __shared__ __align__(16) unsigned char tk_raw[];
-    TkSmem<KCAP> &S = *reinterpret_cast<TkSmem<KCAP> *>(tk_raw);
-    const int tid = threadIdx.x;
-    const int nt = (G.nb + tb - 1) / tb;
-    const int64_t b = blockIdx.x;
-    BinBlock blk;
-    blk.lo[0] = (int)(b % nt) * tb;
-    blk.lo[1] = (int)((b / nt) % nt) * tb;
-    blk.lo[2] = (int)(b / ((int64_t)nt * nt)) * tb;
-    for (int a = 0; a < 3; a++) blk.hi[a] = min(blk.lo[a] + tb - 1, G.nb - 1);
-    // the tile's particles: one contiguous range per (y, z) row of bins
-    const int ry = blk.hi[1] - blk.lo[1] + 1, rz = blk.hi[2] - blk.lo[2] + 1;
-    const int nrow = ry * rz;
-    if (tid == 0) {
-        S.qrow[0] = 0;
-        for (int r = 0; r < nrow; r++) {
-            const int by = blk.lo[1] + r % ry, bz = blk.lo[2] + r / ry;
-            const int row = G.nb * (by + G.nb * bz);
-            const int64_t a0 = G.start[row + blk.lo[0]], a1 = G.start[row + blk.hi[0] + 1];
-            S.qbeg[r] = a0;
-            S.qrow[r + 1] = S.qrow[r] + (int)(a1 - a0);
-        }
-    }
-    __syncthreads();
-    const int total = S.qrow[nrow];
-    for (int r0 = 0; r0 < total; r0 += TK_THREADS) {
-        const int qi = r0 + tid;
-        bool active = qi < total;
-        float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
-        int o = -1;
-        if (active) {
-            int r = 0;
-            while (S.qrow[r + 1] <= qi) r++;
-            p = G.sp[S.qbeg[r] + (qi - S.qrow[r])];
-            o = __float_as_int(p.w);
-            if (mode == 1 && hpart[o] > 0.0f) active = false;
-        }
-        if (!__syncthreads_or(active ? 1 : 0)) continue;
-        const int cnt = tk_query_tile<KCAP>(G, S, blk, active, p.x, p.y, p.z, K);
-        if (active) {
-            const float hk = sqrtf(key_d2(S.list[K - 1][tid]));
-            if (mode == 0) {
-                double bas8 = 0.0;
-                for (int j = 0; j < cnt; j++) bas8 = bas8 + (double)m[key_idx(S.list[j][tid])];
-                const double pi = 3.141592653589793;     // DACOS(-1.D0)
-                part_dens[o] = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(hk, hk), hk)));
-            } else {
-                hpart[o] = hk;
-            }
-        }
-        __syncthreads();
-    }
+    A.u2[c] = (float)(bx / b);
+    A.u3[c] = (float)(by / b);
+    A.u4[c] = (float)(bz / b);
 }
 
 // ---- cells in the ball branch: all particles within DX (src/particles.f90:868-878)
@@ -422,6 +382,30 @@ __global__ void k_tsc_gather(int64_t nc, const int64_t *__restrict__ start, cons
     }
 }
 
+// ---- starting radius of the radius-guided search: the K-th neighbour distance of
+//      a uniform density equal to the particle count of the 3x3x3 bins around ----
+__global__ void k_radius_estimate(KnnGrid G, int K, float fac, float *r0) {
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nb = G.nb;
+    if (b >= (int64_t)nb * nb * nb) return;
+    const int bx = (int)(b % nb), by = (int)((b / nb) % nb), bz = (int)(b / ((int64_t)nb * nb));
+    int64_t n = 0;
+    int vol = 0;
+    for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+                int x = bx + dx, y = by + dy, z = bz + dz;
+                if (G.periodic) { x = wrap_bin(x, nb); y = wrap_bin(y, nb); z = wrap_bin(z, nb); }
+                else if (x < 0 || y < 0 || z < 0 || x >= nb || y >= nb || z >= nb) continue;
+                const int bin = x + nb * (y + nb * z);
+                n += G.start[bin + 1] - G.start[bin];
+                vol++;
+            }
+    // K = n/vol per bin volume * (4/3) pi (r/bw)^3
+    const float dens = fmaxf((float)n / (float)vol, 0.05f);
+    r0[b] = fac * G.bw * cbrtf((float)K / (4.18879020f * dens));
+}
+
 // ---- out-of-box check (src/avism.f90:560-589) ---------------------------------
 __global__ void k_box_check(int64_t n, const float *x, const float *y, const float *z, float half, int *bad) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -437,18 +421,16 @@ __global__ void k_zero_f32(int64_t n, float *a) {
 template <int KCAP>
 static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, const Level &L,
                             const P2G &a, const float *rad_d, bool vel_sph, bool need_h_cells) {
-    const size_t sm = sizeof(TkSmem<KCAP>);
+    const int T = KNN_THREADS(KCAP);
+    const size_t sm = (size_t)KCAP * T * sizeof(unsigned long long);
     const int K = p->kneighbours;
     const int nx = L.g.nx;
     const int64_t nc = (int64_t)nx * nx * nx;
-    AV_CUDA(cudaFuncSetAttribute(k_parts_tiled<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    AV_CUDA(cudaFuncSetAttribute(k_cells_tiled<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    const int tb = 4;                                  // particle tiles: 4^3 bins
-    const int ntb = (G.nb + tb - 1) / tb;
-    const int64_t ptiles = (int64_t)ntb * ntb * ntb;
+    AV_CUDA(cudaFuncSetAttribute(k_ppart_dens<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    AV_CUDA(cudaFuncSetAttribute(k_cells_knn<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    AV_CUDA(cudaFuncSetAttribute(k_fill_h<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     if (vel_sph) {
-        ++c.launches, k_parts_tiled<KCAP><<<(unsigned)ptiles, TK_THREADS, sm, c.stream>>>(G, K, 0, tb, a.m, a.part_dens, a.hpart);
-        AV_CUDA(cudaGetLastError());
+        ++c.launches, k_ppart_dens<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, a.m, a.part_dens);
         c.mark("ppart_dens");
     }
     if (vel_sph || need_h_cells) {
@@ -460,8 +442,9 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
         A.m = a.m; A.vx = a.vx; A.vy = a.vy; A.vz = a.vz; A.part_dens = a.part_dens;
         A.hpart = a.hpart; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
         A.ball_list = ball_list; A.ball_count = cnt_d;
-        const int nt = (nx + 3) / 4;
-        ++c.launches, k_cells_tiled<KCAP><<<(unsigned)((int64_t)nt * nt * nt), TK_THREADS, sm, c.stream>>>(G, A);
+        const int tx = TileDims<T>::x, ty = TileDims<T>::y, tz = TileDims<T>::z;
+        const int64_t nblk = (int64_t)((nx + tx - 1) / tx) * ((nx + ty - 1) / ty) * ((nx + tz - 1) / tz);
+        ++c.launches, k_cells_knn<KCAP><<<(unsigned)nblk, T, sm, c.stream>>>(G, A);
         AV_CUDA(cudaGetLastError());
         c.mark("cells_knn");
         int32_t nball = 0;
@@ -470,10 +453,10 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
         if (nball > 0) ++c.launches, k_cells_ball<<<grid_for(nball, 128), 128, 0, c.stream>>>(G, A, nball);
         AV_CUDA(cudaGetLastError());
         c.mark("cells_ball");
-        ++c.launches, k_parts_tiled<KCAP><<<(unsigned)ptiles, TK_THREADS, sm, c.stream>>>(G, K, 1, tb, a.m, a.part_dens, a.hpart);
-        AV_CUDA(cudaGetLastError());
+        ++c.launches, k_fill_h<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, a.hpart);
         c.mark("fill_h_zeros");
     }
+    AV_CUDA(cudaGetLastError());
 }
 
 void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G &a) {
@@ -507,9 +490,22 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
     TA.rn = L.rad_at(nx) + 0.5f * L.g.dx;
     TA.leng = TA.rn - TA.r1;
     if (vel_sph || dens_sph) {
-        BinnedParticles bp = bin_particles(c, a.n, a.x, a.y, a.z, p->lado0, p->periodic, 1.0f);
+        const char *occ_env = getenv("AVISM_TUNE_OCC");
+        const float occ = occ_env ? (float)atof(occ_env) : 2.0f;
+        BinnedParticles bp = bin_particles(c, a.n, a.x, a.y, a.z, p->lado0, p->periodic, occ);
         KnnGrid G = make_knn_grid(bp);
         c.mark("bin_particles");
+        if (p->learned) {
+            // radius-guided search: a starting radius per bin
+            const int64_t nbins = (int64_t)bp.nb * bp.nb * bp.nb;
+            float *r0 = c.get_t<float>(B_KNN_R0, nbins);
+            const char *fac_env = getenv("AVISM_TUNE_RFAC");
+            const float fac = fac_env ? (float)atof(fac_env) : 1.1f;
+            ++c.launches, k_radius_estimate<<<grid_for(nbins, 256), 256, 0, c.stream>>>(G, K, fac, r0);
+            AV_CUDA(cudaGetLastError());
+            G.r0 = r0;
+            c.mark("radius_estimate");
+        }
         const bool need_h_cells = dens_sph && !vel_sph;
         if (K <= 32) run_sph_kernels<32>(c, G, p, L, a, rad_d, vel_sph, need_h_cells);
         else if (K <= 64) run_sph_kernels<64>(c, G, p, L, a, rad_d, vel_sph, need_h_cells);
