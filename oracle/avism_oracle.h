@@ -8,7 +8,7 @@
  *
  * Parity status: the reference ships no golden vectors and cannot be compiled
  * here (no Fortran compiler), so this oracle is pinned by analytic known-answer
- * cases (tests/test_oracle_kat.py) rather than by reference outputs.
+ * cases (tests/test_oracle_pins.py) rather than by reference outputs.
  *
  * Floating point: compiled with -ffp-contract=off; every f32/f64 operation and
  * promotion point follows the Fortran expression it restates (cited per function).

@@ -163,6 +163,23 @@ def test_run_level_deterministic(gpu, mock1):
         assert np.array_equal(np.asarray(a["cat"][k]), np.asarray(b["cat"][k])), k
 
 
+def test_catalogue_independent_of_binning(gpu, mock1, monkeypatch):
+    """The kNN is exact for any bin size and with the radius-guided start, so
+    the tuning knobs change timing only."""
+    p = Params(nx=64, periodic=1, lado0=100.0)
+    base = gpu.run_level(p, mock1, capacity=100000)
+    variants = [("0.5", 0), ("4", 0), ("2", 1)]
+    for occ, learned in variants:
+        monkeypatch.setenv("AVISM_TUNE_OCC", occ)
+        q = Params(nx=64, periodic=1, lado0=100.0, learned=learned)
+        r = gpu.run_level(q, mock1, capacity=100000)
+        assert r["nvoid"] == base["nvoid"]
+        for k in base["cubes"]:
+            assert np.array_equal(r["cubes"][k], base["cubes"][k]), (occ, learned, k)
+        for k in base["cat"]:
+            assert np.array_equal(np.asarray(r["cat"][k]), np.asarray(base["cat"][k])), (occ, learned, k)
+
+
 def test_out_of_box_is_an_error(gpu, mock_small):
     from avism_b200.avism import AvismError
     parts = {k: np.array(v, copy=True) for k, v in mock_small.items() if isinstance(v, np.ndarray)}
