@@ -8,3 +8,4 @@
 #include "voidfind.cu"
 #include "post.cu"
 #include "capi.cu"
+#include "noalloc.cu"

@@ -191,6 +191,39 @@ int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n,
                         const float *m, avism_cubes *cubes, int32_t *nvoid,
                         avism_voids *voids, float *meandens);
 
+/* ---- kNN without allocation.  No reference counterpart: an extra form of
+ *      avism_gpu_knn (same neighbours, same distances, bit for bit) for callers
+ *      that cannot allocate device memory -- a host whose device memory is
+ *      wholly reserved by another allocator (a framework's caching allocator
+ *      that has claimed the card), or one that cannot take the device-wide
+ *      synchronisation cudaMalloc/cudaFree imply while its other streams run.
+ *      It needs no context and allocates nothing: its scratch is one static
+ *      device array of this library (under 40 MiB per device, present from
+ *      module load), so n <= AVISM_KNN_NOALLOC_MAX_N; a larger n is rejected
+ *      with AVISM_ERR_ARG and its message.
+ *        - x..dist must be device pointers on `device` (AVISM_ERR_ARG otherwise).
+ *        - stream is a cudaStream_t (NULL: the legacy default stream).  The work
+ *          is queued on it and the call returns without waiting, except that
+ *          box_l <= 0 waits once on the stream for the points' bounding cube.
+ *        - the scratch is shared by every call on a device in this process:
+ *          calls whose work overlaps in time (two streams, two host threads)
+ *          race on it and corrupt each other's results.  Serialise them, e.g.
+ *          on one stream.
+ *        - nothing in the scratch needs to start at zero: each call writes
+ *          every scratch word before reading it.
+ *        - the first call on a device sets the device context up and looks the
+ *          scratch address up (cudaGetSymbolAddress), which may load the module
+ *          and allocate inside the CUDA runtime; make that first call before any
+ *          stream capture.
+ *      errbuf (nullable, errlen bytes) receives the failure message, "" on
+ *      success.                                                                 */
+#define AVISM_KNN_NOALLOC_MAX_N 1048576
+int avism_gpu_knn_noalloc(int device, void *stream, int64_t n, const float *x,
+                          const float *y, const float *z, float box_l, int64_t nq,
+                          const float *qx, const float *qy, const float *qz,
+                          int32_t k, int64_t *idx, float *dist, char *errbuf,
+                          int32_t errlen);
+
 #ifdef __cplusplus
 }
 #endif
