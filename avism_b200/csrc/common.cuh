@@ -49,6 +49,7 @@ enum BufId : int {
     B_MARCA, B_PAINT, B_LABMAP, B_LABEL_AUX, B_CCL,
     B_RED0, B_RED1, B_RED2,
     B_QUERY, B_RAD, B_BALL, B_SCAL, B_KNN_R0,
+    B_SV, B_PDENS_S, B_HPART_S,                    // per-particle attributes in binned order
     B_NUM
 };
 

@@ -104,7 +104,7 @@ k_knn_batch(KnnGrid G, int64_t nq, const float *__restrict__ qx, const float *__
     for (int i = 0; i < K; i++) {
         if (i < cnt) {
             const unsigned long long key = col[(size_t)i * S];
-            idx_out[q * K + i] = (int64_t)(uint32_t)(key & 0xffffffffu) + 1;
+            idx_out[q * K + i] = (int64_t)key_orig(G.sp, key) + 1;
             dist_out[q * K + i] = sqrtf(__uint_as_float((uint32_t)(key >> 32)));
         } else {
             idx_out[q * K + i] = -1;

@@ -2,8 +2,9 @@
 //
 // One thread per query.  The current best K keys live in a shared-memory
 // column (stride = blockDim.x, conflict-free), sorted ascending.  A key is
-// (float bits of the squared distance) << 32 | particle index, so ties in
-// distance are broken by the smaller particle index.
+// (float bits of the squared distance) << 32 | position in the binned array;
+// keys order by squared distance, and equal distances by the smaller original
+// particle index (held in sp[pos].w), so the order does not depend on binning.
 #pragma once
 
 #include <cfloat>
@@ -62,11 +63,27 @@ __device__ __forceinline__ float dist2_ref(float px, float py, float pz, float q
     return d;
 }
 
-__device__ __forceinline__ unsigned long long knn_key(float d2, uint32_t idx) {
-    return ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned long long)idx;
+__device__ __forceinline__ unsigned long long knn_key(float d2, uint32_t pos) {
+    return ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned long long)pos;
 }
 __device__ __forceinline__ float key_d2(unsigned long long k) { return __uint_as_float((uint32_t)(k >> 32)); }
-__device__ __forceinline__ uint32_t key_idx(unsigned long long k) { return (uint32_t)(k & 0xffffffffu); }
+// position of the particle in the binned array
+__device__ __forceinline__ uint32_t key_pos(unsigned long long k) { return (uint32_t)(k & 0xffffffffu); }
+// original (input-order, 0-based) index of the particle
+__device__ __forceinline__ uint32_t key_orig(const float4 *sp, unsigned long long k) {
+    return (uint32_t)__float_as_int(sp[key_pos(k)].w);
+}
+// equal squared distances: the smaller original index first (kept out of line,
+// ties are rare and the hot comparisons stay two instructions)
+__device__ __noinline__ bool key_tie_lt(const float4 *sp, unsigned long long a, unsigned long long b) {
+    if (a == b) return false;
+    return key_orig(sp, a) < key_orig(sp, b);
+}
+// a < b in (squared distance, original index) order; ~0 (no key) is above all
+__device__ __forceinline__ bool key_lt(const float4 *sp, unsigned long long a, unsigned long long b) {
+    if ((uint32_t)(a >> 32) != (uint32_t)(b >> 32)) return a < b;
+    return key_tie_lt(sp, a, b);
+}
 
 // allowed bin offsets along one axis for shell radius s
 __device__ __forceinline__ void axis_window(const KnnGrid &G, int b, int s, int &lo, int &hi) {
@@ -84,75 +101,80 @@ __device__ __forceinline__ int wrap_bin(int b, int nb) {
     return b < 0 ? b + nb : b;
 }
 
-template <int KCAP>
-__device__ __forceinline__ void topk_insert(unsigned long long *col, int S, int K, int &cnt,
-                                            unsigned long long key) {
-    int i;
-    if (cnt < K) {
-        i = cnt++;
-    } else {
-        if (key >= col[(size_t)(K - 1) * S]) return;
-        i = K - 1;
-    }
-    while (i > 0) {
-        const unsigned long long prev = col[(size_t)(i - 1) * S];
-        if (prev <= key) break;
-        col[(size_t)i * S] = prev;
-        i--;
-    }
-    col[(size_t)i * S] = key;
+// The current best K keys of one query: a sorted shared-memory column (stride
+// S), its count, and tau = the K-th key once the column is full (before that the
+// proposed-radius bound, or ~0).
+struct TopK {
+    unsigned long long *col;
+    int S, K, cnt;
+    unsigned long long tau;
+    bool tie;                 // a tie in squared distance may decide the result
+};
+
+// Key order of the fast pass is (squared distance, binned position): one 64-bit
+// compare.  It can differ from the exact order (squared distance, original
+// index) only when two keys with equal squared distance are compared, so the
+// fast pass flags every comparison against tau with an equal squared distance
+// and every eviction that leaves tau at the evicted distance; a flagged query
+// is searched again with the exact order.
+template <bool EXACT>
+__device__ __forceinline__ bool key_before(const float4 *sp, unsigned long long a, unsigned long long b) {
+    if constexpr (EXACT) return key_lt(sp, a, b);
+    else return a < b;
 }
 
-// candidates [a, e) of the binned array; tau = current K-th key (or ~0)
+template <bool EXACT>
+__device__ __forceinline__ void topk_offer(const float4 *sp, TopK &T, unsigned long long key) {
+    if constexpr (!EXACT) T.tie |= (uint32_t)(key >> 32) == (uint32_t)(T.tau >> 32);
+    if (!key_before<EXACT>(sp, key, T.tau)) return;
+    int i = T.cnt < T.K ? T.cnt++ : T.K - 1;
+    while (i > 0) {
+        const unsigned long long prev = T.col[(size_t)(i - 1) * T.S];
+        if (!key_before<EXACT>(sp, key, prev)) break;
+        T.col[(size_t)i * T.S] = prev;
+        i--;
+    }
+    T.col[(size_t)i * T.S] = key;
+    if (T.cnt == T.K) {
+        const unsigned long long nt = T.col[(size_t)(T.K - 1) * T.S];
+        if constexpr (!EXACT) T.tie |= (uint32_t)(nt >> 32) == (uint32_t)(T.tau >> 32);
+        T.tau = nt;
+    }
+}
+
+// candidates [a, e) of the binned array
+template <bool EXACT>
 __device__ __forceinline__ void scan_range(const KnnGrid &G, int64_t a, int64_t e, float qx, float qy, float qz,
-                                           unsigned long long *col, int S, int K, int &cnt,
-                                           unsigned long long &tau) {
+                                           TopK &T) {
     int64_t p = a;
     for (; p + 1 < e; p += 2) {                    // two independent loads in flight
         const float4 v0 = G.sp[p], v1 = G.sp[p + 1];
         const float d0 = dist2_ref(v0.x, v0.y, v0.z, qx, qy, qz, G.box, G.periodic);
         const float d1 = dist2_ref(v1.x, v1.y, v1.z, qx, qy, qz, G.box, G.periodic);
-        const unsigned long long k0 = knn_key(d0, (uint32_t)__float_as_int(v0.w));
-        const unsigned long long k1 = knn_key(d1, (uint32_t)__float_as_int(v1.w));
-        if (k0 < tau) {
-            topk_insert<0>(col, S, K, cnt, k0);
-            if (cnt == K) tau = col[(size_t)(K - 1) * S];
-        }
-        if (k1 < tau) {
-            topk_insert<0>(col, S, K, cnt, k1);
-            if (cnt == K) tau = col[(size_t)(K - 1) * S];
-        }
+        topk_offer<EXACT>(G.sp, T, knn_key(d0, (uint32_t)p));
+        topk_offer<EXACT>(G.sp, T, knn_key(d1, (uint32_t)(p + 1)));
     }
     if (p < e) {
         const float4 v = G.sp[p];
         const float d2 = dist2_ref(v.x, v.y, v.z, qx, qy, qz, G.box, G.periodic);
-        const unsigned long long key = knn_key(d2, (uint32_t)__float_as_int(v.w));
-        if (key < tau) {
-            topk_insert<0>(col, S, K, cnt, key);
-            if (cnt == K) tau = col[(size_t)(K - 1) * S];
-        }
+        topk_offer<EXACT>(G.sp, T, knn_key(d2, (uint32_t)p));
     }
 }
 
-__device__ __forceinline__ void scan_bin(const KnnGrid &G, int bin, float qx, float qy, float qz,
-                                         unsigned long long *col, int S, int K, int &cnt) {
-    unsigned long long tau = cnt == K ? col[(size_t)(K - 1) * S] : ~0ULL;
-    scan_range(G, G.start[bin], G.start[bin + 1], qx, qy, qz, col, S, K, cnt, tau);
-}
-
 // bins bx0..bx1 (unwrapped, at most nb of them) of one (by, bz) row
+template <bool EXACT>
 __device__ __forceinline__ void scan_row(const KnnGrid &G, int row, int bx0, int bx1, float qx, float qy, float qz,
-                                         unsigned long long *col, int S, int K, int &cnt, unsigned long long &tau) {
+                                         TopK &T) {
     if (!G.periodic) {
-        scan_range(G, G.start[row + bx0], G.start[row + bx1 + 1], qx, qy, qz, col, S, K, cnt, tau);
+        scan_range<EXACT>(G, G.start[row + bx0], G.start[row + bx1 + 1], qx, qy, qz, T);
         return;
     }
     const int w0 = wrap_bin(bx0, G.nb), n = bx1 - bx0 + 1;
     if (w0 + n <= G.nb) {
-        scan_range(G, G.start[row + w0], G.start[row + w0 + n], qx, qy, qz, col, S, K, cnt, tau);
+        scan_range<EXACT>(G, G.start[row + w0], G.start[row + w0 + n], qx, qy, qz, T);
     } else {                                       // the run wraps around x
-        scan_range(G, G.start[row + w0], G.start[row + G.nb], qx, qy, qz, col, S, K, cnt, tau);
-        scan_range(G, G.start[row], G.start[row + (w0 + n - G.nb)], qx, qy, qz, col, S, K, cnt, tau);
+        scan_range<EXACT>(G, G.start[row + w0], G.start[row + G.nb], qx, qy, qz, T);
+        scan_range<EXACT>(G, G.start[row], G.start[row + (w0 + n - G.nb)], qx, qy, qz, T);
     }
 }
 
@@ -185,125 +207,130 @@ __device__ __forceinline__ float guaranteed_radius(const KnnGrid &G, const int b
     return r - G.margin;
 }
 
-// Exact K nearest of q; returns the number found (K unless fewer particles).
-template <int KCAP>
-__device__ int knn_query(const KnnGrid &G, float qx, float qy, float qz, int K,
-                         unsigned long long *col, int S) {
+// Lower bound of |q - p| along one axis for any particle p binned into the bin
+// with unwrapped index bu: the gap to the bin's slab less the rounding margin.
+__device__ __forceinline__ float axis_gap(const KnnGrid &G, float q, int bu) {
+    const float lo = G.origin + (float)bu * G.bw, hi = lo + G.bw;
+    return fmaxf(fmaxf(fmaxf(lo - q, q - hi), 0.0f) - G.margin, 0.0f);
+}
+
+// K nearest of q in the order of key_before<EXACT>; returns the number found
+// (K unless fewer particles).  Shells of bins outward from q's bin.  While tau
+// is finite, a row of bins whose (y, z) gap exceeds it is skipped, and in a kept
+// row only the bins within the remaining x reach are scanned: tau only
+// decreases, so a skipped bin can never hold a closer particle later.
+// r0 > 0 is a proposed search radius: tau starts just above r0^2, so only
+// particles within r0 are ever inserted.  If the visited block covers the ball
+// of radius r0 and fewer than K particles were found, the search is repeated
+// without the bound; the result is the same either way.
+// The fast pass (EXACT false) sets *tie when equal squared distances may have
+// been ordered by binned position (see topk_offer).
+template <int KCAP, bool EXACT>
+__device__ int knn_search(const KnnGrid &G, float qx, float qy, float qz, int K,
+                          unsigned long long *col, int S, float r0, bool *tie) {
     const int b[3] = {bin_coord(qx, G.origin, G.inv_bw, G.nb), bin_coord(qy, G.origin, G.inv_bw, G.nb),
                       bin_coord(qz, G.origin, G.inv_bw, G.nb)};
     const float q[3] = {qx, qy, qz};
-    int cnt = 0;
-    unsigned long long tau = ~0ULL;
-    for (int s = 0;; s++) {
-        int lz, hz, ly, hy, lx, hx;
-        axis_window(G, b[2], s, lz, hz);
-        axis_window(G, b[1], s, ly, hy);
-        axis_window(G, b[0], s, lx, hx);
-        for (int dz = lz; dz <= hz; dz++) {
-            const int bz = G.periodic ? wrap_bin(b[2] + dz, G.nb) : b[2] + dz;
-            for (int dy = ly; dy <= hy; dy++) {
-                const int by = G.periodic ? wrap_bin(b[1] + dy, G.nb) : b[1] + dy;
-                const bool face = (dz == s || dz == -s || dy == s || dy == -s);
-                const int row = G.nb * (by + G.nb * bz);
-                if (face) {
-                    scan_row(G, row, b[0] + lx, b[0] + hx, qx, qy, qz, col, S, K, cnt, tau);
-                } else {
-                    if (lx == -s) scan_row(G, row, b[0] - s, b[0] - s, qx, qy, qz, col, S, K, cnt, tau);
-                    if (hx == s && s > 0) scan_row(G, row, b[0] + s, b[0] + s, qx, qy, qz, col, S, K, cnt, tau);
+    TopK T;
+    T.col = col;
+    T.S = S;
+    T.K = K;
+    T.tie = false;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        const bool bounded = attempt == 0 && r0 > 0.0f;
+        const float r02 = __fmul_rn(r0, r0);
+        // smallest key with a squared distance above r0^2 (position 0 is a valid index)
+        T.tau = bounded ? knn_key(__uint_as_float(__float_as_uint(r02) + 1u), 0u) : ~0ULL;
+        T.cnt = 0;
+        T.tie = false;
+        bool retry = false;
+        for (int s = 0;; s++) {
+            int lz, hz, ly, hy, lx, hx;
+            axis_window(G, b[2], s, lz, hz);
+            axis_window(G, b[1], s, ly, hy);
+            axis_window(G, b[0], s, lx, hx);
+            // pruning needs the unwrapped geometry to stand for the periodic images
+            const bool prune = !G.periodic || 2 * s + 3 < G.nb;
+            for (int dz = lz; dz <= hz; dz++) {
+                const int bz = G.periodic ? wrap_bin(b[2] + dz, G.nb) : b[2] + dz;
+                const float gz = axis_gap(G, qz, b[2] + dz);
+                const float gz2 = __fmul_rn(gz, gz);
+                if (prune && T.tau != ~0ULL && gz2 > key_d2(T.tau)) continue;
+                for (int dy = ly; dy <= hy; dy++) {
+                    const bool face = (dz == s || dz == -s || dy == s || dy == -s);
+                    int xl = lx, xh = hx;
+                    if (prune && T.tau != ~0ULL) {
+                        const float gy = axis_gap(G, qy, b[1] + dy);
+                        const float yz2 = __fadd_rn(gz2, __fmul_rn(gy, gy));
+                        const float t = key_d2(T.tau);
+                        if (yz2 > t) continue;
+                        const float rx = __fadd_rn(__fsqrt_rn(__fsub_rn(t, yz2)), G.margin);
+                        const int cl = (int)floorf(__fmul_rn(__fsub_rn(__fsub_rn(qx, rx), G.origin), G.inv_bw));
+                        const int ch = (int)floorf(__fmul_rn(__fsub_rn(__fadd_rn(qx, rx), G.origin), G.inv_bw));
+                        // near the periodic seam the images' bins are not monotone in x: keep the shell range
+                        if (!G.periodic || (cl >= 0 && ch <= G.nb - 1)) {
+                            xl = max(xl, cl - b[0]);
+                            xh = min(xh, ch - b[0]);
+                        }
+                    }
+                    const int by = G.periodic ? wrap_bin(b[1] + dy, G.nb) : b[1] + dy;
+                    const int row = G.nb * (by + G.nb * bz);
+                    if (face) {
+                        if (xl <= xh) scan_row<EXACT>(G, row, b[0] + xl, b[0] + xh, qx, qy, qz, T);
+                    } else {
+                        if (lx == -s && xl <= -s) scan_row<EXACT>(G, row, b[0] - s, b[0] - s, qx, qy, qz, T);
+                        if (hx == s && xh >= s) scan_row<EXACT>(G, row, b[0] + s, b[0] + s, qx, qy, qz, T);
+                    }
                 }
             }
+            bool all_done;
+            const float r = guaranteed_radius(G, b, q, s, &all_done);
+            if (all_done) {
+                retry = bounded && T.cnt < K;
+                break;
+            }
+            if (T.cnt == K && r > 0.0f) {
+                const float kth = key_d2(col[(size_t)(K - 1) * S]);
+                if (kth < __fmul_rn(r, r)) break;
+            }
+            if (bounded && T.cnt < K && r > 0.0f && key_d2(T.tau) < __fmul_rn(r, r)) {
+                retry = true;                  // fewer than K particles within r0
+                break;
+            }
         }
-        bool all_done;
-        const float r = guaranteed_radius(G, b, q, s, &all_done);
-        if (all_done) break;
-        if (cnt == K && r > 0.0f) {
-            const float kth = key_d2(col[(size_t)(K - 1) * S]);
-            if (kth < __fmul_rn(r, r)) break;
-        }
+        if (!retry) break;
     }
-    return cnt;
+    if constexpr (!EXACT) {
+        // equal squared distances inside the list are ordered by position
+        for (int i = 1; i < T.cnt; i++)
+            T.tie |= (uint32_t)(col[(size_t)i * S] >> 32) == (uint32_t)(col[(size_t)(i - 1) * S] >> 32);
+        *tie = T.tie;
+    }
+    return T.cnt;
 }
 
-
-// min distance from q to the bin with unwrapped coordinates (bx, by, bz)
-__device__ __forceinline__ float bin_mindist2(const KnnGrid &G, const float q[3], int bx, int by, int bz) {
-    const int b[3] = {bx, by, bz};
-    float d2 = 0.0f;
-    for (int a = 0; a < 3; a++) {
-        const float lo = G.origin + (float)b[a] * G.bw, hi = lo + G.bw;
-        const float g = fmaxf(fmaxf(lo - q[a], q[a] - hi), 0.0f);
-        d2 += g * g;
-    }
-    return d2;
-}
-
-// Exact K nearest of q, starting from the radius estimate r0: scan every bin
-// that meets the ball of radius r (bins met by the previous ball skipped),
-// stop once the K-th distance is <= r (every particle not scanned is farther
-// than r), else grow r by 1.5.  Same results as knn_query.
+// Exact K nearest of q in (squared distance, original index) order: the fast
+// pass, repeated with the exact order when a tie may have decided it.
 template <int KCAP>
-__device__ int knn_query_radius(const KnnGrid &G, float qx, float qy, float qz, int K,
-                                unsigned long long *col, int S, float r0) {
-    const float q[3] = {qx, qy, qz};
-    const int bq[3] = {bin_coord(qx, G.origin, G.inv_bw, G.nb), bin_coord(qy, G.origin, G.inv_bw, G.nb),
-                       bin_coord(qz, G.origin, G.inv_bw, G.nb)};
-    int cnt = 0;
-    float r = fmaxf(r0, 0.5f * G.bw);
-    float rprev2 = -1.0f;                    // bins with mindist2 <= rprev2 were scanned
-    for (int it = 0;; it++) {
-        const float rm = r + G.margin;
-        const float rm2 = rm * rm;
-        int lo[3], hi[3];
-        bool wraps = false, full_all = true;
-        for (int a = 0; a < 3; a++) {
-            // one extra bin each side: the min-distance test decides, so the box
-            // only has to contain every bin that test can accept
-            lo[a] = (int)floorf((q[a] - rm - G.origin) * G.inv_bw) - 1;
-            hi[a] = (int)floorf((q[a] + rm - G.origin) * G.inv_bw) + 1;
-            if (G.periodic) {
-                if (hi[a] - lo[a] + 2 >= G.nb) wraps = true;
-            } else {
-                lo[a] = max(lo[a], 0);
-                hi[a] = min(hi[a], G.nb - 1);
-                if (lo[a] > 0 || hi[a] < G.nb - 1) full_all = false;
-            }
-        }
-        if (wraps) {
-            // the ball reaches around a periodic box: scan every bin once, exactly
-            cnt = 0;
-            const int64_t nbins = (int64_t)G.nb * G.nb * G.nb;
-            for (int64_t bb = 0; bb < nbins; bb++) scan_bin(G, (int)bb, qx, qy, qz, col, S, K, cnt);
-            break;
-        }
-        for (int bz = lo[2]; bz <= hi[2]; bz++)
-            for (int by = lo[1]; by <= hi[1]; by++)
-                for (int bx = lo[0]; bx <= hi[0]; bx++) {
-                    const float md = bin_mindist2(G, q, bx, by, bz);
-                    if (md > rm2 || md <= rprev2) continue;
-                    const int wx = G.periodic ? wrap_bin(bx, G.nb) : bx;
-                    const int wy = G.periodic ? wrap_bin(by, G.nb) : by;
-                    const int wz = G.periodic ? wrap_bin(bz, G.nb) : bz;
-                    scan_bin(G, wx + G.nb * (wy + G.nb * wz), qx, qy, qz, col, S, K, cnt);
-                }
-        if (!G.periodic && full_all) break;           // every bin scanned
-        if (cnt == K && key_d2(col[(size_t)(K - 1) * S]) <= __fmul_rn(r, r)) break;
-        rprev2 = rm2;
-        r *= 1.5f;
-    }
-    return cnt;
+__device__ __forceinline__ int knn_query(const KnnGrid &G, float qx, float qy, float qz, int K,
+                                         unsigned long long *col, int S, float r0 = 0.0f) {
+    bool tie = false;
+    const int cnt = knn_search<KCAP, false>(G, qx, qy, qz, K, col, S, r0, &tie);
+    if (!tie) return cnt;
+    return knn_search<KCAP, true>(G, qx, qy, qz, K, col, S, r0, nullptr);
 }
 
-// exact kNN: shells of bins, or the radius-guided search when a starting
-// radius is available for q's bin
+// exact kNN; with a per-bin proposed radius when one is available
 template <int KCAP>
 __device__ __forceinline__ int knn_any(const KnnGrid &G, float qx, float qy, float qz, int K,
                                        unsigned long long *col, int S) {
+    float r0 = 0.0f;
     if (G.r0) {
         const int b = bin_coord(qx, G.origin, G.inv_bw, G.nb) +
                       G.nb * (bin_coord(qy, G.origin, G.inv_bw, G.nb) + G.nb * bin_coord(qz, G.origin, G.inv_bw, G.nb));
-        return knn_query_radius<KCAP>(G, qx, qy, qz, K, col, S, G.r0[b]);
+        r0 = G.r0[b];
     }
-    return knn_query<KCAP>(G, qx, qy, qz, K, col, S);
+    return knn_query<KCAP>(G, qx, qy, qz, K, col, S, r0);
 }
 
 }  // namespace avism

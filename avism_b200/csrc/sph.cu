@@ -52,7 +52,8 @@ template <> struct TileDims<32> { static constexpr int x = 4, y = 4, z = 2; };
 // ---- PPART_DENS: rho_p = sum_k m / ((4/3) pi h_k^3) ------------------------------
 template <int KCAP>
 __global__ void __launch_bounds__(KNN_THREADS(KCAP))
-k_ppart_dens(KnnGrid G, int64_t n, int K, const float *__restrict__ m, float *__restrict__ part_dens) {
+k_ppart_dens(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float *__restrict__ pd_s,
+             float *__restrict__ part_dens) {
     extern __shared__ unsigned long long knn_smem[];
     const int S = blockDim.x;
     unsigned long long *col = knn_smem + threadIdx.x;
@@ -61,26 +62,44 @@ k_ppart_dens(KnnGrid G, int64_t n, int K, const float *__restrict__ m, float *__
     const float4 p = G.sp[i];
     const int cnt = knn_any<KCAP>(G, p.x, p.y, p.z, K, col, S);
     double bas8 = 0.0;
-    for (int j = 0; j < cnt; j++) bas8 = bas8 + (double)m[key_idx(col[(size_t)j * S])];
+    for (int j = 0; j < cnt; j++) bas8 = bas8 + (double)sv[key_pos(col[(size_t)j * S])].w;
     const float hk = sqrtf(key_d2(col[(size_t)(K - 1) * S]));
     const double pi = 3.141592653589793;     // DACOS(-1.D0)
-    part_dens[__float_as_int(p.w)] = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(hk, hk), hk)));
+    const float rho = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(hk, hk), hk)));
+    pd_s[i] = rho;
+    part_dens[__float_as_int(p.w)] = rho;
 }
 
 // ---- FILL_H_ZEROS: h = k-th neighbour distance where h is still 0 -----------
 template <int KCAP>
 __global__ void __launch_bounds__(KNN_THREADS(KCAP))
-k_fill_h(KnnGrid G, int64_t n, int K, float *__restrict__ hpart) {
+k_fill_h(KnnGrid G, int64_t n, int K, float *__restrict__ hp_s) {
     extern __shared__ unsigned long long knn_smem[];
     const int S = blockDim.x;
     unsigned long long *col = knn_smem + threadIdx.x;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (hp_s[i] > 0.0f) return;
     const float4 p = G.sp[i];
-    const int o = __float_as_int(p.w);
-    if (hpart[o] > 0.0f) return;
     knn_any<KCAP>(G, p.x, p.y, p.z, K, col, S);
-    hpart[o] = sqrtf(key_d2(col[(size_t)(K - 1) * S]));
+    hp_s[i] = sqrtf(key_d2(col[(size_t)(K - 1) * S]));
+}
+
+// per-particle attributes in binned order: (vx, vy, vz, m)
+__global__ void k_sorted_attrs(int64_t n, const float4 *__restrict__ sp, const float *__restrict__ vx,
+                               const float *__restrict__ vy, const float *__restrict__ vz,
+                               const float *__restrict__ m, float4 *__restrict__ sv) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int o = __float_as_int(sp[i].w);
+    sv[i] = make_float4(vx[o], vy[o], vz[o], m[o]);
+}
+
+// binned order -> input order
+__global__ void k_unbin_f32(int64_t n, const float4 *__restrict__ sp, const float *__restrict__ src,
+                            float *__restrict__ dst) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[__float_as_int(sp[i].w)] = src[i];
 }
 
 struct CellArgs {
@@ -88,8 +107,9 @@ struct CellArgs {
     float dx;
     const float *rad;
     const int8_t *smask;
-    const float *m, *vx, *vy, *vz, *part_dens;
-    float *hpart, *u2, *u3, *u4;
+    const float4 *sv;                 // (vx, vy, vz, m) in binned order
+    const float *pd_s;                // particle density in binned order
+    float *hp_s, *u2, *u3, *u4;       // h in binned order
     int do_vel;
     int32_t *ball_list;
     int32_t *ball_count;
@@ -118,20 +138,21 @@ k_cells_knn(KnnGrid G, CellArgs A) {
     }
     for (int i = 0; i < cnt; i++) {
         const unsigned long long key = col[(size_t)i * S];
-        atomic_max_pos(&A.hpart[key_idx(key)], sqrtf(key_d2(key)));
+        atomic_max_pos(&A.hp_s[key_pos(key)], sqrtf(key_d2(key)));
     }
     if (!A.do_vel) return;
     double b = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
     for (int i = 0; i < cnt; i++) {
         const unsigned long long key = col[(size_t)i * S];
-        const uint32_t j = key_idx(key);
+        const uint32_t j = key_pos(key);
+        const float4 a = A.sv[j];
         float w = kernel_m4(hk, sqrtf(key_d2(key)));
-        w = __fmul_rn(w, __fdiv_rn(A.m[j], A.part_dens[j]));
+        w = __fmul_rn(w, __fdiv_rn(a.w, A.pd_s[j]));
         const double w8 = (double)w;
         b = b + w8;
-        bx = bx + w8 * (double)A.vx[j];
-        by = by + w8 * (double)A.vy[j];
-        bz = bz + w8 * (double)A.vz[j];
+        bx = bx + w8 * (double)a.x;
+        by = by + w8 * (double)a.y;
+        bz = bz + w8 * (double)a.z;
     }
     A.u2[c] = (float)(bx / b);
     A.u3[c] = (float)(by / b);
@@ -167,18 +188,18 @@ __global__ void k_cells_ball(KnnGrid G, CellArgs A, int32_t nlist) {
                         const float4 v = G.sp[p];
                         const float d2 = dist2_ref(v.x, v.y, v.z, q[0], q[1], q[2], G.box, G.periodic);
                         if (!(d2 <= r2)) continue;
-                        const int j = __float_as_int(v.w);
                         if (pass == 0) {
                             dmax2 = fmaxf(dmax2, d2);
-                            atomic_max_pos(&A.hpart[j], sqrtf(d2));
+                            atomic_max_pos(&A.hp_s[p], sqrtf(d2));
                         } else {
+                            const float4 a = A.sv[p];
                             float w = kernel_m4(hk, sqrtf(d2));
-                            w = __fmul_rn(w, __fdiv_rn(A.m[j], A.part_dens[j]));
+                            w = __fmul_rn(w, __fdiv_rn(a.w, A.pd_s[p]));
                             const double w8 = (double)w;
                             bs = bs + w8;
-                            bx = bx + w8 * (double)A.vx[j];
-                            by = by + w8 * (double)A.vy[j];
-                            bz = bz + w8 * (double)A.vz[j];
+                            bx = bx + w8 * (double)a.x;
+                            by = by + w8 * (double)a.y;
+                            bz = bz + w8 * (double)a.z;
                         }
                     }
                 }
@@ -197,7 +218,9 @@ __global__ void k_cells_ball(KnnGrid G, CellArgs A, int32_t nlist) {
 struct DdensArgs {
     int nx, rad_lo;
     float dx, rx1;
-    const float *rad, *hpart, *m;
+    const float *rad;
+    const float *hp_s;            // h in binned order
+    const float4 *sv;             // (vx, vy, vz, m) in binned order
     unsigned long long *fix;      // 2 words per cell: low, high
     double scale;
 };
@@ -221,20 +244,19 @@ __global__ void k_ddens(KnnGrid G, int64_t n, DdensArgs A) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 p = G.sp[i];
-    const int o = __float_as_int(p.w);
     const int nx = A.nx;
     const float dx = A.dx;
     const int ix = (int)__fdiv_rn(__fsub_rn(p.x, A.rx1), dx) + 1;
     const int jy = (int)__fdiv_rn(__fsub_rn(p.y, A.rx1), dx) + 1;
     const int kz = (int)__fdiv_rn(__fsub_rn(p.z, A.rx1), dx) + 1;
-    const float h = A.hpart[o];
+    const float h = A.hp_s[i];
     const float inv_h = __fdiv_rn(2.0f, h);
     const float h2max = __fmul_rn(__fmul_rn(4.0f, h), h);
     const int inc = (int)__fadd_rn(__fdiv_rn(__fmul_rn(2.0f, h), dx), 0.5f);
     // only cells with Q < 2 carry weight; rows and planes beyond h are skipped
     const float hh = h * h * 1.00002f + 1e-30f;
     const float *rad = A.rad - A.rad_lo;
-    const float m = A.m[o];
+    const float m = A.sv[i].w;
     const int k_lo = max(kz - inc, 1), k_hi = min(kz + inc, nx);
     const int j_lo = max(jy - inc, 1), j_hi = min(jy + inc, nx);
     const int i_lo = max(ix - inc, 1), i_hi = min(ix + inc, nx);
@@ -420,7 +442,8 @@ __global__ void k_zero_f32(int64_t n, float *a) {
 
 template <int KCAP>
 static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, const Level &L,
-                            const P2G &a, const float *rad_d, bool vel_sph, bool need_h_cells) {
+                            const P2G &a, const float *rad_d, bool vel_sph, bool need_h_cells,
+                            const float4 *sv, float *pd_s, float *hp_s) {
     const int T = KNN_THREADS(KCAP);
     const size_t sm = (size_t)KCAP * T * sizeof(unsigned long long);
     const int K = p->kneighbours;
@@ -430,7 +453,7 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
     AV_CUDA(cudaFuncSetAttribute(k_cells_knn<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     AV_CUDA(cudaFuncSetAttribute(k_fill_h<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     if (vel_sph) {
-        ++c.launches, k_ppart_dens<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, a.m, a.part_dens);
+        ++c.launches, k_ppart_dens<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, sv, pd_s, a.part_dens);
         c.mark("ppart_dens");
     }
     if (vel_sph || need_h_cells) {
@@ -439,8 +462,8 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
         AV_CUDA(cudaMemsetAsync(cnt_d, 0, sizeof(int32_t), c.stream));
         CellArgs A;
         A.nx = nx; A.rad_lo = L.g.rad_lo; A.K = K; A.dx = L.g.dx; A.rad = rad_d; A.smask = a.smask;
-        A.m = a.m; A.vx = a.vx; A.vy = a.vy; A.vz = a.vz; A.part_dens = a.part_dens;
-        A.hpart = a.hpart; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
+        A.sv = sv; A.pd_s = pd_s;
+        A.hp_s = hp_s; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
         A.ball_list = ball_list; A.ball_count = cnt_d;
         const int tx = TileDims<T>::x, ty = TileDims<T>::y, tz = TileDims<T>::z;
         const int64_t nblk = (int64_t)((nx + tx - 1) / tx) * ((nx + ty - 1) / ty) * ((nx + tz - 1) / tz);
@@ -453,8 +476,9 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
         if (nball > 0) ++c.launches, k_cells_ball<<<grid_for(nball, 128), 128, 0, c.stream>>>(G, A, nball);
         AV_CUDA(cudaGetLastError());
         c.mark("cells_ball");
-        ++c.launches, k_fill_h<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, a.hpart);
+        ++c.launches, k_fill_h<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, hp_s);
         c.mark("fill_h_zeros");
+        ++c.launches, k_unbin_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, G.sp, hp_s, a.hpart);
     }
     AV_CUDA(cudaGetLastError());
 }
@@ -494,6 +518,14 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
         const float occ = occ_env ? (float)atof(occ_env) : 2.0f;
         BinnedParticles bp = bin_particles(c, a.n, a.x, a.y, a.z, p->lado0, p->periodic, occ);
         KnnGrid G = make_knn_grid(bp);
+        const int64_t n1 = std::max<int64_t>(a.n, 1);
+        float4 *sv = c.get_t<float4>(B_SV, n1);
+        float *pd_s = c.get_t<float>(B_PDENS_S, n1), *hp_s = c.get_t<float>(B_HPART_S, n1);
+        if (a.n > 0) {
+            ++c.launches, k_sorted_attrs<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, G.sp, a.vx, a.vy, a.vz, a.m, sv);
+            ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, hp_s);
+            ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, pd_s);
+        }
         c.mark("bin_particles");
         if (p->learned) {
             // radius-guided search: a starting radius per bin
@@ -507,10 +539,10 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
             c.mark("radius_estimate");
         }
         const bool need_h_cells = dens_sph && !vel_sph;
-        if (K <= 32) run_sph_kernels<32>(c, G, p, L, a, rad_d, vel_sph, need_h_cells);
-        else if (K <= 64) run_sph_kernels<64>(c, G, p, L, a, rad_d, vel_sph, need_h_cells);
-        else if (K <= 128) run_sph_kernels<128>(c, G, p, L, a, rad_d, vel_sph, need_h_cells);
-        else run_sph_kernels<256>(c, G, p, L, a, rad_d, vel_sph, need_h_cells);
+        if (K <= 32) run_sph_kernels<32>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
+        else if (K <= 64) run_sph_kernels<64>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
+        else if (K <= 128) run_sph_kernels<128>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
+        else run_sph_kernels<256>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
         if (dens_sph) {
             // scale: the largest term m*w/NORM <= m_max stays below 2^62
             float mmax = 0.0f;
@@ -531,7 +563,7 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
             AV_CUDA(cudaMemsetAsync(fix, 0, 2 * nc * sizeof(unsigned long long), c.stream));
             DdensArgs D;
             D.nx = nx; D.rad_lo = L.g.rad_lo; D.dx = L.g.dx; D.rx1 = L.rad_at(1); D.rad = rad_d;
-            D.hpart = a.hpart; D.m = a.m; D.fix = fix; D.scale = scale;
+            D.hp_s = hp_s; D.sv = sv; D.fix = fix; D.scale = scale;
             c.mark("ddens_setup");
             ++c.launches, k_ddens<<<grid_for(a.n, 128), 128, 0, c.stream>>>(G, a.n, D);
             AV_CUDA(cudaGetLastError());
