@@ -13,6 +13,7 @@
 
 #include "common.cuh"
 #include "knn_core.cuh"
+#include "knn_warp.cuh"
 
 namespace avism {
 
@@ -113,6 +114,44 @@ k_knn_batch(KnnGrid G, int64_t nq, const float *__restrict__ qx, const float *__
     }
 }
 
+// warp-per-query form: WQ_WARPS warps per block, WQ_QPW consecutive queries per warp
+constexpr int WQ_WARPS = 8, WQ_QPW = 4;
+
+template <int KMAX>
+__global__ void __launch_bounds__(WQ_WARPS * 32)
+k_knn_batch_w(KnnGrid G, int64_t nq, const float *__restrict__ qx, const float *__restrict__ qy,
+              const float *__restrict__ qz, int K, int64_t *__restrict__ idx_out, float *__restrict__ dist_out) {
+    extern __shared__ __align__(16) unsigned char wq_smem[];
+    WarpKnnSmem<KMAX> &S = reinterpret_cast<WarpKnnSmem<KMAX> *>(wq_smem)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int64_t q0 = ((int64_t)blockIdx.x * WQ_WARPS + (threadIdx.x >> 5)) * WQ_QPW;
+    for (int t = 0; t < WQ_QPW; t++) {
+        const int64_t q = q0 + t;
+        if (q >= nq) break;
+        const int cnt = knn_warp_exact<KMAX>(G, qx[q], qy[q], qz[q], K, 0.0f, S,
+                                             reinterpret_cast<unsigned long long *>(S.d2));
+        for (int i = lane; i < K; i += 32) {
+            if (i < cnt) {
+                idx_out[q * K + i] = (int64_t)__float_as_int(G.sp[S.res_pos[i]].w) + 1;
+                dist_out[q * K + i] = sqrtf(__uint_as_float(S.res_d2[i]));
+            } else {
+                idx_out[q * K + i] = -1;
+                dist_out[q * K + i] = sqrtf(FLT_MAX);     // knn_search initialises dist = HUGE(0.0)
+            }
+        }
+    }
+}
+
+template <int KMAX>
+static void launch_knn_batch_w(Ctx &c, const KnnGrid &G, int64_t nq, const float *qx, const float *qy,
+                               const float *qz, int k, int64_t *idx, float *dist) {
+    const size_t sm = (size_t)WQ_WARPS * sizeof(WarpKnnSmem<KMAX>);
+    AV_CUDA(cudaFuncSetAttribute(k_knn_batch_w<KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    ++c.launches, k_knn_batch_w<KMAX><<<grid_for(nq, WQ_WARPS * WQ_QPW), WQ_WARPS * 32, sm, c.stream>>>(
+        G, nq, qx, qy, qz, k, idx, dist);
+    AV_CUDA(cudaGetLastError());
+}
+
 template <int KCAP>
 static void launch_knn_batch(Ctx &c, const KnnGrid &G, int64_t nq, const float *qx, const float *qy,
                              const float *qz, int k, int64_t *idx, float *dist) {
@@ -127,9 +166,9 @@ void knn_batch(Ctx &c, const BinnedParticles &bp, int64_t nq, const float *qx, c
                const float *qz, int k, int64_t *idx, float *dist) {
     KnnGrid G = make_knn_grid(bp);
     if (nq == 0) return;
-    if (k <= 32) launch_knn_batch<32>(c, G, nq, qx, qy, qz, k, idx, dist);
-    else if (k <= 64) launch_knn_batch<64>(c, G, nq, qx, qy, qz, k, idx, dist);
-    else if (k <= 128) launch_knn_batch<128>(c, G, nq, qx, qy, qz, k, idx, dist);
+    if (k <= 32) launch_knn_batch_w<32>(c, G, nq, qx, qy, qz, k, idx, dist);
+    else if (k <= 64) launch_knn_batch_w<64>(c, G, nq, qx, qy, qz, k, idx, dist);
+    else if (k <= 128) launch_knn_batch_w<128>(c, G, nq, qx, qy, qz, k, idx, dist);
     else if (k <= 256) launch_knn_batch<256>(c, G, nq, qx, qy, qz, k, idx, dist);
     else throw Error{AVISM_ERR_ARG, "kneighbours > 256 is not supported"};
 }

@@ -22,6 +22,8 @@ struct KnnGrid {
     float origin, bw, inv_bw, box, margin;
     int periodic;
     const float *r0;          // per-bin starting radius of the radius-guided search, or null
+    float occ;                // mean particles per bin
+    float dmax;               // no two particles are farther apart than this
 };
 
 inline KnnGrid make_knn_grid(const BinnedParticles &bp) {
@@ -36,6 +38,8 @@ inline KnnGrid make_knn_grid(const BinnedParticles &bp) {
     G.periodic = bp.periodic;
     G.margin = 2e-3f * bp.bw + 1e-6f * bp.box;
     G.r0 = nullptr;
+    G.occ = (float)((double)bp.n / ((double)bp.nb * bp.nb * bp.nb));
+    G.dmax = 1.7321f * bp.box * 1.001f;
     return G;
 }
 

@@ -160,9 +160,18 @@ __global__ void k_ccl_union(PostGrid G, int32_t *P) {
     if (j > 0 && P[e - ne] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - ne));
     if (k > 0 && P[e - (int64_t)ne * ne] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - (int64_t)ne * ne));
 }
+// root of x without path compression: a compressing find racing with another
+// thread's final store could leave that cell pointing at a non-root ancestor
+__device__ __forceinline__ int32_t uf_root(const int32_t *P, int32_t x) {
+    while (true) {
+        const int32_t px = P[x];
+        if (px == x) return x;
+        x = px;
+    }
+}
 __global__ void k_ccl_flatten(int64_t ne3, int32_t *P) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < ne3 && P[e] >= 0) P[e] = uf_find(P, (int32_t)e);
+    if (e < ne3 && P[e] >= 0) P[e] = uf_root(P, (int32_t)e);
 }
 // a hole takes the id of the first non-hole cell in +x (src/voidfinding.f90:1142-1158)
 __global__ void k_fill_holes(PostGrid G, const int32_t *P, const int32_t *marca_in, int32_t *marca_out) {

@@ -12,6 +12,7 @@
 
 #include "common.cuh"
 #include "knn_core.cuh"
+#include "knn_warp.cuh"
 
 namespace avism {
 
@@ -213,6 +214,103 @@ __global__ void k_cells_ball(KnnGrid G, CellArgs A, int32_t nlist) {
     }
 }
 
+// ---- warp-per-query forms of PPART_DENS and VVEL_INTERP_SPH_VW / H_DISTANCE ----
+// Each warp answers SPH_QPW consecutive queries with knn_warp_exact; the sums
+// over the neighbour list stay sequential in list order (REAL*8, as the
+// reference's loops), done by one lane per sum from shared memory.
+constexpr int SPH_WARPS = 8, SPH_QPW = 4;
+
+__device__ __forceinline__ float query_r0(const KnnGrid &G, float qx, float qy, float qz) {
+    if (!G.r0) return 0.0f;
+    const int b = bin_coord(qx, G.origin, G.inv_bw, G.nb) +
+                  G.nb * (bin_coord(qy, G.origin, G.inv_bw, G.nb) + G.nb * bin_coord(qz, G.origin, G.inv_bw, G.nb));
+    return G.r0[b];
+}
+
+template <int KMAX>
+__global__ void __launch_bounds__(SPH_WARPS * 32)
+k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float *__restrict__ pd_s,
+               float *__restrict__ part_dens) {
+    extern __shared__ __align__(16) unsigned char wq_smem[];
+    WarpKnnSmem<KMAX> &S = reinterpret_cast<WarpKnnSmem<KMAX> *>(wq_smem)[threadIdx.x >> 5];
+    double *acc = reinterpret_cast<double *>(S.d2);          // KMAX doubles, free after the select
+    const int lane = threadIdx.x & 31;
+    const int64_t i0 = ((int64_t)blockIdx.x * SPH_WARPS + (threadIdx.x >> 5)) * SPH_QPW;
+    for (int t = 0; t < SPH_QPW; t++) {
+        const int64_t i = i0 + t;
+        if (i >= n) break;
+        const float4 p = G.sp[i];
+        const int cnt = knn_warp_exact<KMAX>(G, p.x, p.y, p.z, K, query_r0(G, p.x, p.y, p.z), S,
+                                             reinterpret_cast<unsigned long long *>(S.d2));
+        for (int j = lane; j < cnt; j += 32) acc[j] = (double)sv[S.res_pos[j]].w;
+        __syncwarp();
+        if (lane == 0) {
+            double bas8 = 0.0;
+            for (int j = 0; j < cnt; j++) bas8 = bas8 + acc[j];
+            const float hk = sqrtf(__uint_as_float(S.res_d2[K - 1]));
+            const double pi = 3.141592653589793;     // DACOS(-1.D0)
+            const float rho = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(hk, hk), hk)));
+            pd_s[i] = rho;
+            part_dens[__float_as_int(p.w)] = rho;
+        }
+    }
+}
+
+template <int KMAX>
+__global__ void __launch_bounds__(SPH_WARPS * 32)
+k_cells_knn_w(KnnGrid G, CellArgs A) {
+    extern __shared__ __align__(16) unsigned char wq_smem[];
+    WarpKnnSmem<KMAX> &S = reinterpret_cast<WarpKnnSmem<KMAX> *>(wq_smem)[threadIdx.x >> 5];
+    double *acc = reinterpret_cast<double *>(S.d2);          // 4 x KMAX doubles, free after the select
+    const int lane = threadIdx.x & 31;
+    const int nx = A.nx;
+    // 4x4x2 tiles of cells, one tile per block, SPH_QPW cells per warp
+    const int ntx = (nx + 3) / 4, nty = (nx + 3) / 4;
+    const int64_t tile = blockIdx.x;
+    const int tx = (int)(tile % ntx), ty = (int)((tile / ntx) % nty), tz = (int)(tile / ((int64_t)ntx * nty));
+    for (int t = 0; t < SPH_QPW; t++) {
+        const int q = (threadIdx.x >> 5) * SPH_QPW + t;        // 0..31 inside the tile
+        const int ix = tx * 4 + (q & 3) + 1, jy = ty * 4 + ((q >> 2) & 3) + 1, kz = tz * 2 + (q >> 4) + 1;
+        if (ix > nx || jy > nx || kz > nx) continue;
+        const int64_t c = (int64_t)(ix - 1) + (int64_t)nx * ((int64_t)(jy - 1) + (int64_t)nx * (kz - 1));
+        if (A.smask && A.smask[c] == 0) continue;
+        const float qx = A.rad[ix - A.rad_lo], qy = A.rad[jy - A.rad_lo], qz = A.rad[kz - A.rad_lo];
+        const int K = A.K;
+        const int cnt = knn_warp_exact<KMAX>(G, qx, qy, qz, K, query_r0(G, qx, qy, qz), S,
+                                             reinterpret_cast<unsigned long long *>(S.d2));
+        const float hk = sqrtf(__uint_as_float(S.res_d2[cnt - 1]));
+        if (!(hk > A.dx)) {                       // ball_search(TREE, TAR, DX) branch
+            if (lane == 0) {
+                const int slot = atomicAdd(A.ball_count, 1);
+                A.ball_list[slot] = (int32_t)c;
+            }
+            continue;
+        }
+        for (int j = lane; j < cnt; j += 32)
+            atomic_max_pos(&A.hp_s[S.res_pos[j]], sqrtf(__uint_as_float(S.res_d2[j])));
+        if (!A.do_vel) continue;
+        for (int j = lane; j < cnt; j += 32) {
+            const uint32_t pj = S.res_pos[j];
+            const float4 a = A.sv[pj];
+            float w = kernel_m4(hk, sqrtf(__uint_as_float(S.res_d2[j])));
+            w = __fmul_rn(w, __fdiv_rn(a.w, A.pd_s[pj]));
+            const double w8 = (double)w;
+            acc[j] = w8;
+            acc[KMAX + j] = w8 * (double)a.x;
+            acc[2 * KMAX + j] = w8 * (double)a.y;
+            acc[3 * KMAX + j] = w8 * (double)a.z;
+        }
+        __syncwarp();
+        double sum = 0.0;
+        if (lane < 4)
+            for (int j = 0; j < cnt; j++) sum = sum + acc[lane * KMAX + j];
+        const double b = __shfl_sync(0xffffffffu, sum, 0);
+        if (lane == 1) A.u2[c] = (float)(sum / b);
+        if (lane == 2) A.u3[c] = (float)(sum / b);
+        if (lane == 3) A.u4[c] = (float)(sum / b);
+    }
+}
+
 // ---- DDENS_INTERP_SPH: per-particle NORM in the reference's loop order, then
 //      a 128-bit fixed-point scatter of m*w/NORM --------------------------------
 struct DdensArgs {
@@ -225,9 +323,13 @@ struct DdensArgs {
     double scale;
 };
 
+// v < 2^62 is added as its two 32-bit halves to two 64-bit counters (low half to
+// word 0, high half to word 1).  Neither counter can overflow for fewer than 2^32
+// additions per cell, no result is needed, so both compile to fire-and-forget
+// reductions; the cell's exact 128-bit sum is word1 * 2^32 + word0.
 __device__ __forceinline__ void add128(unsigned long long *cell, unsigned long long v) {
-    const unsigned long long old = atomicAdd(cell, v);
-    if (old + v < old) atomicAdd(cell + 1, 1ULL);
+    atomicAdd(cell, v & 0xffffffffULL);
+    atomicAdd(cell + 1, v >> 32);
 }
 
 __device__ __forceinline__ float m4_q(float d2, float inv_h) {
@@ -305,7 +407,8 @@ __global__ void k_fix128_to_f32(int64_t nc, const unsigned long long *__restrict
                                 float *__restrict__ out) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
-    const unsigned long long lo = fix[2 * c], hi = fix[2 * c + 1];
+    const unsigned __int128 t = ((unsigned __int128)fix[2 * c + 1] << 32) + (unsigned __int128)fix[2 * c];
+    const unsigned long long lo = (unsigned long long)t, hi = (unsigned long long)(t >> 64);
     const double v = ((double)hi * 18446744073709551616.0 + (double)lo) * inv_scale;
     out[c] = (float)v;
 }
@@ -440,6 +543,54 @@ __global__ void k_zero_f32(int64_t n, float *a) {
     if (i < n) a[i] = 0.0f;
 }
 
+template <int KMAX>
+static void run_sph_kernels_w(Ctx &c, const KnnGrid &G, const avism_params *p, const Level &L,
+                              const P2G &a, const float *rad_d, bool vel_sph, bool need_h_cells,
+                              const float4 *sv, float *pd_s, float *hp_s) {
+    const size_t sm = (size_t)SPH_WARPS * sizeof(WarpKnnSmem<KMAX>);
+    const int K = p->kneighbours;
+    const int nx = L.g.nx;
+    const int64_t nc = (int64_t)nx * nx * nx;
+    AV_CUDA(cudaFuncSetAttribute(k_ppart_dens_w<KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    if (vel_sph) {
+        ++c.launches, k_ppart_dens_w<KMAX><<<grid_for(a.n, SPH_WARPS * SPH_QPW), SPH_WARPS * 32, sm, c.stream>>>(
+            G, a.n, K, sv, pd_s, a.part_dens);
+        AV_CUDA(cudaGetLastError());
+        c.mark("ppart_dens");
+    }
+    if (vel_sph || need_h_cells) {
+        int32_t *ball_list = c.get_t<int32_t>(B_BALL, nc);
+        int32_t *cnt_d = c.get_t<int32_t>(B_SCAL, 4);
+        AV_CUDA(cudaMemsetAsync(cnt_d, 0, sizeof(int32_t), c.stream));
+        CellArgs A;
+        A.nx = nx; A.rad_lo = L.g.rad_lo; A.K = K; A.dx = L.g.dx; A.rad = rad_d; A.smask = a.smask;
+        A.sv = sv; A.pd_s = pd_s;
+        A.hp_s = hp_s; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
+        A.ball_list = ball_list; A.ball_count = cnt_d;
+        const int64_t nblk = (int64_t)((nx + 3) / 4) * ((nx + 3) / 4) * ((nx + 1) / 2);
+        ++c.launches, k_cells_knn_w<KMAX><<<(unsigned)nblk, SPH_WARPS * 32, sm, c.stream>>>(G, A);
+        AV_CUDA(cudaGetLastError());
+        c.mark("cells_knn");
+        int32_t nball = 0;
+        AV_CUDA(cudaMemcpyAsync(&nball, cnt_d, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+        if (nball > 0) ++c.launches, k_cells_ball<<<grid_for(nball, 128), 128, 0, c.stream>>>(G, A, nball);
+        AV_CUDA(cudaGetLastError());
+        c.mark("cells_ball");
+        {
+            constexpr int KC = KMAX;
+            const int T = KNN_THREADS(KC);
+            const size_t smc = (size_t)KC * T * sizeof(unsigned long long);
+            AV_CUDA(cudaFuncSetAttribute(k_fill_h<KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc));
+            ++c.launches, k_fill_h<KC><<<grid_for(a.n, T), T, smc, c.stream>>>(G, a.n, K, hp_s);
+        }
+        c.mark("fill_h_zeros");
+        ++c.launches, k_unbin_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, G.sp, hp_s, a.hpart);
+    }
+    AV_CUDA(cudaGetLastError());
+}
+
 template <int KCAP>
 static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, const Level &L,
                             const P2G &a, const float *rad_d, bool vel_sph, bool need_h_cells,
@@ -539,9 +690,9 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
             c.mark("radius_estimate");
         }
         const bool need_h_cells = dens_sph && !vel_sph;
-        if (K <= 32) run_sph_kernels<32>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
-        else if (K <= 64) run_sph_kernels<64>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
-        else if (K <= 128) run_sph_kernels<128>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
+        if (K <= 32) run_sph_kernels_w<32>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
+        else if (K <= 64) run_sph_kernels_w<64>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
+        else if (K <= 128) run_sph_kernels_w<128>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
         else run_sph_kernels<256>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
         if (dens_sph) {
             // scale: the largest term m*w/NORM <= m_max stays below 2^62
