@@ -30,6 +30,14 @@ SIGNATURES = {
     "avism_gpu_indexx": (C.c_int, [_c_void, _i32, _c_void, _c_void]),
     "avism_gpu_merge_post": (C.c_int, [_c_void, _c_void, _i32, _c_void, _c_void, _f32, _c_void]),
     "avism_gpu_run_level": (C.c_int, [_c_void, _c_void, _i64] + [_c_void] * 7 + [_c_void] * 4),
+    "avism_gpu_knn_counters": (C.c_int, [_c_void, C.c_int, _c_void, C.c_int]),
+    "avism_gpu_proposal_load": (C.c_int, [_c_void, _c_void, _i32]),
+    "avism_gpu_proposal_features": (C.c_int, [_c_void, _c_void, _i64] + [_c_void] * 7 + [_i64, _c_void, _c_void,
+                                                                                       _c_void]),
+    "avism_gpu_proposal_infer": (C.c_int, [_c_void, _i64, _c_void, _c_void, _c_void]),
+    "avism_gpu_proposal_grad": (C.c_int, [_c_void, _i64] + [_c_void] * 6),
+    "avism_gpu_proposal_train": (C.c_int, [_c_void, _i64, _c_void, _c_void, _c_void, _i32, _i32, _f32,
+                                           C.c_uint32, _c_void, _c_void]),
     "avism_gpu_knn_noalloc": (C.c_int, [C.c_int, _c_void, _i64, _c_void, _c_void, _c_void, _f32, _i64,
                                         _c_void, _c_void, _c_void, _i32, _c_void, _c_void, C.c_char_p,
                                         _i32]),

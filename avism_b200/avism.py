@@ -93,6 +93,54 @@ class AvismGPU:
     def launches(self) -> int:
         return int(self.lib.avism_gpu_launches(self.h))
 
+    # ---- warp-kNN counters (instrumentation, no reference counterpart) ---------
+    def knn_counters(self, enable: bool = True) -> dict:
+        """Counters of the last particles_to_grid / run_level call; enable
+        turns collection on (or off) for the following calls."""
+        out = np.zeros(8, np.int64)
+        self._chk(self.lib.avism_gpu_knn_counters(self.h, int(enable), _vp(out), 8))
+        keys = ("queries", "attempts", "scanned", "kept", "fallbacks")
+        return {k: int(out[i]) for i, k in enumerate(keys)}
+
+    # ---- learned proposal (no reference counterpart) -----------------------------
+    def proposal_load(self, params):
+        params = _f32(params)
+        self._chk(self.lib.avism_gpu_proposal_load(self.h, _vp(params), len(params)))
+
+    def proposal_features(self, p: Params, parts: dict):
+        """(features [nb^3, 12], nb, bin width) of the binning particles_to_grid uses."""
+        a = {k: _f32(parts[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        nb, bw = C.c_int32(), C.c_float()
+        pc = p.to_c()
+        args = (self.h, C.byref(pc), len(a["x"]), *(_vp(a[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")))
+        self._chk(self.lib.avism_gpu_proposal_features(*args, 0, None, C.byref(nb), C.byref(bw)))
+        rows = nb.value ** 3
+        feat = np.zeros((rows, 12), np.float32)
+        self._chk(self.lib.avism_gpu_proposal_features(*args, rows, _vp(feat), C.byref(nb), C.byref(bw)))
+        return feat, nb.value, bw.value
+
+    def proposal_infer(self, feat, params):
+        feat = np.ascontiguousarray(feat, np.float32)
+        out = np.zeros((len(feat), 2), np.float32)
+        self._chk(self.lib.avism_gpu_proposal_infer(self.h, len(feat), _vp(feat), _vp(_f32(params)), _vp(out)))
+        return out
+
+    def proposal_grad(self, feat, target, mask, params):
+        feat = np.ascontiguousarray(feat, np.float32)
+        g = np.zeros(len(params), np.float32)
+        loss = C.c_float()
+        self._chk(self.lib.avism_gpu_proposal_grad(self.h, len(feat), _vp(feat), _vp(_f32(target)), _vp(_f32(mask)),
+                                                   _vp(_f32(params)), _vp(g), C.byref(loss)))
+        return loss.value, g
+
+    def proposal_train(self, feat, target, mask, params, steps, batch=4096, lr=1e-3, seed=0):
+        feat = np.ascontiguousarray(feat, np.float32)
+        prm = np.array(params, np.float32, copy=True)
+        curve = np.zeros(max(steps, 1), np.float32)
+        self._chk(self.lib.avism_gpu_proposal_train(self.h, len(feat), _vp(feat), _vp(_f32(target)), _vp(_f32(mask)),
+                                                    steps, batch, lr, seed, _vp(prm), _vp(curve)))
+        return prm, curve[:steps]
+
     # ---- kNN (knn_search, src/kdtree.f90:504-540) ----------------------------
     def knn_search(self, x, y, z, qx, qy, qz, k, box_l=0.0):
         x, y, z, qx, qy, qz = map(_f32, (x, y, z, qx, qy, qz))

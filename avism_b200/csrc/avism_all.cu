@@ -3,6 +3,7 @@
 #include "ctx.cu"
 #include "knn.cu"
 #include "sph.cu"
+#include "proposal.cu"
 #include "fields.cu"
 #include "indexx.cu"
 #include "voidfind.cu"

@@ -267,6 +267,106 @@ int avism_gpu_knn(avism_gpu_ctx *ctx, int64_t n, const float *x, const float *y,
     });
 }
 
+int avism_gpu_knn_counters(avism_gpu_ctx *ctx, int enable, int64_t *out, int n) {
+    return guarded(ctx, [&](Ctx &c) {
+        AV_CHECK(n >= 0 && (n == 0 || out), AVISM_ERR_ARG, "knn_counters: bad arguments");
+        if (n > 0) {
+            unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            if (c.buf[B_KNN_STATS]) {
+                AV_CUDA(cudaMemcpyAsync(h, c.buf[B_KNN_STATS], sizeof h, cudaMemcpyDeviceToHost, c.stream));
+                c.sync();
+            }
+            for (int i = 0; i < n && i < 8; i++) out[i] = (int64_t)h[i];
+        }
+        c.knn_stats = enable != 0;
+    });
+}
+
+int avism_gpu_proposal_load(avism_gpu_ctx *ctx, const float *params, int32_t nparam) {
+    return guarded(ctx, [&](Ctx &c) {
+        AV_CHECK(params && nparam == PROPOSAL_NPARAM, AVISM_ERR_ARG,
+                 "proposal_load: params must hold AVISM_PROPOSAL_NPARAM floats");
+        const float *d = (const float *)to_device(c, B_PR_PARAMS, params, sizeof(float) * PROPOSAL_NPARAM);
+        if (d != c.buf[B_PR_PARAMS]) {
+            float *keep = c.get_t<float>(B_PR_PARAMS, PROPOSAL_NPARAM);
+            AV_CUDA(cudaMemcpyAsync(keep, d, sizeof(float) * PROPOSAL_NPARAM, cudaMemcpyDeviceToDevice, c.stream));
+            d = keep;
+        }
+        proposal_load(c, d);
+    });
+}
+
+int avism_gpu_proposal_features(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x,
+                                const float *y, const float *z, const float *vx, const float *vy,
+                                const float *vz, const float *m, int64_t cap_rows, float *feat, int32_t *nb,
+                                float *bw) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        AV_CHECK(n >= 1 && nb && bw, AVISM_ERR_ARG, "proposal_features: bad arguments");
+        Level L = make_level(p);
+        P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, nullptr);
+        int nbv = 0;
+        float bwv = 0.f;
+        proposal_features(c, p, a, nullptr, &nbv, &bwv);
+        *nb = nbv;
+        *bw = bwv;
+        if (!feat) return;
+        const int64_t rows = (int64_t)nbv * nbv * nbv;
+        AV_CHECK(cap_rows >= rows, AVISM_ERR_ARG, "proposal_features: feat holds fewer rows than bins");
+        float *fd = is_device_ptr(feat) ? feat : c.get_t<float>(B_PR_FEAT, (size_t)rows * 12);
+        proposal_features(c, p, a, fd, &nbv, &bwv);
+        from_device(c, feat, fd, sizeof(float) * 12 * (size_t)rows);
+        c.sync();
+    });
+}
+
+int avism_gpu_proposal_infer(avism_gpu_ctx *ctx, int64_t nrows, const float *feat, const float *params,
+                             float *out) {
+    return guarded(ctx, [&](Ctx &c) {
+        AV_CHECK(nrows >= 0 && feat && params && out, AVISM_ERR_ARG, "proposal_infer: bad arguments");
+        const float *fd = (const float *)to_device(c, B_PR_FEAT, feat, sizeof(float) * 12 * (size_t)std::max<int64_t>(nrows, 1));
+        const float *pd = (const float *)to_device(c, B_PR_TRAIN, params, sizeof(float) * PROPOSAL_NPARAM);
+        float *od = is_device_ptr(out) ? out : c.get_t<float>(B_PR_R0, 2 * (size_t)std::max<int64_t>(nrows, 1));
+        proposal_infer(c, nrows, fd, pd, od);
+        from_device(c, out, od, sizeof(float) * 2 * (size_t)nrows);
+        c.sync();
+    });
+}
+
+int avism_gpu_proposal_grad(avism_gpu_ctx *ctx, int64_t ns, const float *feat, const float *target,
+                            const float *mask, const float *params, float *grad, float *loss) {
+    return guarded(ctx, [&](Ctx &c) {
+        AV_CHECK(ns >= 1 && feat && target && mask && params && grad && loss, AVISM_ERR_ARG,
+                 "proposal_grad: bad arguments");
+        const float *fd = (const float *)to_device(c, B_PR_FEAT, feat, sizeof(float) * 12 * (size_t)ns);
+        const float *td = (const float *)to_device(c, B_PR_W0, target, sizeof(float) * 2 * (size_t)ns);
+        const float *md = (const float *)to_device(c, B_KNN_R0, mask, sizeof(float) * 2 * (size_t)ns);
+        const float *pd = (const float *)to_device(c, B_PR_PARAMS, params, sizeof(float) * PROPOSAL_NPARAM);
+        float *gd = c.get_t<float>(B_PR_GRAD, 3 * (size_t)PROPOSAL_NPARAM);
+        float l = 0.f;
+        proposal_grad(c, ns, fd, td, md, pd, gd, &l);
+        from_device(c, grad, gd, sizeof(float) * PROPOSAL_NPARAM);
+        c.sync();
+        *loss = l;
+    });
+}
+
+int avism_gpu_proposal_train(avism_gpu_ctx *ctx, int64_t ns, const float *feat, const float *target,
+                             const float *mask, int32_t steps, int32_t batch, float lr, uint32_t seed,
+                             float *params, float *loss_curve) {
+    return guarded(ctx, [&](Ctx &c) {
+        AV_CHECK(ns >= 1 && feat && target && mask && params, AVISM_ERR_ARG, "proposal_train: bad arguments");
+        const float *fd = (const float *)to_device(c, B_PR_FEAT, feat, sizeof(float) * 12 * (size_t)ns);
+        const float *td = (const float *)to_device(c, B_PR_W0, target, sizeof(float) * 2 * (size_t)ns);
+        const float *md = (const float *)to_device(c, B_KNN_R0, mask, sizeof(float) * 2 * (size_t)ns);
+        float *pd = c.get_t<float>(B_PR_PARAMS, PROPOSAL_NPARAM);
+        AV_CUDA(cudaMemcpyAsync(pd, params, sizeof(float) * PROPOSAL_NPARAM, cudaMemcpyDefault, c.stream));
+        proposal_train(c, ns, fd, td, md, steps, batch, lr, seed, pd, loss_curve);
+        from_device(c, params, pd, sizeof(float) * PROPOSAL_NPARAM);
+        c.sync();
+    });
+}
+
 int avism_gpu_particles_to_grid(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x,
                                 const float *y, const float *z, const float *vx, const float *vy,
                                 const float *vz, const float *m, const int8_t *smask, float *u_mass,
@@ -402,7 +502,7 @@ int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, co
         particles_to_grid(c, p, L, a);
         float *u1 = c.get_t<float>(B_U1CO, nc), *dv = c.get_t<float>(B_DIVER, nc);
         FieldsOut fo = fields_inner(c, p, L, a.u_mass, a.u2, a.u3, a.u4, u1, dv);
-        c.mark("fields");
+        c.mark("divergence");
         CubesDev cd{};
         const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, nullptr, nullptr, 0, cd);
         HostCubes hc(c, cd, nv);

@@ -50,6 +50,14 @@ enum BufId : int {
     B_RED0, B_RED1, B_RED2,
     B_QUERY, B_RAD, B_BALL, B_SCAL, B_KNN_R0,
     B_SV, B_PDENS_S, B_HPART_S,                    // per-particle attributes in binned order
+    B_PR_PARAMS, B_PR_PACKED, B_PR_PACKED_TMP,     // learned proposal: parameters, packed weights
+    B_PR_TRAIN, B_PR_IDX, B_PR_GRAD, B_PR_ERR,     // training scratch
+    B_PR_PYR0, B_PR_PYR1, B_PR_PYR2, B_PR_PYR3,    // feature pyramid
+    B_PR_R0, B_PR_W0, B_PR_FEAT,                   // per-bin radius / half-width, feature rows
+    B_KNN_STATS,                                   // warp kNN counters
+    B_FLAGS_IN,                                    // flag bytes of the periodic inner grid
+    B_PR_CNT, B_PR_BOX1, B_PR_BOX2, B_PR_BOX4,     // centred box counts of the bins
+    B_PR_TMPA, B_PR_TMPB,
     B_NUM
 };
 
@@ -66,6 +74,10 @@ struct Ctx {
     size_t hpin_cap = 0;
     // number of this library's kernels launched since the context was created
     int64_t launches = 0;
+    // learned-proposal weights loaded (B_PR_PARAMS / B_PR_PACKED hold them)
+    bool prop_loaded = false;
+    // collect warp-kNN counters in particles_to_grid
+    bool knn_stats = false;
     // named stage marks: events recorded on the stream, resolved by stage_close()
     std::vector<cudaEvent_t> marks;
     std::vector<std::string> mark_names;
@@ -199,6 +211,16 @@ void ext_copy(Ctx &c, const Level &L, const float *inner, float *ext);
 void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, const float *dv,
                 int fields_are_ext, const int8_t *smask_ext, const int32_t *marcap_ext,
                 uint8_t *flags);
+
+// learned proposal (proposal.cu)
+void proposal_load(Ctx &c, const float *params_dev);
+void proposal_features(Ctx &c, const avism_params *p, const P2G &a, float *feat_dev, int *nb_out, float *bw_out);
+void proposal_infer(Ctx &c, int64_t ns, const float *feat, const float *prm_dev, float *out);
+void proposal_grad(Ctx &c, int64_t ns, const float *feat, const float *tgt, const float *msk, const float *prm,
+                   float *grad, float *loss);
+void proposal_train(Ctx &c, int64_t ns, const float *feat, const float *tgt, const float *msk, int steps, int batch,
+                    float lr, uint32_t seed, float *prm, float *loss_curve);
+constexpr int PROPOSAL_NPARAM = 9308;
 
 // exact Numerical Recipes INDEXX on device arrays (key f32, idx i32 1-based out)
 void indexx_device(Ctx &c, int32_t n, const float *key_in, int32_t *indx_out);

@@ -6,11 +6,12 @@
 // (src/num.f90:89-133), MARK_ALL (src/voidfinding.f90:13-55) and the six
 // directional flag grids of VOIDFIND (src/voidfinding.f90:256-432).
 //
-// The ext grid is never materialised on the hot path: ghost cells read the
-// inner grids at wrapped coordinates.  Flags are packed into one byte per ext
+// The ext grid of U1CO / DIVERCO is never materialised on the hot path: ghost
+// cells read the inner grids at wrapped coordinates.  Flags are packed into one byte per ext
 // cell: bit0 FLAGV, bit1 X1, bit2 X2, bit3 Y1, bit4 Y2, bit5 Z1, bit6 Z2,
 // bit7 FLAG_SUB.
 #include <cub/cub.cuh>
+#include <cuda.h>
 #include <cmath>
 #include <cstring>
 
@@ -38,6 +39,25 @@ __global__ void k_div_scalar(int64_t nc, float *__restrict__ a, float s) {
 struct ToDouble {
     __host__ __device__ double operator()(float v) const { return (double)v; }
 };
+
+// d v / d axis at a face cell (pos == 1 or nx): periodic wrap or the
+// reference's linear extrapolation (src/divergence.f90:15-46)
+__device__ __forceinline__ float diver_edge(const float *__restrict__ v, int64_t c, int pos, int64_t stride, int nx,
+                                            int periodic) {
+    const float *p = v + c;
+    if (pos > 1 && pos < nx) return __fdiv_rn(__fsub_rn(p[stride], p[-stride]), 2.0f);
+    if (periodic) {
+        const float *pp = pos == nx ? p - (int64_t)(nx - 1) * stride : p + stride;
+        const float *pm = pos == 1 ? p + (int64_t)(nx - 1) * stride : p - stride;
+        return __fdiv_rn(__fsub_rn(*pp, *pm), 2.0f);
+    }
+    if (pos == 1) {
+        const float inner = __fdiv_rn(__fsub_rn(p[2 * stride], p[0]), 2.0f);
+        return __fsub_rn(__fmul_rn(2.0f, __fsub_rn(p[stride], p[0])), inner);
+    }
+    const float inner = __fdiv_rn(__fsub_rn(p[0], p[-2 * stride]), 2.0f);
+    return __fsub_rn(__fmul_rn(2.0f, __fsub_rn(p[0], p[-stride])), inner);
+}
 
 // DIVER_UNIFORM with periodic or extrapolated boundaries
 __global__ void k_diver(int nx, float dx, int periodic, const float *__restrict__ v2,
@@ -67,6 +87,117 @@ __global__ void k_diver(int nx, float dx, int periodic, const float *__restrict_
     diver[c] = __fadd_rn(__fadd_rn(__fdiv_rn(ddx, dx), __fdiv_rn(ddy, dx)), __fdiv_rn(ddz, dx));
 }
 
+// ---- DIVER_UNIFORM on TMA-staged tiles ----------------------------------------
+// A CTA computes a DV_TX x DV_TY x DV_TZ tile of the inner grid.  One elected
+// thread loads three boxes with cp.async.bulk.tensor (v2 with a +-4 x halo, v3
+// with +-1 in y, v4 with +-1 in z; out-of-grid parts are zero-filled and
+// never used) onto one mbarrier; the threads then difference from shared
+// memory.  Cells on the grid's faces (periodic wrap or one-sided
+// extrapolation) take their values from global memory, as k_diver does.
+constexpr int DV_TX = 32, DV_TY = 8, DV_TZ = 8, DV_THREADS = 256;
+constexpr uint32_t DV_WAIT_LIMIT = 1u << 22;
+
+struct __align__(128) DvSmem {
+    float v2[DV_TZ][DV_TY][DV_TX + 8];
+    float v3[DV_TZ][DV_TY + 2][DV_TX];
+    float v4[DV_TZ + 2][DV_TY][DV_TX];
+    uint64_t mbar;
+};
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        :: "r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(map), "r"(x), "r"(y), "r"(z),
+           "r"((uint32_t)__cvta_generic_to_shared(mbar))
+        : "memory");
+}
+
+__global__ void __launch_bounds__(DV_THREADS)
+k_diver_tma(const __grid_constant__ CUtensorMap m2, const __grid_constant__ CUtensorMap m3,
+            const __grid_constant__ CUtensorMap m4, int nx, float dx, int periodic, const float *__restrict__ v2,
+            const float *__restrict__ v3, const float *__restrict__ v4, float *__restrict__ diver, int *err) {
+    __shared__ DvSmem S;
+    const int ntx = nx / DV_TX, nty = nx / DV_TY;
+    const int bx = (int)(blockIdx.x % ntx), by = (int)((blockIdx.x / ntx) % nty), bz = (int)(blockIdx.x / (ntx * nty));
+    const int X0 = bx * DV_TX, Y0 = by * DV_TY, Z0 = bz * DV_TZ;
+    const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&S.mbar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(mb) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const uint32_t bytes = (uint32_t)(sizeof(S.v2) + sizeof(S.v3) + sizeof(S.v4));
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mb), "r"(bytes) : "memory");
+        tma_load_3d(&S.v2[0][0][0], &m2, X0 - 4, Y0, Z0, &S.mbar);
+        tma_load_3d(&S.v3[0][0][0], &m3, X0, Y0 - 1, Z0, &S.mbar);
+        tma_load_3d(&S.v4[0][0][0], &m4, X0, Y0, Z0 - 1, &S.mbar);
+    }
+    __syncthreads();
+    auto wait = [&]() {
+        for (uint32_t it = 0; it < DV_WAIT_LIMIT; it++) {
+            uint32_t r;
+            asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                         "selp.u32 %0, 1, 0, p;\n\t}\n" : "=r"(r) : "r"(mb) : "memory");
+            if (r) return true;
+        }
+        return false;
+    };
+    if (!wait()) {                                 // report, give the copies one more bounded wait, leave
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        wait();
+        return;
+    }
+    const int64_t sy = nx, sz = (int64_t)nx * nx;
+    for (int t = threadIdx.x; t < DV_TX * DV_TY * DV_TZ; t += DV_THREADS) {
+        const int lx = t % DV_TX, ly = (t / DV_TX) % DV_TY, lz = t / (DV_TX * DV_TY);
+        const int i = X0 + lx + 1, j = Y0 + ly + 1, k = Z0 + lz + 1;        // 1-based
+        const int64_t c = (int64_t)(i - 1) + sy * (j - 1) + sz * (k - 1);
+        float ddx, ddy, ddz;
+        if (i > 1 && i < nx) ddx = __fdiv_rn(__fsub_rn(S.v2[lz][ly][lx + 5], S.v2[lz][ly][lx + 3]), 2.0f);
+        else ddx = diver_edge(v2, c, i, 1, nx, periodic);
+        if (j > 1 && j < nx) ddy = __fdiv_rn(__fsub_rn(S.v3[lz][ly + 2][lx], S.v3[lz][ly][lx]), 2.0f);
+        else ddy = diver_edge(v3, c, j, sy, nx, periodic);
+        if (k > 1 && k < nx) ddz = __fdiv_rn(__fsub_rn(S.v4[lz + 2][ly][lx], S.v4[lz][ly][lx]), 2.0f);
+        else ddz = diver_edge(v4, c, k, sz, nx, periodic);
+        diver[c] = __fadd_rn(__fadd_rn(__fdiv_rn(ddx, dx), __fdiv_rn(ddy, dx)), __fdiv_rn(ddz, dx));
+    }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        AV_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        AV_CHECK(p && q == cudaDriverEntryPointSuccess, AVISM_ERR_CUDA, "cuTensorMapEncodeTiled not available");
+        fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// f32 nx^3 grid, box bx x by x bz, zero fill outside the grid
+static CUtensorMap grid_map(const float *g, int nx, int bx, int by, int bz) {
+    CUtensorMap m;
+    const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)nx, (cuuint64_t)nx};
+    const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * nx * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const CUresult r = encode_tiled_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)g, dims, strides, box, es,
+                                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    AV_CHECK(r == CUDA_SUCCESS, AVISM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return m;
+}
+
+// the TMA path needs whole tiles and 16-byte row pitches
+static bool diver_tma_ok(int nx, const float *a, const float *b, const float *c) {
+    auto al = [](const float *p) { return ((uintptr_t)p & 15) == 0; };
+    return nx % DV_TX == 0 && nx % DV_TY == 0 && nx % DV_TZ == 0 && al(a) && al(b) && al(c);
+}
+
 FieldsOut fields_inner(Ctx &c, const avism_params *p, const Level &L, const float *u_mass,
                        const float *u2, const float *u3, const float *u4, float *u1co_in,
                        float *diver_in) {
@@ -86,7 +217,24 @@ FieldsOut fields_inner(Ctx &c, const avism_params *p, const Level &L, const floa
     c.sync();
     const float mean = (float)(sum / (double)nc);
     ++c.launches, k_div_scalar<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u1co_in, mean);
-    ++c.launches, k_diver<<<grid_for(nc, 256), 256, 0, c.stream>>>(nx, dx, p->periodic, u2, u3, u4, diver_in);
+    c.mark("normalise");
+    if (diver_tma_ok(nx, u2, u3, u4)) {
+        const CUtensorMap m2 = grid_map(u2, nx, DV_TX + 8, DV_TY, DV_TZ);
+        const CUtensorMap m3 = grid_map(u3, nx, DV_TX, DV_TY + 2, DV_TZ);
+        const CUtensorMap m4 = grid_map(u4, nx, DV_TX, DV_TY, DV_TZ + 2);
+        int *err = c.get_t<int>(B_SCAL, 4);
+        AV_CUDA(cudaMemsetAsync(err, 0, sizeof(int), c.stream));
+        const unsigned ntiles = (unsigned)((nx / DV_TX) * (nx / DV_TY) * (nx / DV_TZ));
+        ++c.launches, k_diver_tma<<<ntiles, DV_THREADS, 0, c.stream>>>(m2, m3, m4, nx, dx, p->periodic, u2, u3, u4,
+                                                                       diver_in, err);
+        AV_CUDA(cudaGetLastError());
+        int herr = 0;
+        AV_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+        AV_CHECK(herr == 0, AVISM_ERR_TIMEOUT, "divergence: a TMA wait timed out");
+    } else {
+        ++c.launches, k_diver<<<grid_for(nc, 256), 256, 0, c.stream>>>(nx, dx, p->periodic, u2, u3, u4, diver_in);
+    }
     AV_CUDA(cudaGetLastError());
     FieldsOut o;
     const float ul3 = (UL_F * UL_F) * UL_F;
@@ -188,11 +336,8 @@ __device__ __forceinline__ int dir_flag(const FlagArgs &A, const int c[3], int a
     return f;
 }
 
-__global__ void k_flags(FlagArgs A, uint8_t *__restrict__ flags) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int ne = A.ne;
-    if (e >= (int64_t)ne * ne * ne) return;
-    const int c[3] = {(int)(e % ne) + A.low1, (int)((e / ne) % ne) + A.low1, (int)(e / ((int64_t)ne * ne)) + A.low1};
+// flag byte of ext cell e at coordinates c (LOW1..LOW2)
+__device__ __forceinline__ uint8_t flag_byte(const FlagArgs &A, int64_t e, const int c[3]) {
     uint8_t f = 0;
     const int32_t mp = A.marcap ? A.marcap[e] : -1;
     if ((!A.smask || A.smask[e] != 0) && mp != 0) {
@@ -210,7 +355,121 @@ __global__ void k_flags(FlagArgs A, uint8_t *__restrict__ flags) {
         if (r < 0) break;
         if (r) f |= (uint8_t)(1u << bits[d]);
     }
-    flags[e] = f;
+    return f;
+}
+
+__global__ void k_flags(FlagArgs A, uint8_t *__restrict__ flags) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int ne = A.ne;
+    if (e >= (int64_t)ne * ne * ne) return;
+    const int c[3] = {(int)(e % ne) + A.low1, (int)((e / ne) % ne) + A.low1, (int)(e / ((int64_t)ne * ne)) + A.low1};
+    flags[e] = flag_byte(A, e, c);
+}
+
+// ---- flags of the periodic inner grid, spread to the ext grid -------------------
+// Away from the ext grid's faces (every coordinate at least 4 cells inside
+// LOW1..LOW2) a cell's flag byte depends only on U1CO and DIVERCO at wrapped
+// positions, so it equals the byte of the inner cell it wraps to (no mask, no
+// parent map).  k_flags_inner computes those inner bytes once: a CTA holds a
+// 32 x 8 column of cells and marches it along z, with a ring of 7 U1CO planes
+// (+-3 halo) and 3 DIVERCO planes (+-1 halo) in shared memory.  k_flags_spread
+// then writes the ext grid, computing the face shell directly.
+constexpr int FL_TX = 32, FL_TY = 8, FL_TZ = 32, FL_H = 3;
+constexpr int FL_UX = FL_TX + 2 * FL_H, FL_UY = FL_TY + 2 * FL_H;
+constexpr int FL_DX = FL_TX + 2, FL_DY = FL_TY + 2;
+constexpr int FL_UN = FL_UX * FL_UY, FL_DN = FL_DX * FL_DY;
+
+__device__ __forceinline__ int wrapn(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+__global__ void __launch_bounds__(FL_TX * FL_TY)
+k_flags_inner(FlagArgs A, uint8_t *__restrict__ fin) {
+    __shared__ float su[7][FL_UY][FL_UX];
+    __shared__ float sd[3][FL_DY][FL_DX];
+    const int nx = A.nx;
+    const int ntx = nx / FL_TX, nty = nx / FL_TY;
+    const int bx = (int)(blockIdx.x % ntx), by = (int)((blockIdx.x / ntx) % nty), bz = (int)(blockIdx.x / (ntx * nty));
+    const int X0 = bx * FL_TX, Y0 = by * FL_TY, Z0 = bz * FL_TZ;
+    const int tid = threadIdx.x, lx = tid % FL_TX, ly = tid / FL_TX;
+    const int64_t plane = (int64_t)nx * nx;
+    // in-plane offsets of this thread's halo loads (fixed for every plane)
+    int64_t uo[3], dof[2];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const int e = tid + r * FL_TX * FL_TY;
+        const int hx = e % FL_UX, hy = e / FL_UX;
+        uo[r] = e < FL_UN ? (int64_t)wrapn(X0 - FL_H + hx, nx) + (int64_t)nx * wrapn(Y0 - FL_H + hy, nx) : -1;
+    }
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int e = tid + r * FL_TX * FL_TY;
+        const int hx = e % FL_DX, hy = e / FL_DX;
+        dof[r] = e < FL_DN ? (int64_t)wrapn(X0 - 1 + hx, nx) + (int64_t)nx * wrapn(Y0 - 1 + hy, nx) : -1;
+    }
+    auto load_u = [&](int z) {
+        const int slot = (z - Z0 + FL_H) % 7;
+        const float *src = A.u1 + plane * wrapn(z, nx);
+        float *dst = &su[slot][0][0];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+            if (uo[r] >= 0) dst[tid + r * FL_TX * FL_TY] = src[uo[r]];
+    };
+    auto load_d = [&](int z) {
+        const int slot = (z - Z0 + 1) % 3;
+        const float *src = A.dv + plane * wrapn(z, nx);
+        float *dst = &sd[slot][0][0];
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+            if (dof[r] >= 0) dst[tid + r * FL_TX * FL_TY] = src[dof[r]];
+    };
+    for (int z = Z0 - FL_H; z < Z0 + FL_H; z++) load_u(z);
+    load_d(Z0 - 1);
+    load_d(Z0);
+    for (int z = Z0; z < Z0 + FL_TZ; z++) {
+        load_u(z + FL_H);
+        load_d(z + 1);
+        __syncthreads();
+        auto U = [&](int dx, int dy, int dz) { return su[(z + dz - Z0 + FL_H) % 7][ly + FL_H + dy][lx + FL_H + dx]; };
+        auto D = [&](int dx, int dy, int dz) { return sd[(z + dz - Z0 + 1) % 3][ly + 1 + dy][lx + 1 + dx]; };
+        uint8_t f = 0x80;                                        // FLAG_SUB: no mask, no parent map
+        if (U(0, 0, 0) < A.dens1 && D(0, 0, 0) > 0.0f) f |= 0x01;
+        // +X, -X, +Y, -Y, +Z, -Z -> bits 2, 1, 4, 3, 6, 5
+#pragma unroll
+        for (int d = 0; d < 6; d++) {
+            const int ax = d >> 1, sg = (d & 1) ? -1 : 1;
+            const int ex = ax == 0 ? sg : 0, ey = ax == 1 ? sg : 0, ez = ax == 2 ? sg : 0;
+            const float un = U(ex, ey, ez), dn = D(ex, ey, ez);
+            int fl = __fsub_rn(U(2 * ex, 2 * ey, 2 * ez), U(0, 0, 0)) >= A.gthr;
+            if (fl && __fsub_rn(U(3 * ex, 3 * ey, 3 * ez), un) < A.gthr) fl = 0;
+            if (dn < A.div_thre) fl = 1;
+            if (un >= A.dens2) fl = 1;
+            const int bit = 2 * ax + (sg > 0 ? 2 : 1);
+            if (fl) f |= (uint8_t)(1u << bit);
+        }
+        fin[(int64_t)(X0 + lx) + (int64_t)nx * (Y0 + ly) + plane * z] = f;
+        __syncthreads();
+    }
+}
+
+__global__ void k_flags_spread(FlagArgs A, const uint8_t *__restrict__ fin, uint8_t *__restrict__ flags) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ne = A.ne, nx = A.nx;
+    if (i >= ne) return;
+    const int c[3] = {i + A.low1, (int)blockIdx.y + A.low1, (int)blockIdx.z + A.low1};
+    const int64_t e = (int64_t)i + (int64_t)ne * (blockIdx.y + (int64_t)ne * blockIdx.z);
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < 3; a++) inside &= c[a] >= A.low1 + 4 && c[a] <= A.low2 - 4;
+    if (inside) {
+        int w[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            w[a] = c[a];
+            if (w[a] < 1) w[a] += nx; else if (w[a] > nx) w[a] -= nx;
+        }
+        flags[e] = fin[(int64_t)(w[0] - 1) + (int64_t)nx * ((w[1] - 1) + (int64_t)nx * (w[2] - 1))];
+    } else {
+        flags[e] = flag_byte(A, e, c);
+    }
 }
 
 void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, const float *dv,
@@ -223,7 +482,18 @@ void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, 
     A.div_thre = p->div_thre;
     A.gthr = grad_threshold(p->grad_thre, L.g.dx);
     const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
-    ++c.launches, k_flags<<<grid_for(ne3, 256), 256, 0, c.stream>>>(A, flags);
+    const int nx = L.g.nx;
+    const bool tiled = !fields_are_ext && !smask_ext && !marcap_ext && nx % FL_TX == 0 && nx % FL_TY == 0 &&
+                       nx % FL_TZ == 0 && L.g.ne < 65536;
+    if (tiled) {
+        uint8_t *fin = c.get_t<uint8_t>(B_FLAGS_IN, (size_t)nx * nx * nx);
+        const unsigned ntiles = (unsigned)((nx / FL_TX) * (nx / FL_TY) * (nx / FL_TZ));
+        ++c.launches, k_flags_inner<<<ntiles, FL_TX * FL_TY, 0, c.stream>>>(A, fin);
+        const dim3 g((unsigned)((L.g.ne + 127) / 128), (unsigned)L.g.ne, (unsigned)L.g.ne);
+        ++c.launches, k_flags_spread<<<g, 128, 0, c.stream>>>(A, fin, flags);
+    } else {
+        ++c.launches, k_flags<<<grid_for(ne3, 256), 256, 0, c.stream>>>(A, flags);
+    }
     AV_CUDA(cudaGetLastError());
 }
 

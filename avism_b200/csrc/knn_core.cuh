@@ -24,6 +24,7 @@ struct KnnGrid {
     const float *r0;          // per-bin starting radius of the radius-guided search, or null
     float occ;                // mean particles per bin
     float dmax;               // no two particles are farther apart than this
+    unsigned long long *stats;  // warp kNN counters or null: queries, attempts, scanned, kept, fallbacks
 };
 
 inline KnnGrid make_knn_grid(const BinnedParticles &bp) {
@@ -40,6 +41,7 @@ inline KnnGrid make_knn_grid(const BinnedParticles &bp) {
     G.r0 = nullptr;
     G.occ = (float)((double)bp.n / ((double)bp.nb * bp.nb * bp.nb));
     G.dmax = 1.7321f * bp.box * 1.001f;
+    G.stats = nullptr;
     return G;
 }
 

@@ -115,6 +115,89 @@ __device__ __forceinline__ int wq_rows(const KnnGrid &G, const int b[3], float q
     return __shfl_sync(0xffffffffu, li, 31);
 }
 
+__device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int src) {
+    const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)v, src), hi = __shfl_sync(0xffffffffu, (uint32_t)(v >> 32), src);
+    return ((unsigned long long)hi << 32) | lo;
+}
+__device__ __forceinline__ unsigned long long shfl_xor_u64(unsigned long long v, int m) {
+    const uint32_t lo = __shfl_xor_sync(0xffffffffu, (uint32_t)v, m), hi = __shfl_xor_sync(0xffffffffu, (uint32_t)(v >> 32), m);
+    return ((unsigned long long)hi << 32) | lo;
+}
+// ascending bitonic sort of one key per lane
+__device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const unsigned long long b = shfl_xor_u64(v, j);
+            const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+            v = keep_min ? (b < v ? b : v) : (b > v ? b : v);
+        }
+    }
+    return v;
+}
+// the 32 smallest of two ascending 32-key lists, ascending
+__device__ __forceinline__ unsigned long long warp_merge32(unsigned long long a, unsigned long long b) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long br = shfl_u64(b, 31 - lane);
+    unsigned long long v = br < a ? br : a;                 // a bitonic sequence
+#pragma unroll
+    for (int j = 16; j > 0; j >>= 1) {
+        const unsigned long long o = shfl_xor_u64(v, j);
+        v = (lane & j) == 0 ? (o < v ? o : v) : (o > v ? o : v);
+    }
+    return v;
+}
+
+// The K <= 32 nearest of the n <= 128 kept candidates, ordered by (squared
+// distance, buffer slot) with warp bitonic sorts.  That is the exact order
+// unless two of the selected -- or the K-th and a dropped one -- have the same
+// squared distance; then it returns false and the caller ranks exactly.
+template <int KMAX>
+__device__ __forceinline__ bool bitonic_select(const KnnGrid &G, int n, int K, WarpKnnSmem<KMAX> &S) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long k[4];
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        const int e = s * 32 + lane;
+        k[s] = e < n ? (((unsigned long long)S.d2[e] << 32) | (unsigned)e) : ~0ULL;
+    }
+    const int ns = (n + 31) >> 5;
+    k[0] = warp_sort32(k[0]);
+    if (ns > 1) {
+        k[1] = warp_sort32(k[1]);
+        k[0] = warp_merge32(k[0], k[1]);
+    }
+    if (ns > 2) {
+        k[2] = warp_sort32(k[2]);
+        if (ns > 3) {
+            k[3] = warp_sort32(k[3]);
+            k[2] = warp_merge32(k[2], k[3]);
+        }
+        k[0] = warp_merge32(k[0], k[2]);
+    }
+    const int m = min(n, K);
+    // ties: equal squared distances among the first m, or beyond the m-th
+    const uint32_t d = (uint32_t)(k[0] >> 32);
+    const uint32_t dn = __shfl_down_sync(0xffffffffu, d, 1);
+    const uint32_t dk = __shfl_sync(0xffffffffu, d, m - 1);
+    bool tie = lane < m - 1 && d == dn;
+    int le = 0;
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        const int e = s * 32 + lane;
+        le += __popc(__ballot_sync(0xffffffffu, e < n && S.d2[e] <= dk));
+    }
+    if (__any_sync(0xffffffffu, tie) || le > m) return false;
+    if (lane < m) {
+        S.res_d2[lane] = d;
+        S.res_pos[lane] = S.pos[(uint32_t)k[0]];
+    }
+    __syncwarp();
+    return true;
+}
+
 // Exact K nearest of q (K <= KMAX) by the warp; all 32 lanes must call it with
 // the same arguments.  Returns the neighbour count (K unless fewer particles)
 // with S.res_d2 / S.res_pos holding them in ascending order, or -1 when the
@@ -172,6 +255,7 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
                 }
                 count += __popc(m);
             }
+            if (G.stats && lane == 0) atomicAdd(&G.stats[2], (unsigned long long)T);
             __syncwarp();
         }
         if (count > CAP) {                               // too many: shrink
@@ -188,8 +272,16 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
             R = Rn;
             continue;
         }
-        // counting select: rank = #smaller squared distances + #equal ones with a smaller index
         const int n = count;
+        if (G.stats && lane == 0) {
+            atomicAdd(&G.stats[0], 1ULL);
+            atomicAdd(&G.stats[1], (unsigned long long)(attempt + 1));
+            atomicAdd(&G.stats[3], (unsigned long long)n);
+        }
+        if constexpr (KMAX == 32) {
+            if (bitonic_select(G, n, K, S)) return min(n, K);
+        }
+        // counting select: rank = #smaller squared distances + #equal ones with a smaller index
         for (int e = lane; e < n; e += 32) {
             const uint32_t de = S.d2[e];
             int rank = 0, eq = 0;
@@ -208,6 +300,7 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
         __syncwarp();
         return min(n, K);
     }
+    if (G.stats && lane == 0) atomicAdd(&G.stats[4], 1ULL);
     return -1;
 }
 

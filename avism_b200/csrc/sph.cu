@@ -634,6 +634,9 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
     AV_CUDA(cudaGetLastError());
 }
 
+// per-bin starting radius (and half-width) from the learned proposal (proposal.cu)
+void proposal_predict(Ctx &c, const KnnGrid &G, const float4 *sv, int64_t n, float *r0, float *w0);
+
 void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G &a) {
     const int nx = L.g.nx;
     const int64_t nc = (int64_t)nx * nx * nx;
@@ -669,6 +672,10 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
         const float occ = occ_env ? (float)atof(occ_env) : 2.0f;
         BinnedParticles bp = bin_particles(c, a.n, a.x, a.y, a.z, p->lado0, p->periodic, occ);
         KnnGrid G = make_knn_grid(bp);
+        if (c.knn_stats) {
+            G.stats = c.get_t<unsigned long long>(B_KNN_STATS, 8);
+            AV_CUDA(cudaMemsetAsync(G.stats, 0, 8 * sizeof(unsigned long long), c.stream));
+        }
         const int64_t n1 = std::max<int64_t>(a.n, 1);
         float4 *sv = c.get_t<float4>(B_SV, n1);
         float *pd_s = c.get_t<float>(B_PDENS_S, n1), *hp_s = c.get_t<float>(B_HPART_S, n1);
@@ -678,8 +685,16 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
             ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, pd_s);
         }
         c.mark("bin_particles");
-        if (p->learned) {
-            // radius-guided search: a starting radius per bin
+        if (p->learned == 1) {
+            // learned proposal: starting kNN radius per bin from the MLP
+            const int64_t nbins = (int64_t)bp.nb * bp.nb * bp.nb;
+            float *r0 = c.get_t<float>(B_PR_R0, nbins);
+            float *w0 = c.get_t<float>(B_PR_W0, nbins);
+            proposal_predict(c, G, sv, a.n, r0, w0);
+            G.r0 = r0;
+            c.mark("proposal");
+        } else if (p->learned == 2) {
+            // hand-made proposal: a starting radius per bin from the local bin density
             const int64_t nbins = (int64_t)bp.nb * bp.nb * bp.nb;
             float *r0 = c.get_t<float>(B_KNN_R0, nbins);
             const char *fac_env = getenv("AVISM_TUNE_RFAC");

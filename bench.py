@@ -9,7 +9,10 @@ README thresholds.  Synthetic, seeded (1004 + rank).
 
 A step is one pass of the whole level on the GPU: kNN / SPH particle-to-grid,
 normalisation, divergence, flags, candidate ordering, cube growth, merging and
-post-processing, ending with the catalogue on the host.
+post-processing, ending with the catalogue on the host.  The timed path is the
+learned one (params.learned = 1: the trained MLP proposes every bin's starting
+kNN radius); the plain path (learned = 0) is timed beside it and must give the
+identical catalogue.
   value  -- inputs already resident in HBM (device pointers through the C-ABI)
   e2e    -- the same call with pinned host buffers: H2D of the particles and the
             D2H of the catalogue inside the timed region
@@ -185,11 +188,16 @@ def run_reference(a):
 ALG_BYTES = {
     # per cell query: the k neighbours' (x,y,z,m,vx,vy,vz,rho) are compulsory once per
     # particle; per cell 3 velocity components written, per particle h read+written
-    "cells_knn": lambda n, nc: 36 * n + 8 * n + 12 * nc,
-    "ppart_dens": lambda n, nc: 20 * n + 4 * n,
-    "ddens_scatter": lambda n, nc: 24 * n + 16 * nc,
-    "fill_h_zeros": lambda n, nc: 20 * n,
+    "cells_knn": lambda n, nc, ne3: 36 * n + 8 * n + 12 * nc,
+    "ppart_dens": lambda n, nc, ne3: 20 * n + 4 * n,
+    "ddens_scatter": lambda n, nc, ne3: 24 * n + 16 * nc,
+    "fill_h_zeros": lambda n, nc, ne3: 20 * n,
+    # stencils: DIVER_UNIFORM reads 3 velocity grids and writes one; the flag
+    # stencil reads U1CO and DIVERCO and writes one byte per ext cell
+    "divergence": lambda n, nc, ne3: 16 * nc,
+    "flags": lambda n, nc, ne3: 9 * ne3,
 }
+HBM_STAGES = ("divergence", "flags")
 
 
 def run_ours(a):
@@ -202,9 +210,13 @@ def run_ours(a):
     rank, world, local = dist_setup(a.gpus)
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    from avism_b200 import proposal
     p = workload_params(a)
+    p.learned = 1
+    p_plain = workload_params(a)
     n = 2 ** a.log2n
     ncells = a.nx ** 3
+    ne3 = (a.nx + 2 * (a.nx // 8)) ** 3
     with torch.no_grad():
         parts = synth.lognormal_torch(n, min(a.nx, 512), a.box, -1.2, 1.0, 350.0, seed=1004 + rank, device=dev)
         parts = synth.to_reader_units(parts)
@@ -212,13 +224,14 @@ def run_ours(a):
     host_parts = {k: v.cpu().pin_memory() for k, v in dev_parts.items()}
     torch.cuda.synchronize()
     ctx = AvismGPU(local)
+    ctx.proposal_load(proposal.load_weights())    # the trained network (a model load, not timed)
 
-    def step(src):
-        return ctx.run_level(p, src, capacity=p.nvoid_max)
+    def step(src, prm=p):
+        return ctx.run_level(prm, src, capacity=prm.nvoid_max)
 
-    def timed(src, steps, warmup):
+    def timed(src, steps, warmup, prm=p):
         for _ in range(warmup):
-            step(src)
+            step(src, prm)
         barrier(world)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -226,7 +239,7 @@ def run_ours(a):
         stages = []
         e0.record()
         for _ in range(steps):
-            r = step(src)
+            r = step(src, prm)
             stages.append(ctx.stage_times())
         e1.record()
         torch.cuda.synchronize()
@@ -238,10 +251,16 @@ def run_ours(a):
     with sampler:
         ms_dev, res, stages, launches = timed(dev_parts, a.steps, a.warmup)
         ms_e2e, res_h, stages_h, _ = timed(host_parts, max(1, a.steps), 1)
+        ms_plain, res_p, stages_p, _ = timed(dev_parts, max(1, a.steps), 1, p_plain)
     ms_dev = max_over_ranks(ms_dev, world)
     ms_e2e = max_over_ranks(ms_e2e, world)
-    # the catalogue of both paths must be the same
-    same = all(np.array_equal(res["cat"][k], res_h["cat"][k]) for k in ("indice", "uvoid", "ncellv", "volnew", "gxc"))
+    ms_plain = max_over_ranks(ms_plain, world)
+    # host- and device-input runs, and the learned and plain paths, give one catalogue
+    cat_keys = ("indice", "uvoid", "ncellv", "volnew", "gxc", "gyc", "gzc", "eps", "ip", "umean", "mtot")
+    same = all(np.array_equal(res["cat"][k], res_h["cat"][k]) for k in cat_keys)
+    same_plain = (res["nvoid"] == res_p["nvoid"] and
+                  all(np.array_equal(res["cat"][k], res_p["cat"][k]) for k in cat_keys) and
+                  all(np.array_equal(res["cubes"][k], res_p["cubes"][k]) for k in res["cubes"]))
     value = world * ncells / (ms_dev / 1e3)
     e2e = world * ncells / (ms_e2e / 1e3)
     # per-stage mean device time (events on the library's stream)
@@ -252,8 +271,15 @@ def run_ours(a):
     dom = max((k for k in st if k in ALG_BYTES), key=lambda k: st[k])
     peaks = json.load(open(PEAKS)) if os.path.exists(PEAKS) else {}
     peak = peaks.get("hbm_gbs", 6650.0)
-    alg = ALG_BYTES[dom](n, ncells)
+    alg = ALG_BYTES[dom](n, ncells, ne3)
     achieved = alg / (st[dom] / 1e3) / 1e9
+    # the HBM-bound stencil stages against the same peak
+    stencils = {}
+    for k in HBM_STAGES:
+        if st.get(k, 0.0) > 0:
+            gbs = ALG_BYTES[k](n, ncells, ne3) / (st[k] / 1e3) / 1e9
+            stencils[k] = {"ms": round(st[k], 4), "alg_bytes": ALG_BYTES[k](n, ncells, ne3),
+                           "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
     nvoid = res["nvoid"]
     h2d = 7 * 4 * n
     d2h = nvoid * (17 * 4) + nvoid * (15 * 4 + 3 * 4)
@@ -275,8 +301,15 @@ def run_ours(a):
                 "cpu_baseline": cpu,
                 "clocks": sampler.summary(),
                 "gpu_launches": launches,
-                "catalogue": {"cubes": nvoid, "voids": res["cat"]["nvoidt"], "host_vs_device_identical": same},
-                "stages_ms": {k: round(v, 3) for k, v in st.items()}}
+                "catalogue": {"cubes": nvoid, "voids": res["cat"]["nvoidt"], "host_vs_device_identical": same,
+                              "learned_vs_plain_identical": same_plain},
+                "path": "learned (MLP starting kNN radius, params.learned = 1)",
+                "plain": {"ms_per_step": ms_plain, "value": world * ncells / (ms_plain / 1e3), "unit": "cells/s",
+                          "learned_speedup": ms_plain / ms_dev},
+                "roofline_stencils": stencils,
+                "stages_ms": {k: round(v, 3) for k, v in st.items()},
+                "stages_ms_plain": {k: round(statistics.mean(s_.get(k, 0.0) for s_ in stages_p), 3)
+                                    for k in stages_p[0].keys()}}
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

@@ -61,7 +61,7 @@ typedef struct avism_params {
     int32_t flag_dens_interp;   /* 0 TSC, 1 SPH                                   */
     int32_t level;              /* IR                                             */
     int32_t levmin;             /* LEVMIN                                         */
-    int32_t learned;            /* 0: plain search, 1: learned proposals          */
+    int32_t learned;            /* 0: plain search, 1: learned proposal, 2: density estimate */
     int32_t reserved[7];
 } avism_params;
 
@@ -190,6 +190,47 @@ int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n,
                         const float *vx, const float *vy, const float *vz,
                         const float *m, avism_cubes *cubes, int32_t *nvoid,
                         avism_voids *voids, float *meandens);
+
+/* Counters of the warp kNN in the last particles_to_grid / run_level call,
+ * collected while enabled (enable = 1 turns collection on for later calls, 0
+ * off): out[0] queries, [1] radius attempts, [2] candidates scanned, [3]
+ * candidates kept inside the radius, [4] queries that fell back to the shell
+ * search.  No reference counterpart (instrumentation of this library).        */
+int avism_gpu_knn_counters(avism_gpu_ctx *ctx, int enable, int64_t *out, int n);
+
+/* ---- learned proposal.  No reference counterpart: AVISM has no learned part.
+ *      A 12 -> 64 -> 64 -> 64 -> 2 ReLU MLP (BF16 weights, FP32 accumulation)
+ *      predicts, per particle bin, the K-th neighbour distance of a query in the
+ *      bin and the half-width of a cube grown from a centre in it, from 12
+ *      multi-scale features of the binned particles (density, velocity
+ *      divergence and density-gradient magnitude at 1, 2, 4 and 8 bins).  With
+ *      params.learned = 1 the kNN starts from the predicted radius; the search
+ *      grows or shrinks it until the neighbour list is verified, so results are
+ *      identical to learned = 0 (learned = 2 starts from a radius estimated from
+ *      the 27 surrounding bins' counts instead).
+ *      Parameter vector: AVISM_PROPOSAL_NPARAM floats, mu[12], sigma[12],
+ *      W1[64][12], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], W4[2][64],
+ *      b4[2], slack[2] (radius factor, half-width offset).                    */
+#define AVISM_PROPOSAL_NPARAM 9308
+/* weights used by learned = 1 calls on this context */
+int avism_gpu_proposal_load(avism_gpu_ctx *ctx, const float *params, int32_t nparam);
+/* features of every bin of the binning particles_to_grid uses (nb^3 rows of
+ * 12, bin index x fastest); feat may be NULL to query nb and the bin width bw */
+int avism_gpu_proposal_features(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x,
+                                const float *y, const float *z, const float *vx, const float *vy,
+                                const float *vz, const float *m, int64_t cap_rows, float *feat,
+                                int32_t *nb, float *bw);
+/* raw network outputs (nrows x 2) for explicit feature rows, on the tensor cores */
+int avism_gpu_proposal_infer(avism_gpu_ctx *ctx, int64_t nrows, const float *feat, const float *params,
+                             float *out);
+/* loss and gradient of one batch (all ns samples; target / mask ns x 2) */
+int avism_gpu_proposal_grad(avism_gpu_ctx *ctx, int64_t ns, const float *feat, const float *target,
+                            const float *mask, const float *params, float *grad, float *loss);
+/* Adam training on the GPU over random mini-batches; params in: initial, out:
+ * trained; loss_curve (nullable) receives one loss per step                   */
+int avism_gpu_proposal_train(avism_gpu_ctx *ctx, int64_t ns, const float *feat, const float *target,
+                             const float *mask, int32_t steps, int32_t batch, float lr, uint32_t seed,
+                             float *params, float *loss_curve);
 
 /* ---- kNN without allocation.  No reference counterpart: an extra form of
  *      avism_gpu_knn (same neighbours, same distances, bit for bit) for callers

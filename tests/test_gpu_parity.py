@@ -164,11 +164,13 @@ def test_run_level_deterministic(gpu, mock1):
 
 
 def test_catalogue_independent_of_binning(gpu, mock1, monkeypatch):
-    """The kNN is exact for any bin size and with the radius-guided start, so
-    the tuning knobs change timing only."""
+    """The kNN is exact for any bin size and for any starting radius (plain,
+    learned, density estimate), so these knobs change timing only."""
     p = Params(nx=64, periodic=1, lado0=100.0)
     base = gpu.run_level(p, mock1, capacity=100000)
-    variants = [("0.5", 0), ("4", 0), ("2", 1)]
+    from avism_b200 import proposal
+    gpu.proposal_load(proposal.load_weights())
+    variants = [("0.5", 0), ("4", 0), ("2", 1), ("1", 1), ("2", 2)]
     for occ, learned in variants:
         monkeypatch.setenv("AVISM_TUNE_OCC", occ)
         q = Params(nx=64, periodic=1, lado0=100.0, learned=learned)
