@@ -38,6 +38,8 @@ SIGNATURES = {
     "avism_gpu_proposal_grad": (C.c_int, [_c_void, _i64] + [_c_void] * 6),
     "avism_gpu_proposal_train": (C.c_int, [_c_void, _i64, _c_void, _c_void, _c_void, _i32, _i32, _f32,
                                            C.c_uint32, _c_void, _c_void]),
+    "avism_gpu_next_level": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 5),
+    "avism_gpu_run_sublevel": (C.c_int, [_c_void, _c_void, _i64] + [_c_void] * 9 + [_i32] + [_c_void] * 4),
     "avism_gpu_knn_noalloc": (C.c_int, [C.c_int, _c_void, _i64, _c_void, _c_void, _c_void, _f32, _i64,
                                         _c_void, _c_void, _c_void, _i32, _c_void, _c_void, C.c_char_p,
                                         _i32]),

@@ -222,6 +222,35 @@ class AvismGPU:
                                                 _vp(_f32(u1co_ext)), meandens, C.byref(vo.c)))
         return vo.view(nvoid)
 
+    # ---- voids-in-voids (src/avism.f90:2123-2157, 1670-1674) --------------------
+    def next_level(self, p: Params, nvoid, marca_ext, uvoid, req):
+        """(MARCAP2 ext grid of the next level, REQP) from this level's catalogue."""
+        pn = Params(**{**p.__dict__, "nx": 2 * p.nx, "level": p.level + 1})
+        gn, _ = grid_setup(pn)
+        out = np.zeros(gn.ne ** 3, np.int32)
+        rq = np.zeros(max(nvoid, 1), np.float32)
+        self._chk(self.lib.avism_gpu_next_level(self.h, C.byref(p.to_c()), nvoid,
+                                                _vp(np.ascontiguousarray(marca_ext, np.int32)),
+                                                _vp(np.ascontiguousarray(uvoid, np.int32)), _vp(_f32(req)),
+                                                _vp(out), _vp(rq)))
+        return out, rq[:nvoid]
+
+    def run_sublevel(self, p: Params, parts: dict, marcap_ext, reqp, want_marca=False, capacity=None):
+        g, _ = grid_setup(p)
+        cap = int(capacity or p.nvoid_max)
+        a = {k: _f32(parts[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        cubes = Cubes(cap)
+        vo = Voids(cap, g.ne if want_marca else None)
+        nv, md = C.c_int32(), C.c_float()
+        pc = p.to_c()
+        pc.nvoid_max = min(p.nvoid_max, cap)
+        rq = _f32(reqp)
+        self._chk(self.lib.avism_gpu_run_sublevel(
+            self.h, C.byref(pc), len(a["x"]), *(_vp(a[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")),
+            _vp(np.ascontiguousarray(marcap_ext, np.int32)), _vp(rq), len(rq), C.byref(cubes.c), C.byref(nv),
+            C.byref(vo.c), C.byref(md)))
+        return dict(cubes=cubes.view(nv.value), nvoid=nv.value, cat=vo.view(nv.value), meandens=md.value)
+
     # ---- whole level ------------------------------------------------------------
     def run_level(self, p: Params, parts: dict, want_marca=False, want_cubes=True, capacity=None):
         g, _ = grid_setup(p)

@@ -125,7 +125,7 @@ __global__ void k_inner_from_ext(int nx, int low1, int ne, const float *ext, flo
 
 P2G p2g_args(Ctx &c, const avism_params *p, const Level &L, int64_t n, const float *x, const float *y,
              const float *z, const float *vx, const float *vy, const float *vz, const float *m,
-             const int8_t *smask) {
+             const int8_t *smask, bool particle_out = true) {
     const size_t nb = sizeof(float) * (size_t)std::max<int64_t>(n, 1);
     const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
     P2G a;
@@ -142,8 +142,9 @@ P2G p2g_args(Ctx &c, const avism_params *p, const Level &L, int64_t n, const flo
     a.u2 = c.get_t<float>(B_U2, nc);
     a.u3 = c.get_t<float>(B_U3, nc);
     a.u4 = c.get_t<float>(B_U4, nc);
-    a.hpart = c.get_t<float>(B_HPART, std::max<int64_t>(n, 1));
-    a.part_dens = c.get_t<float>(B_PDENS, std::max<int64_t>(n, 1));
+    // per-particle outputs in input order, only when the caller wants them
+    a.hpart = particle_out ? c.get_t<float>(B_HPART, std::max<int64_t>(n, 1)) : nullptr;
+    a.part_dens = particle_out ? c.get_t<float>(B_PDENS, std::max<int64_t>(n, 1)) : nullptr;
     AV_CHECK(x && y && z && m && vx && vy && vz, AVISM_ERR_ARG, "null particle array");
     return a;
 }
@@ -374,7 +375,7 @@ int avism_gpu_particles_to_grid(avism_gpu_ctx *ctx, const avism_params *p, int64
     return guarded(ctx, [&](Ctx &c) {
         check_params(p);
         Level L = make_level(p);
-        P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, smask);
+        P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, smask, hpart || part_dens);
         particles_to_grid(c, p, L, a);
         const size_t gb = sizeof(float) * (size_t)L.g.nx * L.g.nx * L.g.nx;
         from_device(c, u_mass, a.u_mass, gb);
@@ -489,6 +490,91 @@ int avism_gpu_merge_post(avism_gpu_ctx *ctx, const avism_params *p, int32_t nvoi
     });
 }
 
+// a26: parent map of the next level, MARCAP(2NX)^3 = MARCA(coarse cell)
+// (src/avism.f90:2137-2157), extended to the next level's ghost shell as
+// MARCAP2 (src/avism.f90:1670-1674, INT_MAKE_PERIODIC src/num.f90:137-181)
+__global__ void k_next_marcap(int nx, int low1, int ne, const int32_t *__restrict__ marca, int nx2, int low1n,
+                              int ne2, int32_t *__restrict__ out) {
+    const int i2 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i2 >= ne2) return;
+    int c[3] = {i2 + low1n, (int)blockIdx.y + low1n, (int)blockIdx.z + low1n};
+    for (int a = 0; a < 3; a++) {
+        if (c[a] < 1) c[a] += nx2; else if (c[a] > nx2) c[a] -= nx2;
+        c[a] = (c[a] - 1) / 2 + 1;                  // INT((IX-1)/2.)+1
+    }
+    const int64_t e = (int64_t)(c[0] - low1) + (int64_t)ne * ((int64_t)(c[1] - low1) + (int64_t)ne * (c[2] - low1));
+    out[(int64_t)i2 + (int64_t)ne2 * (blockIdx.y + (int64_t)ne2 * blockIdx.z)] = marca[e];
+}
+
+int avism_gpu_next_level(avism_gpu_ctx *ctx, const avism_params *p, int32_t nvoid, const int32_t *marca_ext,
+                         const int32_t *uvoid, const float *req, int32_t *marcap_next_ext, float *reqp_next) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        AV_CHECK(nvoid >= 0 && marca_ext && marcap_next_ext && (nvoid == 0 || (uvoid && req && reqp_next)),
+                 AVISM_ERR_ARG, "next_level: null argument");
+        Level L = make_level(p);
+        avism_params pn = *p;
+        pn.nx = 2 * p->nx;
+        pn.level = p->level + 1;
+        Level Ln = make_level(&pn);
+        const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne, ne3n = (int64_t)Ln.g.ne * Ln.g.ne * Ln.g.ne;
+        AV_CHECK(Ln.g.ne < 65536 && Ln.g.nplus <= Ln.g.nx, AVISM_ERR_ARG, "next_level: grid too large");
+        const int32_t *m = (const int32_t *)to_device(c, B_MARCA, marca_ext, sizeof(int32_t) * (size_t)ne3);
+        int32_t *out = is_device_ptr(marcap_next_ext) ? marcap_next_ext
+                                                       : c.get_t<int32_t>(B_MARCAP, (size_t)ne3n);
+        const dim3 g((unsigned)((Ln.g.ne + 127) / 128), (unsigned)Ln.g.ne, (unsigned)Ln.g.ne);
+        ++c.launches, k_next_marcap<<<g, 128, 0, c.stream>>>(L.g.nx, L.g.low1, L.g.ne, m, Ln.g.nx, Ln.g.low1,
+                                                              Ln.g.ne, out);
+        AV_CUDA(cudaGetLastError());
+        from_device(c, marcap_next_ext, out, sizeof(int32_t) * (size_t)ne3n);
+        // REQP(IND) = REQ(IND) for the main voids (avism.f90:2140-2144), 0 elsewhere
+        if (nvoid > 0) {
+            std::vector<int32_t> uv(nvoid);
+            std::vector<float> rq(nvoid), rp(nvoid, 0.0f);
+            AV_CUDA(cudaMemcpyAsync(uv.data(), uvoid, sizeof(int32_t) * nvoid, cudaMemcpyDefault, c.stream));
+            AV_CUDA(cudaMemcpyAsync(rq.data(), req, sizeof(float) * nvoid, cudaMemcpyDefault, c.stream));
+            c.sync();
+            for (int32_t i = 0; i < nvoid; i++)
+                if (uv[i] == -1) rp[i] = rq[i];
+            AV_CUDA(cudaMemcpyAsync(reqp_next, rp.data(), sizeof(float) * nvoid, cudaMemcpyDefault, c.stream));
+        }
+        c.sync();
+    });
+}
+
+// a level below the first (voids-in-voids): as run_level, with the parent map
+// MARCAP2 and parent radii REQP of avism_gpu_next_level
+int avism_gpu_run_sublevel(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x, const float *y,
+                           const float *z, const float *vx, const float *vy, const float *vz, const float *m,
+                           const int32_t *marcap_ext, const float *reqp, int32_t nreqp, avism_cubes *cubes,
+                           int32_t *nvoid, avism_voids *voids, float *meandens) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        AV_CHECK(nvoid && voids && marcap_ext && nreqp >= 0 && (nreqp == 0 || reqp), AVISM_ERR_ARG,
+                 "run_sublevel: null argument");
+        Level L = make_level(p);
+        const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
+        const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
+        P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, nullptr, false);
+        const int32_t *mp = (const int32_t *)to_device(c, B_MARCAP, marcap_ext, sizeof(int32_t) * (size_t)ne3);
+        const float *rq = nreqp > 0 ? (const float *)to_device(c, B_REQP, reqp, sizeof(float) * (size_t)nreqp) : nullptr;
+        c.mark("h2d");
+        particles_to_grid(c, p, L, a);
+        float *u1 = c.get_t<float>(B_U1CO, nc), *dv = c.get_t<float>(B_DIVER, nc);
+        FieldsOut fo = fields_inner(c, p, L, a.u_mass, a.u2, a.u3, a.u4, u1, dv);
+        c.mark("divergence");
+        CubesDev cd{};
+        const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, mp, rq, nreqp, cd);
+        HostCubes hc(c, cd, nv);
+        if (cubes) cubes_out(c, cd, nv, cubes);
+        c.mark("cubes_d2h");
+        merge_post(c, p, L, nv, &hc.v, u1, fo.meandens, voids, voids->marca);
+        c.mark("catalogue_d2h");
+        *nvoid = nv;
+        if (meandens) *meandens = fo.meandens;
+    });
+}
+
 int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x, const float *y,
                         const float *z, const float *vx, const float *vy, const float *vz, const float *m,
                         avism_cubes *cubes, int32_t *nvoid, avism_voids *voids, float *meandens) {
@@ -497,7 +583,7 @@ int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, co
         AV_CHECK(nvoid && voids, AVISM_ERR_ARG, "run_level: null argument");
         Level L = make_level(p);
         const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
-        P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, nullptr);
+        P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, nullptr, false);
         c.mark("h2d");
         particles_to_grid(c, p, L, a);
         float *u1 = c.get_t<float>(B_U1CO, nc), *dv = c.get_t<float>(B_DIVER, nc);

@@ -182,8 +182,11 @@ struct BinnedParticles {
     const int64_t *start = nullptr;  // nb^3 + 1 offsets
 };
 
+// sv (nullable): receives (vx, vy, vz, m) in binned order
 BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y, const float *z,
-                              float box, int periodic, float occupancy);
+                              float box, int periodic, float occupancy, const float *vx = nullptr,
+                              const float *vy = nullptr, const float *vz = nullptr, const float *m = nullptr,
+                              float4 *sv = nullptr);
 
 void knn_batch(Ctx &c, const BinnedParticles &bp, int64_t nq, const float *qx, const float *qy,
                const float *qz, int k, int64_t *idx_out, float *dist_out);
@@ -193,7 +196,7 @@ struct P2G {
     int64_t n;
     const float *x, *y, *z, *vx, *vy, *vz, *m;
     float *u_mass, *u2, *u3, *u4;    // inner NX^3
-    float *hpart, *part_dens;        // per particle
+    float *hpart, *part_dens;        // per particle, input order; null when not wanted
     const int8_t *smask;             // inner NX^3 or null
 };
 void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G &a);

@@ -30,14 +30,19 @@ __global__ void k_bin_keys(int64_t n, const float *__restrict__ x, const float *
     vals[i] = (int32_t)i;
 }
 
+// binned records (x, y, z, original index) and, when sv is given, the
+// attributes (vx, vy, vz, m) in the same order
 __global__ void k_bin_gather(int64_t n, const uint32_t *__restrict__ keys, const int32_t *__restrict__ vals,
                              const float *__restrict__ x, const float *__restrict__ y,
                              const float *__restrict__ z, float4 *__restrict__ sp,
-                             int64_t *__restrict__ start, int64_t nbins) {
+                             int64_t *__restrict__ start, int64_t nbins, const float *__restrict__ vx = nullptr,
+                             const float *__restrict__ vy = nullptr, const float *__restrict__ vz = nullptr,
+                             const float *__restrict__ m = nullptr, float4 *__restrict__ sv = nullptr) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int32_t v = vals[i];
     sp[i] = make_float4(x[v], y[v], z[v], __int_as_float(v));
+    if (sv) sv[i] = make_float4(vx[v], vy[v], vz[v], m[v]);
     const int64_t cur = keys[i];
     const int64_t prev = i == 0 ? -1 : (int64_t)keys[i - 1];
     for (int64_t b = prev + 1; b <= cur; b++) start[b] = i;
@@ -51,7 +56,8 @@ __global__ void k_empty_start(int64_t *start, int64_t nbins) {
 }
 
 BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y, const float *z,
-                              float box, int periodic, float occupancy) {
+                              float box, int periodic, float occupancy, const float *vx, const float *vy,
+                              const float *vz, const float *m, float4 *sv) {
     BinnedParticles bp;
     bp.n = n;
     bp.periodic = periodic;
@@ -85,7 +91,7 @@ BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y,
     void *t = c.get(B_CUB_TMP, tmp);
     AV_CUDA(cub::DeviceRadixSort::SortPairs(t, tmp, dk, dv, (int)n, 0, end_bit, c.stream));
     ++c.launches, k_bin_gather<<<grid_for(n, 256), 256, 0, c.stream>>>(n, dk.Current(), dv.Current(), x, y, z, sp,
-                                                           start, nbins);
+                                                           start, nbins, vx, vy, vz, m, sv);
     AV_CUDA(cudaGetLastError());
     return bp;
 }

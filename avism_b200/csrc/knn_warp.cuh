@@ -14,6 +14,8 @@
 // therefore only a starting point: the neighbour lists do not depend on it.
 #pragma once
 
+#include <climits>
+
 #include "knn_core.cuh"
 
 namespace avism {
@@ -231,18 +233,20 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
             int nseg;
             const int T = wq_rows(G, b, qx, qy, qz, R2, prune, lx, hx, ly, ny, lz, nrows, rbase, S.seg_start,
                                   S.seg_end, &nseg);
+            int k0 = 0;                                  // first segment ending after this chunk's start
             for (int cb = 0; cb < T; cb += 32) {
                 const int g = cb + lane;
+                // segment of candidate g = number of segment ends <= g: the ends in
+                // [cb, cb + 31] as one OR-reduced mask (ends are distinct, so at most 32)
+                const int e = k0 + lane < nseg ? S.seg_end[k0 + lane] : INT_MAX;
+                const unsigned endmask = __reduce_or_sync(0xffffffffu, e - cb <= 31 ? 1u << (e - cb) : 0u);
+                const int seg = k0 + __popc(endmask & ((2u << lane) - 1u));
+                k0 += __popc(endmask);
                 bool pass = false;
                 uint32_t d2b = 0, p = 0;
                 if (g < T) {
-                    int lo = 0, hi = nseg - 1;           // first segment whose end exceeds g
-                    while (lo < hi) {
-                        const int mid = (lo + hi) >> 1;
-                        if (S.seg_end[mid] > g) hi = mid; else lo = mid + 1;
-                    }
-                    const int begin = lo == 0 ? 0 : S.seg_end[lo - 1];
-                    p = S.seg_start[lo] + (uint32_t)(g - begin);
+                    const int begin = seg == 0 ? 0 : S.seg_end[seg - 1];
+                    p = S.seg_start[seg] + (uint32_t)(g - begin);
                     const float4 v = G.sp[p];
                     const float d2 = dist2_ref(v.x, v.y, v.z, qx, qy, qz, G.box, G.periodic);
                     pass = d2 <= R2;

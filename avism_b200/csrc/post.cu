@@ -9,8 +9,8 @@
 //    applied by one relabel pass instead of a WHERE per void);
 //  * VOID_SHAPE inertia sums, JACOBI / SORT on the host (src/shape.f90);
 //  * SIMPLE_CONNECTION_FAST as union-find connected components of the non-void
-//    cells: everything not connected to the LOW1 corner is a hole, filled with
-//    the id of the first void cell in +x;
+//    cells (shared-memory tiles, then the tile faces): everything not connected
+//    to the LOW1 corner is a hole, filled with the id of the first void cell in +x;
 //  * VOID_PERIODIC: overlap counts of every outer-centred void computed in one
 //    pass, then validated in catalogue order on the host; a void whose inputs
 //    an earlier merge could have changed is recounted on the device;
@@ -111,9 +111,19 @@ __global__ void k_inertia(PostGrid G, const int32_t *marca, const float *rad, in
             t[5] = -__fmul_rn(r1, r2);
         }
     }
+    if (__all_sync(0xffffffffu, m == 0)) return;            // no void cell in this warp
     const unsigned grp = __match_any_sync(0xffffffffu, m);
     const int lane = threadIdx.x & 31;
     const int leader = __ffs(grp) - 1;
+    if (__all_sync(0xffffffffu, grp == 0xffffffffu)) {
+        // one label in the whole warp: a shuffle tree in FP64
+        for (int q = 0; q < 6; q++) {
+            double s = (double)t[q];
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) atomicAdd(&inert[(size_t)(m - 1) * 6 + q], s);
+        }
+        return;
+    }
     for (int q = 0; q < 6; q++) {
         // sum in lane order inside the group
         double s = 0.0;
@@ -146,20 +156,102 @@ __device__ __forceinline__ void uf_union(int32_t *P, int32_t a, int32_t b) {
         a = old;
     }
 }
-__global__ void k_ccl_init(int64_t ne3, const int32_t *marca, int32_t *P) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < ne3) P[e] = marca[e] > 0 ? -1 : (int32_t)e;
+// Union-find in shared memory over one CL_TX x CL_TY x CL_TZ tile, then every
+// non-void cell points at its tile component's smallest cell (global index);
+// k_ccl_border joins components across the tiles' low faces.  Local and
+// global indices are both (z, y, x)-lexicographic, so the local minimum is the
+// global minimum and parents keep pointing to smaller indices.
+constexpr int CL_TX = 16, CL_TY = 8, CL_TZ = 8, CL_N = CL_TX * CL_TY * CL_TZ, CL_THREADS = 256;
+
+__device__ __forceinline__ int32_t luf_find(int32_t *L, int32_t x) {
+    volatile int32_t *V = L;
+    while (true) {                                  // path halving, as uf_find
+        const int32_t px = V[x];
+        if (px == x) return x;
+        const int32_t ppx = V[px];
+        if (ppx != px) V[x] = ppx;
+        x = px;
+    }
 }
-__global__ void k_ccl_union(PostGrid G, int32_t *P) {
+__device__ __forceinline__ void luf_union(int32_t *L, int32_t a, int32_t b) {
+    while (true) {
+        a = luf_find(L, a);
+        b = luf_find(L, b);
+        if (a == b) return;
+        if (a < b) { const int32_t t = a; a = b; b = t; }
+        const int32_t old = atomicCAS(&L[a], a, b);
+        if (old == a) return;
+        a = old;
+    }
+}
+
+__global__ void __launch_bounds__(CL_THREADS) k_ccl_local(PostGrid G, const int32_t *__restrict__ marca,
+                                                          int32_t *__restrict__ P) {
+    __shared__ int32_t L[CL_N];
+    const int ne = G.ne;
+    const int ntx = (ne + CL_TX - 1) / CL_TX, nty = (ne + CL_TY - 1) / CL_TY;
+    const int bx = (int)(blockIdx.x % ntx), by = (int)((blockIdx.x / ntx) % nty), bz = (int)(blockIdx.x / (ntx * nty));
+    const int X0 = bx * CL_TX, Y0 = by * CL_TY, Z0 = bz * CL_TZ;
+    auto gidx = [&](int li) -> int64_t {
+        const int x = X0 + li % CL_TX, y = Y0 + (li / CL_TX) % CL_TY, z = Z0 + li / (CL_TX * CL_TY);
+        if (x >= ne || y >= ne || z >= ne) return -1;
+        return (int64_t)x + (int64_t)ne * (y + (int64_t)ne * z);
+    };
+    for (int li = threadIdx.x; li < CL_N; li += CL_THREADS) {
+        const int64_t e = gidx(li);
+        L[li] = (e >= 0 && marca[e] <= 0) ? li : -1;
+    }
+    __syncthreads();
+    // x-runs of non-void cells point at their first cell
+    int32_t start[CL_N / CL_THREADS];
+#pragma unroll
+    for (int q = 0; q < CL_N / CL_THREADS; q++) {
+        const int li = threadIdx.x + q * CL_THREADS;
+        int r = li;
+        if (L[li] >= 0)
+            while (r % CL_TX > 0 && L[r - 1] >= 0) r--;
+        start[q] = r;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < CL_N / CL_THREADS; q++) {
+        const int li = threadIdx.x + q * CL_THREADS;
+        if (L[li] >= 0) L[li] = start[q];
+    }
+    __syncthreads();
+    for (int li = threadIdx.x; li < CL_N; li += CL_THREADS) {
+        if (L[li] < 0) continue;
+        const int ly = (li / CL_TX) % CL_TY, lz = li / (CL_TX * CL_TY);
+        if (ly > 0 && L[li - CL_TX] >= 0) luf_union(L, li, li - CL_TX);
+        if (lz > 0 && L[li - CL_TX * CL_TY] >= 0) luf_union(L, li, li - CL_TX * CL_TY);
+    }
+    __syncthreads();
+    for (int li = threadIdx.x; li < CL_N; li += CL_THREADS) {
+        const int64_t e = gidx(li);
+        if (e < 0) continue;
+        int32_t r = li;
+        if (L[li] < 0) {
+            P[e] = -1;
+            continue;
+        }
+        while (L[r] != r) r = L[r];
+        P[e] = (int32_t)gidx(r);
+    }
+}
+
+__global__ void k_ccl_border(PostGrid G, int32_t *P) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int ne = G.ne;
     const int64_t ne3 = (int64_t)ne * ne * ne;
-    if (e >= ne3 || P[e] < 0) return;
+    if (e >= ne3) return;
     const int i = (int)(e % ne), j = (int)((e / ne) % ne), k = (int)(e / ((int64_t)ne * ne));
-    if (i > 0 && P[e - 1] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - 1));
-    if (j > 0 && P[e - ne] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - ne));
-    if (k > 0 && P[e - (int64_t)ne * ne] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - (int64_t)ne * ne));
+    const bool fx = i > 0 && i % CL_TX == 0, fy = j > 0 && j % CL_TY == 0, fz = k > 0 && k % CL_TZ == 0;
+    if (!(fx || fy || fz) || P[e] < 0) return;
+    if (fx && P[e - 1] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - 1));
+    if (fy && P[e - ne] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - ne));
+    if (fz && P[e - (int64_t)ne * ne] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - (int64_t)ne * ne));
 }
+
 // root of x without path compression: a compressing find racing with another
 // thread's final store could leave that cell pointing at a non-root ancestor
 __device__ __forceinline__ int32_t uf_root(const int32_t *P, int32_t x) {
@@ -252,8 +344,22 @@ __global__ void k_final_props(PostGrid G, const int32_t *marca, const int32_t *u
             mt = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(u, meandens), dx), dx), dx), rete3);
         }
     }
+    if (__all_sync(0xffffffffu, m == 0)) return;            // no void cell in this warp
     const unsigned grp = __match_any_sync(0xffffffffu, m);
     const int lane = threadIdx.x & 31;
+    if (__all_sync(0xffffffffu, grp == 0xffffffffu)) {
+        double su = (double)u, sm = (double)mt;
+        for (int o = 16; o > 0; o >>= 1) {
+            su += __shfl_xor_sync(0xffffffffu, su, o);
+            sm += __shfl_xor_sync(0xffffffffu, sm, o);
+        }
+        if (lane == 0) {
+            atomicAdd(&ncell[m - 1], 32);
+            atomicAdd(&sums[(size_t)(m - 1) * 2], su);
+            atomicAdd(&sums[(size_t)(m - 1) * 2 + 1], sm);
+        }
+        return;
+    }
     double su = 0.0, sm = 0.0;
     for (int src = 0; src < 32; src++) {
         const float a = __shfl_sync(0xffffffffu, u, src), b = __shfl_sync(0xffffffffu, mt, src);
@@ -578,8 +684,9 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
     {
         int32_t *P = c.get_t<int32_t>(B_CCL, ne3);
         int32_t *m2 = c.get_t<int32_t>(B_PAINT, ne3);
-        ++c.launches, k_ccl_init<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, P);
-        ++c.launches, k_ccl_union<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, P);
+        const int64_t ntl = (int64_t)((ne + CL_TX - 1) / CL_TX) * ((ne + CL_TY - 1) / CL_TY) * ((ne + CL_TZ - 1) / CL_TZ);
+        ++c.launches, k_ccl_local<<<(unsigned)ntl, CL_THREADS, 0, c.stream>>>(PG, marca, P);
+        ++c.launches, k_ccl_border<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, P);
         ++c.launches, k_ccl_flatten<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, P);
         ++c.launches, k_fill_holes<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, P, marca, m2);
         AV_CUDA(cudaMemcpyAsync(marca, m2, (size_t)ne3 * 4, cudaMemcpyDeviceToDevice, c.stream));

@@ -9,6 +9,7 @@
 // independent, so the grid does not depend on thread timing.
 #include <cub/cub.cuh>
 #include <cfloat>
+#include <climits>
 
 #include "common.cuh"
 #include "knn_core.cuh"
@@ -68,7 +69,7 @@ k_ppart_dens(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float *
     const double pi = 3.141592653589793;     // DACOS(-1.D0)
     const float rho = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(hk, hk), hk)));
     pd_s[i] = rho;
-    part_dens[__float_as_int(p.w)] = rho;
+    if (part_dens) part_dens[__float_as_int(p.w)] = rho;
 }
 
 // ---- FILL_H_ZEROS: h = k-th neighbour distance where h is still 0 -----------
@@ -251,7 +252,7 @@ k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float
             const double pi = 3.141592653589793;     // DACOS(-1.D0)
             const float rho = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(hk, hk), hk)));
             pd_s[i] = rho;
-            part_dens[__float_as_int(p.w)] = rho;
+            if (part_dens) part_dens[__float_as_int(p.w)] = rho;
         }
     }
 }
@@ -586,7 +587,7 @@ static void run_sph_kernels_w(Ctx &c, const KnnGrid &G, const avism_params *p, c
             ++c.launches, k_fill_h<KC><<<grid_for(a.n, T), T, smc, c.stream>>>(G, a.n, K, hp_s);
         }
         c.mark("fill_h_zeros");
-        ++c.launches, k_unbin_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, G.sp, hp_s, a.hpart);
+        if (a.hpart) ++c.launches, k_unbin_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, G.sp, hp_s, a.hpart);
     }
     AV_CUDA(cudaGetLastError());
 }
@@ -629,7 +630,7 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
         c.mark("cells_ball");
         ++c.launches, k_fill_h<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, hp_s);
         c.mark("fill_h_zeros");
-        ++c.launches, k_unbin_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, G.sp, hp_s, a.hpart);
+        if (a.hpart) ++c.launches, k_unbin_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, G.sp, hp_s, a.hpart);
     }
     AV_CUDA(cudaGetLastError());
 }
@@ -658,8 +659,8 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
     float *rad_d = c.get_t<float>(B_RAD, L.rad.size());
     AV_CUDA(cudaMemcpyAsync(rad_d, L.rad.data(), L.rad.size() * sizeof(float), cudaMemcpyHostToDevice, c.stream));
     for (float *g : {a.u_mass, a.u2, a.u3, a.u4}) ++c.launches, k_zero_f32<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, g);
-    ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.hpart);
-    ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.part_dens);
+    if (a.hpart) ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.hpart);
+    if (a.part_dens) ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.part_dens);
     c.mark("p2g_setup");
     const bool vel_sph = p->flag_vel_interp == 1, dens_sph = p->flag_dens_interp == 1;
     TscArgs TA;
@@ -670,17 +671,17 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
     if (vel_sph || dens_sph) {
         const char *occ_env = getenv("AVISM_TUNE_OCC");
         const float occ = occ_env ? (float)atof(occ_env) : 2.0f;
-        BinnedParticles bp = bin_particles(c, a.n, a.x, a.y, a.z, p->lado0, p->periodic, occ);
+        const int64_t n1 = std::max<int64_t>(a.n, 1);
+        float4 *sv = c.get_t<float4>(B_SV, n1);
+        BinnedParticles bp = bin_particles(c, a.n, a.x, a.y, a.z, p->lado0, p->periodic, occ, a.vx, a.vy, a.vz,
+                                           a.m, sv);
         KnnGrid G = make_knn_grid(bp);
         if (c.knn_stats) {
             G.stats = c.get_t<unsigned long long>(B_KNN_STATS, 8);
             AV_CUDA(cudaMemsetAsync(G.stats, 0, 8 * sizeof(unsigned long long), c.stream));
         }
-        const int64_t n1 = std::max<int64_t>(a.n, 1);
-        float4 *sv = c.get_t<float4>(B_SV, n1);
         float *pd_s = c.get_t<float>(B_PDENS_S, n1), *hp_s = c.get_t<float>(B_HPART_S, n1);
         if (a.n > 0) {
-            ++c.launches, k_sorted_attrs<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, G.sp, a.vx, a.vy, a.vz, a.m, sv);
             ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, hp_s);
             ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, pd_s);
         }

@@ -232,6 +232,26 @@ int avism_gpu_proposal_train(avism_gpu_ctx *ctx, int64_t ns, const float *feat, 
                              const float *mask, int32_t steps, int32_t batch, float lr, uint32_t seed,
                              float *params, float *loss_curve);
 
+/* ---- a26: voids-in-voids.  The next level's parent map: MARCAP(2NX)^3 =
+ *      MARCA of the coarse cell and REQP = REQ of the main voids (replaces
+ *      src/avism.f90:2123-2157), extended over the next level's ghost shell as
+ *      MARCAP2 (src/avism.f90:1670-1674, INT_MAKE_PERIODIC src/num.f90:137-181).
+ *      p describes the current level; marca_ext is its final MARCA (ext grid),
+ *      uvoid / req its catalogue columns (nvoid entries).  marcap_next_ext
+ *      receives the ext grid of the level with 2*nx cells per side, reqp_next
+ *      nvoid radii (0 for voids that are not main voids).                      */
+int avism_gpu_next_level(avism_gpu_ctx *ctx, const avism_params *p, int32_t nvoid, const int32_t *marca_ext,
+                         const int32_t *uvoid, const float *req, int32_t *marcap_next_ext, float *reqp_next);
+/* A level below the first, particles in and catalogue out (as run_level), with
+ * the parent map and radii of avism_gpu_next_level: growth stays inside the
+ * parent voids (src/voidfinding.f90:34-36, 487-529).  In the reference only
+ * AMR input reaches this path (particle arrays are freed inside the level
+ * loop, src/avism.f90:1613-1629); here the particles are passed again.       */
+int avism_gpu_run_sublevel(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x, const float *y,
+                           const float *z, const float *vx, const float *vy, const float *vz, const float *m,
+                           const int32_t *marcap_ext, const float *reqp, int32_t nreqp, avism_cubes *cubes,
+                           int32_t *nvoid, avism_voids *voids, float *meandens);
+
 /* ---- kNN without allocation.  No reference counterpart: an extra form of
  *      avism_gpu_knn (same neighbours, same distances, bit for bit) for callers
  *      that cannot allocate device memory -- a host whose device memory is

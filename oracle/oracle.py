@@ -174,3 +174,36 @@ def run_level(p: Params, parts: dict):
     vf = voidfind(p, u1, dv)
     cat = merge_post(p, vf["nvoid"], vf["cubes"], u1, md)
     return dict(grid=pg, u1co=u1, diverco=dv, meandens=md, vf=vf, cat=cat)
+
+
+def next_level(p: Params, nvoid, marca_ext, uvoid, req):
+    """Parent map and radii of the next level (numpy restatement).
+
+    MARCAP(2NX)^3 = MARCA(INT((IX-1)/2.)+1, ...) and REQP(IND) = REQ(IND) for
+    main voids (src/avism.f90:2123-2157), then MARCAP2 = MARCAP on 1..2NX with
+    the periodic ghost shell of INT_MAKE_PERIODIC (src/avism.f90:1670-1674,
+    src/num.f90:137-181).  Returns (MARCAP2 flattened x-fastest, REQP)."""
+    g, _ = grid_setup(p)
+    pn = Params(**{**p.__dict__, "nx": 2 * p.nx, "level": p.level + 1})
+    gn, _ = grid_setup(pn)
+    ne, nx = g.ne, g.nx
+    m = np.asarray(marca_ext, np.int32).reshape(ne, ne, ne)          # [k][j][i]
+    lo = 1 - g.low1                                                   # offset of inner cell 1
+    inner = m[lo:lo + nx, lo:lo + nx, lo:lo + nx]
+    fine = inner.repeat(2, 0).repeat(2, 1).repeat(2, 2)                # MARCAP(2NX)^3
+    nx2 = 2 * nx
+    idx = (np.arange(gn.low1, gn.low2 + 1) - 1) % nx2                  # periodic ghost fill
+    ext = fine[np.ix_(idx, idx, idx)]
+    uv = np.asarray(uvoid, np.int32)[:nvoid]
+    rq = np.where(uv == -1, np.asarray(req, np.float32)[:nvoid], np.float32(0.0)).astype(np.float32)
+    return np.ascontiguousarray(ext).ravel(), rq
+
+
+def run_sublevel(p: Params, parts: dict, marcap_ext, reqp):
+    """A level below the first: particles -> catalogue with the parent map."""
+    pg = particles_to_grid(p, *(parts[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")))
+    u1, dv, md = fields(p, pg["u_mass"], pg["u2"], pg["u3"], pg["u4"])
+    vf = voidfind(p, u1, dv, marcap_ext=marcap_ext, reqp=reqp)
+    cat = merge_post(p, vf["nvoid"], vf["cubes"], u1, md)
+    return dict(u1co=u1, diverco=dv, meandens=md, vf=vf, cat=cat)
+

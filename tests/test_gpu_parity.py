@@ -212,3 +212,39 @@ def test_nvoid_max_matches_reference_stop(gpu, fields_pair):
             with pytest.raises(AvismError) as e:
                 gpu.voidfind(p, o[0], o[1], capacity=cap)
             assert e.value.code == 4
+
+
+def test_next_level_parent_map(gpu, mock1, oracle_mock1):
+    """a26: the next level's MARCAP2 and REQP from the level-0 catalogue."""
+    for per in (1, 0):
+        p = Params(nx=64, periodic=per, lado0=100.0)
+        o = oracle_mock1[per]
+        nv = o["vf"]["nvoid"]
+        mg, rg = gpu.next_level(p, nv, o["cat"]["marca"], o["cat"]["uvoid"], o["cat"]["req"])
+        mo, ro = O.next_level(p, nv, o["cat"]["marca"], o["cat"]["uvoid"], o["cat"]["req"])
+        assert np.array_equal(mg, mo) and np.array_equal(rg, ro)
+
+
+def test_voids_in_voids_two_levels(gpu):
+    """Level 0 at 32^3, then level 1 at 64^3 inside the level-0 voids, against
+    the oracle's same sequence (cubes and catalogue ids bit-exact)."""
+    from avism_b200 import synth
+    parts = synth.to_reader_units(synth.mock_spheres(n=2 ** 17, box=64.0, nsph=4, rmin=7.0, rmax=11.0, seed=77))
+    p0 = Params(nx=32, periodic=1, lado0=64.0, rmin=2.0, rmin_sub=2.0)
+    o0 = O.run_level(p0, parts)
+    g0 = gpu.run_level(p0, parts, capacity=100000, want_marca=True)
+    assert np.array_equal(g0["cat"]["marca"], o0["cat"]["marca"])
+    nv = o0["vf"]["nvoid"]
+    mp, rq = O.next_level(p0, nv, o0["cat"]["marca"], o0["cat"]["uvoid"], o0["cat"]["req"])
+    assert np.any(mp > 0)
+    p1 = Params(nx=64, periodic=1, lado0=64.0, rmin=2.0, rmin_sub=2.0, level=1)
+    o1 = O.run_sublevel(p1, parts, mp, rq)
+    g1 = gpu.run_sublevel(p1, parts, mp, rq, capacity=100000, want_marca=True)
+    assert g1["nvoid"] == o1["vf"]["nvoid"]
+    for k in g1["cubes"]:
+        assert np.array_equal(g1["cubes"][k], o1["vf"]["cubes"][k]), k
+    for k in ("indice", "uvoid", "ncellv", "marca", "volnew", "req", "gxc", "gyc", "gzc"):
+        assert np.array_equal(g1["cat"][k], o1["cat"][k]), k
+    # every level-1 cube grows inside a level-0 void
+    father = np.asarray(g1["cubes"]["father"])
+    assert np.all(father > 0)
