@@ -48,8 +48,11 @@ __device__ __forceinline__ float knn_uniform_radius(const KnnGrid &G, int K) {
 
 // One batch of up to 32 rows (row r = rbase + lane): write their particle
 // segments to smem and return the total number of candidates.
+// b in [-nb, 2nb): the bin it wraps to
+__device__ __forceinline__ int wrap_near(int b, int nb) { return b < 0 ? b + nb : (b >= nb ? b - nb : b); }
+
 __device__ __forceinline__ int wq_rows(const KnnGrid &G, const int b[3], float qx, float qy, float qz,
-                                       float R2, bool prune, int lx, int hx, int ly, int ny, int lz,
+                                       float R2, bool prune, int lx, int hx, int ly, int ny, float inv_ny, int lz,
                                        int nrows, int rbase, uint32_t *seg_start, int32_t *seg_end,
                                        int *nseg_out) {
     const int lane = threadIdx.x & 31;
@@ -57,7 +60,9 @@ __device__ __forceinline__ int wq_rows(const KnnGrid &G, const int b[3], float q
     uint32_t s0 = 0, s1 = 0;
     int l0 = 0, l1 = 0;
     if (r < nrows) {
-        const int dy = ly + r % ny, dz = lz + r / ny;
+        // r = ry + ny * rz; the float quotient is exact here (r, ny < 2^12)
+        const int rz = (int)(((float)r + 0.5f) * inv_ny);
+        const int dy = ly + (r - rz * ny), dz = lz + rz;
         bool keep = true;
         int xl = lx, xh = hx;
         if (prune) {
@@ -68,7 +73,9 @@ __device__ __forceinline__ int wq_rows(const KnnGrid &G, const int b[3], float q
             if (gz2 > R2 || yz2 > R2) {
                 keep = false;
             } else {
-                const float rx = __fadd_rn(__fsqrt_rn(__fsub_rn(R2, yz2)), G.margin);
+                // the reach only prunes (with the margin), so an approximate root does
+                const float rem = R2 - yz2;
+                const float rx = (rem > 0.0f ? rem * rsqrtf(rem) * 1.000001f : 0.0f) + G.margin;
                 const int cl = (int)floorf(__fmul_rn(__fsub_rn(__fsub_rn(qx, rx), G.origin), G.inv_bw));
                 const int ch = (int)floorf(__fmul_rn(__fsub_rn(__fadd_rn(qx, rx), G.origin), G.inv_bw));
                 // near the periodic seam the images' bins are not monotone in x: keep the window
@@ -79,15 +86,15 @@ __device__ __forceinline__ int wq_rows(const KnnGrid &G, const int b[3], float q
             }
         }
         if (keep && xl <= xh) {
-            const int bz = G.periodic ? wrap_bin(b[2] + dz, G.nb) : b[2] + dz;
-            const int by = G.periodic ? wrap_bin(b[1] + dy, G.nb) : b[1] + dy;
+            const int bz = G.periodic ? wrap_near(b[2] + dz, G.nb) : b[2] + dz;
+            const int by = G.periodic ? wrap_near(b[1] + dy, G.nb) : b[1] + dy;
             const int64_t row = (int64_t)G.nb * (by + (int64_t)G.nb * bz);
             const int bx0 = b[0] + xl, n = xh - xl + 1;
             if (!G.periodic) {
                 s0 = (uint32_t)G.start[row + bx0];
                 l0 = (int)(G.start[row + bx0 + n] - G.start[row + bx0]);
             } else {
-                const int w0 = wrap_bin(bx0, G.nb);
+                const int w0 = wrap_near(bx0, G.nb);
                 if (w0 + n <= G.nb) {
                     s0 = (uint32_t)G.start[row + w0];
                     l0 = (int)(G.start[row + w0 + n] - G.start[row + w0]);
@@ -117,84 +124,82 @@ __device__ __forceinline__ int wq_rows(const KnnGrid &G, const int b[3], float q
     return __shfl_sync(0xffffffffu, li, 31);
 }
 
-__device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int src) {
-    const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)v, src), hi = __shfl_sync(0xffffffffu, (uint32_t)(v >> 32), src);
-    return ((unsigned long long)hi << 32) | lo;
-}
-__device__ __forceinline__ unsigned long long shfl_xor_u64(unsigned long long v, int m) {
-    const uint32_t lo = __shfl_xor_sync(0xffffffffu, (uint32_t)v, m), hi = __shfl_xor_sync(0xffffffffu, (uint32_t)(v >> 32), m);
-    return ((unsigned long long)hi << 32) | lo;
-}
-// ascending bitonic sort of one key per lane
-__device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v) {
+// ascending bitonic sort of one (key, payload) per lane; equal keys keep their
+// lanes' order undefined (the caller detects equal squared distances)
+__device__ __forceinline__ void warp_sort32(uint32_t &key, uint32_t &val) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
         for (int j = k >> 1; j > 0; j >>= 1) {
-            const unsigned long long b = shfl_xor_u64(v, j);
+            const uint32_t bk = __shfl_xor_sync(0xffffffffu, key, j), bv = __shfl_xor_sync(0xffffffffu, val, j);
             const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
-            v = keep_min ? (b < v ? b : v) : (b > v ? b : v);
+            const bool take = keep_min ? bk < key : bk > key;
+            key = take ? bk : key;
+            val = take ? bv : val;
         }
     }
-    return v;
 }
-// the 32 smallest of two ascending 32-key lists, ascending
-__device__ __forceinline__ unsigned long long warp_merge32(unsigned long long a, unsigned long long b) {
+// the 32 smallest of two ascending 32-entry lists, ascending
+__device__ __forceinline__ void warp_merge32(uint32_t &ak, uint32_t &av, uint32_t bk, uint32_t bv) {
     const int lane = threadIdx.x & 31;
-    const unsigned long long br = shfl_u64(b, 31 - lane);
-    unsigned long long v = br < a ? br : a;                 // a bitonic sequence
+    const uint32_t rk = __shfl_sync(0xffffffffu, bk, 31 - lane), rv = __shfl_sync(0xffffffffu, bv, 31 - lane);
+    const bool t0 = rk < ak;                              // a bitonic sequence
+    ak = t0 ? rk : ak;
+    av = t0 ? rv : av;
 #pragma unroll
     for (int j = 16; j > 0; j >>= 1) {
-        const unsigned long long o = shfl_xor_u64(v, j);
-        v = (lane & j) == 0 ? (o < v ? o : v) : (o > v ? o : v);
+        const uint32_t ok = __shfl_xor_sync(0xffffffffu, ak, j), ov = __shfl_xor_sync(0xffffffffu, av, j);
+        const bool take = (lane & j) == 0 ? ok < ak : ok > ak;
+        ak = take ? ok : ak;
+        av = take ? ov : av;
     }
-    return v;
 }
 
-// The K <= 32 nearest of the n <= 128 kept candidates, ordered by (squared
-// distance, buffer slot) with warp bitonic sorts.  That is the exact order
+// The K <= 32 nearest of the n <= 128 kept candidates ordered by squared
+// distance with warp bitonic sorts on 32-bit keys.  That is the exact order
 // unless two of the selected -- or the K-th and a dropped one -- have the same
 // squared distance; then it returns false and the caller ranks exactly.
 template <int KMAX>
 __device__ __forceinline__ bool bitonic_select(const KnnGrid &G, int n, int K, WarpKnnSmem<KMAX> &S) {
     const int lane = threadIdx.x & 31;
-    unsigned long long k[4];
+    uint32_t k[4], v[4];
 #pragma unroll
-    for (int s = 0; s < 4; s++) {
-        const int e = s * 32 + lane;
-        k[s] = e < n ? (((unsigned long long)S.d2[e] << 32) | (unsigned)e) : ~0ULL;
+    for (int q = 0; q < 4; q++) {
+        const int e = q * 32 + lane;
+        k[q] = e < n ? S.d2[e] : 0xffffffffu;
+        v[q] = (uint32_t)e;
     }
     const int ns = (n + 31) >> 5;
-    k[0] = warp_sort32(k[0]);
+    warp_sort32(k[0], v[0]);
     if (ns > 1) {
-        k[1] = warp_sort32(k[1]);
-        k[0] = warp_merge32(k[0], k[1]);
+        warp_sort32(k[1], v[1]);
+        warp_merge32(k[0], v[0], k[1], v[1]);
     }
     if (ns > 2) {
-        k[2] = warp_sort32(k[2]);
+        warp_sort32(k[2], v[2]);
         if (ns > 3) {
-            k[3] = warp_sort32(k[3]);
-            k[2] = warp_merge32(k[2], k[3]);
+            warp_sort32(k[3], v[3]);
+            warp_merge32(k[2], v[2], k[3], v[3]);
         }
-        k[0] = warp_merge32(k[0], k[2]);
+        warp_merge32(k[0], v[0], k[2], v[2]);
     }
     const int m = min(n, K);
     // ties: equal squared distances among the first m, or beyond the m-th
-    const uint32_t d = (uint32_t)(k[0] >> 32);
+    const uint32_t d = k[0];
     const uint32_t dn = __shfl_down_sync(0xffffffffu, d, 1);
     const uint32_t dk = __shfl_sync(0xffffffffu, d, m - 1);
     bool tie = lane < m - 1 && d == dn;
     int le = 0;
 #pragma unroll
-    for (int s = 0; s < 4; s++) {
-        const int e = s * 32 + lane;
+    for (int q = 0; q < 4; q++) {
+        const int e = q * 32 + lane;
         le += __popc(__ballot_sync(0xffffffffu, e < n && S.d2[e] <= dk));
     }
     if (__any_sync(0xffffffffu, tie) || le > m) return false;
     if (lane < m) {
         S.res_d2[lane] = d;
-        S.res_pos[lane] = S.pos[(uint32_t)k[0]];
+        S.res_pos[lane] = S.pos[v[0]];
     }
     __syncwarp();
     return true;
@@ -223,6 +228,12 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
         axis_window(G, b[0], s, lx, hx);
         const int ny = hy - ly + 1, nz = hz - lz + 1;
         const int nrows = ny * nz;
+        const float inv_ny = 1.0f / (float)ny;
+        // no wrapped image inside the window: |dx| < L/2 for every candidate, so
+        // min(|dx|, L - |dx|) = |dx| and the plain distance has the same bits
+        const bool plain_d = !G.periodic || (b[0] + lx >= 0 && b[0] + hx < G.nb && b[1] + ly >= 0 &&
+                                             b[1] + hy < G.nb && b[2] + lz >= 0 && b[2] + hz < G.nb &&
+                                             4 * s + 2 <= G.nb);
         bool all_done;
         if (G.periodic) all_done = 2 * s + 1 >= G.nb;
         else all_done = b[0] + lx == 0 && b[0] + hx == G.nb - 1 && b[1] + ly == 0 && b[1] + hy == G.nb - 1 &&
@@ -231,8 +242,8 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
         int count = 0;
         for (int rbase = 0; rbase < nrows; rbase += 32) {
             int nseg;
-            const int T = wq_rows(G, b, qx, qy, qz, R2, prune, lx, hx, ly, ny, lz, nrows, rbase, S.seg_start,
-                                  S.seg_end, &nseg);
+            const int T = wq_rows(G, b, qx, qy, qz, R2, prune, lx, hx, ly, ny, inv_ny, lz, nrows, rbase,
+                                  S.seg_start, S.seg_end, &nseg);
             int k0 = 0;                                  // first segment ending after this chunk's start
             for (int cb = 0; cb < T; cb += 32) {
                 const int g = cb + lane;
@@ -248,7 +259,7 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
                     const int begin = seg == 0 ? 0 : S.seg_end[seg - 1];
                     p = S.seg_start[seg] + (uint32_t)(g - begin);
                     const float4 v = G.sp[p];
-                    const float d2 = dist2_ref(v.x, v.y, v.z, qx, qy, qz, G.box, G.periodic);
+                    const float d2 = dist2_ref(v.x, v.y, v.z, qx, qy, qz, G.box, plain_d ? 0 : 1);
                     pass = d2 <= R2;
                     d2b = __float_as_uint(d2);
                 }

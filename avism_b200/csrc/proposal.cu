@@ -98,7 +98,7 @@ __device__ __forceinline__ float4 pyr_at(const Pyramid &P, int l, int x, int y, 
     x = pyr_wrap(x, n, P.periodic);
     y = pyr_wrap(y, n, P.periodic);
     z = pyr_wrap(z, n, P.periodic);
-    return P.lev[l][x + (int64_t)n * (y + (int64_t)n * z)];
+    return P.lev[l][(uint32_t)x + (uint32_t)n * ((uint32_t)y + (uint32_t)n * (uint32_t)z)];
 }
 
 __global__ void k_counts(int64_t nb3, const float4 *__restrict__ lev0, float *__restrict__ cnt) {
@@ -106,13 +106,14 @@ __global__ void k_counts(int64_t nb3, const float4 *__restrict__ lev0, float *__
     if (b < nb3) cnt[b] = lev0[b].x;
 }
 
-// one separable pass of a (2w+1)-wide box sum along `axis` (wrapped or clamped)
+// one separable pass of a (2w+1)-wide box sum along `axis` (wrapped or
+// clamped); grid (ceil(nb / blockDim), nb, nb), x along threads
 __global__ void k_box_pass(int nb, int w, int axis, int periodic, const float *__restrict__ in,
                            float *__restrict__ out) {
-    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t nb3 = (int64_t)nb * nb * nb;
-    if (b >= nb3) return;
-    const int c[3] = {(int)(b % nb), (int)((b / nb) % nb), (int)(b / ((int64_t)nb * nb))};
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= nb) return;
+    const int c[3] = {x, (int)blockIdx.y, (int)blockIdx.z};
+    const int64_t b = (int64_t)x + (int64_t)nb * (blockIdx.y + (int64_t)nb * blockIdx.z);
     const int64_t stride = axis == 0 ? 1 : (axis == 1 ? nb : (int64_t)nb * nb);
     float s = 0.f;
     for (int d = -w; d <= w; d++) {
@@ -130,7 +131,7 @@ __device__ __forceinline__ float cbox_at(const Pyramid &P, int s, int nb, int x,
     x = pyr_wrap(x, nb, P.periodic);
     y = pyr_wrap(y, nb, P.periodic);
     z = pyr_wrap(z, nb, P.periodic);
-    return P.cbox[s][x + (int64_t)nb * (y + (int64_t)nb * z)];
+    return P.cbox[s][(uint32_t)x + (uint32_t)nb * ((uint32_t)y + (uint32_t)nb * (uint32_t)z)];
 }
 
 // The 12 features of bin (bx, by, bz): f0..f3 the log density of the centred
@@ -469,7 +470,10 @@ __global__ void k_features_tiles(Pyramid P, int nb, const float *__restrict__ mu
     const int64_t ntile_rows = (nb3 + TC_M - 1) / TC_M * TC_M;
     if (b >= ntile_rows) return;
     float f[PR_NF];
-    if (b < nb3) bin_features(P, nb, (int)(b % nb), (int)((b / nb) % nb), (int)(b / ((int64_t)nb * nb)), f);
+    if (b < nb3) {
+        const uint32_t u = (uint32_t)b, un = (uint32_t)nb, q = u / un;     // nb^3 < 2^32
+        bin_features(P, nb, (int)(u - q * un), (int)(q % un), (int)(q / un), f);
+    }
     __align__(16) __nv_bfloat16 v[16];
 #pragma unroll
     for (int k = 0; k < 16; k++) {
@@ -767,9 +771,10 @@ Pyramid build_pyramid(Ctx &c, const KnnGrid &G, const float4 *sv, int64_t n) {
     for (int s = 1; s < 4; s++) {
         float *out = c.get_t<float>(bid[s - 1], (size_t)nb3);
         const int w = box_w(s);
-        ++c.launches, k_box_pass<<<grid_for(nb3, 256), 256, 0, c.stream>>>(G.nb, w, 0, G.periodic, cnt, ta);
-        ++c.launches, k_box_pass<<<grid_for(nb3, 256), 256, 0, c.stream>>>(G.nb, w, 1, G.periodic, ta, tb);
-        ++c.launches, k_box_pass<<<grid_for(nb3, 256), 256, 0, c.stream>>>(G.nb, w, 2, G.periodic, tb, out);
+        const dim3 bg((unsigned)((G.nb + 127) / 128), (unsigned)G.nb, (unsigned)G.nb);
+        ++c.launches, k_box_pass<<<bg, 128, 0, c.stream>>>(G.nb, w, 0, G.periodic, cnt, ta);
+        ++c.launches, k_box_pass<<<bg, 128, 0, c.stream>>>(G.nb, w, 1, G.periodic, ta, tb);
+        ++c.launches, k_box_pass<<<bg, 128, 0, c.stream>>>(G.nb, w, 2, G.periodic, tb, out);
         P.cbox[s] = out;
     }
     // velocity scale of the divergence features: v_rms of the particles

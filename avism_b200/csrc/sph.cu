@@ -356,8 +356,9 @@ __global__ void k_ddens(KnnGrid G, int64_t n, DdensArgs A) {
     const float inv_h = __fdiv_rn(2.0f, h);
     const float h2max = __fmul_rn(__fmul_rn(4.0f, h), h);
     const int inc = (int)__fadd_rn(__fdiv_rn(__fmul_rn(2.0f, h), dx), 0.5f);
-    // only cells with Q < 2 carry weight; rows and planes beyond h are skipped
+    // only cells with Q <= 2 (d <= h) carry weight; rows and planes beyond h are skipped
     const float hh = h * h * 1.00002f + 1e-30f;
+    const float inv_dx = 1.0f / dx;
     const float *rad = A.rad - A.rad_lo;
     const float m = A.sv[i].w;
     const int k_lo = max(kz - inc, 1), k_hi = min(kz + inc, nx);
@@ -374,13 +375,16 @@ __global__ void k_ddens(KnnGrid G, int64_t n, DdensArgs A) {
                 const float dy2 = __fmul_rn(ty, ty);
                 const float rem = hh - dz2 - dy2;
                 if (rem < 0.0f) continue;
-                const float R = sqrtf(rem) * 1.00001f + 1e-6f * dx;
-                const int a = max(i_lo, (int)floorf((p.x - R - A.rx1) / dx) + 1 - 1);
-                const int e = min(i_hi, (int)ceilf((p.x + R - A.rx1) / dx) + 1 + 1);
+                // conservative x range (one spare cell each side absorbs the rounding
+                // of the approximate root and of the reciprocal)
+                const float R = (rem > 0.0f ? rem * rsqrtf(rem) : 0.0f) * 1.00001f + 1e-6f * dx;
+                const int a = max(i_lo, (int)floorf((p.x - R - A.rx1) * inv_dx) + 1 - 1);
+                const int e = min(i_hi, (int)ceilf((p.x + R - A.rx1) * inv_dx) + 1 + 1);
                 for (int i2 = a; i2 <= e; i2++) {
                     const float tx = __fsub_rn(p.x, rad[i2]);
                     const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), dy2), dz2);
-                    if (d2 > h2max) continue;
+                    // beyond the M4 support (d > h) the weight is exactly 0: skip the root
+                    if (d2 > hh || d2 > h2max) continue;
                     const float w = m4_q(d2, inv_h);
                     if (pass == 0) {
                         norm = __fadd_rn(norm, w);
