@@ -364,13 +364,22 @@ __global__ void k_ddens(KnnGrid G, int64_t n, DdensArgs A) {
     const int k_lo = max(kz - inc, 1), k_hi = min(kz + inc, nx);
     const int j_lo = max(jy - inc, 1), j_hi = min(jy + inc, nx);
     const int i_lo = max(ix - inc, 1), i_hi = min(ix + inc, nx);
+    // planes and rows that can meet the support, straight from its radius (one
+    // spare cell each side, as for the x range); everything else has weight 0
+    const float hr = (hh > 0.0f ? hh * rsqrtf(hh) : 0.0f) * 1.00001f + 1e-6f * dx;
+    const int k_a = max(k_lo, (int)floorf((p.z - hr - A.rx1) * inv_dx) + 1 - 1);
+    const int k_b = min(k_hi, (int)ceilf((p.z + hr - A.rx1) * inv_dx) + 1 + 1);
     float norm = 0.0f;
     for (int pass = 0; pass < 2; pass++) {
-        for (int k2 = k_lo; k2 <= k_hi; k2++) {
+        for (int k2 = k_a; k2 <= k_b; k2++) {
             const float tz = __fsub_rn(p.z, rad[k2]);
             const float dz2 = __fmul_rn(tz, tz);
             if (dz2 > hh) continue;
-            for (int j2 = j_lo; j2 <= j_hi; j2++) {
+            const float remz = hh - dz2;
+            const float ry = (remz > 0.0f ? remz * rsqrtf(remz) : 0.0f) * 1.00001f + 1e-6f * dx;
+            const int j_a = max(j_lo, (int)floorf((p.y - ry - A.rx1) * inv_dx) + 1 - 1);
+            const int j_b = min(j_hi, (int)ceilf((p.y + ry - A.rx1) * inv_dx) + 1 + 1);
+            for (int j2 = j_a; j2 <= j_b; j2++) {
                 const float ty = __fsub_rn(p.y, rad[j2]);
                 const float dy2 = __fmul_rn(ty, ty);
                 const float rem = hh - dz2 - dy2;
