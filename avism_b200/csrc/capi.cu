@@ -558,13 +558,15 @@ int avism_gpu_run_sublevel(avism_gpu_ctx *ctx, const avism_params *p, int64_t n,
         P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, nullptr, false);
         const int32_t *mp = (const int32_t *)to_device(c, B_MARCAP, marcap_ext, sizeof(int32_t) * (size_t)ne3);
         const float *rq = nreqp > 0 ? (const float *)to_device(c, B_REQP, reqp, sizeof(float) * (size_t)nreqp) : nullptr;
+        WidthProposal wp;
+        a.wprop = &wp;
         c.mark("h2d");
         particles_to_grid(c, p, L, a);
         float *u1 = c.get_t<float>(B_U1CO, nc), *dv = c.get_t<float>(B_DIVER, nc);
         FieldsOut fo = fields_inner(c, p, L, a.u_mass, a.u2, a.u3, a.u4, u1, dv);
         c.mark("divergence");
         CubesDev cd{};
-        const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, mp, rq, nreqp, cd);
+        const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, mp, rq, nreqp, cd, &wp);
         HostCubes hc(c, cd, nv);
         if (cubes) cubes_out(c, cd, nv, cubes);
         c.mark("cubes_d2h");
@@ -584,13 +586,15 @@ int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, co
         Level L = make_level(p);
         const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
         P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, nullptr, false);
+        WidthProposal wp;
+        a.wprop = &wp;
         c.mark("h2d");
         particles_to_grid(c, p, L, a);
         float *u1 = c.get_t<float>(B_U1CO, nc), *dv = c.get_t<float>(B_DIVER, nc);
         FieldsOut fo = fields_inner(c, p, L, a.u_mass, a.u2, a.u3, a.u4, u1, dv);
         c.mark("divergence");
         CubesDev cd{};
-        const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, nullptr, nullptr, 0, cd);
+        const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, nullptr, nullptr, 0, cd, &wp);
         HostCubes hc(c, cd, nv);
         if (cubes) cubes_out(c, cd, nv, cubes);
         c.mark("cubes_d2h");

@@ -191,6 +191,13 @@ BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y,
 void knn_batch(Ctx &c, const BinnedParticles &bp, int64_t nq, const float *qx, const float *qy,
                const float *qz, int k, int64_t *idx_out, float *dist_out);
 
+// per-bin proposed cube half-widths of the learned proposal, with the binning
+struct WidthProposal {
+    const float *w0 = nullptr;
+    int nb = 0, periodic = 0;
+    float origin = 0.f, inv_bw = 0.f, box = 0.f;
+};
+
 // particles -> grid (SPH/TSC).  All pointers are device pointers.
 struct P2G {
     int64_t n;
@@ -198,6 +205,7 @@ struct P2G {
     float *u_mass, *u2, *u3, *u4;    // inner NX^3
     float *hpart, *part_dens;        // per particle, input order; null when not wanted
     const int8_t *smask;             // inner NX^3 or null
+    WidthProposal *wprop = nullptr;  // receives the half-width proposal (learned = 1), nullable
 };
 void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G &a);
 
@@ -237,7 +245,7 @@ struct CubesDev {
 int32_t voidfind_device(Ctx &c, const avism_params *p, const Level &L, const float *u1,
                         const float *dv, int fields_are_ext, const int8_t *smask_ext,
                         const int32_t *marcap_ext, const float *reqp, int32_t nreqp,
-                        CubesDev &cubes);
+                        CubesDev &cubes, const WidthProposal *wp = nullptr);
 
 // merge + post-processing; cubes in host memory (copied), outputs host arrays
 void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nvoid,

@@ -367,33 +367,43 @@ __global__ void k_ddens(KnnGrid G, int64_t n, DdensArgs A) {
     // planes and rows that can meet the support, straight from its radius (one
     // spare cell each side, as for the x range); everything else has weight 0
     const float hr = (hh > 0.0f ? hh * rsqrtf(hh) : 0.0f) * 1.00001f + 1e-6f * dx;
-    const int k_a = max(k_lo, (int)floorf((p.z - hr - A.rx1) * inv_dx) + 1 - 1);
-    const int k_b = min(k_hi, (int)ceilf((p.z + hr - A.rx1) * inv_dx) + 1 + 1);
+    int k_a = max(k_lo, (int)floorf((p.z - hr - A.rx1) * inv_dx) + 1 - 1);
+    int k_b = min(k_hi, (int)ceilf((p.z + hr - A.rx1) * inv_dx) + 1 + 1);
+    // trim the spare planes: the support is convex and RADX monotone, so only
+    // the ends can lie outside it (dz^2 > hh, weight 0 everywhere)
+    auto dz2_of = [&](int k2) { const float t = __fsub_rn(p.z, rad[k2]); return __fmul_rn(t, t); };
+    while (k_a <= k_b && dz2_of(k_a) > hh) k_a++;
+    while (k_b >= k_a && dz2_of(k_b) > hh) k_b--;
     float norm = 0.0f;
     for (int pass = 0; pass < 2; pass++) {
         for (int k2 = k_a; k2 <= k_b; k2++) {
-            const float tz = __fsub_rn(p.z, rad[k2]);
-            const float dz2 = __fmul_rn(tz, tz);
-            if (dz2 > hh) continue;
+            const float dz2 = dz2_of(k2);
             const float remz = hh - dz2;
             const float ry = (remz > 0.0f ? remz * rsqrtf(remz) : 0.0f) * 1.00001f + 1e-6f * dx;
-            const int j_a = max(j_lo, (int)floorf((p.y - ry - A.rx1) * inv_dx) + 1 - 1);
-            const int j_b = min(j_hi, (int)ceilf((p.y + ry - A.rx1) * inv_dx) + 1 + 1);
+            int j_a = max(j_lo, (int)floorf((p.y - ry - A.rx1) * inv_dx) + 1 - 1);
+            int j_b = min(j_hi, (int)ceilf((p.y + ry - A.rx1) * inv_dx) + 1 + 1);
+            auto rem_of = [&](int j2) { const float t = __fsub_rn(p.y, rad[j2]); return hh - dz2 - __fmul_rn(t, t); };
+            while (j_a <= j_b && rem_of(j_a) < 0.0f) j_a++;
+            while (j_b >= j_a && rem_of(j_b) < 0.0f) j_b--;
             for (int j2 = j_a; j2 <= j_b; j2++) {
                 const float ty = __fsub_rn(p.y, rad[j2]);
                 const float dy2 = __fmul_rn(ty, ty);
                 const float rem = hh - dz2 - dy2;
-                if (rem < 0.0f) continue;
                 // conservative x range (one spare cell each side absorbs the rounding
-                // of the approximate root and of the reciprocal)
+                // of the approximate root and of the reciprocal), then trimmed to the
+                // cells inside the support: d^2 <= hh (beyond it the weight is exactly 0)
                 const float R = (rem > 0.0f ? rem * rsqrtf(rem) : 0.0f) * 1.00001f + 1e-6f * dx;
-                const int a = max(i_lo, (int)floorf((p.x - R - A.rx1) * inv_dx) + 1 - 1);
-                const int e = min(i_hi, (int)ceilf((p.x + R - A.rx1) * inv_dx) + 1 + 1);
+                int a = max(i_lo, (int)floorf((p.x - R - A.rx1) * inv_dx) + 1 - 1);
+                int e = min(i_hi, (int)ceilf((p.x + R - A.rx1) * inv_dx) + 1 + 1);
+                auto d2_of = [&](int i2) {
+                    const float t = __fsub_rn(p.x, rad[i2]);
+                    return __fadd_rn(__fadd_rn(__fmul_rn(t, t), dy2), dz2);
+                };
+                while (a <= e && d2_of(a) > hh) a++;
+                while (e >= a && d2_of(e) > hh) e--;
                 for (int i2 = a; i2 <= e; i2++) {
-                    const float tx = __fsub_rn(p.x, rad[i2]);
-                    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), dy2), dz2);
-                    // beyond the M4 support (d > h) the weight is exactly 0: skip the root
-                    if (d2 > hh || d2 > h2max) continue;
+                    const float d2 = d2_of(i2);
+                    if (d2 > h2max) continue;            // never, as hh < h2max; kept as in the reference
                     const float w = m4_q(d2, inv_h);
                     if (pass == 0) {
                         norm = __fadd_rn(norm, w);
@@ -706,6 +716,14 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
             float *w0 = c.get_t<float>(B_PR_W0, nbins);
             proposal_predict(c, G, sv, a.n, r0, w0);
             G.r0 = r0;
+            if (a.wprop) {
+                a.wprop->w0 = w0;
+                a.wprop->nb = bp.nb;
+                a.wprop->periodic = bp.periodic;
+                a.wprop->origin = bp.origin;
+                a.wprop->inv_bw = bp.inv_bw;
+                a.wprop->box = bp.box;
+            }
             c.mark("proposal");
         } else if (p->learned == 2) {
             // hand-made proposal: a starting radius per bin from the local bin density

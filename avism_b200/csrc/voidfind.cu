@@ -16,6 +16,7 @@
 #include <cub/cub.cuh>
 
 #include "common.cuh"
+#include "knn_core.cuh"
 
 namespace avism {
 
@@ -36,6 +37,10 @@ struct VfArgs {
     uint8_t *cover;             // ext grid: covered by a cube accepted in an earlier window
     unsigned long long *umin;   // ext grid: (epoch, rank) min of open cubes
     unsigned long long *amin;   // ext grid: (window, rank) min of this window's accepted cubes
+    // learned proposal of the half-width (per particle bin), or null
+    const float *w0;
+    int nb, periodic_bins;
+    float rx1, dx, bin_origin, inv_bw, box;
 };
 
 __device__ __forceinline__ int32_t rank_pos(const VfArgs &A, int32_t r) {
@@ -81,6 +86,54 @@ __device__ bool faces_pass_warp(const VfArgs &A, const int c[3], int w, int32_t 
     return true;
 }
 
+// First shell in 0..cap whose faces fail, or cap + 1: every face cell of the
+// cube of half-width cap checked at once.  A cell at Chebyshev distance d lies
+// on the face of shell d along each axis where its offset is +-d (all six
+// directions for the centre), and is checked there exactly as faces_pass_warp
+// checks it; the first failing shell is the smallest failing d.
+__device__ int first_failing_shell(const VfArgs &A, const int c[3], int cap, int32_t indv, int lane) {
+    const int side = 2 * cap + 1;
+    const int64_t total = (int64_t)side * side * side;
+    int fail = cap + 1;
+    for (int64_t t = lane; t < total; t += 32) {
+        const int o[3] = {(int)(t % side) - cap, (int)((t / side) % side) - cap, (int)(t / ((int64_t)side * side)) - cap};
+        const int d = max(abs(o[0]), max(abs(o[1]), abs(o[2])));
+        if (d >= fail) continue;
+        const int cell[3] = {c[0] + o[0], c[1] + o[1], c[2] + o[2]};
+        const uint8_t fc = A.flags[eidx(A, cell[0], cell[1], cell[2])];
+        bool ok = true;
+        for (int a = 0; a < 3 && ok; a++) {
+            for (int s = -1; s <= 1 && ok; s += 2) {
+                if (d > 0 ? o[a] != s * d : false) continue;
+                int nb[3] = {cell[0], cell[1], cell[2]};
+                nb[a] += s;
+                const int64_t en = eidx(A, nb[0], nb[1], nb[2]);
+                const int bit = 1 + 2 * a + (s > 0 ? 1 : 0);
+                const int32_t mp = A.marcap ? A.marcap[en] : -1;
+                ok = (A.flags[en] & 0x80) && mp == indv && !(fc & (1u << bit));
+            }
+        }
+        if (!ok) fail = d;
+    }
+    return __reduce_min_sync(0xffffffffu, fail);
+}
+
+// proposed half-width for the centre cell c: the bin of its position
+__device__ __forceinline__ int proposed_width(const VfArgs &A, const int c[3]) {
+    if (!A.w0) return 0;
+    int b[3];
+    for (int a = 0; a < 3; a++) {
+        float x = A.rx1 + (float)(c[a] - 1) * A.dx;
+        if (A.periodic_bins) {
+            if (x < A.bin_origin) x += A.box;
+            else if (x >= A.bin_origin + A.box) x -= A.box;
+        }
+        b[a] = bin_coord(x, A.bin_origin, A.inv_bw, A.nb);
+    }
+    const float w = A.w0[b[0] + (int64_t)A.nb * (b[1] + (int64_t)A.nb * b[2])];
+    return w > 0.0f ? min((int)w, 64) : 0;
+}
+
 // Phase 1: drop edge / covered candidates of the window, grow the others.
 __global__ void k_phase1(VfArgs A, int32_t r0, int32_t r1, int32_t *open_list, int32_t *n_open) {
     const int lane = threadIdx.x & 31;
@@ -103,6 +156,15 @@ __global__ void k_phase1(VfArgs A, int32_t r0, int32_t r1, int32_t *open_list, i
         if (indv > 0 && A.reqp && indv <= A.nreqp && A.reqp[indv - 1] < A.rmin_sub) flag1 = true;
         bool f2 = false;
         if (!flag1) {
+            // with a proposed half-width, shells 0..cap are checked in one sweep
+            // (cap stops short of the first shell that touches the edge region)
+            int cap = proposed_width(A, c);
+            for (int a = 0; a < 3; a++)
+                cap = min(cap, min(c[a] - (A.low1 + 1), (A.low2 - 1) - c[a]) - 1);
+            if (cap > 0) {
+                const int f = first_failing_shell(A, c, cap, indv, lane);
+                w = min(f, cap);           // shells below w pass; the loop resumes at w
+            }
             for (;;) {
                 if (!faces_pass_warp(A, c, w, indv, lane)) break;
                 w++;
@@ -269,7 +331,7 @@ __global__ void k_nvoid_check(const uint8_t *st, const int32_t *ids, int32_t nra
 
 int32_t voidfind_device(Ctx &c, const avism_params *p, const Level &L, const float *u1, const float *dv,
                         int fields_are_ext, const int8_t *smask_ext, const int32_t *marcap_ext,
-                        const float *reqp, int32_t nreqp, CubesDev &cubes) {
+                        const float *reqp, int32_t nreqp, CubesDev &cubes, const WidthProposal *wp) {
     const int ne = L.g.ne;
     const int64_t ne3 = (int64_t)ne * ne * ne;
     AV_CHECK(ne3 < (int64_t)INT32_MAX, AVISM_ERR_ARG, "ext grid larger than 2^31 cells");
@@ -280,6 +342,11 @@ int32_t voidfind_device(Ctx &c, const avism_params *p, const Level &L, const flo
     VfArgs A;
     A.low1 = L.g.low1; A.low2 = L.g.low2; A.ne = ne; A.nx = L.g.nx; A.ext = fields_are_ext;
     A.flags = flags; A.marcap = marcap_ext; A.reqp = reqp; A.nreqp = nreqp; A.rmin_sub = p->rmin_sub;
+    A.w0 = nullptr;
+    if (wp && wp->w0) {
+        A.w0 = wp->w0; A.nb = wp->nb; A.periodic_bins = wp->periodic; A.bin_origin = wp->origin;
+        A.inv_bw = wp->inv_bw; A.box = wp->box; A.rx1 = L.rad_at(1); A.dx = L.g.dx;
+    }
 
     // candidates in K,J,I order
     int32_t *pos = c.get_t<int32_t>(B_CAND_POS, ne3);
