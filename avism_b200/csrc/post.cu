@@ -307,11 +307,20 @@ __global__ void k_bbox(PostGrid G, const int32_t *marca, int32_t *bb /* 6 per la
 // shifted-cell overlap counts of every outer-centred void against its IND2;
 // labmap maps stored labels to the current ones (identity for the first pass);
 // only_label > 0 restricts the pass to one (current) label
+// (box: when bdim[0] > 0 only the cells of the box starting at ext offsets
+// blo are visited -- the bounding box of the one label being recounted)
 __global__ void k_periodic_counts(PostGrid G, const int32_t *marca, const int32_t *labmap, const int8_t *shift,
-                                  const int32_t *ind2, int32_t only_label, int32_t *cnt /* 2 per label */) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+                                  const int32_t *ind2, int32_t only_label, int32_t *cnt /* 2 per label */,
+                                  int3 blo = make_int3(0, 0, 0), int3 bdim = make_int3(0, 0, 0)) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int ne = G.ne;
-    if (e >= (int64_t)ne * ne * ne) return;
+    if (bdim.x > 0) {
+        if (e >= (int64_t)bdim.x * bdim.y * bdim.z) return;
+        const int bx = (int)(e % bdim.x), by = (int)((e / bdim.x) % bdim.y), bz = (int)(e / ((int64_t)bdim.x * bdim.y));
+        e = (int64_t)(blo.x + bx) + (int64_t)ne * ((blo.y + by) + (int64_t)ne * (blo.z + bz));
+    } else if (e >= (int64_t)ne * ne * ne) {
+        return;
+    }
     int32_t m = marca[e];
     if (m <= 0) return;
     m = labmap[m];
@@ -809,7 +818,15 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
                     int32_t *i2d = dev_upload<int32_t>(c, B_RED1, i2v.data(), nvs);
                     int32_t *one = c.get_t<int32_t>(B_RED2, (size_t)nvs * 2);
                     AV_CUDA(cudaMemsetAsync(one + (size_t)(ind - 1) * 2, 0, 8, c.stream));
-                    ++c.launches, k_periodic_counts<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, lm_d, sh_d, i2d, ind, one);
+                    // the label's cells lie in its bounding box (merges extend it)
+                    const auto &bx = curbb[ind];
+                    if (bx[0] <= bx[3]) {
+                        const int3 blo = make_int3(bx[0] - g.low1, bx[1] - g.low1, bx[2] - g.low1);
+                        const int3 bd = make_int3(bx[3] - bx[0] + 1, bx[4] - bx[1] + 1, bx[5] - bx[2] + 1);
+                        const int64_t nbox = (int64_t)bd.x * bd.y * bd.z;
+                        ++c.launches, k_periodic_counts<<<grid_for(nbox, 256), 256, 0, c.stream>>>(
+                            PG, marca, lm_d, sh_d, i2d, ind, one, blo, bd);
+                    }
                     int32_t r2[2];
                     dev_download(c, r2, one + (size_t)(ind - 1) * 2, 2);
                     counter = r2[0];

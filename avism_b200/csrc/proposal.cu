@@ -139,15 +139,18 @@ __device__ __forceinline__ float cbox_at(const Pyramid &P, int s, int nb, int x,
 // density gradient over +-max(w, 1) bins; f8..f11 the velocity divergence of
 // the pyramid cells of 1, 2, 4, 8 bins, in units of v_rms / bw.
 __device__ void bin_features(const Pyramid &P, int nb, int bx, int by, int bz, float f[PR_NF]) {
+    // features only steer where a search starts, so fast intrinsics are used;
+    // training and inference share this function
+    const float inv_occ = 1.0f / P.occ;
 #pragma unroll
     for (int s = 0; s < 4; s++) {
         const int w = box_w(s), sp = w > 0 ? w : 1;
-        const float vol = P.occ * (float)((2 * w + 1) * (2 * w + 1) * (2 * w + 1));
-        f[s] = logf(0.05f + cbox_at(P, s, nb, bx, by, bz) / vol);
+        const float inv_vol = inv_occ / (float)((2 * w + 1) * (2 * w + 1) * (2 * w + 1));
+        f[s] = __logf(0.05f + cbox_at(P, s, nb, bx, by, bz) * inv_vol);
         const float gx = cbox_at(P, s, nb, bx + sp, by, bz) - cbox_at(P, s, nb, bx - sp, by, bz);
         const float gy = cbox_at(P, s, nb, bx, by + sp, bz) - cbox_at(P, s, nb, bx, by - sp, bz);
         const float gz = cbox_at(P, s, nb, bx, by, bz + sp) - cbox_at(P, s, nb, bx, by, bz - sp);
-        f[4 + s] = sqrtf(gx * gx + gy * gy + gz * gz) / (2.f * (float)sp * vol);
+        f[4 + s] = sqrtf(gx * gx + gy * gy + gz * gz) * (inv_vol * (0.5f / (float)sp));
     }
 #pragma unroll
     for (int l = 0; l < PR_LEVELS; l++) {
@@ -158,10 +161,10 @@ __device__ void bin_features(const Pyramid &P, int nb, int bx, int by, int bz, f
             const float4 p = pyr_at(P, l, x + d[a][0], y + d[a][1], z + d[a][2]);
             const float4 m = pyr_at(P, l, x - d[a][0], y - d[a][1], z - d[a][2]);
             const float vp = a == 0 ? p.y : a == 1 ? p.z : p.w, vm = a == 0 ? m.y : a == 1 ? m.z : m.w;
-            const float up = p.x > 0.f ? vp / p.x : 0.f, um = m.x > 0.f ? vm / m.x : 0.f;
-            div += (up - um) / (2.f * (float)(1 << l));
+            const float up = p.x > 0.f ? __fdividef(vp, p.x) : 0.f, um = m.x > 0.f ? __fdividef(vm, m.x) : 0.f;
+            div += up - um;
         }
-        f[8 + l] = div * P.inv_vscale;
+        f[8 + l] = div * (P.inv_vscale * (0.5f / (float)(1 << l)));
     }
 }
 

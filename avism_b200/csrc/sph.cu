@@ -257,8 +257,10 @@ k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float
     }
 }
 
+// five blocks per SM (48 registers): the cell kernel gains more from the extra
+// warps than it loses to spills (the particle kernel does not)
 template <int KMAX>
-__global__ void __launch_bounds__(SPH_WARPS * 32)
+__global__ void __launch_bounds__(SPH_WARPS * 32, 5)
 k_cells_knn_w(KnnGrid G, CellArgs A) {
     extern __shared__ __align__(16) unsigned char wq_smem[];
     WarpKnnSmem<KMAX> &S = reinterpret_cast<WarpKnnSmem<KMAX> *>(wq_smem)[threadIdx.x >> 5];
