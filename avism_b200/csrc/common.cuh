@@ -58,6 +58,7 @@ enum BufId : int {
     B_FLAGS_IN,                                    // flag bytes of the periodic inner grid
     B_PR_CNT, B_PR_BOX1, B_PR_BOX2, B_PR_BOX4,     // centred box counts of the bins
     B_PR_TMPA, B_PR_TMPB,
+    B_PX4, B_PV4,                                  // packed (x, y, z, m), (vx, vy, vz, 0) in input order
     B_NUM
 };
 

@@ -164,71 +164,4 @@ void merge_cubes_host(const MergeIn &in, MergeOut &out) {
     out.nvoid2 = nvoid2;
 }
 
-// ---- JACOBI / SORT of src/shape.f90 (REAL*4 with the REAL*8 literal promotions)
-void jacobi3_ref(float a[3][3], float d[3]) {
-    const int n = 3;
-    float b[3], z[3];
-    for (int ip = 0; ip < n; ip++) { b[ip] = a[ip][ip]; d[ip] = b[ip]; z[ip] = 0.0f; }
-    for (int it = 1; it <= 50; it++) {
-        float sm = 0.0f;
-        for (int ip = 0; ip < n - 1; ip++)
-            for (int iq = ip + 1; iq < n; iq++) sm = sm + std::fabs(a[ip][iq]);
-        if (sm == 0.0f) return;
-        const float tresh = it < 4 ? (float)(0.2 * (double)(sm * sm)) : 0.0f;
-        for (int ip = 0; ip < n - 1; ip++)
-            for (int iq = ip + 1; iq < n; iq++) {
-                const float g = (float)(100.0 * (double)std::fabs(a[ip][iq]));
-                if (it > 4 && std::fabs(d[ip]) + g == std::fabs(d[ip]) && std::fabs(d[iq]) + g == std::fabs(d[iq])) {
-                    a[ip][iq] = 0.0f;
-                    continue;
-                }
-                if (!(std::fabs(a[ip][iq]) > tresh)) continue;
-                float h = d[iq] - d[ip];
-                float t;
-                if (std::fabs(h) + g == std::fabs(h)) {
-                    t = a[ip][iq] / h;
-                } else {
-                    const float theta = (float)(0.5 * (double)h / (double)a[ip][iq]);
-                    t = (float)(1.0 / ((double)std::fabs(theta) + std::sqrt(1.0 + (double)(theta * theta))));
-                    if (theta < 0.0f) t = -t;
-                }
-                const float c = (float)(1.0 / std::sqrt(1.0 + (double)(t * t)));
-                const float s = t * c;
-                const float tau = (float)((double)s / (1.0 + (double)c));
-                h = t * a[ip][iq];
-                z[ip] = z[ip] - h;
-                z[iq] = z[iq] + h;
-                d[ip] = d[ip] - h;
-                d[iq] = d[iq] + h;
-                a[ip][iq] = 0.0f;
-                for (int j = 0; j < ip; j++) {
-                    const float gg = a[j][ip], hh = a[j][iq];
-                    a[j][ip] = gg - s * (hh + gg * tau);
-                    a[j][iq] = hh + s * (gg - hh * tau);
-                }
-                for (int j = ip + 1; j < iq; j++) {
-                    const float gg = a[ip][j], hh = a[j][iq];
-                    a[ip][j] = gg - s * (hh + gg * tau);
-                    a[j][iq] = hh + s * (gg - hh * tau);
-                }
-                for (int j = iq + 1; j < n; j++) {
-                    const float gg = a[ip][j], hh = a[iq][j];
-                    a[ip][j] = gg - s * (hh + gg * tau);
-                    a[iq][j] = hh + s * (gg - hh * tau);
-                }
-            }
-        for (int ip = 0; ip < n; ip++) { b[ip] = b[ip] + z[ip]; d[ip] = b[ip]; z[ip] = 0.0f; }
-    }
-}
-
-void sort_desc3_ref(float d[3]) {
-    for (int i = 0; i < 2; i++) {
-        int k = i;
-        float p = d[i];
-        for (int j = i + 1; j < 3; j++)
-            if (d[j] >= p) { k = j; p = d[j]; }
-        if (k != i) { d[k] = d[i]; d[i] = p; }
-    }
-}
-
 }  // namespace avism

@@ -34,7 +34,5 @@ struct MergeOut {
 };
 
 void merge_cubes_host(const MergeIn &in, MergeOut &out);
-void jacobi3_ref(float a[3][3], float d[3]);
-void sort_desc3_ref(float d[3]);
 
 }  // namespace avism

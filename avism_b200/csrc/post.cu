@@ -135,6 +135,108 @@ __global__ void k_inertia(PostGrid G, const int32_t *marca, const float *rad, in
     }
 }
 
+// ---- VOID_SHAPE axes: one thread per main void (src/shape.f90:198-232) -----
+// JACOBI (src/shape.f90:46-134, Numerical Recipes) and SORT (src/shape.f90:2-29)
+// in REAL*4 with the REAL*8 promotions of their literals.  The library is built
+// with --fmad=false and IEEE division and square roots, so every operation
+// rounds as the Fortran's does.
+__device__ void jacobi3(float a[3][3], float d[3]) {
+    const int n = 3;
+    float b[3], z[3];
+    for (int ip = 0; ip < n; ip++) { b[ip] = a[ip][ip]; d[ip] = b[ip]; z[ip] = 0.0f; }
+    for (int it = 1; it <= 50; it++) {
+        float sm = 0.0f;
+        for (int ip = 0; ip < n - 1; ip++)
+            for (int iq = ip + 1; iq < n; iq++) sm = sm + fabsf(a[ip][iq]);
+        if (sm == 0.0f) return;
+        const float tresh = it < 4 ? (float)(0.2 * (double)(sm * sm)) : 0.0f;
+        for (int ip = 0; ip < n - 1; ip++)
+            for (int iq = ip + 1; iq < n; iq++) {
+                const float g = (float)(100.0 * (double)fabsf(a[ip][iq]));
+                if (it > 4 && fabsf(d[ip]) + g == fabsf(d[ip]) && fabsf(d[iq]) + g == fabsf(d[iq])) {
+                    a[ip][iq] = 0.0f;
+                    continue;
+                }
+                if (!(fabsf(a[ip][iq]) > tresh)) continue;
+                float h = d[iq] - d[ip];
+                float t;
+                if (fabsf(h) + g == fabsf(h)) {
+                    t = a[ip][iq] / h;
+                } else {
+                    const float theta = (float)(0.5 * (double)h / (double)a[ip][iq]);
+                    t = (float)(1.0 / ((double)fabsf(theta) + sqrt(1.0 + (double)(theta * theta))));
+                    if (theta < 0.0f) t = -t;
+                }
+                const float c = (float)(1.0 / sqrt(1.0 + (double)(t * t)));
+                const float s = t * c;
+                const float tau = (float)((double)s / (1.0 + (double)c));
+                h = t * a[ip][iq];
+                z[ip] = z[ip] - h;
+                z[iq] = z[iq] + h;
+                d[ip] = d[ip] - h;
+                d[iq] = d[iq] + h;
+                a[ip][iq] = 0.0f;
+                for (int j = 0; j < ip; j++) {
+                    const float gg = a[j][ip], hh = a[j][iq];
+                    a[j][ip] = gg - s * (hh + gg * tau);
+                    a[j][iq] = hh + s * (gg - hh * tau);
+                }
+                for (int j = ip + 1; j < iq; j++) {
+                    const float gg = a[ip][j], hh = a[j][iq];
+                    a[ip][j] = gg - s * (hh + gg * tau);
+                    a[j][iq] = hh + s * (gg - hh * tau);
+                }
+                for (int j = iq + 1; j < n; j++) {
+                    const float gg = a[ip][j], hh = a[iq][j];
+                    a[ip][j] = gg - s * (hh + gg * tau);
+                    a[iq][j] = hh + s * (gg - hh * tau);
+                }
+            }
+        for (int ip = 0; ip < n; ip++) { b[ip] = b[ip] + z[ip]; d[ip] = b[ip]; z[ip] = 0.0f; }
+    }
+}
+
+__device__ __forceinline__ void sort_desc3(float d[3]) {
+    for (int i = 0; i < 2; i++) {
+        int k = i;
+        float p = d[i];
+        for (int j = i + 1; j < 3; j++)
+            if (d[j] >= p) { k = j; p = d[j]; }
+        if (k != i) { d[k] = d[i]; d[i] = p; }
+    }
+}
+
+
+__global__ void k_void_axes(int32_t nv, const int32_t *__restrict__ uvoid, const int32_t *__restrict__ ncellv,
+                            const double *__restrict__ inert, float dx, double pi, float *__restrict__ eps,
+                            float *__restrict__ ipv) {
+    const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nv) return;
+    float e = 0.0f, ip = 0.0f;
+    if (uvoid[v] == -1) {
+        const double *s = &inert[(size_t)v * 6];
+        const float n = (float)ncellv[v];
+        float a[3][3];
+        a[0][0] = (float)s[0] / n; a[1][1] = (float)s[1] / n; a[2][2] = (float)s[2] / n;
+        a[0][1] = a[1][0] = (float)s[3] / n;
+        a[0][2] = a[2][0] = (float)s[4] / n;
+        a[1][2] = a[2][1] = (float)s[5] / n;
+        float ev[3] = {0.0f, 0.0f, 0.0f}, ax[3];
+        jacobi3(a, ev);
+        ax[0] = sqrtf(2.5f * fabsf((ev[1] + ev[2]) - ev[0]));
+        ax[1] = sqrtf(2.5f * fabsf((ev[2] + ev[0]) - ev[1]));
+        ax[2] = sqrtf(2.5f * fabsf((ev[0] + ev[1]) - ev[2]));
+        sort_desc3(ax);
+        e = 1.0f - ax[2] / ax[0];
+        const float volm = (((float)ncellv[v] * dx) * dx) * dx;
+        const float vell = (float)(((((double)(4.0f / 3.0f) * pi) * (double)ax[0]) * (double)ax[1]) * (double)ax[2]);
+        ip = volm / vell;
+        if (ip > 1.0f) { ip = -99.0f; e = -99.0f; }
+    }
+    eps[v] = e;
+    ipv[v] = ip;
+}
+
 // ---- SIMPLE_CONNECTION_FAST: union-find of non-void cells --------------------
 __device__ __forceinline__ int32_t uf_find(int32_t *P, int32_t x) {
     while (true) {
@@ -631,33 +733,16 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         AV_CUDA(cudaMemcpyAsync(gc_d + 2 * nvs, mo.gzc.data(), sizeof(float) * nv, cudaMemcpyHostToDevice, c.stream));
         double *in_d = c.get_t<double>(B_SCAN_A, (size_t)nvs * 6);
         AV_CUDA(cudaMemsetAsync(in_d, 0, sizeof(double) * 6 * (size_t)nvs, c.stream));
+        c.mark("shape_setup");
         ++c.launches, k_inertia<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, rad_d, g.rad_lo, gc_d, gc_d + nvs, gc_d + 2 * nvs, in_d);
-        std::vector<double> inert((size_t)nvs * 6);
-        dev_download(c, inert.data(), in_d, (size_t)nv * 6);
-        for (int32_t I = 0; I < nv; I++) {
-            const int32_t ind = indice[I];
-            if (uvoid[ind - 1] != -1) continue;
-            const double *s = &inert[(size_t)(ind - 1) * 6];
-            const float n = (float)ncellv[ind - 1];
-            float a[3][3];
-            a[0][0] = (float)s[0] / n; a[1][1] = (float)s[1] / n; a[2][2] = (float)s[2] / n;
-            a[0][1] = a[1][0] = (float)s[3] / n;
-            a[0][2] = a[2][0] = (float)s[4] / n;
-            a[1][2] = a[2][1] = (float)s[5] / n;
-            float ev[3] = {0.0f, 0.0f, 0.0f}, ax[3];
-            jacobi3_ref(a, ev);
-            ax[0] = std::sqrt(2.5f * std::fabs((ev[1] + ev[2]) - ev[0]));
-            ax[1] = std::sqrt(2.5f * std::fabs((ev[2] + ev[0]) - ev[1]));
-            ax[2] = std::sqrt(2.5f * std::fabs((ev[0] + ev[1]) - ev[2]));
-            sort_desc3_ref(ax);
-            float e = 1.0f - ax[2] / ax[0];
-            const float volm = (((float)ncellv[ind - 1] * dx) * dx) * dx;
-            const float vell = (float)(((((double)(4.0f / 3.0f) * pi) * (double)ax[0]) * (double)ax[1]) * (double)ax[2]);
-            float ip = volm / vell;
-            if (ip > 1.0f) { ip = -99.0f; e = -99.0f; }
-            eps[ind - 1] = e;
-            ipv[ind - 1] = ip;
-        }
+        c.mark("shape_inertia");
+        int32_t *nc_d = dev_upload<int32_t>(c, B_RED2, ncellv.data(), (size_t)nv);
+        push_uvoid();
+        float *ax_d = gc_d;                          // the centres are consumed by k_inertia
+        ++c.launches, k_void_axes<<<grid_for(nv, 128), 128, 0, c.stream>>>(nv, uv_d, nc_d, in_d, dx, pi, ax_d, ax_d + nvs);
+        dev_download(c, eps.data(), ax_d, nv);
+        dev_download(c, ipv.data(), ax_d + nvs, nv);
+        c.mark("shape_axes");
     }
     const float cellv = (dx * dx) * dx;
     const double vmin = ((double)(4.0f / 3.0f) * pi) * (double)((p->rmin * p->rmin) * p->rmin);
