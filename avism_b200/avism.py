@@ -99,7 +99,7 @@ class AvismGPU:
         turns collection on (or off) for the following calls."""
         out = np.zeros(8, np.int64)
         self._chk(self.lib.avism_gpu_knn_counters(self.h, int(enable), _vp(out), 8))
-        keys = ("queries", "attempts", "scanned", "kept", "fallbacks")
+        keys = ("queries", "attempts", "scanned", "kept", "fallbacks", "exact_ranks")
         return {k: int(out[i]) for i, k in enumerate(keys)}
 
     # ---- learned proposal (no reference counterpart) -----------------------------

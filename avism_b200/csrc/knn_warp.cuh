@@ -124,82 +124,86 @@ __device__ __forceinline__ int wq_rows(const KnnGrid &G, const int b[3], float q
     return __shfl_sync(0xffffffffu, li, 31);
 }
 
-// ascending bitonic sort of one (key, payload) per lane; equal keys keep their
-// lanes' order undefined (the caller detects equal squared distances)
-__device__ __forceinline__ void warp_sort32(uint32_t &key, uint32_t &val) {
+// Bitonic sort of one 32-bit key per lane, ascending (DESC: descending).  The
+// keys carry their payload in the low bits, so a stage is one shuffle and a
+// min or max.
+template <bool DESC>
+__device__ __forceinline__ void warp_sort32(uint32_t &key) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
         for (int j = k >> 1; j > 0; j >>= 1) {
-            const uint32_t bk = __shfl_xor_sync(0xffffffffu, key, j), bv = __shfl_xor_sync(0xffffffffu, val, j);
-            const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
-            const bool take = keep_min ? bk < key : bk > key;
-            key = take ? bk : key;
-            val = take ? bv : val;
+            const uint32_t o = __shfl_xor_sync(0xffffffffu, key, j);
+            const bool keep_min = (((lane & j) == 0) == ((lane & k) == 0)) != DESC;
+            key = keep_min ? min(key, o) : max(key, o);
         }
     }
 }
-// the 32 smallest of two ascending 32-entry lists, ascending
-__device__ __forceinline__ void warp_merge32(uint32_t &ak, uint32_t &av, uint32_t bk, uint32_t bv) {
+// a ascending, b descending: the 32 smallest of both, ascending (DESC: descending).
+// The lane-wise minimum is a bitonic sequence holding them; half-cleaners sort it.
+template <bool DESC>
+__device__ __forceinline__ void warp_merge32(uint32_t &a, uint32_t b) {
     const int lane = threadIdx.x & 31;
-    const uint32_t rk = __shfl_sync(0xffffffffu, bk, 31 - lane), rv = __shfl_sync(0xffffffffu, bv, 31 - lane);
-    const bool t0 = rk < ak;                              // a bitonic sequence
-    ak = t0 ? rk : ak;
-    av = t0 ? rv : av;
+    a = min(a, b);
 #pragma unroll
     for (int j = 16; j > 0; j >>= 1) {
-        const uint32_t ok = __shfl_xor_sync(0xffffffffu, ak, j), ov = __shfl_xor_sync(0xffffffffu, av, j);
-        const bool take = (lane & j) == 0 ? ok < ak : ok > ak;
-        ak = take ? ok : ak;
-        av = take ? ov : av;
+        const uint32_t o = __shfl_xor_sync(0xffffffffu, a, j);
+        const bool keep_min = ((lane & j) == 0) != DESC;
+        a = keep_min ? min(a, o) : max(a, o);
     }
 }
 
-// The K <= 32 nearest of the n <= 128 kept candidates ordered by squared
-// distance with warp bitonic sorts on 32-bit keys.  That is the exact order
-// unless two of the selected -- or the K-th and a dropped one -- have the same
-// squared distance; then it returns false and the caller ranks exactly.
+// The K <= 32 nearest of the n <= 128 kept candidates.  Each key packs the
+// squared distance's bits (shifted past the always-zero sign bit, low seven
+// bits dropped) above the candidate's 7-bit slot, and the keys are sorted with
+// warp bitonic networks.  The result is then verified on the full squared
+// distances: the first m = min(n, K) must be strictly ascending (no tie, no pair
+// misordered by the dropped bits) and exactly m kept candidates may lie at or
+// below the m-th.  Then they are the m nearest in the exact order; otherwise it
+// returns false and the caller ranks exactly.
 template <int KMAX>
 __device__ __forceinline__ bool bitonic_select(const KnnGrid &G, int n, int K, WarpKnnSmem<KMAX> &S) {
+    static_assert(WarpKnnSmem<KMAX>::CAP <= 128, "slots must fit in 7 bits");
     const int lane = threadIdx.x & 31;
-    uint32_t k[4], v[4];
+    uint32_t k[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const int e = q * 32 + lane;
-        k[q] = e < n ? S.d2[e] : 0xffffffffu;
-        v[q] = (uint32_t)e;
+        k[q] = e < n ? (((S.d2[e] << 1) & ~0x7fu) | (uint32_t)e) : 0xffffffffu;
     }
     const int ns = (n + 31) >> 5;
-    warp_sort32(k[0], v[0]);
+    warp_sort32<false>(k[0]);
     if (ns > 1) {
-        warp_sort32(k[1], v[1]);
-        warp_merge32(k[0], v[0], k[1], v[1]);
+        warp_sort32<true>(k[1]);
+        warp_merge32<false>(k[0], k[1]);
     }
     if (ns > 2) {
-        warp_sort32(k[2], v[2]);
         if (ns > 3) {
-            warp_sort32(k[3], v[3]);
-            warp_merge32(k[2], v[2], k[3], v[3]);
+            warp_sort32<false>(k[2]);
+            warp_sort32<true>(k[3]);
+            warp_merge32<true>(k[2], k[3]);
+        } else {
+            warp_sort32<true>(k[2]);
         }
-        warp_merge32(k[0], v[0], k[2], v[2]);
+        warp_merge32<false>(k[0], k[2]);
     }
     const int m = min(n, K);
-    // ties: equal squared distances among the first m, or beyond the m-th
-    const uint32_t d = k[0];
+    const uint32_t slot = k[0] & 0x7fu;
+    const uint32_t d = lane < m ? S.d2[slot] : 0xffffffffu;
     const uint32_t dn = __shfl_down_sync(0xffffffffu, d, 1);
     const uint32_t dk = __shfl_sync(0xffffffffu, d, m - 1);
-    bool tie = lane < m - 1 && d == dn;
+    const bool bad = lane < m - 1 && !(d < dn);
     int le = 0;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const int e = q * 32 + lane;
         le += __popc(__ballot_sync(0xffffffffu, e < n && S.d2[e] <= dk));
     }
-    if (__any_sync(0xffffffffu, tie) || le > m) return false;
+    if (__any_sync(0xffffffffu, bad) || le > m) return false;
     if (lane < m) {
         S.res_d2[lane] = d;
-        S.res_pos[lane] = S.pos[v[0]];
+        S.res_pos[lane] = S.pos[slot];
     }
     __syncwarp();
     return true;
@@ -295,6 +299,7 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
         }
         if constexpr (KMAX == 32) {
             if (bitonic_select(G, n, K, S)) return min(n, K);
+            if (G.stats && lane == 0) atomicAdd(&G.stats[5], 1ULL);
         }
         // counting select: rank = #smaller squared distances + #equal ones with a smaller index
         for (int e = lane; e < n; e += 32) {

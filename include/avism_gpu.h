@@ -195,7 +195,9 @@ int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n,
  * collected while enabled (enable = 1 turns collection on for later calls, 0
  * off): out[0] queries, [1] radius attempts, [2] candidates scanned, [3]
  * candidates kept inside the radius, [4] queries that fell back to the shell
- * search.  No reference counterpart (instrumentation of this library).        */
+ * search, [5] queries (K <= 32) ranked by the exact counting select after the
+ * bitonic order failed its check.  No reference counterpart (instrumentation of
+ * this library).                                                              */
 int avism_gpu_knn_counters(avism_gpu_ctx *ctx, int enable, int64_t *out, int n);
 
 /* ---- learned proposal.  No reference counterpart: AVISM has no learned part.
