@@ -258,7 +258,8 @@ int avism_gpu_knn(avism_gpu_ctx *ctx, int64_t n, const float *x, const float *y,
             }
             box = 2.0f * lim * 1.0001f + 1e-6f;
         }
-        BinnedParticles bp = bin_particles(c, n, dx, dy, dz, box, periodic, 4.0f);
+        BinnedParticles bp = bin_particles(c, n, dx, dy, dz, box, periodic, 4.0f, nullptr, nullptr, nullptr,
+                                           nullptr, nullptr, true);
         int64_t *di = (int64_t *)(is_device_ptr(idx) ? (void *)idx : c.get(B_LIST_A, sizeof(int64_t) * (size_t)std::max<int64_t>(nq * k, 1)));
         float *dd = (float *)(is_device_ptr(dist) ? (void *)dist : c.get(B_LIST_B, sizeof(float) * (size_t)std::max<int64_t>(nq * k, 1)));
         knn_batch(c, bp, nq, dqx, dqy, dqz, k, di, dd);

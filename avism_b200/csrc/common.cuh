@@ -59,6 +59,7 @@ enum BufId : int {
     B_PR_CNT, B_PR_BOX1, B_PR_BOX2, B_PR_BOX4,     // centred box counts of the bins
     B_PR_TMPA, B_PR_TMPB,
     B_PX4, B_PV4,                                  // packed (x, y, z, m), (vx, vy, vz, 0) in input order
+    B_FSTART,                                      // int32 offsets of quarter-bin x cells
     B_NUM
 };
 
@@ -181,13 +182,16 @@ struct BinnedParticles {
     int periodic = 0;
     const float4 *sp = nullptr;      // binned particles (x, y, z, orig idx bits)
     const int64_t *start = nullptr;  // nb^3 + 1 offsets
+    // offsets of quarter-bin cells along x (4 nb^3 + 1), or null: the kNN then
+    // trims each row of bins to the query's reach at a quarter of a bin
+    const int32_t *fstart = nullptr;
 };
 
 // sv (nullable): receives (vx, vy, vz, m) in binned order
 BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y, const float *z,
                               float box, int periodic, float occupancy, const float *vx = nullptr,
                               const float *vy = nullptr, const float *vz = nullptr, const float *m = nullptr,
-                              float4 *sv = nullptr);
+                              float4 *sv = nullptr, bool fine = false);
 
 void knn_batch(Ctx &c, const BinnedParticles &bp, int64_t nq, const float *qx, const float *qy,
                const float *qz, int k, int64_t *idx_out, float *dist_out);

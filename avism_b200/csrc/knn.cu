@@ -30,6 +30,28 @@ __global__ void k_bin_keys(int64_t n, const float *__restrict__ x, const float *
     vals[i] = (int32_t)i;
 }
 
+// keys of quarter-bin x cells: fine x + 4 nb (y + nb z); key / 4 is the bin
+__global__ void k_bin_keys_fine(int64_t n, const float *__restrict__ x, const float *__restrict__ y,
+                                const float *__restrict__ z, float origin, float inv_bw, int nb,
+                                uint32_t *__restrict__ keys, int32_t *__restrict__ vals) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int fx = fine_coord(x[i], origin, inv_bw, nb);
+    const int by = bin_coord(y[i], origin, inv_bw, nb);
+    const int bz = bin_coord(z[i], origin, inv_bw, nb);
+    keys[i] = (uint32_t)fx + (uint32_t)(KNN_XF * nb) * ((uint32_t)by + (uint32_t)nb * (uint32_t)bz);
+    vals[i] = (int32_t)i;
+}
+
+// offsets of the key cells [prev + 1, cur] start at i; the last particle closes the rest
+template <class T>
+__device__ __forceinline__ void fill_starts(T *start, int64_t i, int64_t n, int64_t prev, int64_t cur,
+                                            int64_t ncells) {
+    for (int64_t b = prev + 1; b <= cur; b++) start[b] = (T)i;
+    if (i == n - 1)
+        for (int64_t b = cur + 1; b <= ncells; b++) start[b] = (T)n;
+}
+
 // binned records (x, y, z, original index) and the bin offsets
 __global__ void k_bin_gather(int64_t n, const uint32_t *__restrict__ keys, const int32_t *__restrict__ vals,
                              const float *__restrict__ x, const float *__restrict__ y,
@@ -59,22 +81,32 @@ __global__ void k_pack_particles(int64_t n, const float *__restrict__ x, const f
     pb[i] = make_float4(vx[i], vy[i], vz[i], 0.0f);
 }
 
-// k_bin_gather with the attributes, from the packed records
-__global__ void k_bin_gather_packed(int64_t n, const uint32_t *__restrict__ keys, const int32_t *__restrict__ vals,
-                                    const float4 *__restrict__ pa, const float4 *__restrict__ pb,
-                                    float4 *__restrict__ sp, float4 *__restrict__ sv, int64_t *__restrict__ start,
-                                    int64_t nbins) {
+// k_bin_gather with the attributes from the packed records (pa non-null) and,
+// for FINE keys, the quarter-bin offsets as well
+template <bool FINE>
+__global__ void k_bin_gather2(int64_t n, const uint32_t *__restrict__ keys, const int32_t *__restrict__ vals,
+                              const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
+                              const float4 *__restrict__ pa, const float4 *__restrict__ pb, float4 *__restrict__ sp,
+                              float4 *__restrict__ sv, int64_t *__restrict__ start, int64_t nbins,
+                              int32_t *__restrict__ fstart) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int32_t v = vals[i];
-    const float4 a = pa[v], b = pb[v];
-    sp[i] = make_float4(a.x, a.y, a.z, __int_as_float(v));
-    sv[i] = make_float4(b.x, b.y, b.z, a.w);
+    if (pa) {
+        const float4 a = pa[v], b = pb[v];
+        sp[i] = make_float4(a.x, a.y, a.z, __int_as_float(v));
+        sv[i] = make_float4(b.x, b.y, b.z, a.w);
+    } else {
+        sp[i] = make_float4(x[v], y[v], z[v], __int_as_float(v));
+    }
     const int64_t cur = keys[i];
     const int64_t prev = i == 0 ? -1 : (int64_t)keys[i - 1];
-    for (int64_t b2 = prev + 1; b2 <= cur; b2++) start[b2] = i;
-    if (i == n - 1)
-        for (int64_t b2 = cur + 1; b2 <= nbins; b2++) start[b2] = n;
+    if (FINE) {
+        fill_starts(fstart, i, n, prev, cur, (int64_t)KNN_XF * nbins);
+        fill_starts(start, i, n, prev < 0 ? -1 : prev / KNN_XF, cur / KNN_XF, nbins);
+    } else {
+        fill_starts(start, i, n, prev, cur, nbins);
+    }
 }
 
 __global__ void k_empty_start(int64_t *start, int64_t nbins) {
@@ -84,7 +116,7 @@ __global__ void k_empty_start(int64_t *start, int64_t nbins) {
 
 BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y, const float *z,
                               float box, int periodic, float occupancy, const float *vx, const float *vy,
-                              const float *vz, const float *m, float4 *sv) {
+                              const float *vz, const float *m, float4 *sv, bool fine) {
     BinnedParticles bp;
     bp.n = n;
     bp.periodic = periodic;
@@ -105,26 +137,39 @@ BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y,
         return bp;
     }
     AV_CHECK(n < (int64_t)INT32_MAX, AVISM_ERR_ARG, "more than 2^31-1 particles");
+    // quarter-bin keys while 4 nb^3 offsets stay below 2^31
+    fine = fine && (int64_t)KNN_XF * nbins < (int64_t)INT32_MAX;
+    const int64_t nkeys = fine ? (int64_t)KNN_XF * nbins : nbins;
     uint32_t *ka = c.get_t<uint32_t>(B_KEYS_A, n), *kb = c.get_t<uint32_t>(B_KEYS_B, n);
     int32_t *va = c.get_t<int32_t>(B_VALS_A, n), *vb = c.get_t<int32_t>(B_VALS_B, n);
-    ++c.launches, k_bin_keys<<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, y, z, bp.origin, bp.inv_bw, nb, ka, va);
+    if (fine)
+        ++c.launches, k_bin_keys_fine<<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, y, z, bp.origin, bp.inv_bw, nb,
+                                                                              ka, va);
+    else
+        ++c.launches, k_bin_keys<<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, y, z, bp.origin, bp.inv_bw, nb, ka, va);
     AV_CUDA(cudaGetLastError());
     cub::DoubleBuffer<uint32_t> dk(ka, kb);
     cub::DoubleBuffer<int32_t> dv(va, vb);
     int end_bit = 1;
-    while ((1LL << end_bit) < nbins) end_bit++;
+    while ((1LL << end_bit) < nkeys) end_bit++;
     size_t tmp = 0;
     AV_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, (int)n, 0, end_bit, c.stream));
     void *t = c.get(B_CUB_TMP, tmp);
     AV_CUDA(cub::DeviceRadixSort::SortPairs(t, tmp, dk, dv, (int)n, 0, end_bit, c.stream));
+    float4 *pa = nullptr, *pb = nullptr;
     if (sv) {
-        float4 *pa = c.get_t<float4>(B_PX4, n), *pb = c.get_t<float4>(B_PV4, n);
+        pa = c.get_t<float4>(B_PX4, n);
+        pb = c.get_t<float4>(B_PV4, n);
         ++c.launches, k_pack_particles<<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, y, z, m, vx, vy, vz, pa, pb);
-        ++c.launches, k_bin_gather_packed<<<grid_for(n, 256), 256, 0, c.stream>>>(n, dk.Current(), dv.Current(), pa,
-                                                                                pb, sp, sv, start, nbins);
+    }
+    if (fine) {
+        int32_t *fstart = c.get_t<int32_t>(B_FSTART, nkeys + 1);
+        bp.fstart = fstart;
+        ++c.launches, k_bin_gather2<true><<<grid_for(n, 256), 256, 0, c.stream>>>(
+            n, dk.Current(), dv.Current(), x, y, z, pa, pb, sp, sv, start, nbins, fstart);
     } else {
-        ++c.launches, k_bin_gather<<<grid_for(n, 256), 256, 0, c.stream>>>(n, dk.Current(), dv.Current(), x, y, z,
-                                                                         sp, start, nbins);
+        ++c.launches, k_bin_gather2<false><<<grid_for(n, 256), 256, 0, c.stream>>>(
+            n, dk.Current(), dv.Current(), x, y, z, pa, pb, sp, sv, start, nbins, nullptr);
     }
     AV_CUDA(cudaGetLastError());
     return bp;

@@ -18,6 +18,7 @@ namespace avism {
 struct KnnGrid {
     const float4 *sp;
     const int64_t *start;
+    const int32_t *fstart;    // quarter-bin x offsets (BinnedParticles::fstart) or null
     int nb;
     float origin, bw, inv_bw, box, margin;
     int periodic;
@@ -31,6 +32,7 @@ inline KnnGrid make_knn_grid(const BinnedParticles &bp) {
     KnnGrid G;
     G.sp = bp.sp;
     G.start = bp.start;
+    G.fstart = bp.fstart;
     G.nb = bp.nb;
     G.origin = bp.origin;
     G.bw = bp.bw;
@@ -48,6 +50,12 @@ inline KnnGrid make_knn_grid(const BinnedParticles &bp) {
 __host__ __device__ __forceinline__ int bin_coord(float x, float origin, float inv_bw, int nb) {
     int b = (int)floorf((x - origin) * inv_bw);
     return b < 0 ? 0 : (b >= nb ? nb - 1 : b);
+}
+// quarter-bin cell along x: 4t is exact, so fine_coord / 4 == bin_coord
+constexpr int KNN_XF = 4;
+__host__ __device__ __forceinline__ int fine_coord(float x, float origin, float inv_bw, int nb) {
+    const float f = ((x - origin) * inv_bw) * (float)KNN_XF;
+    return f < 0.0f ? 0 : (f >= (float)(KNN_XF * nb) ? KNN_XF * nb - 1 : (int)floorf(f));
 }
 
 // squared distance exactly as distance() in src/kdtree.f90:1441-1465:

@@ -65,6 +65,7 @@ __device__ __forceinline__ int wq_rows(const KnnGrid &G, const int b[3], float q
         const int dy = ly + (r - rz * ny), dz = lz + rz;
         bool keep = true;
         int xl = lx, xh = hx;
+        int fl = INT_MIN, fh = INT_MAX;                 // quarter-bin x range (G.fstart)
         if (prune) {
             const float gz = axis_gap(G, qz, b[2] + dz);
             const float gz2 = __fmul_rn(gz, gz);
@@ -76,12 +77,16 @@ __device__ __forceinline__ int wq_rows(const KnnGrid &G, const int b[3], float q
                 // the reach only prunes (with the margin), so an approximate root does
                 const float rem = R2 - yz2;
                 const float rx = (rem > 0.0f ? rem * rsqrtf(rem) * 1.000001f : 0.0f) + G.margin;
-                const int cl = (int)floorf(__fmul_rn(__fsub_rn(__fsub_rn(qx, rx), G.origin), G.inv_bw));
-                const int ch = (int)floorf(__fmul_rn(__fsub_rn(__fadd_rn(qx, rx), G.origin), G.inv_bw));
+                const float tl = __fmul_rn(__fsub_rn(__fsub_rn(qx, rx), G.origin), G.inv_bw);
+                const float th = __fmul_rn(__fsub_rn(__fadd_rn(qx, rx), G.origin), G.inv_bw);
+                const int cl = (int)floorf(tl), ch = (int)floorf(th);
                 // near the periodic seam the images' bins are not monotone in x: keep the window
                 if (!G.periodic || (cl >= 0 && ch <= G.nb - 1)) {
                     xl = max(xl, cl - b[0]);
                     xh = min(xh, ch - b[0]);
+                    // particles' quarter-bin cells are floor(4 t) of the same t: monotone in x
+                    fl = (int)floorf(tl * (float)KNN_XF);
+                    fh = (int)floorf(th * (float)KNN_XF);
                 }
             }
         }
@@ -90,7 +95,31 @@ __device__ __forceinline__ int wq_rows(const KnnGrid &G, const int b[3], float q
             const int by = G.periodic ? wrap_near(b[1] + dy, G.nb) : b[1] + dy;
             const int64_t row = (int64_t)G.nb * (by + (int64_t)G.nb * bz);
             const int bx0 = b[0] + xl, n = xh - xl + 1;
-            if (!G.periodic) {
+            if (G.fstart) {
+                // the same rows at a quarter of a bin along x; the cells' offsets are
+                // in bin order, so a wrapped window splits as the bins' does
+                const int nf = KNN_XF * G.nb;
+                const int f0 = max(KNN_XF * bx0, fl), f1 = min(KNN_XF * (bx0 + n) - 1, fh);
+                const int fn = f1 - f0 + 1;
+                const int64_t frow = (int64_t)nf * (by + (int64_t)G.nb * bz);
+                const int32_t *F = G.fstart + frow;
+                if (fn <= 0) {
+                } else if (!G.periodic) {
+                    s0 = (uint32_t)F[f0];
+                    l0 = F[f0 + fn] - F[f0];
+                } else {
+                    const int w0 = wrap_near(f0, nf);
+                    if (w0 + fn <= nf) {
+                        s0 = (uint32_t)F[w0];
+                        l0 = F[w0 + fn] - F[w0];
+                    } else {
+                        s0 = (uint32_t)F[w0];
+                        l0 = F[nf] - F[w0];
+                        s1 = (uint32_t)F[0];
+                        l1 = F[w0 + fn - nf] - F[0];
+                    }
+                }
+            } else if (!G.periodic) {
                 s0 = (uint32_t)G.start[row + bx0];
                 l0 = (int)(G.start[row + bx0 + n] - G.start[row + bx0]);
             } else {

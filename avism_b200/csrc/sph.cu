@@ -698,8 +698,10 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
         const float occ = occ_env ? (float)atof(occ_env) : 2.0f;
         const int64_t n1 = std::max<int64_t>(a.n, 1);
         float4 *sv = c.get_t<float4>(B_SV, n1);
+        const char *fine_env = getenv("AVISM_TUNE_FINE");
+        const bool fine = fine_env ? atoi(fine_env) != 0 : true;
         BinnedParticles bp = bin_particles(c, a.n, a.x, a.y, a.z, p->lado0, p->periodic, occ, a.vx, a.vy, a.vz,
-                                           a.m, sv);
+                                           a.m, sv, fine);
         KnnGrid G = make_knn_grid(bp);
         if (c.knn_stats) {
             G.stats = c.get_t<unsigned long long>(B_KNN_STATS, 8);
