@@ -345,10 +345,9 @@ __device__ __forceinline__ float m4_q(float d2, float inv_h) {
     return 0.0f;
 }
 
-__global__ void k_ddens(KnnGrid G, int64_t n, DdensArgs A) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4 p = G.sp[i];
+// one particle with nested row loops (both passes): particles whose support
+// has more rows than k_ddens holds, or offsets beyond 8 bits
+__device__ __noinline__ void ddens_nested(const DdensArgs &A, const float4 p, int64_t i) {
     const int nx = A.nx;
     const float dx = A.dx;
     const int ix = (int)__fdiv_rn(__fsub_rn(p.x, A.rx1), dx) + 1;
@@ -425,6 +424,135 @@ __global__ void k_ddens(KnnGrid G, int64_t n, DdensArgs A) {
                 add128(A.fix + 2 * cid, (unsigned long long)llrint((double)m * A.scale));
             }
             break;
+        }
+    }
+}
+
+
+// DDENS_INTERP_SPH, one thread per particle.  The rows of the particle's support
+// (planes and rows trimmed to d^2 <= hh, x ranges trimmed likewise) are listed
+// once in shared memory, packed (k - k_lo, j - j_lo, a - i_lo, length) in 8 bits
+// each; both passes then walk the cells as one flat loop, so the lanes of a warp
+// stay busy until the largest support is done instead of idling at the end of
+// every plane and row.  NORM still sums in the reference's (k, j, i) order.
+constexpr int DD_THREADS = 256, DD_RMAX = 40;
+
+__global__ void __launch_bounds__(DD_THREADS) k_ddens(KnnGrid G, int64_t n, DdensArgs A) {
+    __shared__ uint32_t rows[DD_RMAX * DD_THREADS];
+    uint32_t *my = rows + threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = G.sp[i];
+    const int nx = A.nx;
+    const float dx = A.dx;
+    const int ix = (int)__fdiv_rn(__fsub_rn(p.x, A.rx1), dx) + 1;
+    const int jy = (int)__fdiv_rn(__fsub_rn(p.y, A.rx1), dx) + 1;
+    const int kz = (int)__fdiv_rn(__fsub_rn(p.z, A.rx1), dx) + 1;
+    const float h = A.hp_s[i];
+    const float inv_h = __fdiv_rn(2.0f, h);
+    const int inc = (int)__fadd_rn(__fdiv_rn(__fmul_rn(2.0f, h), dx), 0.5f);
+    const float hh = h * h * 1.00002f + 1e-30f;
+    const float inv_dx = 1.0f / dx;
+    const float *rad = A.rad - A.rad_lo;
+    const int k_lo = max(kz - inc, 1), k_hi = min(kz + inc, nx);
+    const int j_lo = max(jy - inc, 1), j_hi = min(jy + inc, nx);
+    const int i_lo = max(ix - inc, 1), i_hi = min(ix + inc, nx);
+    const float hr = (hh > 0.0f ? hh * rsqrtf(hh) : 0.0f) * 1.00001f + 1e-6f * dx;
+    int k_a = max(k_lo, (int)floorf((p.z - hr - A.rx1) * inv_dx) + 1 - 1);
+    int k_b = min(k_hi, (int)ceilf((p.z + hr - A.rx1) * inv_dx) + 1 + 1);
+    auto dz2_of = [&](int k2) { const float t = __fsub_rn(p.z, rad[k2]); return __fmul_rn(t, t); };
+    while (k_a <= k_b && dz2_of(k_a) > hh) k_a++;
+    while (k_b >= k_a && dz2_of(k_b) > hh) k_b--;
+    // the support's rows, as ddens_nested walks them
+    int nrows = 0, ncell = 0;
+    bool over = false;
+    for (int k2 = k_a; k2 <= k_b && !over; k2++) {
+        const float dz2 = dz2_of(k2);
+        const float remz = hh - dz2;
+        const float ry = (remz > 0.0f ? remz * rsqrtf(remz) : 0.0f) * 1.00001f + 1e-6f * dx;
+        int j_a = max(j_lo, (int)floorf((p.y - ry - A.rx1) * inv_dx) + 1 - 1);
+        int j_b = min(j_hi, (int)ceilf((p.y + ry - A.rx1) * inv_dx) + 1 + 1);
+        auto rem_of = [&](int j2) { const float t = __fsub_rn(p.y, rad[j2]); return hh - dz2 - __fmul_rn(t, t); };
+        while (j_a <= j_b && rem_of(j_a) < 0.0f) j_a++;
+        while (j_b >= j_a && rem_of(j_b) < 0.0f) j_b--;
+        for (int j2 = j_a; j2 <= j_b; j2++) {
+            const float ty = __fsub_rn(p.y, rad[j2]);
+            const float dy2 = __fmul_rn(ty, ty);
+            const float rem = hh - dz2 - dy2;
+            const float R = (rem > 0.0f ? rem * rsqrtf(rem) : 0.0f) * 1.00001f + 1e-6f * dx;
+            int a = max(i_lo, (int)floorf((p.x - R - A.rx1) * inv_dx) + 1 - 1);
+            int e = min(i_hi, (int)ceilf((p.x + R - A.rx1) * inv_dx) + 1 + 1);
+            auto d2_of = [&](int i2) {
+                const float t = __fsub_rn(p.x, rad[i2]);
+                return __fadd_rn(__fadd_rn(__fmul_rn(t, t), dy2), dz2);
+            };
+            while (a <= e && d2_of(a) > hh) a++;
+            while (e >= a && d2_of(e) > hh) e--;
+            if (a > e) continue;
+            const int len = e - a + 1;
+            if (nrows == DD_RMAX || k2 - k_lo > 255 || j2 - j_lo > 255 || a - i_lo > 255 || len > 255) {
+                over = true;
+                break;
+            }
+            my[nrows * DD_THREADS] = (uint32_t)(k2 - k_lo) | (uint32_t)(j2 - j_lo) << 8 |
+                                     (uint32_t)(a - i_lo) << 16 | (uint32_t)len << 24;
+            nrows++;
+            ncell += len;
+        }
+    }
+    if (over) {
+        ddens_nested(A, p, i);
+        return;
+    }
+    int k2 = 0, j2 = 0, i2 = 0, ie = -1;
+    float dy2 = 0.0f, dz2 = 0.0f;
+    auto load_row = [&](int r) {
+        const uint32_t d = my[r * DD_THREADS];
+        k2 = k_lo + (int)(d & 255u);
+        j2 = j_lo + (int)((d >> 8) & 255u);
+        i2 = i_lo + (int)((d >> 16) & 255u);
+        ie = i2 + (int)(d >> 24) - 1;
+        dz2 = dz2_of(k2);
+        const float ty = __fsub_rn(p.y, rad[j2]);
+        dy2 = __fmul_rn(ty, ty);
+    };
+    // pass 0: NORM (cells outside the support add exactly 0 in the reference)
+    float norm = 0.0f;
+    if (ncell > 0) {
+        int r = 0;
+        load_row(0);
+        for (int t = 0; t < ncell; t++) {
+            const float tx = __fsub_rn(p.x, rad[i2]);
+            const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), dy2), dz2);
+            norm = __fadd_rn(norm, m4_q(d2, inv_h));
+            if (++i2 > ie && t + 1 < ncell) load_row(++r);
+        }
+    }
+    const float m = A.sv[i].w;
+    if (norm == 0.0f) {
+        // the particle only contributes to its own cell
+        if (ix >= 1 && ix <= nx && jy >= 1 && jy <= nx && kz >= 1 && kz <= nx) {
+            const int64_t cid = (int64_t)(ix - 1) + (int64_t)nx * ((int64_t)(jy - 1) + (int64_t)nx * (kz - 1));
+            add128(A.fix + 2 * cid, (unsigned long long)llrint((double)m * A.scale));
+        }
+        return;
+    }
+    // pass 1: m * w / NORM in 128-bit fixed point
+    int r = 0;
+    load_row(0);
+    int64_t rowc = (int64_t)nx * ((int64_t)(j2 - 1) + (int64_t)nx * (k2 - 1)) - 1;
+    for (int t = 0; t < ncell; t++) {
+        const float tx = __fsub_rn(p.x, rad[i2]);
+        const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), dy2), dz2);
+        const float w = m4_q(d2, inv_h);
+        if (w != 0.0f) {
+            const float contrib = __fdiv_rn(__fmul_rn(w, m), norm);
+            const unsigned long long v = (unsigned long long)llrint((double)contrib * A.scale);
+            add128(A.fix + 2 * (rowc + i2), v);
+        }
+        if (++i2 > ie && t + 1 < ncell) {
+            load_row(++r);
+            rowc = (int64_t)nx * ((int64_t)(j2 - 1) + (int64_t)nx * (k2 - 1)) - 1;
         }
     }
 }
@@ -767,7 +895,7 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
             D.nx = nx; D.rad_lo = L.g.rad_lo; D.dx = L.g.dx; D.rx1 = L.rad_at(1); D.rad = rad_d;
             D.hp_s = hp_s; D.sv = sv; D.fix = fix; D.scale = scale;
             c.mark("ddens_setup");
-            ++c.launches, k_ddens<<<grid_for(a.n, 128), 128, 0, c.stream>>>(G, a.n, D);
+            ++c.launches, k_ddens<<<grid_for(a.n, DD_THREADS), DD_THREADS, 0, c.stream>>>(G, a.n, D);
             AV_CUDA(cudaGetLastError());
             c.mark("ddens_scatter");
             ++c.launches, k_fix128_to_f32<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, fix, 1.0 / scale, a.u_mass);
