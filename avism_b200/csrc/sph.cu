@@ -228,32 +228,68 @@ __device__ __forceinline__ float query_r0(const KnnGrid &G, float qx, float qy, 
     return G.r0[b];
 }
 
+// the particle kernel stages its queries' neighbour masses per warp and sums
+// them after the searches, one lane per query; (KMAX + 2)-double rows keep the
+// summing lanes' 16-byte loads on distinct banks
+template <int KMAX> constexpr int SPH_ROW = KMAX + 2;
+template <int KMAX>
+constexpr size_t sph_smem_bytes() {
+    return (size_t)SPH_WARPS * sizeof(WarpKnnSmem<KMAX>) +
+           (size_t)SPH_WARPS * SPH_QPW * SPH_ROW<KMAX> * sizeof(double);
+}
+template <int KMAX>
+__device__ __forceinline__ double *sph_rows(unsigned char *smem, int warp) {
+    return reinterpret_cast<double *>(smem + SPH_WARPS * sizeof(WarpKnnSmem<KMAX>)) +
+           (size_t)warp * SPH_QPW * SPH_ROW<KMAX>;
+}
+// sequential REAL*8 sum of row[0..n) in order, two values per 16-byte load
+__device__ __forceinline__ double seq_sum(const double *row, int n) {
+    const double2 *r2 = reinterpret_cast<const double2 *>(row);
+    double s = 0.0;
+    int j = 0;
+    for (; j + 2 <= n; j += 2) {
+        const double2 v = r2[j >> 1];
+        s = s + v.x;
+        s = s + v.y;
+    }
+    if (j < n) s = s + row[j];
+    return s;
+}
+
 template <int KMAX>
 __global__ void __launch_bounds__(SPH_WARPS * 32)
 k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float *__restrict__ pd_s,
                float *__restrict__ part_dens) {
     extern __shared__ __align__(16) unsigned char wq_smem[];
-    WarpKnnSmem<KMAX> &S = reinterpret_cast<WarpKnnSmem<KMAX> *>(wq_smem)[threadIdx.x >> 5];
-    double *acc = reinterpret_cast<double *>(S.d2);          // KMAX doubles, free after the select
+    const int warp = threadIdx.x >> 5;
+    WarpKnnSmem<KMAX> &S = reinterpret_cast<WarpKnnSmem<KMAX> *>(wq_smem)[warp];
+    double *acc = sph_rows<KMAX>(wq_smem, warp);              // one row of masses per query
     const int lane = threadIdx.x & 31;
-    const int64_t i0 = ((int64_t)blockIdx.x * SPH_WARPS + (threadIdx.x >> 5)) * SPH_QPW;
+    const int64_t i0 = ((int64_t)blockIdx.x * SPH_WARPS + warp) * SPH_QPW;
+    int my_cnt = 0;                                           // lane t: query t's count and h
+    float my_hk = 0.0f;
     for (int t = 0; t < SPH_QPW; t++) {
         const int64_t i = i0 + t;
         if (i >= n) break;
         const float4 p = G.sp[i];
         const int cnt = knn_warp_exact<KMAX>(G, p.x, p.y, p.z, K, query_r0(G, p.x, p.y, p.z), S,
                                              reinterpret_cast<unsigned long long *>(S.d2));
-        for (int j = lane; j < cnt; j += 32) acc[j] = (double)sv[S.res_pos[j]].w;
-        __syncwarp();
-        if (lane == 0) {
-            double bas8 = 0.0;
-            for (int j = 0; j < cnt; j++) bas8 = bas8 + acc[j];
-            const float hk = sqrtf(__uint_as_float(S.res_d2[K - 1]));
-            const double pi = 3.141592653589793;     // DACOS(-1.D0)
-            const float rho = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(hk, hk), hk)));
-            pd_s[i] = rho;
-            if (part_dens) part_dens[__float_as_int(p.w)] = rho;
+        for (int j = lane; j < cnt; j += 32) acc[t * SPH_ROW<KMAX> + j] = (double)sv[S.res_pos[j]].w;
+        const float hk = sqrtf(__uint_as_float(S.res_d2[K - 1]));
+        if (lane == t) {
+            my_cnt = cnt;
+            my_hk = hk;
         }
+    }
+    __syncwarp();
+    // the queries' sums side by side, one lane each
+    const int64_t i = i0 + lane;
+    if (lane < SPH_QPW && i < n) {
+        const double bas8 = seq_sum(acc + lane * SPH_ROW<KMAX>, my_cnt);
+        const double pi = 3.141592653589793;     // DACOS(-1.D0)
+        const float rho = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(my_hk, my_hk), my_hk)));
+        pd_s[i] = rho;
+        if (part_dens) part_dens[__float_as_int(G.sp[i].w)] = rho;
     }
 }
 
@@ -701,7 +737,7 @@ template <int KMAX>
 static void run_sph_kernels_w(Ctx &c, const KnnGrid &G, const avism_params *p, const Level &L,
                               const P2G &a, const float *rad_d, bool vel_sph, bool need_h_cells,
                               const float4 *sv, float *pd_s, float *hp_s) {
-    const size_t sm = (size_t)SPH_WARPS * sizeof(WarpKnnSmem<KMAX>);
+    const size_t sm = sph_smem_bytes<KMAX>();
     const int K = p->kneighbours;
     const int nx = L.g.nx;
     const int64_t nc = (int64_t)nx * nx * nx;
