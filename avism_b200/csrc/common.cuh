@@ -60,6 +60,7 @@ enum BufId : int {
     B_PR_TMPA, B_PR_TMPB,
     B_PX4, B_PV4,                                  // packed (x, y, z, m), (vx, vy, vz, 0) in input order
     B_FSTART,                                      // int32 offsets of quarter-bin x cells
+    B_PER_CELL, B_PER_LAB, B_PER_PAIRS,            // VOID_PERIODIC: centre cells, their labels, label-map updates
     B_NUM
 };
 

@@ -413,7 +413,8 @@ __global__ void k_bbox(PostGrid G, const int32_t *marca, int32_t *bb /* 6 per la
 // blo are visited -- the bounding box of the one label being recounted)
 __global__ void k_periodic_counts(PostGrid G, const int32_t *marca, const int32_t *labmap, const int8_t *shift,
                                   const int32_t *ind2, int32_t only_label, int32_t *cnt /* 2 per label */,
-                                  int3 blo = make_int3(0, 0, 0), int3 bdim = make_int3(0, 0, 0)) {
+                                  int3 blo = make_int3(0, 0, 0), int3 bdim = make_int3(0, 0, 0),
+                                  int32_t only_ind2 = 0) {
     int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int ne = G.ne;
     if (bdim.x > 0) {
@@ -436,7 +437,18 @@ __global__ void k_periodic_counts(PostGrid G, const int32_t *marca, const int32_
     atomicAdd(&cnt[(size_t)(m - 1) * 2 + 1], 1);
     int32_t lab = marca[pidx(G, i, j, k)];
     if (lab > 0) lab = labmap[lab];
-    if (lab == ind2[m - 1]) atomicAdd(&cnt[(size_t)(m - 1) * 2], 1);
+    if (lab == (only_label > 0 ? only_ind2 : ind2[m - 1])) atomicAdd(&cnt[(size_t)(m - 1) * 2], 1);
+}
+// out[i] = src[idx[i]]
+__global__ void k_gather_i32(int32_t n, const int64_t *__restrict__ idx, const int32_t *__restrict__ src,
+                             int32_t *__restrict__ out) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = src[idx[i]];
+}
+// dst[pairs[2i]] = pairs[2i + 1]
+__global__ void k_scatter_pairs(int32_t n, const int32_t *__restrict__ pairs, int32_t *__restrict__ dst) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[pairs[2 * i]] = pairs[2 * i + 1];
 }
 
 // ---- global properties on the inner cells (src/avism.f90:1917-1933) ------------
@@ -830,14 +842,18 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
             outer.push_back(ind);
         }
         if (!outer.empty()) {
-            // labels at the shifted centres, initial state
-            std::vector<int32_t> m0(outer.size());
-            for (size_t q = 0; q < outer.size(); q++) {
-                AV_CUDA(cudaMemcpyAsync(&m0[q], marca + centre_cell[outer[q] - 1], sizeof(int32_t),
-                                        cudaMemcpyDeviceToHost, c.stream));
+            // labels at the shifted centres, initial state (one gather)
+            const int32_t nout = (int32_t)outer.size();
+            std::vector<int32_t> m0(nout);
+            {
+                std::vector<int64_t> cells(nout);
+                for (int32_t q = 0; q < nout; q++) cells[q] = centre_cell[outer[q] - 1];
+                const int64_t *cells_d = dev_upload<int64_t>(c, B_PER_CELL, cells.data(), nout);
+                int32_t *m0_d = c.get_t<int32_t>(B_PER_LAB, nout);
+                ++c.launches, k_gather_i32<<<grid_for(nout, 256), 256, 0, c.stream>>>(nout, cells_d, marca, m0_d);
+                dev_download(c, m0.data(), m0_d, nout);
             }
-            c.sync();
-            for (size_t q = 0; q < outer.size(); q++) ind2spec[outer[q] - 1] = m0[q];
+            for (int32_t q = 0; q < nout; q++) ind2spec[outer[q] - 1] = m0[q];
             std::vector<int32_t> labmap(nvs + 1);
             for (int32_t i = 0; i <= nv; i++) labmap[i] = i;
             int32_t *lm_d = dev_upload<int32_t>(c, B_LABMAP, labmap.data(), nv + 1);
@@ -871,7 +887,18 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
                 for (int a = 0; a < 6; a++) curbb[i][a] = bb[(size_t)(i - 1) * 6 + a];
             }
             std::vector<std::array<int32_t, 6>> changed_bb;
-            bool lm_dirty = false;
+            // (label, new root) pairs not yet applied to the device label map
+            std::vector<int32_t> lm_pend;
+            // voids by the main void they belong to (uvoid > 0): linked lists, so
+            // CHANGE_BELONG moves a void's members without scanning all voids
+            std::vector<int32_t> lhead(nvs + 1, -1), ltail(nvs + 1, -1), lnext(nvs, -1);
+            auto lpush = [&](int32_t v, int32_t i) {
+                lnext[i] = -1;
+                if (ltail[v] < 0) lhead[v] = i; else lnext[ltail[v]] = i;
+                ltail[v] = i;
+            };
+            for (int32_t i = 0; i < nv; i++)
+                if (uvoid[i] > 0) lpush(uvoid[i], i);
             for (int32_t ind : outer) {
                 const int8_t *s = &shift[(size_t)(ind - 1) * 3];
                 int32_t i2 = ind2spec[ind - 1];
@@ -892,15 +919,12 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
                 }
                 int64_t counter = cnt[(size_t)(ind - 1) * 2], counter2 = cnt[(size_t)(ind - 1) * 2 + 1];
                 if (affected) {
-                    if (lm_dirty) {
-                        std::vector<int32_t> flat(nvs + 1);
-                        for (int32_t i = 0; i <= nv; i++) flat[i] = i == 0 ? 0 : find(i);
-                        AV_CUDA(cudaMemcpyAsync(lm_d, flat.data(), sizeof(int32_t) * (size_t)(nv + 1), cudaMemcpyHostToDevice, c.stream));
-                        lm_dirty = false;
+                    if (!lm_pend.empty()) {
+                        const int32_t np = (int32_t)(lm_pend.size() / 2);
+                        const int32_t *pr_d = dev_upload<int32_t>(c, B_PER_PAIRS, lm_pend.data(), lm_pend.size());
+                        ++c.launches, k_scatter_pairs<<<grid_for(np, 256), 256, 0, c.stream>>>(np, pr_d, lm_d);
+                        lm_pend.clear();
                     }
-                    std::vector<int32_t> i2v(nvs, 0);
-                    i2v[ind - 1] = i2;
-                    int32_t *i2d = dev_upload<int32_t>(c, B_RED1, i2v.data(), nvs);
                     int32_t *one = c.get_t<int32_t>(B_RED2, (size_t)nvs * 2);
                     AV_CUDA(cudaMemsetAsync(one + (size_t)(ind - 1) * 2, 0, 8, c.stream));
                     // the label's cells lie in its bounding box (merges extend it)
@@ -910,7 +934,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
                         const int3 bd = make_int3(bx[3] - bx[0] + 1, bx[4] - bx[1] + 1, bx[5] - bx[2] + 1);
                         const int64_t nbox = (int64_t)bd.x * bd.y * bd.z;
                         ++c.launches, k_periodic_counts<<<grid_for(nbox, 256), 256, 0, c.stream>>>(
-                            PG, marca, lm_d, sh_d, i2d, ind, one, blo, bd);
+                            PG, marca, lm_d, sh_d, i2_d, ind, one, blo, bd, i2);
                     }
                     int32_t r2[2];
                     dev_download(c, r2, one + (size_t)(ind - 1) * 2, 2);
@@ -919,9 +943,25 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
                 }
                 const float inter = counter2 == 0 ? 0.0f : (float)counter / (float)counter2;
                 if (inter > 0.4f) {                                  // CHANGE_BELONG(IND2, IND)
+                    // UVOID(IND) = IND2, then every void with UVOID == IND follows
                     uvoid[ind - 1] = i2;
-                    for (int32_t i = 0; i < nv; i++) if (uvoid[i] == ind) uvoid[i] = i2;
                     if (i2 != ind) {
+                        for (int32_t i = lhead[ind]; i >= 0; i = lnext[i]) uvoid[i] = i2;
+                        if (lhead[ind] >= 0) {
+                            if (ltail[i2] < 0) lhead[i2] = lhead[ind]; else lnext[ltail[i2]] = lhead[ind];
+                            ltail[i2] = ltail[ind];
+                            lhead[ind] = ltail[ind] = -1;
+                        }
+                    }
+                    lpush(i2, ind - 1);
+                    if (i2 != ind) {
+                        // IND's set (IND and what it absorbed) now resolves to IND2
+                        lm_pend.push_back(ind);
+                        lm_pend.push_back(i2);
+                        for (int32_t mm : members[ind]) {
+                            lm_pend.push_back(mm);
+                            lm_pend.push_back(i2);
+                        }
                         parent[ind] = i2;
                         members[i2].push_back(ind);
                         for (int32_t mm : members[ind]) members[i2].push_back(mm);
@@ -931,7 +971,6 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
                             tb[3 + a] = std::max(tb[3 + a], b[3 + a]);
                         }
                         changed_bb.push_back(b);
-                        lm_dirty = true;
                     }
                     volnew[ind - 1] = 0.0f;
                 }
