@@ -19,7 +19,8 @@ namespace avism {
 
 __device__ __forceinline__ float kernel_m4(float h, float dist) {
     // KERNEL_FUNC, M4 branch: Q = DIST/(H/2)
-    const float q = __fdiv_rn(dist, __fdiv_rn(h, 2.0f));
+    // H/2 as h * 0.5: both are the correctly rounded h/2, so the bits agree
+    const float q = __fdiv_rn(dist, __fmul_rn(h, 0.5f));
     if (q <= 1.0f) return __fsub_rn(1.0f, __fmul_rn(__fmul_rn(1.5f, __fmul_rn(q, q)), __fsub_rn(1.0f, __fmul_rn(0.5f, q))));
     if (q <= 2.0f) {
         const float t = __fsub_rn(2.0f, q);
@@ -256,8 +257,10 @@ __device__ __forceinline__ double seq_sum(const double *row, int n) {
     return s;
 }
 
+// five blocks per SM (48 registers, a few spills): more warps in flight pay
+// for the spills (171 against 187 ms with four blocks at 512^3)
 template <int KMAX>
-__global__ void __launch_bounds__(SPH_WARPS * 32)
+__global__ void __launch_bounds__(SPH_WARPS * 32, 5)
 k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float *__restrict__ pd_s,
                float *__restrict__ part_dens) {
     extern __shared__ __align__(16) unsigned char wq_smem[];
@@ -294,13 +297,16 @@ k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float
 }
 
 // five blocks per SM (48 registers): the cell kernel gains more from the extra
-// warps than it loses to spills (the particle kernel does not)
+// warps than it loses to spills (six blocks at 40 registers spill too much)
 template <int KMAX>
 __global__ void __launch_bounds__(SPH_WARPS * 32, 5)
 k_cells_knn_w(KnnGrid G, CellArgs A) {
     extern __shared__ __align__(16) unsigned char wq_smem[];
     WarpKnnSmem<KMAX> &S = reinterpret_cast<WarpKnnSmem<KMAX> *>(wq_smem)[threadIdx.x >> 5];
-    double *acc = reinterpret_cast<double *>(S.d2);          // 4 x KMAX doubles, free after the select
+    // 4 rows of SPH_ROW doubles (b, bx, by, bz) over d2, pos and the segment
+    // lists, which are free after the select (res_* lie beyond them)
+    static_assert(4 * SPH_ROW<KMAX> * sizeof(double) <= offsetof(WarpKnnSmem<KMAX>, res_d2), "rows overlap res_d2");
+    double *acc = reinterpret_cast<double *>(S.d2);
     const int lane = threadIdx.x & 31;
     const int nx = A.nx;
     // 4x4x2 tiles of cells, one tile per block, SPH_QPW cells per warp
@@ -335,14 +341,13 @@ k_cells_knn_w(KnnGrid G, CellArgs A) {
             w = __fmul_rn(w, __fdiv_rn(a.w, A.pd_s[pj]));
             const double w8 = (double)w;
             acc[j] = w8;
-            acc[KMAX + j] = w8 * (double)a.x;
-            acc[2 * KMAX + j] = w8 * (double)a.y;
-            acc[3 * KMAX + j] = w8 * (double)a.z;
+            acc[SPH_ROW<KMAX> + j] = w8 * (double)a.x;
+            acc[2 * SPH_ROW<KMAX> + j] = w8 * (double)a.y;
+            acc[3 * SPH_ROW<KMAX> + j] = w8 * (double)a.z;
         }
         __syncwarp();
         double sum = 0.0;
-        if (lane < 4)
-            for (int j = 0; j < cnt; j++) sum = sum + acc[lane * KMAX + j];
+        if (lane < 4) sum = seq_sum(acc + lane * SPH_ROW<KMAX>, cnt);
         const double b = __shfl_sync(0xffffffffu, sum, 0);
         if (lane == 1) A.u2[c] = (float)(sum / b);
         if (lane == 2) A.u3[c] = (float)(sum / b);
