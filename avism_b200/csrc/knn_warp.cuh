@@ -28,7 +28,8 @@ struct __align__(16) WarpKnnSmem {
     static constexpr int CAP = 4 * KMAX;    // kept candidates per attempt
     uint32_t d2[CAP];                       // float bits of the squared distance
     uint32_t pos[CAP];                      // position in the binned array
-    uint32_t seg_start[WQ_SEGS];            // first binned position of each segment
+    uint32_t seg_base[WQ_SEGS];             // binned position of each segment's first candidate
+                                            // minus its offset in the batch (mod 2^32)
     int32_t seg_end[WQ_SEGS];               // running end offset of each segment
     uint32_t res_d2[KMAX];                  // result, ascending (squared distance, index)
     uint32_t res_pos[KMAX];
@@ -53,7 +54,7 @@ __device__ __forceinline__ int wrap_near(int b, int nb) { return b < 0 ? b + nb 
 
 __device__ __forceinline__ int wq_rows(const KnnGrid &G, const int b[3], float qx, float qy, float qz,
                                        float R2, bool prune, int lx, int hx, int ly, int ny, float inv_ny, int lz,
-                                       int nrows, int rbase, uint32_t *seg_start, int32_t *seg_end,
+                                       int nrows, int rbase, uint32_t *seg_base, int32_t *seg_end,
                                        int *nseg_out) {
     const int lane = threadIdx.x & 31;
     const int r = rbase + lane;
@@ -146,8 +147,8 @@ __device__ __forceinline__ int wq_rows(const KnnGrid &G, const int b[3], float q
         if (lane >= o) { si += a; li += c; }
     }
     int k = si - ns, off = li - lt;
-    if (l0 > 0) { seg_start[k] = s0; seg_end[k] = off + l0; k++; off += l0; }
-    if (l1 > 0) { seg_start[k] = s1; seg_end[k] = off + l1; }
+    if (l0 > 0) { seg_base[k] = s0 - (uint32_t)off; seg_end[k] = off + l0; k++; off += l0; }
+    if (l1 > 0) { seg_base[k] = s1 - (uint32_t)off; seg_end[k] = off + l1; }
     *nseg_out = __shfl_sync(0xffffffffu, si, 31);
     __syncwarp();
     return __shfl_sync(0xffffffffu, li, 31);
@@ -276,7 +277,7 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
         for (int rbase = 0; rbase < nrows; rbase += 32) {
             int nseg;
             const int T = wq_rows(G, b, qx, qy, qz, R2, prune, lx, hx, ly, ny, inv_ny, lz, nrows, rbase,
-                                  S.seg_start, S.seg_end, &nseg);
+                                  S.seg_base, S.seg_end, &nseg);
             int k0 = 0;                                  // first segment ending after this chunk's start
             for (int cb = 0; cb < T; cb += 32) {
                 const int g = cb + lane;
@@ -289,8 +290,7 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
                 bool pass = false;
                 uint32_t d2b = 0, p = 0;
                 if (g < T) {
-                    const int begin = seg == 0 ? 0 : S.seg_end[seg - 1];
-                    p = S.seg_start[seg] + (uint32_t)(g - begin);
+                    p = S.seg_base[seg] + (uint32_t)g;
                     const float4 v = G.sp[p];
                     const float d2 = dist2_ref(v.x, v.y, v.z, qx, qy, qz, G.box, plain_d ? 0 : 1);
                     pass = d2 <= R2;

@@ -365,6 +365,7 @@ struct DdensArgs {
     const float4 *sv;             // (vx, vy, vz, m) in binned order
     unsigned long long *fix;      // 2 words per cell: low, high
     double scale;
+    float scale_f;                // the same power of two
 };
 
 // v < 2^62 is added as its two 32-bit halves to two 64-bit counters (low half to
@@ -588,7 +589,9 @@ __global__ void __launch_bounds__(DD_THREADS) k_ddens(KnnGrid G, int64_t n, Dden
         const float w = m4_q(d2, inv_h);
         if (w != 0.0f) {
             const float contrib = __fdiv_rn(__fmul_rn(w, m), norm);
-            const unsigned long long v = (unsigned long long)llrint((double)contrib * A.scale);
+            // contrib * 2^k is exact in f32 (below 2^62, no overflow), so
+            // rounding it to an integer in f32 gives llrint((double)contrib * scale)
+            const unsigned long long v = __float2ull_rn(__fmul_rn(contrib, A.scale_f));
             add128(A.fix + 2 * (rowc + i2), v);
         }
         if (++i2 > ie && t + 1 < ncell) {
@@ -934,7 +937,7 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
             AV_CUDA(cudaMemsetAsync(fix, 0, 2 * nc * sizeof(unsigned long long), c.stream));
             DdensArgs D;
             D.nx = nx; D.rad_lo = L.g.rad_lo; D.dx = L.g.dx; D.rx1 = L.rad_at(1); D.rad = rad_d;
-            D.hp_s = hp_s; D.sv = sv; D.fix = fix; D.scale = scale;
+            D.hp_s = hp_s; D.sv = sv; D.fix = fix; D.scale = scale; D.scale_f = (float)scale;
             c.mark("ddens_setup");
             ++c.launches, k_ddens<<<grid_for(a.n, DD_THREADS), DD_THREADS, 0, c.stream>>>(G, a.n, D);
             AV_CUDA(cudaGetLastError());
