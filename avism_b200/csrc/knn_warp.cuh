@@ -170,6 +170,21 @@ __device__ __forceinline__ void warp_sort32(uint32_t &key) {
         }
     }
 }
+// a ascending and b descending in lockstep: one lane predicate per stage and two
+// independent shuffle chains
+__device__ __forceinline__ void warp_sort32x2(uint32_t &a, uint32_t &b) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t oa = __shfl_xor_sync(0xffffffffu, a, j), ob = __shfl_xor_sync(0xffffffffu, b, j);
+            const bool lo = ((lane & j) == 0) == ((lane & k) == 0);
+            a = lo ? min(a, oa) : max(a, oa);
+            b = lo ? max(b, ob) : min(b, ob);
+        }
+    }
+}
 // a ascending, b descending: the 32 smallest of both, ascending (DESC: descending).
 // The lane-wise minimum is a bitonic sequence holding them; half-cleaners sort it.
 template <bool DESC>
@@ -203,15 +218,15 @@ __device__ __forceinline__ bool bitonic_select(const KnnGrid &G, int n, int K, W
         k[q] = e < n ? (((S.d2[e] << 1) & ~0x7fu) | (uint32_t)e) : 0xffffffffu;
     }
     const int ns = (n + 31) >> 5;
-    warp_sort32<false>(k[0]);
     if (ns > 1) {
-        warp_sort32<true>(k[1]);
+        warp_sort32x2(k[0], k[1]);
         warp_merge32<false>(k[0], k[1]);
+    } else {
+        warp_sort32<false>(k[0]);
     }
     if (ns > 2) {
         if (ns > 3) {
-            warp_sort32<false>(k[2]);
-            warp_sort32<true>(k[3]);
+            warp_sort32x2(k[2], k[3]);
             warp_merge32<true>(k[2], k[3]);
         } else {
             warp_sort32<true>(k[2]);
