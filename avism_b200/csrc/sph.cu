@@ -221,6 +221,7 @@ __global__ void k_cells_ball(KnnGrid G, CellArgs A, int32_t nlist) {
 // over the neighbour list stay sequential in list order (REAL*8, as the
 // reference's loops), done by one lane per sum from shared memory.
 constexpr int SPH_WARPS = 8, SPH_QPW = 4;
+constexpr int PP_QPW = 8;                      // particle queries per warp (their sums run side by side)
 
 __device__ __forceinline__ float query_r0(const KnnGrid &G, float qx, float qy, float qz) {
     if (!G.r0) return 0.0f;
@@ -236,12 +237,12 @@ template <int KMAX> constexpr int SPH_ROW = KMAX + 2;
 template <int KMAX>
 constexpr size_t sph_smem_bytes() {
     return (size_t)SPH_WARPS * sizeof(WarpKnnSmem<KMAX>) +
-           (size_t)SPH_WARPS * SPH_QPW * SPH_ROW<KMAX> * sizeof(double);
+           (size_t)SPH_WARPS * PP_QPW * SPH_ROW<KMAX> * sizeof(double);
 }
 template <int KMAX>
 __device__ __forceinline__ double *sph_rows(unsigned char *smem, int warp) {
     return reinterpret_cast<double *>(smem + SPH_WARPS * sizeof(WarpKnnSmem<KMAX>)) +
-           (size_t)warp * SPH_QPW * SPH_ROW<KMAX>;
+           (size_t)warp * PP_QPW * SPH_ROW<KMAX>;
 }
 // sequential REAL*8 sum of row[0..n) in order, two values per 16-byte load
 __device__ __forceinline__ double seq_sum(const double *row, int n) {
@@ -268,10 +269,10 @@ k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float
     WarpKnnSmem<KMAX> &S = reinterpret_cast<WarpKnnSmem<KMAX> *>(wq_smem)[warp];
     double *acc = sph_rows<KMAX>(wq_smem, warp);              // one row of masses per query
     const int lane = threadIdx.x & 31;
-    const int64_t i0 = ((int64_t)blockIdx.x * SPH_WARPS + warp) * SPH_QPW;
+    const int64_t i0 = ((int64_t)blockIdx.x * SPH_WARPS + warp) * PP_QPW;
     int my_cnt = 0;                                           // lane t: query t's count and h
     float my_hk = 0.0f;
-    for (int t = 0; t < SPH_QPW; t++) {
+    for (int t = 0; t < PP_QPW; t++) {
         const int64_t i = i0 + t;
         if (i >= n) break;
         const float4 p = G.sp[i];
@@ -287,7 +288,7 @@ k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float
     __syncwarp();
     // the queries' sums side by side, one lane each
     const int64_t i = i0 + lane;
-    if (lane < SPH_QPW && i < n) {
+    if (lane < PP_QPW && i < n) {
         const double bas8 = seq_sum(acc + lane * SPH_ROW<KMAX>, my_cnt);
         const double pi = 3.141592653589793;     // DACOS(-1.D0)
         const float rho = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(my_hk, my_hk), my_hk)));
@@ -750,9 +751,11 @@ static void run_sph_kernels_w(Ctx &c, const KnnGrid &G, const avism_params *p, c
     const int nx = L.g.nx;
     const int64_t nc = (int64_t)nx * nx * nx;
     AV_CUDA(cudaFuncSetAttribute(k_ppart_dens_w<KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    // the cell kernel stages its sums inside WarpKnnSmem: no extra rows, more L1
+    const size_t sm_cells = (size_t)SPH_WARPS * sizeof(WarpKnnSmem<KMAX>);
+    AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cells));
     if (vel_sph) {
-        ++c.launches, k_ppart_dens_w<KMAX><<<grid_for(a.n, SPH_WARPS * SPH_QPW), SPH_WARPS * 32, sm, c.stream>>>(
+        ++c.launches, k_ppart_dens_w<KMAX><<<grid_for(a.n, SPH_WARPS * PP_QPW), SPH_WARPS * 32, sm, c.stream>>>(
             G, a.n, K, sv, pd_s, a.part_dens);
         AV_CUDA(cudaGetLastError());
         c.mark("ppart_dens");
@@ -767,7 +770,7 @@ static void run_sph_kernels_w(Ctx &c, const KnnGrid &G, const avism_params *p, c
         A.hp_s = hp_s; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
         A.ball_list = ball_list; A.ball_count = cnt_d;
         const int64_t nblk = (int64_t)((nx + 3) / 4) * ((nx + 3) / 4) * ((nx + 1) / 2);
-        ++c.launches, k_cells_knn_w<KMAX><<<(unsigned)nblk, SPH_WARPS * 32, sm, c.stream>>>(G, A);
+        ++c.launches, k_cells_knn_w<KMAX><<<(unsigned)nblk, SPH_WARPS * 32, sm_cells, c.stream>>>(G, A);
         AV_CUDA(cudaGetLastError());
         c.mark("cells_knn");
         int32_t nball = 0;
