@@ -230,19 +230,21 @@ __device__ __forceinline__ float query_r0(const KnnGrid &G, float qx, float qy, 
     return G.r0[b];
 }
 
-// the particle kernel stages its queries' neighbour masses per warp and sums
-// them after the searches, one lane per query; (KMAX + 2)-double rows keep the
+// rows of staged sums: (KMAX + 2) doubles or (KMAX + 4) floats keep the
 // summing lanes' 16-byte loads on distinct banks
 template <int KMAX> constexpr int SPH_ROW = KMAX + 2;
+template <int KMAX> constexpr int SPH_ROWF = KMAX + 4;
+// the particle kernel stages its queries' neighbour masses (f32, as stored) per
+// warp and sums them after the searches, one lane per query
 template <int KMAX>
 constexpr size_t sph_smem_bytes() {
     return (size_t)SPH_WARPS * sizeof(WarpKnnSmem<KMAX>) +
-           (size_t)SPH_WARPS * PP_QPW * SPH_ROW<KMAX> * sizeof(double);
+           (size_t)SPH_WARPS * PP_QPW * SPH_ROWF<KMAX> * sizeof(float);
 }
 template <int KMAX>
-__device__ __forceinline__ double *sph_rows(unsigned char *smem, int warp) {
-    return reinterpret_cast<double *>(smem + SPH_WARPS * sizeof(WarpKnnSmem<KMAX>)) +
-           (size_t)warp * PP_QPW * SPH_ROW<KMAX>;
+__device__ __forceinline__ float *sph_rows(unsigned char *smem, int warp) {
+    return reinterpret_cast<float *>(smem + SPH_WARPS * sizeof(WarpKnnSmem<KMAX>)) +
+           (size_t)warp * PP_QPW * SPH_ROWF<KMAX>;
 }
 // sequential REAL*8 sum of row[0..n) in order, two values per 16-byte load
 __device__ __forceinline__ double seq_sum(const double *row, int n) {
@@ -257,6 +259,21 @@ __device__ __forceinline__ double seq_sum(const double *row, int n) {
     if (j < n) s = s + row[j];
     return s;
 }
+// the same REAL*8 sum of f32 values, four per 16-byte load
+__device__ __forceinline__ double seq_sum(const float *row, int n) {
+    const float4 *r4 = reinterpret_cast<const float4 *>(row);
+    double s = 0.0;
+    int j = 0;
+    for (; j + 4 <= n; j += 4) {
+        const float4 v = r4[j >> 2];
+        s = s + (double)v.x;
+        s = s + (double)v.y;
+        s = s + (double)v.z;
+        s = s + (double)v.w;
+    }
+    for (; j < n; j++) s = s + (double)row[j];
+    return s;
+}
 
 // five blocks per SM (48 registers, a few spills): more warps in flight pay
 // for the spills (171 against 187 ms with four blocks at 512^3)
@@ -267,7 +284,7 @@ k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float
     extern __shared__ __align__(16) unsigned char wq_smem[];
     const int warp = threadIdx.x >> 5;
     WarpKnnSmem<KMAX> &S = reinterpret_cast<WarpKnnSmem<KMAX> *>(wq_smem)[warp];
-    double *acc = sph_rows<KMAX>(wq_smem, warp);              // one row of masses per query
+    float *acc = sph_rows<KMAX>(wq_smem, warp);               // one row of masses per query
     const int lane = threadIdx.x & 31;
     const int64_t i0 = ((int64_t)blockIdx.x * SPH_WARPS + warp) * PP_QPW;
     int my_cnt = 0;                                           // lane t: query t's count and h
@@ -278,7 +295,7 @@ k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float
         const float4 p = G.sp[i];
         const int cnt = knn_warp_exact<KMAX>(G, p.x, p.y, p.z, K, query_r0(G, p.x, p.y, p.z), S,
                                              reinterpret_cast<unsigned long long *>(S.d2));
-        for (int j = lane; j < cnt; j += 32) acc[t * SPH_ROW<KMAX> + j] = (double)sv[S.res_pos[j]].w;
+        for (int j = lane; j < cnt; j += 32) acc[t * SPH_ROWF<KMAX> + j] = sv[S.res_pos[j]].w;
         const float hk = sqrtf(__uint_as_float(S.res_d2[K - 1]));
         if (lane == t) {
             my_cnt = cnt;
@@ -289,7 +306,7 @@ k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float
     // the queries' sums side by side, one lane each
     const int64_t i = i0 + lane;
     if (lane < PP_QPW && i < n) {
-        const double bas8 = seq_sum(acc + lane * SPH_ROW<KMAX>, my_cnt);
+        const double bas8 = seq_sum(acc + lane * SPH_ROWF<KMAX>, my_cnt);
         const double pi = 3.141592653589793;     // DACOS(-1.D0)
         const float rho = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(my_hk, my_hk), my_hk)));
         pd_s[i] = rho;
@@ -751,9 +768,14 @@ static void run_sph_kernels_w(Ctx &c, const KnnGrid &G, const avism_params *p, c
     const int nx = L.g.nx;
     const int64_t nc = (int64_t)nx * nx * nx;
     AV_CUDA(cudaFuncSetAttribute(k_ppart_dens_w<KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    // the cell kernel stages its sums inside WarpKnnSmem: no extra rows, more L1
+    // the cell kernel stages its sums inside WarpKnnSmem: no extra rows, and a
+    // shared-memory carveout just large enough for its five blocks leaves the
+    // rest to L1, where the candidate records are read (K <= 32: 40%, 1% faster
+    // than the default at 512^3)
     const size_t sm_cells = (size_t)SPH_WARPS * sizeof(WarpKnnSmem<KMAX>);
+    const int carve = std::min(100, (int)((100 * 5 * (sm_cells + 1024) + 228 * 1024 - 1) / (228 * 1024)) + 5);
     AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cells));
+    AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
     if (vel_sph) {
         ++c.launches, k_ppart_dens_w<KMAX><<<grid_for(a.n, SPH_WARPS * PP_QPW), SPH_WARPS * 32, sm, c.stream>>>(
             G, a.n, K, sv, pd_s, a.part_dens);
