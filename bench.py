@@ -99,7 +99,9 @@ class ClockSampler:
 
 
 # ---- distributed plumbing -----------------------------------------------------
-def dist_setup(n_gpus: int):
+def dist_setup(n_gpus: int, backend: str | None = None):
+    """(rank, world, local rank) from the torchrun environment; joins the
+    process group when world > 1 (NCCL on GPUs, gloo otherwise)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -107,10 +109,19 @@ def dist_setup(n_gpus: int):
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=timedelta(seconds=600))
     return rank, world, local
+
+
+def replica_seed(rank: int) -> int:
+    """Seed of rank's snapshot: each rank runs its own iteration."""
+    return 1004 + rank
 
 
 def barrier(world):
@@ -124,7 +135,7 @@ def max_over_ranks(v: float, world: int) -> float:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -218,7 +229,7 @@ def run_ours(a):
     ncells = a.nx ** 3
     ne3 = (a.nx + 2 * (a.nx // 8)) ** 3
     with torch.no_grad():
-        parts = synth.lognormal_torch(n, min(a.nx, 512), a.box, -1.2, 1.0, 350.0, seed=1004 + rank, device=dev)
+        parts = synth.lognormal_torch(n, min(a.nx, 512), a.box, -1.2, 1.0, 350.0, seed=replica_seed(rank), device=dev)
         parts = synth.to_reader_units(parts)
     dev_parts = {k: parts[k].contiguous() for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
     host_parts = {k: v.cpu().pin_memory() for k, v in dev_parts.items()}
