@@ -209,6 +209,12 @@ ALG_BYTES = {
     "flags": lambda n, nc, ne3: 9 * ne3,
 }
 HBM_STAGES = ("divergence", "flags")
+# DRAM bytes (read + write) per unit of the dominant stage from one ncu capture
+# of k_cells_knn_w on the 256^3 / 2^24-particle case of this workload: 0.857 GB
+# read + 0.260 GB written for 2^24 cell queries.  The capture is too large to
+# take at 512^3 under the profiling size rule; the queries and particles both
+# scale by 8, so the traffic is scaled by the cells of the launch.
+TRAFFIC_PER_CELL = {"cells_knn": (0.857047040e9 + 0.260322560e9) / 2 ** 24}
 
 
 def run_ours(a):
@@ -306,7 +312,8 @@ def run_ours(a):
                 "e2e": {"value": e2e, "unit": "cells/s", "ms_per_step": ms_e2e,
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                             "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                             "unit": "GB/s", "frac": achieved / peak,
+                             "traffic": TRAFFIC_PER_CELL[dom] * ncells if dom in TRAFFIC_PER_CELL else None,
                              "alg_bytes_per_launch": alg, "ms_per_launch": st[dom],
                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback"},
                 "cpu_baseline": cpu,
