@@ -495,9 +495,11 @@ __device__ __noinline__ void ddens_nested(const DdensArgs &A, const float4 p, in
 // each; both passes then walk the cells as one flat loop, so the lanes of a warp
 // stay busy until the largest support is done instead of idling at the end of
 // every plane and row.  NORM still sums in the reference's (k, j, i) order.
-constexpr int DD_THREADS = 256, DD_RMAX = 40;
+// 28 rows per thread (28 KB per block) and six blocks per SM at 40 registers:
+// occupancy pays more than the particles whose longer lists go to ddens_nested
+constexpr int DD_THREADS = 256, DD_RMAX = 28;
 
-__global__ void __launch_bounds__(DD_THREADS) k_ddens(KnnGrid G, int64_t n, DdensArgs A) {
+__global__ void __launch_bounds__(DD_THREADS, 6) k_ddens(KnnGrid G, int64_t n, DdensArgs A) {
     __shared__ uint32_t rows[DD_RMAX * DD_THREADS];
     uint32_t *my = rows + threadIdx.x;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
