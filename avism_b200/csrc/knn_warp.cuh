@@ -3,12 +3,14 @@
 // One warp answers one query.  Given a radius R, the warp lists every row of
 // bins that the ball of radius R around the query can touch (one row per lane,
 // pruned in y/z by the row's gap and in x by the remaining reach, exactly as
-// knn_search prunes), concatenates the rows' particle ranges and scans them 32
+// knn_search prunes; with quarter-bin offsets the x range is cut at a quarter
+// of a bin), concatenates the rows' particle ranges and scans them 32
 // candidates at a time with all lanes busy.  Candidates with squared distance
 // <= R^2 are kept in a shared-memory buffer.  If at least K were kept, the K
 // nearest overall are the K smallest kept ones (nothing outside the ball can be
 // closer), and they are ranked exactly by (squared distance, original particle
-// index) -- the order of knn_search -- with a counting select.  If fewer than K
+// index) -- the order of knn_search -- by a bitonic sort verified on the full
+// squared distances, or by a counting select when that check fails.  If fewer than K
 // were kept the radius grows; if more than the buffer holds it shrinks; after a
 // bounded number of attempts the query falls back to knn_search.  The radius is
 // therefore only a starting point: the neighbour lists do not depend on it.
