@@ -260,7 +260,9 @@ __device__ __forceinline__ bool bitonic_select(const KnnGrid &G, int n, int K, W
 // the same arguments.  Returns the neighbour count (K unless fewer particles)
 // with S.res_d2 / S.res_pos holding them in ascending order, or -1 when the
 // attempts ran out (the caller then runs knn_search).
-template <int KMAX>
+// STATS: count queries, attempts and candidates into G.stats (a separate
+// instantiation, so the counters cost nothing when they are off)
+template <int KMAX, bool STATS = false>
 __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, float r0, WarpKnnSmem<KMAX> &S) {
     constexpr int CAP = WarpKnnSmem<KMAX>::CAP;
     const int lane = threadIdx.x & 31;
@@ -320,7 +322,7 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
                 }
                 count += __popc(m);
             }
-            if (G.stats && lane == 0) atomicAdd(&G.stats[2], (unsigned long long)T);
+            if (STATS && lane == 0) atomicAdd(&G.stats[2], (unsigned long long)T);
             __syncwarp();
         }
         if (count > CAP) {                               // too many: shrink
@@ -338,14 +340,14 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
             continue;
         }
         const int n = count;
-        if (G.stats && lane == 0) {
+        if (STATS && lane == 0) {
             atomicAdd(&G.stats[0], 1ULL);
             atomicAdd(&G.stats[1], (unsigned long long)(attempt + 1));
             atomicAdd(&G.stats[3], (unsigned long long)n);
         }
         if constexpr (KMAX == 32) {
             if (bitonic_select(G, n, K, S)) return min(n, K);
-            if (G.stats && lane == 0) atomicAdd(&G.stats[5], 1ULL);
+            if (STATS && lane == 0) atomicAdd(&G.stats[5], 1ULL);
         }
         // counting select: rank = #smaller squared distances + #equal ones with a smaller index
         for (int e = lane; e < n; e += 32) {
@@ -366,7 +368,7 @@ __device__ int knn_warp(const KnnGrid &G, float qx, float qy, float qz, int K, f
         __syncwarp();
         return min(n, K);
     }
-    if (G.stats && lane == 0) atomicAdd(&G.stats[4], 1ULL);
+    if (STATS && lane == 0) atomicAdd(&G.stats[4], 1ULL);
     return -1;
 }
 
@@ -387,10 +389,10 @@ __device__ int knn_warp_fallback(const KnnGrid &G, float qx, float qy, float qz,
 }
 
 // exact kNN of one query by the whole warp
-template <int KMAX>
+template <int KMAX, bool STATS = false>
 __device__ __forceinline__ int knn_warp_exact(const KnnGrid &G, float qx, float qy, float qz, int K, float r0,
                                               WarpKnnSmem<KMAX> &S, unsigned long long *col) {
-    const int cnt = knn_warp<KMAX>(G, qx, qy, qz, K, r0, S);
+    const int cnt = knn_warp<KMAX, STATS>(G, qx, qy, qz, K, r0, S);
     if (cnt >= 0) return cnt;
     return knn_warp_fallback<KMAX>(G, qx, qy, qz, K, S, col);
 }

@@ -277,7 +277,7 @@ __device__ __forceinline__ double seq_sum(const float *row, int n) {
 
 // five blocks per SM (48 registers, a few spills): more warps in flight pay
 // for the spills (171 against 187 ms with four blocks at 512^3)
-template <int KMAX>
+template <int KMAX, bool STATS>
 __global__ void __launch_bounds__(SPH_WARPS * 32, 5)
 k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float *__restrict__ pd_s,
                float *__restrict__ part_dens) {
@@ -293,7 +293,7 @@ k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float
         const int64_t i = i0 + t;
         if (i >= n) break;
         const float4 p = G.sp[i];
-        const int cnt = knn_warp_exact<KMAX>(G, p.x, p.y, p.z, K, query_r0(G, p.x, p.y, p.z), S,
+        const int cnt = knn_warp_exact<KMAX, STATS>(G, p.x, p.y, p.z, K, query_r0(G, p.x, p.y, p.z), S,
                                              reinterpret_cast<unsigned long long *>(S.d2));
         for (int j = lane; j < cnt; j += 32) acc[t * SPH_ROWF<KMAX> + j] = sv[S.res_pos[j]].w;
         const float hk = sqrtf(__uint_as_float(S.res_d2[K - 1]));
@@ -316,7 +316,7 @@ k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float
 
 // five blocks per SM (48 registers): the cell kernel gains more from the extra
 // warps than it loses to spills (six blocks at 40 registers spill too much)
-template <int KMAX>
+template <int KMAX, bool STATS>
 __global__ void __launch_bounds__(SPH_WARPS * 32, 5)
 k_cells_knn_w(KnnGrid G, CellArgs A) {
     extern __shared__ __align__(16) unsigned char wq_smem[];
@@ -339,7 +339,7 @@ k_cells_knn_w(KnnGrid G, CellArgs A) {
         if (A.smask && A.smask[c] == 0) continue;
         const float qx = A.rad[ix - A.rad_lo], qy = A.rad[jy - A.rad_lo], qz = A.rad[kz - A.rad_lo];
         const int K = A.K;
-        const int cnt = knn_warp_exact<KMAX>(G, qx, qy, qz, K, query_r0(G, qx, qy, qz), S,
+        const int cnt = knn_warp_exact<KMAX, STATS>(G, qx, qy, qz, K, query_r0(G, qx, qy, qz), S,
                                              reinterpret_cast<unsigned long long *>(S.d2));
         const float hk = sqrtf(__uint_as_float(S.res_d2[cnt - 1]));
         if (!(hk > A.dx)) {                       // ball_search(TREE, TAR, DX) branch
@@ -761,25 +761,25 @@ __global__ void k_zero_f32(int64_t n, float *a) {
     if (i < n) a[i] = 0.0f;
 }
 
-template <int KMAX>
-static void run_sph_kernels_w(Ctx &c, const KnnGrid &G, const avism_params *p, const Level &L,
+template <int KMAX, bool STATS>
+static void run_sph_kernels_ws(Ctx &c, const KnnGrid &G, const avism_params *p, const Level &L,
                               const P2G &a, const float *rad_d, bool vel_sph, bool need_h_cells,
                               const float4 *sv, float *pd_s, float *hp_s) {
     const size_t sm = sph_smem_bytes<KMAX>();
     const int K = p->kneighbours;
     const int nx = L.g.nx;
     const int64_t nc = (int64_t)nx * nx * nx;
-    AV_CUDA(cudaFuncSetAttribute(k_ppart_dens_w<KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    AV_CUDA(cudaFuncSetAttribute(k_ppart_dens_w<KMAX, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     // the cell kernel stages its sums inside WarpKnnSmem: no extra rows, and a
     // shared-memory carveout just large enough for its five blocks leaves the
     // rest to L1, where the candidate records are read (K <= 32: 40%, 1% faster
     // than the default at 512^3)
     const size_t sm_cells = (size_t)SPH_WARPS * sizeof(WarpKnnSmem<KMAX>);
     const int carve = std::min(100, (int)((100 * 5 * (sm_cells + 1024) + 228 * 1024 - 1) / (228 * 1024)) + 5);
-    AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cells));
-    AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+    AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cells));
+    AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX, STATS>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
     if (vel_sph) {
-        ++c.launches, k_ppart_dens_w<KMAX><<<grid_for(a.n, SPH_WARPS * PP_QPW), SPH_WARPS * 32, sm, c.stream>>>(
+        ++c.launches, k_ppart_dens_w<KMAX, STATS><<<grid_for(a.n, SPH_WARPS * PP_QPW), SPH_WARPS * 32, sm, c.stream>>>(
             G, a.n, K, sv, pd_s, a.part_dens);
         AV_CUDA(cudaGetLastError());
         c.mark("ppart_dens");
@@ -794,7 +794,7 @@ static void run_sph_kernels_w(Ctx &c, const KnnGrid &G, const avism_params *p, c
         A.hp_s = hp_s; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
         A.ball_list = ball_list; A.ball_count = cnt_d;
         const int64_t nblk = (int64_t)((nx + 3) / 4) * ((nx + 3) / 4) * ((nx + 1) / 2);
-        ++c.launches, k_cells_knn_w<KMAX><<<(unsigned)nblk, SPH_WARPS * 32, sm_cells, c.stream>>>(G, A);
+        ++c.launches, k_cells_knn_w<KMAX, STATS><<<(unsigned)nblk, SPH_WARPS * 32, sm_cells, c.stream>>>(G, A);
         AV_CUDA(cudaGetLastError());
         c.mark("cells_knn");
         int32_t nball = 0;
@@ -814,6 +814,15 @@ static void run_sph_kernels_w(Ctx &c, const KnnGrid &G, const avism_params *p, c
         if (a.hpart) ++c.launches, k_unbin_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, G.sp, hp_s, a.hpart);
     }
     AV_CUDA(cudaGetLastError());
+}
+
+// the counters' instantiation only when they are on
+template <int KMAX>
+static void run_sph_kernels_w(Ctx &c, const KnnGrid &G, const avism_params *p, const Level &L, const P2G &a,
+                              const float *rad_d, bool vel_sph, bool need_h_cells, const float4 *sv, float *pd_s,
+                              float *hp_s) {
+    if (G.stats) run_sph_kernels_ws<KMAX, true>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
+    else run_sph_kernels_ws<KMAX, false>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
 }
 
 template <int KCAP>
