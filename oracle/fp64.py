@@ -1,6 +1,6 @@
-"""FP64 restatement of the SPH particle-to-grid path (test infrastructure only).
+"""FP64 restatement of the particle-to-grid path (test infrastructure only).
 
-The definitions are those of orc_interp.c (src/particles.f90: PPART_DENS
+The definitions are those of orc_interp.c (src/particles.f90: TSC 16-271, PPART_DENS
 742-801, VVEL_INTERP_SPH_VW 806-929 with KERNEL_FUNC 935-963, FILL_H_ZEROS
 398-430, DDENS_INTERP_SPH 434-617), but every quantity is double precision and
 the neighbour searches rank double-precision distances (scipy's cKDTree).  It
@@ -113,3 +113,49 @@ def _ddens(x, y, z, h, mm, rad, off, nx, dx, chunk_cells=2 ** 24):
             lone = lone[inside]
             np.add.at(u, (ix[lone] - 1) + nx * ((jy[lone] - 1) + nx * (kz[lone] - 1)), mm[lone])
     return u
+
+
+def _tsc_axis(v, rad, off, nx, dx, periodic):
+    """TSC cell and the three weights of one coordinate (particles.f90:56-96)."""
+    r1 = rad[1 - off] - 0.5 * dx
+    rn = rad[nx - off] + 0.5 * dx
+    if periodic:
+        leng = rn - r1
+        v = np.where(v < r1, v + leng, v)
+        v = np.where(v >= rn, v - leng, v)
+    i = np.floor((v - rad[1 - off]) / dx + 0.49999).astype(np.int64) + 1
+    t0 = 1.5 - np.abs(rad[i - 1 - off] - v) / dx
+    t1 = np.abs(rad[i - off] - v) / dx
+    t2 = 1.5 - np.abs(rad[i + 1 - off] - v) / dx
+    return i, (0.5 * t0 * t0, 0.75 - t1 * t1, 0.5 * t2 * t2)
+
+
+def tsc_fp64(p, x, y, z, vx, vy, vz, m):
+    """(u_mass, u2, u3, u4) of DENS_INTERP_TSC and VEL_INTERP_TSC in FP64
+    (particles.f90:16-271; non-periodic cells outside 1..NX are dropped)."""
+    from .oracle import grid_setup
+    g, radx = grid_setup(p)
+    nx, per = int(p.nx), bool(p.periodic)
+    dx = float(g.dx)
+    rad = np.asarray(radx, np.float64)
+    off = int(g.rad_lo)
+    x, y, z, vx, vy, vz, mm = (np.asarray(a, np.float64) for a in (x, y, z, vx, vy, vz, m))
+    (ci, wx), (cj, wy), (ck, wz) = (_tsc_axis(v, rad, off, nx, dx, per) for v in (x, y, z))
+    nc = nx ** 3
+    um, s2, s3, s4, wt = (np.zeros(nc) for _ in range(5))
+    for a in range(3):
+        for b in range(3):
+            for c in range(3):
+                i3, j3, k3 = ci + c - 1, cj + b - 1, ck + a - 1
+                if per:
+                    i3, j3, k3 = ((t - 1) % nx + 1 for t in (i3, j3, k3))
+                ok = (i3 >= 1) & (i3 <= nx) & (j3 >= 1) & (j3 <= nx) & (k3 >= 1) & (k3 <= nx)
+                cid = ((i3 - 1) + nx * ((j3 - 1) + nx * (k3 - 1)))[ok]
+                w = (wx[c] * wy[b] * wz[a])[ok]
+                um += np.bincount(cid, weights=mm[ok] * w, minlength=nc)
+                s2 += np.bincount(cid, weights=vx[ok] * w, minlength=nc)
+                s3 += np.bincount(cid, weights=vy[ok] * w, minlength=nc)
+                s4 += np.bincount(cid, weights=vz[ok] * w, minlength=nc)
+                wt += np.bincount(cid, weights=w, minlength=nc)
+    wei = np.where(wt == 0.0, 1.0, wt)
+    return dict(u_mass=um, u2=s2 / wei, u3=s3 / wei, u4=s4 / wei)

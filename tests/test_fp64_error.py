@@ -49,3 +49,17 @@ def test_fp64_restatement_conserves_mass(pair):
     # DDENS does not wrap: only mass whose support leaves the grid is lost
     total = np.sum(np.asarray(parts["m"], np.float64))
     assert 0.9 * total < np.sum(f64["u_mass"]) <= total * (1 + 1e-12)
+
+
+@pytest.mark.parametrize("periodic", [1, 0])
+def test_tsc_fields_close_to_fp64(periodic):
+    """TSC density and velocity (the GPU's are within 1e-5 of the oracle's)."""
+    from oracle.fp64 import tsc_fp64
+    parts = synth.to_reader_units(synth.mock_spheres(n=2 ** 15, box=50.0, seed=1001))
+    p = Params(nx=32, periodic=periodic, lado0=50.0, flag_vel_interp=0, flag_dens_interp=0)
+    args = [parts[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")]
+    f32, f64 = O.particles_to_grid(p, *args), tsc_fp64(p, *args)
+    r = _rel(f32["u_mass"], f64["u_mass"])
+    assert np.quantile(r, 0.99) < 1e-6 and np.max(r) < 1e-4
+    for k in ("u2", "u3", "u4"):
+        assert np.max(_rel(f32[k], f64[k], add_mean=True)) < 1e-5, k
