@@ -4,8 +4,9 @@ The definitions are those of orc_interp.c (src/particles.f90: TSC 16-271, PPART_
 742-801, VVEL_INTERP_SPH_VW 806-929 with KERNEL_FUNC 935-963, FILL_H_ZEROS
 398-430, DDENS_INTERP_SPH 434-617), but every quantity is double precision and
 the neighbour searches rank double-precision distances (scipy's cKDTree).  It
-states the error of the REAL*4 path -- the oracle, which the GPU path equals
-bit for bit -- against the same method in FP64, field by field.
+states the error of the REAL*4 path -- the oracle, which the GPU's SPH fields
+equal bit for bit and its TSC fields within 1e-5 -- against the same method in
+FP64, field by field.
 
 Only the arithmetic differs from the REAL*4 path: grid coordinates are the
 REAL*4 RADX values, the ball fallback is taken where the K-th distance is at
