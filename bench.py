@@ -325,6 +325,7 @@ def run_ours(a):
                 "plain": {"ms_per_step": ms_plain, "value": world * ncells / (ms_plain / 1e3), "unit": "cells/s",
                           "learned_speedup": ms_plain / ms_dev},
                 "roofline_stencils": stencils,
+                "particles_per_s": {"value": world * n / (ms_dev / 1e3), "e2e": world * n / (ms_e2e / 1e3)},
                 "stages_ms": {k: round(v, 3) for k, v in st.items()},
                 "stages_ms_plain": {k: round(statistics.mean(s_.get(k, 0.0) for s_ in stages_p), 3)
                                     for k in stages_p[0].keys()}}
