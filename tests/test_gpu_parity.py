@@ -248,3 +248,25 @@ def test_voids_in_voids_two_levels(gpu):
     # every level-1 cube grows inside a level-0 void
     father = np.asarray(g1["cubes"]["father"])
     assert np.all(father > 0)
+
+
+@pytest.mark.parametrize("case", ["straddling", "overlapping"])
+def test_known_answer_fields_match_oracle(gpu, case):
+    """The oracle's known-answer voids (a void across the periodic boundary, two
+    overlapping holes merged into one) give the same catalogue on the GPU."""
+    import test_oracle_pins as K
+    L = 64.0
+    if case == "straddling":
+        parts = K._void_field(2 ** 16, L, [(np.array([L / 2 - 2.0, 5.0, -7.0]), 12.0)], 0.1, 0.5, seed=21)
+    else:
+        parts = K._void_field(2 ** 16, L, [(np.array([-5.0, 0.0, 0.0]), 9.0), (np.array([5.0, 0.0, 0.0]), 9.0)],
+                              0.1, 0.5, seed=22)
+    p = Params(nx=32, lado0=L, periodic=1, rmin=2.0)
+    o = O.run_level(p, parts)
+    g = gpu.run_level(p, parts, capacity=100000)
+    assert g["nvoid"] == o["vf"]["nvoid"]
+    for k in ("indice", "uvoid", "ncellv"):
+        assert np.array_equal(np.asarray(g["cat"][k]), np.asarray(o["cat"][k])), k
+    for k in ("volnew", "gxc", "gyc", "gzc"):
+        assert np.array_equal(np.asarray(g["cat"][k]), np.asarray(o["cat"][k])), k
+    assert g["cat"]["nvoidt"] == o["cat"]["nvoidt"]

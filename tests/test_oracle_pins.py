@@ -181,3 +181,66 @@ def test_single_tophat_void():
     assert np.linalg.norm(centre - c) < 4.0          # within two cells of the planted centre
     assert 6.0 < cat["req"][big] < 16.0
     assert cat["umean"][big] < 0.5
+
+
+def _void_field(n, L, holes, contrast, outflow, seed):
+    """Poisson particles in a periodic box with underdense spheres (centre, radius),
+    which may straddle the box boundary; radial outflow inside each sphere."""
+    from avism_b200 import synth
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(-L / 2, L / 2, (4 * n, 3))
+    keep = np.ones(len(x), bool)
+    vel = rng.normal(0.0, 30.0, x.shape)
+    for c, r in holes:
+        dv = x - np.asarray(c)
+        dv -= L * np.round(dv / L)                          # minimum image
+        inside = np.sqrt((dv ** 2).sum(1)) < r
+        keep &= ~inside | (rng.random(len(x)) < contrast)
+        vel[inside] += outflow * 100.0 * dv[inside]
+    x, vel = x[keep][:n], vel[keep][:n]
+    parts = dict(x=x[:, 0], y=x[:, 1], z=x[:, 2], vx=vel[:, 0], vy=vel[:, 1], vz=vel[:, 2],
+                 m=np.full(len(x), synth._mean_mass(len(x), L)))
+    return synth.to_reader_units({k: np.asarray(v, np.float32) for k, v in parts.items()})
+
+
+def _main_voids(cat):
+    main = np.flatnonzero(cat["uvoid"] == -1)
+    return main, np.stack([cat["gxc"][main], cat["gyc"][main], cat["gzc"][main]], 1)
+
+
+def test_void_straddling_the_periodic_boundary():
+    """A void centred 2 cMpc inside the +x face wraps onto the -x side: it is
+    found once, at its centre modulo the box, not as two half-voids."""
+    L = 64.0
+    c = np.array([L / 2 - 2.0, 5.0, -7.0])
+    parts = _void_field(2 ** 16, L, [(c, 12.0)], 0.1, 0.5, seed=21)
+    r = O.run_level(Params(nx=32, lado0=L, periodic=1, rmin=2.0), parts)
+    main, centres = _main_voids(r["cat"])
+    dv = centres - c
+    dv -= L * np.round(dv / L)
+    near = np.sqrt((dv ** 2).sum(1)) < 8.0
+    assert near.sum() == 1, centres[near]
+    big = main[near][0]
+    assert np.sqrt((dv[near][0] ** 2).sum()) < 4.0
+    assert 6.0 < r["cat"]["req"][big] < 16.0
+
+
+def test_two_overlapping_holes_merge_into_one_void():
+    """Two overlapping underdense spheres give cubes at both lobes; MERGE_VOID
+    joins them into one main void that owns the other lobe's cubes."""
+    L = 64.0
+    a, b = np.array([-5.0, 0.0, 0.0]), np.array([5.0, 0.0, 0.0])
+    parts = _void_field(2 ** 16, L, [(a, 9.0), (b, 9.0)], 0.1, 0.5, seed=22)
+    r = O.run_level(Params(nx=32, lado0=L, periodic=1, rmin=2.0), parts)
+    cat, cubes = r["cat"], r["vf"]["cubes"]
+    main, centres = _main_voids(cat)
+    near = np.sqrt((centres ** 2).sum(1)) < 12.0            # main voids around the pair
+    assert near.sum() == 1, centres[near]
+    owner = main[near][0] + 1                                 # 1-based void id
+    # the main void owns cubes grown in both lobes
+    g, _ = O.grid_setup(Params(nx=32, lado0=L, periodic=1))
+    cx = g.rx1 + (np.asarray(cubes["icx"], np.float64) - 1) * g.dx
+    uvoid = np.asarray(cat["uvoid"])
+    owned = (uvoid == owner) | (np.arange(len(uvoid)) + 1 == owner)
+    assert owned.sum() >= 2
+    assert cx[owned].min() < -2.0 and cx[owned].max() > 2.0
