@@ -270,3 +270,32 @@ def test_known_answer_fields_match_oracle(gpu, case):
     for k in ("volnew", "gxc", "gyc", "gzc"):
         assert np.array_equal(np.asarray(g["cat"][k]), np.asarray(o["cat"][k])), k
     assert g["cat"]["nvoidt"] == o["cat"]["nvoidt"]
+
+
+def test_survey_mask_paths(gpu, mock1):
+    """SMASK (survey mode's observed-cell mask): no SPH interpolation in masked
+    cells, and no flag, centre or growth through them -- as in the oracle."""
+    p = Params(nx=64, periodic=1, lado0=100.0)
+    g, radx = O.grid_setup(p)
+    rad = radx.astype(np.float64)
+
+    def sphere_mask(lo, n):                       # observed: within 35 cMpc of the origin
+        i = np.arange(n ** 3)
+        c = [rad[(i // n ** a) % n + lo - g.rad_lo] for a in range(3)]
+        return ((c[0] ** 2 + c[1] ** 2 + c[2] ** 2) < 35.0 ** 2).astype(np.int8)
+
+    smask = sphere_mask(1, g.nx)
+    args = [mock1[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")]
+    o = O.particles_to_grid(p, *args, smask=smask)
+    gg = gpu.particles_to_grid(p, mock1, smask=smask)
+    for k in ("part_dens", "hpart", "u2", "u3", "u4", "u_mass"):
+        assert np.array_equal(o[k], gg[k]), k
+    assert np.all(o["u2"][smask == 0] == 0.0)
+    smask_ext = sphere_mask(g.low1, g.ne)
+    u1, dv, _ = O.fields(p, o["u_mass"], o["u2"], o["u3"], o["u4"])
+    vo = O.voidfind(p, u1, dv, smask_ext=smask_ext)
+    assert np.array_equal(vo["flags"], gpu.mark_all(p, u1, dv, smask_ext=smask_ext))
+    cubes, nv = gpu.voidfind(p, u1, dv, smask_ext=smask_ext)
+    assert nv == vo["nvoid"] > 0
+    for k in cubes:
+        assert np.array_equal(cubes[k], vo["cubes"][k]), k
