@@ -299,3 +299,14 @@ def test_survey_mask_paths(gpu, mock1):
     assert nv == vo["nvoid"] > 0
     for k in cubes:
         assert np.array_equal(cubes[k], vo["cubes"][k]), k
+
+
+@pytest.mark.parametrize("k,periodic", [(16, 1), (48, 1), (48, 0), (100, 1)])
+def test_sph_fields_other_k(gpu, mock_small, k, periodic):
+    """The SPH fields for k other than 32 (the 64- and 128-wide warp kNN
+    instantiations and the counting select), periodic and not."""
+    p = Params(nx=32, periodic=periodic, lado0=64.0, kneighbours=k)
+    o = O.particles_to_grid(p, *(mock_small[q] for q in ("x", "y", "z", "vx", "vy", "vz", "m")))
+    g = gpu.particles_to_grid(p, mock_small)
+    for key in ("part_dens", "hpart", "u2", "u3", "u4", "u_mass"):
+        assert np.array_equal(o[key], g[key]), key
