@@ -63,3 +63,40 @@ def test_tsc_fields_close_to_fp64(periodic):
     assert np.quantile(r, 0.99) < 1e-6 and np.max(r) < 1e-4
     for k in ("u2", "u3", "u4"):
         assert np.max(_rel(f32[k], f64[k], add_mean=True)) < 1e-5, k
+
+
+def test_fp64_restatement_against_brute_force():
+    """Pin oracle/fp64.py itself: PPART_DENS, one cell's VVEL and one particle's
+    DDENS support recomputed with plain loops over all particles / cells."""
+    rng = np.random.default_rng(3)
+    L, nx, K, n = 16.0, 8, 8, 600
+    x, y, z = (rng.uniform(-L / 2, L / 2, n).astype(np.float32) for _ in range(3))
+    vx, vy, vz = (rng.normal(0, 100, n).astype(np.float32) for _ in range(3))
+    m = np.full(n, 2.0, np.float32)
+    p = Params(nx=nx, periodic=1, lado0=L, kneighbours=K)
+    f = particles_to_grid_fp64(p, x, y, z, vx, vy, vz, m)
+    P = np.stack([x, y, z], 1).astype(np.float64)
+
+    def dist(a, b):
+        d = np.abs(a - b)
+        d = np.minimum(d, L - d)
+        return np.sqrt((d ** 2).sum(-1))
+
+    # PPART_DENS of particle 5: K nearest (itself included), mass over the ball of the K-th distance
+    d5 = np.sort(dist(P, P[5]))
+    assert np.isclose(f["part_dens"][5], 2.0 * K / (4.0 / 3.0 * np.pi * d5[K - 1] ** 3), rtol=1e-12)
+    # VVEL of cell (3, 4, 5): M4 weights over its K nearest, m / rho_p
+    g, radx = O.grid_setup(p)
+    rad = radx.astype(np.float64)
+    q = np.array([rad[3 - g.rad_lo], rad[4 - g.rad_lo], rad[5 - g.rad_lo]])
+    dq = dist(P, q)
+    nn = np.argsort(dq, kind="stable")[:K]
+    h = dq[nn].max()
+    assert h > float(g.dx)                                  # the kNN branch, not the ball
+    qq = dq[nn] / (h / 2)
+    w = np.where(qq <= 1, 1 - 1.5 * qq ** 2 * (1 - 0.5 * qq), np.where(qq <= 2, 0.25 * (2 - qq) ** 3, 0))
+    w = w * 2.0 / f["part_dens"][nn]
+    c = (3 - 1) + nx * ((4 - 1) + nx * (5 - 1))
+    assert np.isclose(f["u2"][c], (w * vx[nn]).sum() / w.sum(), rtol=1e-12)
+    # DDENS: the grid total is the mass of the particles whose supports stay in the grid
+    assert 0.5 * m.sum() < f["u_mass"].sum() <= m.sum() * (1 + 1e-12)
