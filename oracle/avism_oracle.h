@@ -6,9 +6,11 @@
  * __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the checker.
  * The product (avism_b200/, libavism_gpu.so) never links, loads or calls it.
  *
- * Parity status: the reference ships no golden vectors and cannot be compiled
- * here (no Fortran compiler), so this oracle is pinned by analytic known-answer
- * cases (tests/test_oracle_pins.py) rather than by reference outputs.
+ * Parity status: parity unpinned by the reference.  The reference ships no
+ * golden vectors and cannot be compiled here (no Fortran compiler), so this
+ * oracle is pinned by analytic known-answer cases (tests/test_oracle_pins.py),
+ * brute-force kNN and an independent INDEXX restatement rather than by
+ * reference outputs.
  *
  * Floating point: compiled with -ffp-contract=off; every f32/f64 operation and
  * promotion point follows the Fortran expression it restates (cited per function).

@@ -1,5 +1,8 @@
 """ctypes wrapper of the C oracle (oracle/liboracle.so) -- test infrastructure.
 
+Parity unpinned by the reference: it cannot be built here (Fortran) and ships
+no golden vectors; the oracle is pinned by known-answer cases instead.
+
 Every function restates a reference routine; see the C sources for the
 file:line each follows.  Arrays are numpy, grids Fortran column-major and
 flattened (x fastest), index outputs keep the reference's values.
