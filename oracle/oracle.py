@@ -24,10 +24,9 @@ _lib = None
 
 
 def build(force: bool = False) -> str:
-    """Compile liboracle.so with the committed Makefile."""
-    if force or not os.path.exists(_LIB):
-        subprocess.run(["make", "-C", _HERE, "-B" if force else "liboracle.so"],
-                       check=True, capture_output=True)
+    """Compile liboracle.so with the committed Makefile (make rebuilds it when a
+    source or header is newer than the library)."""
+    subprocess.run(["make", "-C", _HERE, "-B" if force else "liboracle.so"], check=True, capture_output=True)
     return _LIB
 
 

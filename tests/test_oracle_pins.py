@@ -244,3 +244,21 @@ def test_two_overlapping_holes_merge_into_one_void():
     owned = (uvoid == owner) | (np.arange(len(uvoid)) + 1 == owner)
     assert owned.sum() >= 2
     assert cx[owned].min() < -2.0 and cx[owned].max() > 2.0
+
+
+def test_req_follows_the_fortran_promotions():
+    """REQ = ((3.*VOLM)/(4.*PI))**(1./3.) (src/avism.f90:2071): 3.*VOLM rounds in
+    REAL*4, the quotient and the power are REAL*8 with the REAL*4 exponent 1./3."""
+    from avism_b200 import synth
+    parts = synth.to_reader_units(synth.mock_spheres(n=2 ** 16, box=64.0, nsph=8, rmin=4.0, rmax=8.0, seed=5))
+    r = O.run_level(Params(nx=48, lado0=64.0, periodic=1, rmin=1.0), parts)   # dx^3 not a power of two
+    cat = r["cat"]
+    main = np.flatnonzero(cat["uvoid"] == -1)
+    v = cat["volnew"][main].astype(np.float32)
+    third = np.float64(np.float32(1.0) / np.float32(3.0))
+    four_pi = 4.0 * np.arccos(-1.0)
+    expect = np.power((np.float32(3.0) * v).astype(np.float64) / four_pi, third).astype(np.float32)
+    assert np.array_equal(cat["req"][main], expect)
+    # the case is one where the REAL*8 product 3*VOLM would give another REQ
+    wrong = np.power(3.0 * v.astype(np.float64) / four_pi, third).astype(np.float32)
+    assert np.any(wrong != expect)
