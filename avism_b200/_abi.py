@@ -18,7 +18,7 @@ AVISM_OK = 0
 STATUS_NAMES = {
     0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_OOM", 4: "ERR_NVOID_MAX",
     5: "ERR_OUT_OF_BOX", 6: "ERR_TIMEOUT", 7: "ERR_NO_DEVICE", 8: "ERR_UNSUPPORTED",
-    9: "ERR_INTERNAL",
+    9: "ERR_INTERNAL", 10: "ERR_IO",
 }
 # messages of the reference's STOP statements for the codes that have one
 STOP_TEXT = {

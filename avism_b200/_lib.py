@@ -43,6 +43,11 @@ SIGNATURES = {
     "avism_gpu_knn_noalloc": (C.c_int, [C.c_int, _c_void, _i64, _c_void, _c_void, _c_void, _f32, _i64,
                                         _c_void, _c_void, _c_void, _i32, _c_void, _c_void, C.c_char_p,
                                         _i32]),
+    "avism_io_particle_header": (C.c_int, [C.c_char_p, _c_void, _c_void]),
+    "avism_io_read_particles": (C.c_int, [C.c_char_p, _i64] + [_c_void] * 7),
+    "avism_io_write_headers": (C.c_int, [C.c_char_p, C.c_char_p] + [_i32] * 6 + [_f32]),
+    "avism_io_append_level": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, _c_void, _i32, _i32, _f32]
+                              + [_c_void] * 5),
 }
 
 _lib = None

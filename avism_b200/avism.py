@@ -9,6 +9,7 @@ stops, its STOP text.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -53,6 +54,61 @@ def grid_setup(p: Params):
     rad = np.zeros(g.rad_hi - g.rad_lo + 1, np.float32)
     lib.avism_gpu_grid_setup(C.byref(pc), C.byref(g), _vp(rad))
     return g, rad
+
+
+# ---- on-disk formats (host only) ---------------------------------------------
+def _io_chk(st, what):
+    if st != AVISM_OK:
+        raise AvismError(st, what)
+
+
+def _path(p):
+    return None if p is None else os.fsencode(p)
+
+
+def read_particle_file(path) -> dict:
+    """A READ_BINARY_PART_1 particle file (src/reader.f90:410-460): x, y, z, vx,
+    vy, vz, m as stored (cMpc, km/s, Msun) and the redshift zeta."""
+    lib = _lib.load()
+    n, zeta = C.c_int64(), C.c_float()
+    _io_chk(lib.avism_io_particle_header(_path(path), C.byref(n), C.byref(zeta)), f"particle file {path}")
+    keys = ("x", "y", "z", "vx", "vy", "vz", "m")
+    out = {k: np.zeros(n.value, np.float32) for k in keys}
+    _io_chk(lib.avism_io_read_particles(_path(path), n.value, *(_vp(out[k]) for k in keys)), f"particle file {path}")
+    out["zeta"] = zeta.value
+    return out
+
+
+def write_catalogue_headers(voids_path, cubes_path, nlev, levmin, levmax, ncox, ncoy, ncoz, lado0):
+    """First lines of the voids (and cubes) files of one iteration (src/avism.f90:710-722)."""
+    _io_chk(_lib.load().avism_io_write_headers(_path(voids_path), _path(cubes_path), nlev, levmin, levmax,
+                                               ncox, ncoy, ncoz, lado0), "catalogue headers")
+
+
+def append_catalogue_level(voids_path, p: Params, res: dict, nvoidp: int = 0, req_parent=None, cubes_path=None,
+                           map_path=None, u1co_ext=None, diverco_ext=None):
+    """One level of a run_level / run_sublevel result (``cubes``, ``nvoid``,
+    ``cat``, ``meandens``) into the voids, cubes and map files
+    (src/avism.f90:2026-2085)."""
+    nv = int(res["nvoid"])
+    cb = Cubes.from_dict(res["cubes"], nv) if res.get("cubes") is not None else None
+    cat = res["cat"]
+    vo = Voids(max(nv, 1), None)
+    for k in vo.arr:
+        vo.arr[k][:nv] = np.asarray(cat[k])[:nv]
+    marca = cat.get("marca")
+    if marca is not None:
+        vo.marca = np.ascontiguousarray(marca, np.int32)
+        vo.c.marca = ptr(vo.marca, C.c_int32)
+    vo.c.nvoid2, vo.c.nvoidt, vo.c.volt_clean = int(cat["nvoid2"]), int(cat["nvoidt"]), float(cat["volt_clean"])
+    rp = None if req_parent is None else _f32(req_parent)
+    u1 = None if u1co_ext is None else _f32(u1co_ext)
+    dv = None if diverco_ext is None else _f32(diverco_ext)
+    pc = p.to_c()
+    _io_chk(_lib.load().avism_io_append_level(
+        _path(voids_path), _path(cubes_path), _path(map_path), C.byref(pc), nv, int(nvoidp),
+        float(res["meandens"]), C.byref(cb.c) if cb else None, C.byref(vo.c), _vp(rp), _vp(u1), _vp(dv)),
+        "catalogue level")
 
 
 class AvismGPU:

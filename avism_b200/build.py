@@ -25,7 +25,7 @@ NVCC_FLAGS = [
 
 
 def sources():
-    return [os.path.join(CSRC, "avism_all.cu"), os.path.join(CSRC, "merge.cpp")]
+    return [os.path.join(CSRC, "avism_all.cu"), os.path.join(CSRC, "merge.cpp"), os.path.join(CSRC, "io.cpp")]
 
 
 def _stale() -> bool:

@@ -38,7 +38,9 @@ enum {
     AVISM_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up            */
     AVISM_ERR_NO_DEVICE = 7,    /* no CUDA device / wrong architecture           */
     AVISM_ERR_UNSUPPORTED = 8,  /* option not implemented by this library        */
-    AVISM_ERR_INTERNAL = 9      /* internal consistency check failed             */
+    AVISM_ERR_INTERNAL = 9,     /* internal consistency check failed             */
+    AVISM_ERR_IO = 10           /* a file could not be opened, read or written,  */
+                                /* or its records are not the expected ones      */
 };
 
 /* ---- parameters: POD mirror of config/voids.dat (src/avism.f90:173-254) -- */
@@ -286,6 +288,46 @@ int avism_gpu_knn_noalloc(int device, void *stream, int64_t n, const float *x,
                           const float *qx, const float *qy, const float *qz,
                           int32_t k, int64_t *idx, float *dist, char *errbuf,
                           int32_t errlen);
+
+/* ---- on-disk formats at the boundary (host only: no context, no GPU) ------
+ * Particle files of READ_BINARY_PART_1 (src/reader.f90:410-460): Fortran
+ * sequential unformatted records with 4-byte length markers -- [int64 NPARTT,
+ * REAL*4 ZETA], then x, y, z [cMpc], vx, vy, vz [km/s] and m [Msun], NPARTT
+ * REAL*4 values each.  The values come back as stored; the reference divides
+ * masses by UM and velocities by UV right after reading (src/reader.f90:455-458).
+ * avism_io_read_particles fails with AVISM_ERR_ARG when NPARTT > capacity
+ * (the reference's 'NPARTT > PARTIRED' stop) and AVISM_ERR_IO on any record
+ * whose markers do not frame the expected length.                            */
+int avism_io_particle_header(const char *path, int64_t *n, float *zeta);
+int avism_io_read_particles(const char *path, int64_t capacity, float *x, float *y, float *z,
+                            float *vx, float *vy, float *vz, float *m);
+
+/* The voids / cubes catalogues and the map file of one iteration
+ * (src/avism.f90:710-722 and 2026-2085), as tools/read_voids.py reads them.
+ * avism_io_write_headers creates the voids file (and the cubes file when
+ * cubes_path is not NULL) with their first lines: NLEV LEVMIN LEVMAX NCOX NCOY
+ * NCOZ LADO0, and NLEV LEVMIN LEVMAX.
+ * avism_io_append_level appends one level, as run_level / run_sublevel left it:
+ *  - voids: IR NVOID NVOIDT NVOIDP VOLT_CLEAN/LADO0^3 MEANDENS, then for every
+ *    main void in INDICE order: IND XC YC ZC GXC GYC GZC VOLM REQ UMEAN EPS IP
+ *    INDP REQPP MTOT, with INDP = FATHER(IND) and REQPP its parent's REQ above
+ *    LEVMIN (req_parent: the parent level's REQ by parent id), 0 at LEVMIN.
+ *    The reference reads REQPP from its shared REQ array, which this level's
+ *    loop may already have overwritten at that index; the parent's own value
+ *    is written here;
+ *  - cubes (cubes_path not NULL): IR NVOID NVOIDT, then every cube in INDICE
+ *    order: IND UVOID INICIOX FINALX INICIOY FINALY INICIOZ FINALZ RINIXCO
+ *    RFINXCO RINIYCO RFINYCO RINIZCO RFINZCO;
+ *  - map (map_path not NULL): MARCA, U1CO - 1 and DIVERCO on the inner NX^3
+ *    cells, column-major, raw (STREAM access), from voids->marca and the ext
+ *    grids of avism_gpu_fields.
+ * Reals are written with 9 (REAL*8: 17) significant digits.                   */
+int avism_io_write_headers(const char *voids_path, const char *cubes_path, int32_t nlev, int32_t levmin,
+                           int32_t levmax, int32_t ncox, int32_t ncoy, int32_t ncoz, float lado0);
+int avism_io_append_level(const char *voids_path, const char *cubes_path, const char *map_path,
+                          const avism_params *p, int32_t nvoid, int32_t nvoidp, float meandens,
+                          const avism_cubes *cubes, const avism_voids *voids, const float *req_parent,
+                          const float *u1co_ext, const float *diverco_ext);
 
 #ifdef __cplusplus
 }

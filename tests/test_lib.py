@@ -14,7 +14,7 @@ def declared_functions():
     names = set()
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         text = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
-        names |= set(re.findall(r"\b(avism_gpu_\w+)\s*\(", text))
+        names |= set(re.findall(r"\b(avism_(?:gpu|io)_\w+)\s*\(", text))
     return sorted(names)
 
 
