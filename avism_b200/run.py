@@ -1,0 +1,94 @@
+"""Standalone run of one iteration without the Fortran driver.
+
+A READ_BINARY_PART_1 particle file in; the voids, cubes and map files of the
+iteration out, for levels LEVMIN..LEVMAX (each level at twice the previous
+grid, inside the previous level's voids), in the layout tools/read_voids.py
+reads.  It is the reference's level loop (src/avism.f90:742-2181) for particle
+input, with the particle arrays kept across levels::
+
+    python -m avism_b200.run input_data/bin_file_part00001 --nx 64 --lado0 100 \\
+        --levels 2 --out output_files --iter 1 --cubes --map
+
+Masses and velocities are divided by UM and UV after reading, as
+src/reader.f90:455-458 does.  The work runs on the GPU through the C-ABI.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+
+from ._abi import Params
+from .avism import append_catalogue_level, read_particle_file, write_catalogue_headers
+
+
+def run_iteration(particle_path, p: Params, out_dir, it: int = 1, nlev: int = 1, cubes: bool = False,
+                  maps: bool = False, engine=None) -> dict:
+    """Run levels p.levmin .. p.levmin + nlev - 1 and write their files; returns
+    the paths and each level's result.  ``engine`` is an AvismGPU (default:
+    device 0) or anything with its run_level / run_sublevel / next_level /
+    particles_to_grid / fields methods."""
+    from . import synth
+    parts = read_particle_file(particle_path)
+    p = Params(**{**p.__dict__, "zeta": float(parts.pop("zeta")), "level": p.levmin})
+    parts = synth.to_reader_units(parts)
+    if engine is None:
+        from .avism import AvismGPU
+        engine = AvismGPU(0)
+        if p.learned == 1:
+            from . import proposal
+            engine.proposal_load(proposal.load_weights())
+    os.makedirs(out_dir, exist_ok=True)
+    vp = os.path.join(out_dir, f"voids{it:05d}")
+    cp = os.path.join(out_dir, f"cubes{it:05d}") if cubes else None
+    mp = os.path.join(out_dir, f"map{it:05d}") if maps else None
+    write_catalogue_headers(vp, cp, nlev, p.levmin, p.levmin + nlev - 1, p.nx, p.nx, p.nx, p.lado0)
+    if mp:
+        open(mp, "wb").close()
+    results = []
+    req_parent, nvoidp, marcap, reqp = None, 0, None, None
+    for lev in range(nlev):
+        q = Params(**{**p.__dict__, "nx": p.nx * 2 ** lev, "level": p.levmin + lev})
+        keep_marca = maps or lev + 1 < nlev
+        if lev == 0:
+            res = engine.run_level(q, parts, want_marca=keep_marca)
+        else:
+            res = engine.run_sublevel(q, parts, marcap, reqp, want_marca=keep_marca)
+        u1 = dv = None
+        if maps:
+            grid = engine.particles_to_grid(q, parts)
+            u1, dv, _ = engine.fields(q, grid["u_mass"], grid["u2"], grid["u3"], grid["u4"])
+        append_catalogue_level(vp, q, res, nvoidp=nvoidp, req_parent=req_parent, cubes_path=cp, map_path=mp,
+                               u1co_ext=u1, diverco_ext=dv)
+        results.append(res)
+        if lev + 1 < nlev:
+            cat = res["cat"]
+            marcap, reqp = engine.next_level(q, res["nvoid"], cat["marca"], cat["uvoid"], cat["req"])
+            req_parent, nvoidp = reqp, res["nvoid"]          # REQP and NVOIDP = NVOID (avism.f90:2139-2146)
+    return dict(voids=vp, cubes=cp, map=mp, levels=results)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("particles")
+    ap.add_argument("--nx", type=int, required=True)
+    ap.add_argument("--lado0", type=float, required=True)
+    ap.add_argument("--periodic", type=int, default=1)
+    ap.add_argument("--kneighbours", type=int, default=32)
+    ap.add_argument("--levels", type=int, default=1)
+    ap.add_argument("--learned", type=int, default=0, choices=[0, 1, 2])
+    ap.add_argument("--nvoid-max", type=int, default=4_000_000)
+    ap.add_argument("--out", default="output_files")
+    ap.add_argument("--iter", type=int, default=1)
+    ap.add_argument("--cubes", action="store_true")
+    ap.add_argument("--map", action="store_true")
+    a = ap.parse_args(argv)
+    p = Params(nx=a.nx, lado0=a.lado0, periodic=a.periodic, kneighbours=a.kneighbours, learned=a.learned,
+               nvoid_max=a.nvoid_max)
+    r = run_iteration(a.particles, p, a.out, it=a.iter, nlev=a.levels, cubes=a.cubes, maps=a.map)
+    for lev in r["levels"]:
+        print(f"level: {lev['nvoid']} cubes, {lev['cat']['nvoidt']} voids")
+    print(f"wrote {r['voids']}" + (f", {r['cubes']}" if r["cubes"] else "") + (f", {r['map']}" if r["map"] else ""))
+
+
+if __name__ == "__main__":
+    main()
