@@ -1,4 +1,5 @@
 // capi.cu -- the extern "C" entry points declared in include/avism_gpu.h.
+#include <cub/cub.cuh>
 #include <cstring>
 #include <exception>
 #include <vector>

@@ -89,7 +89,7 @@ __device__ __forceinline__ uint32_t key_orig(const float4 *sp, unsigned long lon
 }
 // equal squared distances: the smaller original index first (kept out of line,
 // ties are rare and the hot comparisons stay two instructions)
-__device__ __noinline__ bool key_tie_lt(const float4 *sp, unsigned long long a, unsigned long long b) {
+static __device__ __noinline__ bool key_tie_lt(const float4 *sp, unsigned long long a, unsigned long long b) {
     if (a == b) return false;
     return key_orig(sp, a) < key_orig(sp, b);
 }

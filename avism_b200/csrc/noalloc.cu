@@ -19,6 +19,7 @@
 
 #include "common.cuh"
 #include "knn_core.cuh"
+#include "bin_kernels.cuh"
 
 namespace avism {
 namespace noalloc {

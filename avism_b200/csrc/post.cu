@@ -1016,9 +1016,10 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
     for (int32_t i = 0; i < nv; i++) {
         if (uvoid[i] != -1) continue;
         nvoidt++;
-        // ((3.*VOLM)/(4.*PI))**(1./3.) (src/avism.f90:2071): 3.*VOLM is a REAL*4
-        // product, 4.*PI and the quotient REAL*8, 1./3. a REAL*4 quotient
-        req[i] = (float)std::pow((double)(3.0f * volnew[i]) / (4.0 * pi), (double)(1.0f / 3.0f));
+        // ((3.*VOLM)/(4.*PI))**(1./3.) (src/avism.f90:2071): VOLM is REAL*8
+        // (src/avism.f90:73), so 3.*VOLM, 4.*PI and the quotient are REAL*8
+        // products; 1./3. is a REAL*4 quotient widened for the power
+        req[i] = (float)std::pow((3.0 * (double)volnew[i]) / (4.0 * pi), (double)(1.0f / 3.0f));
     }
 
     // ---- outputs

@@ -27,6 +27,7 @@
 
 #include "common.cuh"
 #include "knn_core.cuh"
+#include "bin_kernels.cuh"
 
 namespace avism {
 

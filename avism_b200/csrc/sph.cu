@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "knn_core.cuh"
 #include "knn_warp.cuh"
+#include "bin_kernels.cuh"
 
 namespace avism {
 
@@ -86,16 +87,6 @@ k_fill_h(KnnGrid G, int64_t n, int K, float *__restrict__ hp_s) {
     const float4 p = G.sp[i];
     knn_any<KCAP>(G, p.x, p.y, p.z, K, col, S);
     hp_s[i] = sqrtf(key_d2(col[(size_t)(K - 1) * S]));
-}
-
-// per-particle attributes in binned order: (vx, vy, vz, m)
-__global__ void k_sorted_attrs(int64_t n, const float4 *__restrict__ sp, const float *__restrict__ vx,
-                               const float *__restrict__ vy, const float *__restrict__ vz,
-                               const float *__restrict__ m, float4 *__restrict__ sv) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int o = __float_as_int(sp[i].w);
-    sv[i] = make_float4(vx[o], vy[o], vz[o], m[o]);
 }
 
 // binned order -> input order

@@ -460,8 +460,9 @@ int orc_merge_post(const avism_params *p, int32_t nvoid, const avism_cubes *cb,
         out->req[i] = 0.0f;
         if (uvoid[i] == -1) {
             nvoidt++;
-            /* ((3.*VOLM)/(4.*PI))**(1./3.), src/avism.f90:2071: 3.*VOLM in REAL*4 */
-            out->req[i] = (float)pow((double)(3.0f * volnew[i]) / (4.0 * pi), (double)(1.0f / 3.0f));
+            /* ((3.*VOLM)/(4.*PI))**(1./3.), src/avism.f90:2071: VOLM is REAL*8
+               (src/avism.f90:73), so 3.*VOLM is a REAL*8 product */
+            out->req[i] = (float)pow((3.0 * (double)volnew[i]) / (4.0 * pi), (double)(1.0f / 3.0f));
         }
     }
     out->nvoidt = nvoidt;

@@ -247,8 +247,10 @@ def test_two_overlapping_holes_merge_into_one_void():
 
 
 def test_req_follows_the_fortran_promotions():
-    """REQ = ((3.*VOLM)/(4.*PI))**(1./3.) (src/avism.f90:2071): 3.*VOLM rounds in
-    REAL*4, the quotient and the power are REAL*8 with the REAL*4 exponent 1./3."""
+    """REQ = ((3.*VOLM)/(4.*PI))**(1./3.) (src/avism.f90:2071).  VOLM is REAL*8
+    (src/avism.f90:73: 'REAL*8 :: VOLT_CLEAN, VOLM') and PI REAL*8
+    (src/commondata.f90:16), so 3.*VOLM, 4.*PI and the quotient are REAL*8; the
+    exponent 1./3. is a REAL*4 quotient widened for the power."""
     from avism_b200 import synth
     parts = synth.to_reader_units(synth.mock_spheres(n=2 ** 16, box=64.0, nsph=8, rmin=4.0, rmax=8.0, seed=5))
     r = O.run_level(Params(nx=48, lado0=64.0, periodic=1, rmin=1.0), parts)   # dx^3 not a power of two
@@ -257,8 +259,8 @@ def test_req_follows_the_fortran_promotions():
     v = cat["volnew"][main].astype(np.float32)
     third = np.float64(np.float32(1.0) / np.float32(3.0))
     four_pi = 4.0 * np.arccos(-1.0)
-    expect = np.power((np.float32(3.0) * v).astype(np.float64) / four_pi, third).astype(np.float32)
+    expect = np.power(3.0 * v.astype(np.float64) / four_pi, third).astype(np.float32)
     assert np.array_equal(cat["req"][main], expect)
-    # the case is one where the REAL*8 product 3*VOLM would give another REQ
-    wrong = np.power(3.0 * v.astype(np.float64) / four_pi, third).astype(np.float32)
+    # the case is one where a REAL*4 product 3.*VOLNEW would give another REQ
+    wrong = np.power((np.float32(3.0) * v).astype(np.float64) / four_pi, third).astype(np.float32)
     assert np.any(wrong != expect)
