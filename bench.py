@@ -155,17 +155,21 @@ def config_dict(a, world):
 
 
 # ---- CPU baseline: the oracle on a bounded sample of the same workload -------
-def cpu_sample_run(steps: int, warmup: int, seed: int = 1004):
+def cpu_sample_run(steps: int, warmup: int, seed: int = 1004, nx: int = 128):
     """The C oracle (restatement of the reference's algorithms: k-d tree kNN,
-    scatter SPH, serial growth and merge) on a 128^3 sub-box with the same cell
-    size and particle density (2^21 particles, L = 125 cMpc, periodic)."""
+    scatter SPH, serial growth and merge) on a sub-box of the workload with the
+    same cell size and particle density: nx^3 cells, L = nx * 500/512 cMpc,
+    2^27 (nx/512)^3 particles, periodic.  Returns (cells/s, cores, s per level,
+    sample description)."""
     from avism_b200 import synth
     from avism_b200._abi import Params
     from oracle import oracle as O
-    nx, box, n = 128, 125.0, 2 ** 21
-    parts = synth.to_reader_units(synth.lognormal(n=n, ng=128, box=box, index=-1.2, sigma_ln=1.0,
+    box = nx * 500.0 / 512
+    n = int(round(2 ** 27 * (nx / 512) ** 3))
+    parts = synth.to_reader_units(synth.lognormal(n=n, ng=nx, box=box, index=-1.2, sigma_ln=1.0,
                                                   vrms=350.0, seed=seed))
     p = Params(nx=nx, periodic=1, lado0=box, kneighbours=32, nvoid_max=4_000_000)
+    g, _ = O.grid_setup(p)
     times = []
     for i in range(warmup + steps):
         t0 = time.perf_counter()
@@ -175,27 +179,44 @@ def cpu_sample_run(steps: int, warmup: int, seed: int = 1004):
             times.append(dt)
     t = statistics.mean(times)
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return nx ** 3 / t, cores, t, f"oracle port, full level on a {nx}^3 sub-box (2^21 particles, L={box:g}, " \
-                                   f"ext {nx + 2 * 51}^3), same cell size and density; {t:.2f} s per level"
+    return nx ** 3 / t, cores, t, (f"oracle port (k-d tree kNN, scatter SPH, serial growth and merge), one full "
+                                   f"level per step on a {nx}^3 sub-box ({n} particles, L={box:g} cMpc periodic, "
+                                   f"ext {g.ne}^3) with the cell size and particle density of the 512^3 workload; "
+                                   f"{t:.2f} s per level; cells/s = {nx}^3 / that time, a per-cell rate "
+                                   f"extrapolated to 512^3")
+
+
+REF_NX = 96     # reference-arm sub-box: one level takes a few seconds on 16 host cores
 
 
 def run_reference(a):
-    rank, world, _ = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0
+    """The reference arm: the oracle port on the host cores, every one of the
+    --warmup + --steps steps a full level on a REF_NX^3 sub-box of the workload
+    (rank 0 only; other ranks exit without work)."""
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-    value, cores, t, sample = cpu_sample_run(max(1, min(a.steps, 3)), 1 if a.warmup > 0 else 0)
+    value, cores, t, sample = cpu_sample_run(a.steps, a.warmup, nx=REF_NX)
+    box = REF_NX * 500.0 / 512
+    cfg = {"workload": f"particles->void catalogue on a {REF_NX}^3 sub-box of the 512^3 workload "
+                       f"(L={box:g} cMpc periodic, same cell size and particle density, k=32, SPH/SPH); "
+                       f"cells/s is extrapolated per cell to the 512^3 level",
+           "grid": REF_NX, "particles": int(round(2 ** 27 * (REF_NX / 512) ** 3)), "box_cmpc": box,
+           "kneighbours": 32, "field": "lognormal GRF P(k)~k^-1.2 sigma_ln=1, linear-theory v 350 km/s rms",
+           "parallelism": "host threads (OpenMP)"}
     line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": config_dict(a, 1),
+            "config": cfg,
             "cpu_baseline": {"value": value, "unit": "cells/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 # ---- our arm ----------------------------------------------------------------
-# algorithmic bytes per unit of the dominant stages
+# algorithmic bytes per unit of the dominant stages: compulsory reads and writes
+# of each stage's inputs and outputs, counted once
 ALG_BYTES = {
     # per cell query: the k neighbours' (x,y,z,m,vx,vy,vz,rho) are compulsory once per
     # particle; per cell 3 velocity components written, per particle h read+written

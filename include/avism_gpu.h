@@ -280,6 +280,9 @@ int avism_gpu_run_sublevel(avism_gpu_ctx *ctx, const avism_params *p, int64_t n,
  *          scratch address up (cudaGetSymbolAddress), which may load the module
  *          and allocate inside the CUDA runtime; make that first call before any
  *          stream capture.
+ *        - the address is kept for the life of the process: do not call this
+ *          entry point again after cudaDeviceReset() (or any teardown of the
+ *          device's primary context), which invalidates it.
  *      errbuf (nullable, errlen bytes) receives the failure message, "" on
  *      success.                                                                 */
 #define AVISM_KNN_NOALLOC_MAX_N 1048576

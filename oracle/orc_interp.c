@@ -11,10 +11,15 @@
  *   - DDENS / DENS_TSC: FP64 accumulation in particle order, then rounded;
  *   - VEL_TSC: FP32 accumulation in particle order (the reference uses FP32
  *     atomics, src/particles.f90:241-248, so its own result varies per run).
+ * The scatter loops run in parallel over z-slabs of cells (slab_of), each
+ * thread walking every particle in index order, so these orders hold.
  */
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include "avism_oracle.h"
 
 #define RAD(i) radx[(i) - g->rad_lo]
@@ -156,6 +161,22 @@ int orc_fill_h_zeros(const orc_kdtree *t, int64_t n, const float *x, const float
     return AVISM_OK;
 }
 
+/* Cells are split into z-slabs, one per thread; every thread walks all the
+ * particles in index order and adds only the contributions that fall in its
+ * slab, so each cell still receives its terms in particle order (the rule that
+ * replaces the reference's OpenMP atomics).  A particle whose support spans two
+ * slabs has its NORM computed by both threads, identically. */
+static void slab_of(int nx, int *k0, int *k1)
+{
+    int nt = 1, t = 0;
+#ifdef _OPENMP
+    nt = omp_get_num_threads();
+    t = omp_get_thread_num();
+#endif
+    *k0 = 1 + (int)(((int64_t)nx * t) / nt);
+    *k1 = (int)(((int64_t)nx * (t + 1)) / nt);
+}
+
 int orc_ddens_interp_sph(const avism_grid *g, const float *radx, int64_t n,
                          const float *x, const float *y, const float *z,
                          const float *hpart, const float *m, float *u)
@@ -166,44 +187,51 @@ int orc_ddens_interp_sph(const avism_grid *g, const float *radx, int64_t n,
     const int64_t nc = (int64_t)nx * nx * nx;
     double *u8 = (double *)calloc((size_t)nc, sizeof(double));
     if (!u8) return AVISM_ERR_OOM;
-    for (int64_t p = 0; p < n; p++) {
-        const int ix = (int)((x[p] - rx1) / dx) + 1;
-        const int jy = (int)((y[p] - rx1) / dx) + 1;
-        const int kz = (int)((z[p] - rx1) / dx) + 1;
-        const float h = hpart[p];
-        const float inv_h = 2.0f / h;
-        const float h2max = (4.0f * h) * h;
-        const int inc = (int)((2.0f * h) / dx + 0.5f);
-        float norm = 0.0f;
-        for (int pass = 0; pass < 2; pass++) {
-            for (int k2 = kz - inc; k2 <= kz + inc; k2++) {
-                if (k2 < 1 || k2 > nx) continue;
-                const float tz = z[p] - RAD(k2);
-                const float dz2 = tz * tz;
-                for (int j2 = jy - inc; j2 <= jy + inc; j2++) {
-                    if (j2 < 1 || j2 > nx) continue;
-                    const float ty = y[p] - RAD(j2);
-                    const float dy2 = ty * ty;
-                    for (int i2 = ix - inc; i2 <= ix + inc; i2++) {
-                        if (i2 < 1 || i2 > nx) continue;
-                        const float tx = x[p] - RAD(i2);
-                        const float dx2 = tx * tx;
-                        const float d2 = (dx2 + dy2) + dz2;
-                        if (d2 > h2max) continue;
-                        const float q = sqrtf(d2) * inv_h;
-                        float w;
-                        if (q <= 1.0f) w = 1.0f - (1.5f * (q * q)) * (1.0f - 0.5f * q);
-                        else if (q <= 2.0f) { const float s = 2.0f - q; w = 0.25f * ((s * s) * s); }
-                        else w = 0.0f;
-                        if (pass == 0) norm = norm + w;
-                        else u8[cell_id(nx, i2, j2, k2)] += (double)((w * m[p]) / norm);
+    #pragma omp parallel
+    {
+        int ks0, ks1;
+        slab_of(nx, &ks0, &ks1);
+        for (int64_t p = 0; p < n && ks0 <= ks1; p++) {
+            const int ix = (int)((x[p] - rx1) / dx) + 1;
+            const int jy = (int)((y[p] - rx1) / dx) + 1;
+            const int kz = (int)((z[p] - rx1) / dx) + 1;
+            const float h = hpart[p];
+            const int inc = (int)((2.0f * h) / dx + 0.5f);
+            if (kz + inc < ks0 || kz - inc > ks1) continue;
+            const float inv_h = 2.0f / h;
+            const float h2max = (4.0f * h) * h;
+            float norm = 0.0f;
+            for (int pass = 0; pass < 2; pass++) {
+                for (int k2 = kz - inc; k2 <= kz + inc; k2++) {
+                    if (k2 < 1 || k2 > nx) continue;
+                    if (pass == 1 && (k2 < ks0 || k2 > ks1)) continue;
+                    const float tz = z[p] - RAD(k2);
+                    const float dz2 = tz * tz;
+                    for (int j2 = jy - inc; j2 <= jy + inc; j2++) {
+                        if (j2 < 1 || j2 > nx) continue;
+                        const float ty = y[p] - RAD(j2);
+                        const float dy2 = ty * ty;
+                        for (int i2 = ix - inc; i2 <= ix + inc; i2++) {
+                            if (i2 < 1 || i2 > nx) continue;
+                            const float tx = x[p] - RAD(i2);
+                            const float dx2 = tx * tx;
+                            const float d2 = (dx2 + dy2) + dz2;
+                            if (d2 > h2max) continue;
+                            const float q = sqrtf(d2) * inv_h;
+                            float w;
+                            if (q <= 1.0f) w = 1.0f - (1.5f * (q * q)) * (1.0f - 0.5f * q);
+                            else if (q <= 2.0f) { const float s = 2.0f - q; w = 0.25f * ((s * s) * s); }
+                            else w = 0.0f;
+                            if (pass == 0) norm = norm + w;
+                            else u8[cell_id(nx, i2, j2, k2)] += (double)((w * m[p]) / norm);
+                        }
                     }
                 }
-            }
-            if (pass == 0 && norm == 0.0f) {
-                if (ix >= 1 && ix <= nx && jy >= 1 && jy <= nx && kz >= 1 && kz <= nx)
-                    u8[cell_id(nx, ix, jy, kz)] += (double)m[p];
-                break;
+                if (pass == 0 && norm == 0.0f) {
+                    if (ix >= 1 && ix <= nx && jy >= 1 && jy <= nx && kz >= ks0 && kz <= ks1 && kz <= nx)
+                        u8[cell_id(nx, ix, jy, kz)] += (double)m[p];
+                    break;
+                }
             }
         }
     }
@@ -251,7 +279,11 @@ int orc_dens_interp_tsc(const avism_grid *g, const float *radx, int periodic, in
     const int64_t nc = (int64_t)nx * nx * nx;
     double *u8 = (double *)calloc((size_t)nc, sizeof(double));
     if (!u8) return AVISM_ERR_OOM;
-    for (int64_t p = 0; p < n; p++) {
+    #pragma omp parallel
+    {
+    int ks0, ks1;
+    slab_of(nx, &ks0, &ks1);
+    for (int64_t p = 0; p < n && ks0 <= ks1; p++) {
         int ci, cj, ck; float wx[3], wy[3], wz[3];
         tsc_axis(g, radx, periodic, x[p], &ci, wx);
         tsc_axis(g, radx, periodic, y[p], &cj, wy);
@@ -265,9 +297,11 @@ int orc_dens_interp_tsc(const avism_grid *g, const float *radx, int periodic, in
                     /* non-periodic cells outside 1..NX: the reference writes out of
                        bounds there; the oracle drops the contribution */
                     if (i3 < 1 || i3 > nx || j3 < 1 || j3 > nx || k3 < 1 || k3 > nx) continue;
+                    if (k3 < ks0 || k3 > ks1) continue;
                     const float inc = ((m[p] * wx[c]) * wy[b]) * wz[a];
                     u8[cell_id(nx, i3, j3, k3)] += (double)inc;
                 }
+    }
     }
     for (int64_t c = 0; c < nc; c++) u[c] = (float)u8[c];
     free(u8);
@@ -283,7 +317,11 @@ int orc_vel_interp_tsc(const avism_grid *g, const float *radx, int periodic, int
     float *wt = (float *)calloc((size_t)nc, sizeof(float));
     if (!wt) return AVISM_ERR_OOM;
     for (int64_t c = 0; c < nc; c++) { u2[c] = 0.0f; u3[c] = 0.0f; u4[c] = 0.0f; }
-    for (int64_t p = 0; p < n; p++) {
+    #pragma omp parallel
+    {
+    int ks0, ks1;
+    slab_of(nx, &ks0, &ks1);
+    for (int64_t p = 0; p < n && ks0 <= ks1; p++) {
         int ci, cj, ck; float wx[3], wy[3], wz[3];
         tsc_axis(g, radx, periodic, x[p], &ci, wx);
         tsc_axis(g, radx, periodic, y[p], &cj, wy);
@@ -295,6 +333,7 @@ int orc_vel_interp_tsc(const avism_grid *g, const float *radx, int periodic, int
                     const int j3 = tsc_wrap(cj + b - 1, nx, periodic);
                     const int k3 = tsc_wrap(ck + a - 1, nx, periodic);
                     if (i3 < 1 || i3 > nx || j3 < 1 || j3 > nx || k3 < 1 || k3 > nx) continue;
+                    if (k3 < ks0 || k3 > ks1) continue;
                     const float w = (wx[c] * wy[b]) * wz[a];
                     const int64_t id = cell_id(nx, i3, j3, k3);
                     u2[id] = u2[id] + vx[p] * w;
@@ -302,6 +341,7 @@ int orc_vel_interp_tsc(const avism_grid *g, const float *radx, int periodic, int
                     u4[id] = u4[id] + vz[p] * w;
                     wt[id] = wt[id] + w;
                 }
+    }
     }
     for (int64_t c = 0; c < nc; c++) {
         float wei = wt[c];

@@ -15,7 +15,10 @@ from avism_b200.avism import (AvismError, append_catalogue_level, read_particle_
                               write_catalogue_headers)
 from oracle import oracle as O
 
-READ_VOIDS = "/root/reference/tools/read_voids.py"
+# tools/read_voids.py of the reference checkout named by AVISM_REFERENCE_ROOT
+# (unset: the test that runs the tool is skipped)
+_REF = os.environ.get("AVISM_REFERENCE_ROOT")
+READ_VOIDS = os.path.join(_REF, "tools", "read_voids.py") if _REF else ""
 
 
 def _fortran_records(path, records):
@@ -144,7 +147,8 @@ def test_sublevel_parent_columns(tmp_path, level):
     assert np.array_equal(rows[:, 13], req_parent[cubes["father"][main] - 1])
 
 
-@pytest.mark.skipif(not os.path.exists(READ_VOIDS), reason="reference tools not mounted")
+@pytest.mark.skipif(not (READ_VOIDS and os.path.exists(READ_VOIDS)),
+                    reason="AVISM_REFERENCE_ROOT does not name a reference checkout with tools/read_voids.py")
 def test_reference_reader_reads_the_files(tmp_path, level):
     """tools/read_voids.py itself parses the voids, cubes and map files."""
     p, res, u1, dv = level

@@ -84,3 +84,26 @@ def test_noalloc_rejects_oversize_and_host_pointers(gpu):
     st = lib.avism_gpu_knn_noalloc(0, C.c_void_p(stream), 16, p, p, p, 10.0, 4, q[0].data_ptr(),
                                    q[1].data_ptr(), q[2].data_ptr(), 8, idx.data_ptr(), dist.data_ptr(), err, 256)
     assert st == 1 and b"not a device pointer" in err.value, (st, err.value)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k,box_l", [(8, 0.0), (100, 60.0), (100, 0.0), (200, 60.0), (200, 0.0)])
+def test_noalloc_matches_oracle(k, box_l):
+    """Against the CPU oracle's kNN (k-d tree, ties by particle index) on the
+    same points, over the 32-, 128- and 256-wide instantiations, periodic and
+    not; two calls in a row with different inputs."""
+    import torch
+    from avism_b200 import _lib
+    from oracle import oracle as O
+    lib = _lib.load()
+    dev = torch.device("cuda:0")
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    for seed in (k, k + 1):
+        pts, qs = _case(seed, 30000, 2000, box_l, 30.0)
+        d = [torch.from_numpy(a.copy()).to(dev) for a in (*pts, *qs)]
+        st, msg, idx, dist = _noalloc(lib, d, box_l, k, stream)
+        assert st == 0 and msg == "", (st, msg)
+        torch.cuda.current_stream(dev).synchronize()
+        ref_idx, ref_dist = O.knn(*pts, *qs, k, box_l)
+        assert np.array_equal(idx.cpu().numpy().reshape(-1, k), ref_idx)
+        assert np.array_equal(dist.cpu().numpy().reshape(-1, k).view(np.uint32), ref_dist.view(np.uint32))
