@@ -45,6 +45,12 @@ SIGNATURES = {
                                         _i32]),
     "avism_io_particle_header": (C.c_int, [C.c_char_p, _c_void, _c_void]),
     "avism_io_read_particles": (C.c_int, [C.c_char_p, _i64] + [_c_void] * 7),
+    "avism_io_read_particles_novel": (C.c_int, [C.c_char_p, _i64] + [_c_void] * 4),
+    "avism_io_read_grid": (C.c_int, [C.c_char_p, _i32] + [_c_void] * 5),
+    "avism_io_read_mask": (C.c_int, [C.c_char_p, _i32, _i32, _c_void, _c_void]),
+    "avism_io_randoms_header": (C.c_int, [C.c_char_p, _c_void]),
+    "avism_io_read_randoms": (C.c_int, [C.c_char_p, _i32] + [_c_void] * 4),
+    "avism_io_write_vel_cube": (C.c_int, [C.c_char_p, _i32] + [_c_void] * 3),
     "avism_io_write_headers": (C.c_int, [C.c_char_p, C.c_char_p] + [_i32] * 6 + [_f32]),
     "avism_io_append_level": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, _c_void, _i32, _i32, _f32]
                               + [_c_void] * 5),

@@ -79,6 +79,58 @@ def read_particle_file(path) -> dict:
     return out
 
 
+def read_particle_file_novel(path) -> dict:
+    """A READ_BINARY_PART_2 particle file (src/reader.f90:465-519): x, y, z, m
+    as stored, no velocities, and the redshift zeta."""
+    lib = _lib.load()
+    n, zeta = C.c_int64(), C.c_float()
+    _io_chk(lib.avism_io_particle_header(_path(path), C.byref(n), C.byref(zeta)), f"particle file {path}")
+    keys = ("x", "y", "z", "m")
+    out = {k: np.zeros(n.value, np.float32) for k in keys}
+    _io_chk(lib.avism_io_read_particles_novel(_path(path), n.value, *(_vp(out[k]) for k in keys)),
+            f"particle file {path}")
+    out["zeta"] = zeta.value
+    return out
+
+
+def read_grid_file(path, nx) -> dict:
+    """A READ_BINARY_GRID file (src/reader.f90:523-552): the density contrast
+    u1 and velocities u2..u4 (km/s) on nx^3 cells as stored, and zeta."""
+    nc = int(nx) ** 3
+    out = {k: np.zeros(nc, np.float32) for k in ("u1", "u2", "u3", "u4")}
+    zeta = C.c_float()
+    _io_chk(_lib.load().avism_io_read_grid(_path(path), int(nx), C.byref(zeta),
+                                           *(_vp(out[k]) for k in ("u1", "u2", "u3", "u4"))), f"grid file {path}")
+    out["zeta"] = zeta.value
+    return out
+
+
+def read_mask_file(path, ncox, nx):
+    """The survey mask (src/avism.f90:403-418, 873-901) on the level's nx^3
+    inner cells (int8) and (MASKLOW, MASKUPPER, MASKSIDE)."""
+    sm = np.zeros(int(nx) ** 3, np.int8)
+    lims = np.zeros(3, np.float32)
+    _io_chk(_lib.load().avism_io_read_mask(_path(path), int(ncox), int(nx), _vp(sm), _vp(lims)), f"mask {path}")
+    return sm, lims
+
+
+def read_randoms_file(path) -> dict:
+    """The survey randoms (src/avism.f90:1425-1444): x, y, z and weights w."""
+    lib = _lib.load()
+    n = C.c_int32()
+    _io_chk(lib.avism_io_randoms_header(_path(path), C.byref(n)), f"randoms {path}")
+    out = {k: np.zeros(n.value, np.float32) for k in ("x", "y", "z", "w")}
+    _io_chk(lib.avism_io_read_randoms(_path(path), n.value, *(_vp(out[k]) for k in ("x", "y", "z", "w"))),
+            f"randoms {path}")
+    return out
+
+
+def write_vel_cube(path, nx, u2, u3, u4):
+    """vel_cube.dat (src/avism.f90:1198-1202): the three velocity grids raw."""
+    _io_chk(_lib.load().avism_io_write_vel_cube(_path(path), int(nx), *(_vp(_f32(u)) for u in (u2, u3, u4))),
+            f"vel_cube {path}")
+
+
 def write_catalogue_headers(voids_path, cubes_path, nlev, levmin, levmax, ncox, ncoy, ncoz, lado0):
     """First lines of the voids (and cubes) files of one iteration (src/avism.f90:710-722)."""
     _io_chk(_lib.load().avism_io_write_headers(_path(voids_path), _path(cubes_path), nlev, levmin, levmax,

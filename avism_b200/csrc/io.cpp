@@ -3,7 +3,15 @@
 //  * particle files of READ_BINARY_PART_1 (src/reader.f90:410-460): Fortran
 //    sequential unformatted records, each framed by 4-byte length markers:
 //    [int64 NPARTT, REAL*4 ZETA], then x, y, z, vx, vy, vz, m (NPARTT REAL*4
-//    each), as written by the reference's input tools;
+//    each), as written by the reference's input tools; READ_BINARY_PART_2
+//    (src/reader.f90:465-519) without the three velocity records;
+//  * grid files of READ_BINARY_GRID (src/reader.f90:523-552): [REAL*4 ZETA],
+//    then the density contrast and the three velocity grids;
+//  * survey inputs: the stream mask file (src/avism.f90:403-418, mapped onto
+//    the level's grid as src/avism.f90:873-901) and the randoms file
+//    (src/avism.f90:1425-1444);
+//  * the vel_cube.dat side dump of the SPH velocity grids
+//    (src/avism.f90:1198-1202, STREAM access);
 //  * the voids / cubes catalogues and the map of one iteration
 //    (src/avism.f90:710-722 headers, 2026-2085 per level): whitespace-separated
 //    text lines with the reference's columns, and the map as raw STREAM arrays
@@ -11,6 +19,7 @@
 //    column-major).  Reals are printed with enough digits to read back the same
 //    REAL*4 (or REAL*8) value; the reference's list-directed spacing is not kept,
 //    readers split on whitespace.
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -25,12 +34,39 @@ struct File {
     ~File() { if (f) std::fclose(f); }
 };
 
-// one record: 4-byte marker, payload, the same marker
-bool read_record(FILE *f, void *dst, uint32_t bytes) {
-    uint32_t a = 0, b = 0;
-    if (std::fread(&a, 4, 1, f) != 1 || a != bytes) return false;
-    if (bytes && std::fread(dst, 1, bytes, f) != bytes) return false;
-    return std::fread(&b, 4, 1, f) == 1 && b == bytes;
+// Largest payload of one gfortran subrecord with 4-byte markers.  A longer
+// record is written as a chain of subrecords: each carries its own leading and
+// trailing length markers, and a negative leading marker says that another
+// subrecord of the same record follows (the trailing marker of a continuation
+// is negative too; only its magnitude is checked here).
+constexpr uint64_t MAX_SUBRECORD = 2147483639ull;
+
+// one logical record of exactly `bytes` payload bytes, as one record or a chain
+// of subrecords
+bool read_record(FILE *f, void *dst, uint64_t bytes) {
+    unsigned char *out = static_cast<unsigned char *>(dst);
+    uint64_t got = 0;
+    for (;;) {
+        int32_t head = 0, tail = 0;
+        if (std::fread(&head, 4, 1, f) != 1 || head == INT32_MIN) return false;
+        const uint64_t len = (uint64_t)(head < 0 ? -(int64_t)head : head);
+        if (got + len > bytes) return false;
+        if (len && std::fread(out + got, 1, len, f) != len) return false;
+        if (std::fread(&tail, 4, 1, f) != 1 || tail == INT32_MIN) return false;
+        if ((uint64_t)(tail < 0 ? -(int64_t)tail : tail) != len) return false;
+        got += len;
+        if (head >= 0) break;
+    }
+    return got == bytes;
+}
+
+// the leading record [int64 NPARTT, REAL*4 ZETA] of the particle files
+bool read_particle_head(FILE *f, int64_t *n, float *zeta) {
+    unsigned char rec[12];
+    if (!read_record(f, rec, 12)) return false;
+    std::memcpy(n, rec, 8);
+    std::memcpy(zeta, rec + 8, 4);
+    return *n >= 0;
 }
 
 // 9 significant digits read back as the same REAL*4
@@ -44,31 +80,118 @@ int avism_io_particle_header(const char *path, int64_t *n, float *zeta) {
     if (!path || !n || !zeta) return AVISM_ERR_ARG;
     File in(path, "rb");
     if (!in.f) return AVISM_ERR_IO;
-    unsigned char rec[12];
-    if (!read_record(in.f, rec, 12)) return AVISM_ERR_IO;
-    std::memcpy(n, rec, 8);
-    std::memcpy(zeta, rec + 8, 4);
-    return *n >= 0 ? AVISM_OK : AVISM_ERR_IO;
+    return read_particle_head(in.f, n, zeta) ? AVISM_OK : AVISM_ERR_IO;
 }
 
-int avism_io_read_particles(const char *path, int64_t capacity, float *x, float *y, float *z, float *vx,
-                            float *vy, float *vz, float *m) {
-    float *dst[7] = {x, y, z, vx, vy, vz, m};
-    for (float *d : dst)
-        if (!d) return AVISM_ERR_ARG;
+namespace {
+
+// READ_BINARY_PART_1 / _2: the header, then one record of NPARTT REAL*4 per
+// destination array, in order
+int read_particle_columns(const char *path, int64_t capacity, float *const *dst, int ncol) {
+    for (int i = 0; i < ncol; i++)
+        if (!dst[i]) return AVISM_ERR_ARG;
     if (!path) return AVISM_ERR_ARG;
     File in(path, "rb");
     if (!in.f) return AVISM_ERR_IO;
-    unsigned char rec[12];
-    if (!read_record(in.f, rec, 12)) return AVISM_ERR_IO;
     int64_t n;
-    std::memcpy(&n, rec, 8);
-    if (n < 0) return AVISM_ERR_IO;
+    float zeta;
+    if (!read_particle_head(in.f, &n, &zeta)) return AVISM_ERR_IO;
     if (n > capacity) return AVISM_ERR_ARG;                              // 'ERROR: NPARTT > PARTIRED'
-    if ((uint64_t)n * 4 > 0xffffffffull) return AVISM_ERR_UNSUPPORTED;   // would need a split record
-    for (float *d : dst)
-        if (!read_record(in.f, d, (uint32_t)(n * 4))) return AVISM_ERR_IO;
+    for (int i = 0; i < ncol; i++)
+        if (!read_record(in.f, dst[i], (uint64_t)n * 4)) return AVISM_ERR_IO;
     return AVISM_OK;
+}
+
+}  // namespace
+
+int avism_io_read_particles(const char *path, int64_t capacity, float *x, float *y, float *z, float *vx,
+                            float *vy, float *vz, float *m) {
+    float *const dst[7] = {x, y, z, vx, vy, vz, m};
+    return read_particle_columns(path, capacity, dst, 7);
+}
+
+int avism_io_read_particles_novel(const char *path, int64_t capacity, float *x, float *y, float *z, float *m) {
+    float *const dst[4] = {x, y, z, m};
+    return read_particle_columns(path, capacity, dst, 4);
+}
+
+int avism_io_read_grid(const char *path, int32_t nx, float *zeta, float *u1, float *u2, float *u3, float *u4) {
+    float *const dst[4] = {u1, u2, u3, u4};
+    if (!path || !zeta || nx < 1) return AVISM_ERR_ARG;
+    for (float *d : dst)
+        if (!d) return AVISM_ERR_ARG;
+    File in(path, "rb");
+    if (!in.f) return AVISM_ERR_IO;
+    if (!read_record(in.f, zeta, 4)) return AVISM_ERR_IO;
+    const uint64_t bytes = (uint64_t)nx * (uint64_t)nx * (uint64_t)nx * 4;
+    for (float *d : dst)
+        if (!read_record(in.f, d, bytes)) return AVISM_ERR_IO;
+    return AVISM_OK;
+}
+
+int avism_io_read_mask(const char *path, int32_t ncox, int32_t nx, int8_t *smask, float *lims) {
+    if (!path || !smask || ncox < 1 || nx < 1) return AVISM_ERR_ARG;
+    File in(path, "rb");
+    if (!in.f) return AVISM_ERR_IO;
+    int32_t nmask = 0;
+    float hdr[3];
+    if (std::fread(&nmask, 4, 1, in.f) != 1) return AVISM_ERR_IO;
+    if (nmask != ncox) return AVISM_ERR_ARG;       // 'MASK grid does not coincide with AVISM coarse grid'
+    if (std::fread(hdr, 4, 3, in.f) != 3) return AVISM_ERR_IO;
+    if (lims) std::memcpy(lims, hdr, sizeof hdr);
+    const size_t nm = (size_t)nmask;
+    std::vector<int8_t> m2(nm * nm * nm);
+    if (std::fread(m2.data(), 1, m2.size(), in.f) != m2.size()) return AVISM_ERR_IO;
+    int ndown = 1;
+    if (nx > nmask) {
+        ndown = nx / nmask;
+        if (ndown % 2 != 0) return AVISM_ERR_ARG;  // 'STH WRONG IN MASK INTERPOLATION'
+    } else if (nx != nmask) {
+        return AVISM_ERR_ARG;
+    }
+    const size_t n = (size_t)nx;
+    for (size_t k = 0; k < n; k++)
+        for (size_t j = 0; j < n; j++)
+            for (size_t i = 0; i < n; i++) {
+                const size_t i2 = i / ndown, j2 = j / ndown, k2 = k / ndown;
+                int8_t v = m2[i2 + nm * (j2 + nm * k2)];
+                if (v > 0) v = 1;                  // WHERE (SMASK > 0) SMASK = 1
+                smask[i + n * (j + n * k)] = v;
+            }
+    return AVISM_OK;
+}
+
+int avism_io_randoms_header(const char *path, int32_t *nrand) {
+    if (!path || !nrand) return AVISM_ERR_ARG;
+    File in(path, "rb");
+    if (!in.f) return AVISM_ERR_IO;
+    if (!read_record(in.f, nrand, 4)) return AVISM_ERR_IO;
+    return *nrand >= 0 ? AVISM_OK : AVISM_ERR_IO;
+}
+
+int avism_io_read_randoms(const char *path, int32_t capacity, float *x, float *y, float *z, float *w) {
+    float *const dst[4] = {x, y, z, w};
+    if (!path) return AVISM_ERR_ARG;
+    for (float *d : dst)
+        if (!d) return AVISM_ERR_ARG;
+    File in(path, "rb");
+    if (!in.f) return AVISM_ERR_IO;
+    int32_t n = 0;
+    if (!read_record(in.f, &n, 4) || n < 0) return AVISM_ERR_IO;
+    if (n > capacity) return AVISM_ERR_ARG;
+    for (float *d : dst)
+        if (!read_record(in.f, d, (uint64_t)n * 4)) return AVISM_ERR_IO;
+    return AVISM_OK;
+}
+
+int avism_io_write_vel_cube(const char *path, int32_t nx, const float *u2, const float *u3, const float *u4) {
+    if (!path || nx < 1 || !u2 || !u3 || !u4) return AVISM_ERR_ARG;
+    File out(path, "wb");
+    if (!out.f) return AVISM_ERR_IO;
+    const size_t nc = (size_t)nx * (size_t)nx * (size_t)nx;
+    for (const float *u : {u2, u3, u4})
+        if (std::fwrite(u, 4, nc, out.f) != nc) return AVISM_ERR_IO;
+    return std::fflush(out.f) == 0 ? AVISM_OK : AVISM_ERR_IO;
 }
 
 int avism_io_write_headers(const char *voids_path, const char *cubes_path, int32_t nlev, int32_t levmin,

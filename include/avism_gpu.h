@@ -304,6 +304,35 @@ int avism_gpu_knn_noalloc(int device, void *stream, int64_t n, const float *x,
 int avism_io_particle_header(const char *path, int64_t *n, float *zeta);
 int avism_io_read_particles(const char *path, int64_t capacity, float *x, float *y, float *z,
                             float *vx, float *vy, float *vz, float *m);
+/* READ_BINARY_PART_2 (src/reader.f90:465-519): the same file without the three
+ * velocity records (x, y, z, m); the driver then takes the no-velocity path
+ * (avism_params.no_velocities = 1).  Header via avism_io_particle_header.
+ * Records longer than a gfortran subrecord (2147483639 bytes) are read as the
+ * chain of subrecords gfortran writes for them, in every reader here.        */
+int avism_io_read_particles_novel(const char *path, int64_t capacity, float *x, float *y, float *z,
+                                  float *m);
+/* READ_BINARY_GRID (src/reader.f90:523-552): [REAL*4 ZETA], then U1G (density
+ * contrast delta), U2G, U3G, U4G (velocities in km/s), nx^3 REAL*4 each,
+ * column-major, as stored.  The reference then takes U1G + 1 and divides the
+ * velocities by UV (src/reader.f90:546-550); avism_gpu_run_level_grid expects
+ * those converted values.                                                     */
+int avism_io_read_grid(const char *path, int32_t nx, float *zeta, float *u1, float *u2, float *u3, float *u4);
+/* Survey mask (src/avism.f90:403-418): a stream file [int32 NMASK, REAL*4
+ * MASKLOW, MASKUPPER, MASKSIDE, INTEGER*1 SMASK2(NMASK^3)].  NMASK must equal
+ * ncox (the coarse grid, else AVISM_ERR_ARG as the reference's stop); the mask
+ * is mapped onto the level's nx^3 cells by integer refinement NDOWN = nx/NMASK
+ * (even, src/avism.f90:873-892), and positive values become 1
+ * (src/avism.f90:898).  smask: inner nx^3 (int8); lims (nullable, 3 floats)
+ * receives MASKLOW, MASKUPPER, MASKSIDE.                                      */
+int avism_io_read_mask(const char *path, int32_t ncox, int32_t nx, int8_t *smask, float *lims);
+/* Survey randoms (src/avism.f90:1425-1444): sequential unformatted [INTEGER*4
+ * NRAND], then RANDX, RANDY, RANDZ [cMpc] and the weights MASSRAND [Msun], as
+ * stored (the reference divides the weights by UM).                          */
+int avism_io_randoms_header(const char *path, int32_t *nrand);
+int avism_io_read_randoms(const char *path, int32_t capacity, float *x, float *y, float *z, float *w);
+/* vel_cube.dat (src/avism.f90:1198-1202): the SPH velocity grids U2, U3, U4
+ * (inner nx^3 each, column-major) written raw, STREAM access.                 */
+int avism_io_write_vel_cube(const char *path, int32_t nx, const float *u2, const float *u3, const float *u4);
 
 /* The voids / cubes catalogues and the map file of one iteration
  * (src/avism.f90:710-722 and 2026-2085), as tools/read_voids.py reads them.

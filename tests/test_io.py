@@ -171,3 +171,107 @@ def test_reference_reader_reads_the_files(tmp_path, level):
     o, nx, ne = 1 - g.low1, g.nx, g.ne
     ext = np.asarray(cat["marca"]).reshape((ne,) * 3, order="F")
     assert np.array_equal(marca[0], ext[o:o + nx, o:o + nx, o:o + nx])
+
+
+def _fortran_subrecords(f, payload, chunk):
+    """One logical record written as gfortran's chain of subrecords of at most
+    `chunk` bytes: a negative leading marker when another subrecord follows, a
+    negative trailing marker on every subrecord after the first."""
+    parts = [payload[i:i + chunk] for i in range(0, len(payload), chunk)] or [b""]
+    for i, part in enumerate(parts):
+        head = -len(part) if i < len(parts) - 1 else len(part)
+        tail = -len(part) if i > 0 else len(part)
+        f.write(np.int32(head).tobytes() + part + np.int32(tail).tobytes())
+
+
+def test_particle_file_with_split_records(tmp_path):
+    """Records written as subrecord chains (gfortran splits records above
+    2147483639 bytes) read back as the whole record."""
+    rng = np.random.default_rng(3)
+    n = 777
+    cols = [rng.normal(0, 10, n).astype(np.float32) for _ in range(7)]
+    path = tmp_path / "split"
+    with open(path, "wb") as f:
+        _fortran_subrecords(f, np.int64(n).tobytes() + np.float32(1.5).tobytes(), 12)
+        for i, c in enumerate(cols):
+            _fortran_subrecords(f, c.tobytes(), [4, 1000, 3108, 400, 1, 7, 64][i])
+    r = read_particle_file(path)
+    assert r["zeta"] == np.float32(1.5)
+    for k, c in zip(("x", "y", "z", "vx", "vy", "vz", "m"), cols):
+        assert np.array_equal(r[k], c), k
+    bad = tmp_path / "badsplit"                      # chain whose trailing marker lies
+    with open(bad, "wb") as f:
+        _fortran_subrecords(f, np.int64(n).tobytes() + np.float32(1.5).tobytes(), 12)
+        b = cols[0].tobytes()
+        f.write(np.int32(-100).tobytes() + b[:100] + np.int32(-99).tobytes())
+    lib = _lib.load()
+    bufs = [np.zeros(n, np.float32) for _ in range(7)]
+    assert lib.avism_io_read_particles(os.fsencode(bad), n, *(C.c_void_p(b.ctypes.data) for b in bufs)) == 10
+
+
+def test_particle_file_without_velocities(tmp_path):
+    from avism_b200.avism import read_particle_file_novel
+    rng = np.random.default_rng(4)
+    n = 500
+    cols = [rng.uniform(-50, 50, n).astype(np.float32) for _ in range(3)] + [np.full(n, 3e9, np.float32)]
+    path = tmp_path / "bin_file_part2"
+    _fortran_records(path, [np.int64(n).tobytes() + np.float32(0.25).tobytes()] + cols)
+    r = read_particle_file_novel(path)
+    assert r["zeta"] == np.float32(0.25) and set(r) == {"x", "y", "z", "m", "zeta"}
+    for k, c in zip(("x", "y", "z", "m"), cols):
+        assert np.array_equal(r[k], c), k
+
+
+def test_grid_file(tmp_path):
+    from avism_b200.avism import read_grid_file
+    rng = np.random.default_rng(5)
+    nx = 12
+    grids = [rng.normal(0, 1, nx ** 3).astype(np.float32) for _ in range(4)]
+    path = tmp_path / "bin_file_grid00001"
+    _fortran_records(path, [np.float32(0.0).tobytes()] + grids)
+    r = read_grid_file(path, nx)
+    for k, g in zip(("u1", "u2", "u3", "u4"), grids):
+        assert np.array_equal(r[k], g), k
+    with pytest.raises(AvismError):
+        read_grid_file(path, nx + 1)                  # records shorter than (nx+1)^3
+
+
+def test_mask_file_maps_to_level(tmp_path):
+    """mask.dat at the coarse grid, mapped onto a level 4x finer by integer
+    refinement; positive values become 1, zero and negative ones stay."""
+    from avism_b200.avism import read_mask_file
+    rng = np.random.default_rng(6)
+    nm = 8
+    m2 = rng.integers(-2, 4, nm ** 3).astype(np.int8)
+    path = tmp_path / "mask.dat"
+    with open(path, "wb") as f:
+        f.write(np.int32(nm).tobytes() + np.array([-1.0, 1.0, 2.0], np.float32).tobytes() + m2.tobytes())
+    sm, lims = read_mask_file(path, nm, nm)
+    assert np.array_equal(lims, np.array([-1.0, 1.0, 2.0], np.float32))
+    assert np.array_equal(sm, np.where(m2 > 0, 1, m2).astype(np.int8))
+    fine, _ = read_mask_file(path, nm, 4 * nm)
+    m3 = np.where(m2 > 0, 1, m2).reshape(nm, nm, nm)                     # [k][j][i]
+    want = m3.repeat(4, 0).repeat(4, 1).repeat(4, 2).ravel()
+    assert np.array_equal(fine, want)
+    with pytest.raises(AvismError):
+        read_mask_file(path, nm + 1, nm + 1)          # 'MASK grid does not coincide'
+    with pytest.raises(AvismError):
+        read_mask_file(path, nm, 3 * nm)              # odd refinement
+
+
+def test_randoms_file_and_vel_cube(tmp_path):
+    from avism_b200.avism import read_randoms_file, write_vel_cube
+    rng = np.random.default_rng(7)
+    n = 321
+    cols = [rng.uniform(-9, 9, n).astype(np.float32) for _ in range(3)] + [rng.uniform(0.5, 2, n).astype(np.float32)]
+    path = tmp_path / "rands.dat"
+    _fortran_records(path, [np.int32(n).tobytes()] + cols)
+    r = read_randoms_file(path)
+    for k, c in zip(("x", "y", "z", "w"), cols):
+        assert np.array_equal(r[k], c), k
+    nx = 6
+    g = [rng.normal(0, 1, nx ** 3).astype(np.float32) for _ in range(3)]
+    vp = tmp_path / "vel_cube.dat"
+    write_vel_cube(vp, nx, *g)
+    raw = np.fromfile(vp, np.float32)
+    assert np.array_equal(raw, np.concatenate(g))
