@@ -40,7 +40,8 @@ class AvismParams(C.Structure):
         ("rmin_sub", C.c_float), ("kneighbours", C.c_int32),
         ("flag_vel_interp", C.c_int32), ("flag_dens_interp", C.c_int32),
         ("level", C.c_int32), ("levmin", C.c_int32), ("learned", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("kernel_mode", C.c_int32), ("no_velocities", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -152,6 +153,8 @@ class Params:
     level: int = 0
     levmin: int = 0
     learned: int = 0
+    kernel_mode: int = 1
+    no_velocities: int = 0
     extra: dict = field(default_factory=dict)
 
     def to_c(self) -> AvismParams:

@@ -205,9 +205,10 @@ class AvismGPU:
     def knn_counters(self, enable: bool = True) -> dict:
         """Counters of the last particles_to_grid / run_level call; enable
         turns collection on (or off) for the following calls."""
-        out = np.zeros(8, np.int64)
-        self._chk(self.lib.avism_gpu_knn_counters(self.h, int(enable), _vp(out), 8))
-        keys = ("queries", "attempts", "scanned", "kept", "fallbacks", "exact_ranks")
+        out = np.zeros(9, np.int64)
+        self._chk(self.lib.avism_gpu_knn_counters(self.h, int(enable), _vp(out), 9))
+        keys = ("queries", "attempts", "scanned", "kept", "fallbacks", "exact_ranks", "ball_cells", "orphans",
+                "norm0")
         return {k: int(out[i]) for i, k in enumerate(keys)}
 
     # ---- learned proposal (no reference counterpart) -----------------------------
@@ -217,7 +218,7 @@ class AvismGPU:
 
     def proposal_features(self, p: Params, parts: dict):
         """(features [nb^3, 12], nb, bin width) of the binning particles_to_grid uses."""
-        a = {k: _f32(parts[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        a = {k: (_f32(parts[k]) if parts.get(k) is not None else None) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
         nb, bw = C.c_int32(), C.c_float()
         pc = p.to_c()
         args = (self.h, C.byref(pc), len(a["x"]), *(_vp(a[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")))
@@ -261,7 +262,7 @@ class AvismGPU:
 
     # ---- PPART_DENS / VVEL_INTERP_SPH_VW / FILL_H_ZEROS / DDENS_INTERP_SPH / TSC
     def particles_to_grid(self, p: Params, parts: dict, smask=None):
-        a = {k: _f32(parts[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        a = {k: (_f32(parts[k]) if parts.get(k) is not None else None) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
         n = len(a["x"])
         nc = p.nx ** 3
         out = [np.zeros(nc, np.float32) for _ in range(4)]
@@ -282,7 +283,8 @@ class AvismGPU:
         dv = np.zeros(ne3, np.float32)
         md = C.c_float()
         pc = p.to_c()
-        self._chk(self.lib.avism_gpu_fields(self.h, C.byref(pc), *(_vp(_f32(v)) for v in (u_mass, u2, u3, u4)),
+        self._chk(self.lib.avism_gpu_fields(self.h, C.byref(pc),
+                                            *(_vp(None if v is None else _f32(v)) for v in (u_mass, u2, u3, u4)),
                                             _vp(u1), _vp(dv), C.byref(md)))
         return u1, dv, md.value
 
@@ -346,7 +348,7 @@ class AvismGPU:
     def run_sublevel(self, p: Params, parts: dict, marcap_ext, reqp, want_marca=False, capacity=None):
         g, _ = grid_setup(p)
         cap = int(capacity or p.nvoid_max)
-        a = {k: _f32(parts[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        a = {k: (_f32(parts[k]) if parts.get(k) is not None else None) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
         cubes = Cubes(cap)
         vo = Voids(cap, g.ne if want_marca else None)
         nv, md = C.c_int32(), C.c_float()
@@ -363,7 +365,7 @@ class AvismGPU:
     def run_level(self, p: Params, parts: dict, want_marca=False, want_cubes=True, capacity=None):
         g, _ = grid_setup(p)
         cap = int(capacity or p.nvoid_max)
-        a = {k: _f32(parts[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        a = {k: (_f32(parts[k]) if parts.get(k) is not None else None) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
         n = len(a["x"])
         cubes = Cubes(cap) if want_cubes else None
         vo = Voids(cap, g.ne if want_marca else None)

@@ -134,6 +134,12 @@ P2G p2g_args(Ctx &c, const avism_params *p, const Level &L, int64_t n, const flo
     a.x = (const float *)to_device(c, B_PX, x, nb);
     a.y = (const float *)to_device(c, B_PY, y, nb);
     a.z = (const float *)to_device(c, B_PZ, z, nb);
+    if (p->no_velocities && !(vx && vy && vz)) {
+        // READ_BINARY_PART_2 input: no velocities; zeros stand in for them
+        float *zv = c.get_t<float>(B_PVX, (size_t)std::max<int64_t>(n, 1));
+        AV_CUDA(cudaMemsetAsync(zv, 0, nb, c.stream));
+        vx = vy = vz = zv;
+    }
     a.vx = (const float *)to_device(c, B_PVX, vx, nb);
     a.vy = (const float *)to_device(c, B_PVY, vy, nb);
     a.vz = (const float *)to_device(c, B_PVZ, vz, nb);
@@ -157,6 +163,8 @@ void check_params(const avism_params *p) {
     AV_CHECK(p->flag_vel_interp == 0 || p->flag_vel_interp == 1, AVISM_ERR_ARG, "FLAG_VEL_INTERP must be 0 or 1");
     AV_CHECK(p->flag_dens_interp == 0 || p->flag_dens_interp == 1, AVISM_ERR_ARG, "FLAG_DENS_INTERP must be 0 or 1");
     AV_CHECK(p->nvoid_max >= 1, AVISM_ERR_ARG, "NVOID_MAX must be positive");
+    AV_CHECK(p->kernel_mode >= 0 && p->kernel_mode <= 2, AVISM_ERR_ARG, "KERNEL_MODE must be 1 (M4) or 2 (Gaussian)");
+    AV_CHECK(p->no_velocities == 0 || p->no_velocities == 1, AVISM_ERR_ARG, "no_velocities must be 0 or 1");
 }
 
 }  // namespace
@@ -279,7 +287,8 @@ int avism_gpu_knn_counters(avism_gpu_ctx *ctx, int enable, int64_t *out, int n) 
                 AV_CUDA(cudaMemcpyAsync(h, c.buf[B_KNN_STATS], sizeof h, cudaMemcpyDeviceToHost, c.stream));
                 c.sync();
             }
-            for (int i = 0; i < n && i < 8; i++) out[i] = (int64_t)h[i];
+            for (int i = 0; i < n && i < 6; i++) out[i] = (int64_t)h[i];
+            for (int i = 6; i < n && i < 9; i++) out[i] = c.path_counts[i - 6];
         }
         c.knn_stats = enable != 0;
     });

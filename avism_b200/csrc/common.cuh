@@ -81,6 +81,9 @@ struct Ctx {
     bool prop_loaded = false;
     // collect warp-kNN counters in particles_to_grid
     bool knn_stats = false;
+    // branch counters of the last particles_to_grid with counters on: cells on
+    // the ball fallback, FILL_H_ZEROS orphans, DDENS particles with NORM = 0
+    int64_t path_counts[3] = {0, 0, 0};
     // named stage marks: events recorded on the stream, resolved by stage_close()
     std::vector<cudaEvent_t> marks;
     std::vector<std::string> mark_names;

@@ -36,6 +36,12 @@ __global__ void k_div_scalar(int64_t nc, float *__restrict__ a, float s) {
     if (c < nc) a[c] = __fdiv_rn(a[c], s);
 }
 
+// linear-theory divergence from the density contrast: -(coef * (U1CO - 1))
+__global__ void k_lin_div(int64_t nc, const float *__restrict__ u1, float coef, float *__restrict__ dv) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nc) dv[c] = -__fmul_rn(coef, __fsub_rn(u1[c], 1.0f));
+}
+
 struct ToDouble {
     __host__ __device__ double operator()(float v) const { return (double)v; }
 };
@@ -218,7 +224,12 @@ FieldsOut fields_inner(Ctx &c, const avism_params *p, const Level &L, const floa
     const float mean = (float)(sum / (double)nc);
     ++c.launches, k_div_scalar<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u1co_in, mean);
     c.mark("normalise");
-    if (diver_tma_ok(nx, u2, u3, u4)) {
+    if (p->no_velocities) {
+        // DIVERCO = -OMEGA0**(0.6)*RETE*HTE*(U1CO - 1.0) (src/avism.f90:1647-1650),
+        // the REAL*4 coefficient with the host libm's powf, as the reference's
+        const float coef = (::powf(p->omega0, 0.6f) * L.g.rete) * L.g.hte;
+        ++c.launches, k_lin_div<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u1co_in, coef, diver_in);
+    } else if (diver_tma_ok(nx, u2, u3, u4)) {
         const CUtensorMap m2 = grid_map(u2, nx, DV_TX + 8, DV_TY, DV_TZ);
         const CUtensorMap m3 = grid_map(u3, nx, DV_TX, DV_TY + 2, DV_TZ);
         const CUtensorMap m4 = grid_map(u4, nx, DV_TX, DV_TY, DV_TZ + 2);

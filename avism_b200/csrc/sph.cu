@@ -30,6 +30,17 @@ __device__ __forceinline__ float kernel_m4(float h, float dist) {
     return 0.0f;
 }
 
+// KERNEL_FUNC with KERNEL_MODE = 2 (src/particles.f90:955-956): Q = DIST/(H/2),
+// EXP(-Q**2).  expf is CUDA's (within 2 ulp); the Gaussian fields agree with a
+// host libm to the interpolation tolerance, not bit for bit.
+__device__ __forceinline__ float kernel_w(bool gauss, float h, float dist) {
+    if (gauss) {
+        const float q = __fdiv_rn(dist, __fmul_rn(h, 0.5f));
+        return expf(-__fmul_rn(q, q));
+    }
+    return kernel_m4(h, dist);
+}
+
 // HPART(j) = MAX(HPART(j), d): non-negative floats order as their int bits
 __device__ __forceinline__ void atomic_max_pos(float *a, float v) {
     atomicMax((int *)a, __float_as_int(v));
@@ -89,6 +100,14 @@ k_fill_h(KnnGrid G, int64_t n, int K, float *__restrict__ hp_s) {
     hp_s[i] = sqrtf(key_d2(col[(size_t)(K - 1) * S]));
 }
 
+// particles whose h is still 0 (FILL_H_ZEROS will search for them)
+__global__ void k_count_zero(int64_t n, const float *__restrict__ h, unsigned long long *cnt) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool z = i < n && h[i] == 0.0f;
+    const unsigned b = __ballot_sync(0xffffffffu, z);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(cnt, (unsigned long long)__popc(b));
+}
+
 // binned order -> input order
 __global__ void k_unbin_f32(int64_t n, const float4 *__restrict__ sp, const float *__restrict__ src,
                             float *__restrict__ dst) {
@@ -105,6 +124,7 @@ struct CellArgs {
     const float *pd_s;                // particle density in binned order
     float *hp_s, *u2, *u3, *u4;       // h in binned order
     int do_vel;
+    int gauss;                        // KERNEL_MODE = 2
     int32_t *ball_list;
     int32_t *ball_count;
 };
@@ -140,7 +160,7 @@ k_cells_knn(KnnGrid G, CellArgs A) {
         const unsigned long long key = col[(size_t)i * S];
         const uint32_t j = key_pos(key);
         const float4 a = A.sv[j];
-        float w = kernel_m4(hk, sqrtf(key_d2(key)));
+        float w = kernel_w(A.gauss, hk, sqrtf(key_d2(key)));
         w = __fmul_rn(w, __fdiv_rn(a.w, A.pd_s[j]));
         const double w8 = (double)w;
         b = b + w8;
@@ -154,10 +174,14 @@ k_cells_knn(KnnGrid G, CellArgs A) {
 }
 
 // ---- cells in the ball branch: all particles within DX (src/particles.f90:868-878)
-__global__ void k_cells_ball(KnnGrid G, CellArgs A, int32_t nlist) {
-    const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
-    if (t >= nlist) return;
-    const int64_t c = A.ball_list[t];
+// ball_search returns the ball sorted by distance (src/kdtree.f90:1015-1212), and
+// the velocity sums run over it in that order.  Here the members of every ball
+// cell are listed with 64-bit keys (squared-distance bits above the particle
+// index, the tie rule), sorted per cell, and summed in that order:
+//   k_ball_scan (count, h = max distance, K-th distance) -> scan of the counts
+//   -> k_ball_fill (keys, binned positions) -> segmented sort -> k_ball_sum.
+template <class F>
+__device__ __forceinline__ void ball_walk(const KnnGrid &G, const CellArgs &A, int64_t c, F &&f) {
     const int nx = A.nx;
     const int ix = (int)(c % nx) + 1, jy = (int)((c / nx) % nx) + 1, kz = (int)(c / ((int64_t)nx * nx)) + 1;
     const float q[3] = {A.rad[ix - A.rad_lo], A.rad[jy - A.rad_lo], A.rad[kz - A.rad_lo]};
@@ -167,44 +191,106 @@ __global__ void k_cells_ball(KnnGrid G, CellArgs A, int32_t nlist) {
     const int sb = (int)ceilf(A.dx * G.inv_bw) + 1;
     int lo[3], hi[3];
     for (int a = 0; a < 3; a++) axis_window(G, b[a], sb, lo[a], hi[a]);
-    float dmax2 = -1.0f;
-    for (int pass = 0; pass < (A.do_vel ? 2 : 1); pass++) {
-        const float hk = sqrtf(dmax2);
-        double bs = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
-        for (int dz = lo[2]; dz <= hi[2]; dz++) {
-            const int bz_ = G.periodic ? wrap_bin(b[2] + dz, G.nb) : b[2] + dz;
-            for (int dy = lo[1]; dy <= hi[1]; dy++) {
-                const int by_ = G.periodic ? wrap_bin(b[1] + dy, G.nb) : b[1] + dy;
-                for (int dx = lo[0]; dx <= hi[0]; dx++) {
-                    const int bx_ = G.periodic ? wrap_bin(b[0] + dx, G.nb) : b[0] + dx;
-                    const int bin = bx_ + G.nb * (by_ + G.nb * bz_);
-                    for (int64_t p = G.start[bin]; p < G.start[bin + 1]; p++) {
-                        const float4 v = G.sp[p];
-                        const float d2 = dist2_ref(v.x, v.y, v.z, q[0], q[1], q[2], G.box, G.periodic);
-                        if (!(d2 <= r2)) continue;
-                        if (pass == 0) {
-                            dmax2 = fmaxf(dmax2, d2);
-                            atomic_max_pos(&A.hp_s[p], sqrtf(d2));
-                        } else {
-                            const float4 a = A.sv[p];
-                            float w = kernel_m4(hk, sqrtf(d2));
-                            w = __fmul_rn(w, __fdiv_rn(a.w, A.pd_s[p]));
-                            const double w8 = (double)w;
-                            bs = bs + w8;
-                            bx = bx + w8 * (double)a.x;
-                            by = by + w8 * (double)a.y;
-                            bz = bz + w8 * (double)a.z;
-                        }
-                    }
+    for (int dz = lo[2]; dz <= hi[2]; dz++) {
+        const int bz_ = G.periodic ? wrap_bin(b[2] + dz, G.nb) : b[2] + dz;
+        for (int dy = lo[1]; dy <= hi[1]; dy++) {
+            const int by_ = G.periodic ? wrap_bin(b[1] + dy, G.nb) : b[1] + dy;
+            for (int dx = lo[0]; dx <= hi[0]; dx++) {
+                const int bx_ = G.periodic ? wrap_bin(b[0] + dx, G.nb) : b[0] + dx;
+                const int bin = bx_ + G.nb * (by_ + G.nb * bz_);
+                for (int64_t p = G.start[bin]; p < G.start[bin + 1]; p++) {
+                    const float4 v = G.sp[p];
+                    const float d2 = dist2_ref(v.x, v.y, v.z, q[0], q[1], q[2], G.box, G.periodic);
+                    if (d2 <= r2) f(p, v, d2);
                 }
             }
         }
-        if (pass == 1) {
-            A.u2[c] = (float)(bx / bs);
-            A.u3[c] = (float)(by / bs);
-            A.u4[c] = (float)(bz / bs);
-        }
     }
+}
+
+// members per ball cell, h = MAX(h, d) of every member, the largest distance
+__global__ void k_ball_scan(KnnGrid G, CellArgs A, int32_t nlist, int32_t *__restrict__ cnt,
+                            float *__restrict__ dmax) {
+    const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (t >= nlist) return;
+    int32_t m = 0;
+    float dm2 = -1.0f;
+    ball_walk(G, A, A.ball_list[t], [&](int64_t p, const float4 &, float d2) {
+        m++;
+        dm2 = fmaxf(dm2, d2);
+        atomic_max_pos(&A.hp_s[p], sqrtf(d2));
+    });
+    cnt[t] = m;
+    dmax[t] = sqrtf(dm2);
+}
+
+__global__ void k_ball_fill(KnnGrid G, CellArgs A, int32_t nlist, const int64_t *__restrict__ off,
+                            unsigned long long *__restrict__ keys, int32_t *__restrict__ pos) {
+    const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (t >= nlist) return;
+    int64_t o = off[t];
+    ball_walk(G, A, A.ball_list[t], [&](int64_t p, const float4 &v, float d2) {
+        keys[o] = ((unsigned long long)__float_as_uint(d2) << 32) | (uint32_t)__float_as_int(v.w);
+        pos[o] = (int32_t)p;
+        o++;
+    });
+}
+
+// the velocity sums over each ball in (distance, particle index) order, REAL*8
+__global__ void k_ball_sum(CellArgs A, int32_t nlist, const int64_t *__restrict__ off,
+                           const unsigned long long *__restrict__ keys, const int32_t *__restrict__ pos,
+                           const float *__restrict__ dmax) {
+    const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (t >= nlist) return;
+    const int64_t c = A.ball_list[t];
+    const float hk = dmax[t];
+    double bs = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
+    for (int64_t o = off[t]; o < off[t + 1]; o++) {
+        const int32_t p = pos[o];
+        const float4 a = A.sv[p];
+        float w = kernel_w(A.gauss, hk, sqrtf(__uint_as_float((uint32_t)(keys[o] >> 32))));
+        w = __fmul_rn(w, __fdiv_rn(a.w, A.pd_s[p]));
+        const double w8 = (double)w;
+        bs = bs + w8;
+        bx = bx + w8 * (double)a.x;
+        by = by + w8 * (double)a.y;
+        bz = bz + w8 * (double)a.z;
+    }
+    A.u2[c] = (float)(bx / bs);
+    A.u3[c] = (float)(by / bs);
+    A.u4[c] = (float)(bz / bs);
+}
+
+static void cells_ball(Ctx &c, const KnnGrid &G, const CellArgs &A, int32_t nball) {
+    if (nball <= 0) return;
+    int32_t *cnt = c.get_t<int32_t>(B_LIST_A, (size_t)nball + 1);
+    float *dmax = c.get_t<float>(B_LIST_B, (size_t)nball);
+    int64_t *off = c.get_t<int64_t>(B_SEG_A, (size_t)nball + 1);
+    ++c.launches, k_ball_scan<<<grid_for(nball, 128), 128, 0, c.stream>>>(G, A, nball, cnt, dmax);
+    AV_CUDA(cudaGetLastError());
+    if (!A.do_vel) return;
+    AV_CUDA(cudaMemsetAsync(cnt + nball, 0, sizeof(int32_t), c.stream));
+    size_t tmp = 0;
+    AV_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt, off, nball + 1, c.stream));
+    AV_CUDA(cub::DeviceScan::ExclusiveSum(c.get(B_CUB_TMP, tmp), tmp, cnt, off, nball + 1, c.stream));
+    int64_t total = 0;
+    AV_CUDA(cudaMemcpyAsync(&total, off + nball, sizeof total, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    AV_CHECK(total < (int64_t)INT32_MAX, AVISM_ERR_UNSUPPORTED, "ball fallback: more than 2^31 members");
+    const int64_t m = std::max<int64_t>(total, 1);
+    unsigned long long *ka = c.get_t<unsigned long long>(B_SORT_KEY, 2 * (size_t)m);
+    int32_t *pa = c.get_t<int32_t>(B_SORT_IDX, 2 * (size_t)m);
+    ++c.launches, k_ball_fill<<<grid_for(nball, 128), 128, 0, c.stream>>>(G, A, nball, off, ka, pa);
+    AV_CUDA(cudaGetLastError());
+    cub::DoubleBuffer<unsigned long long> dk(ka, ka + m);
+    cub::DoubleBuffer<int32_t> dv(pa, pa + m);
+    tmp = 0;
+    AV_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, tmp, dk, dv, (int)total, nball, off, off + 1, c.stream));
+    AV_CUDA(cub::DeviceSegmentedSort::SortPairs(c.get(B_CUB_TMP, tmp), tmp, dk, dv, (int)total, nball, off,
+                                                off + 1, c.stream));
+    ++c.launches, k_ball_sum<<<grid_for(nball, 128), 128, 0, c.stream>>>(A, nball, off, dk.Current(),
+                                                                          dv.Current(), dmax);
+    AV_CUDA(cudaGetLastError());
 }
 
 // ---- warp-per-query forms of PPART_DENS and VVEL_INTERP_SPH_VW / H_DISTANCE ----
@@ -346,7 +432,7 @@ k_cells_knn_w(KnnGrid G, CellArgs A) {
         for (int j = lane; j < cnt; j += 32) {
             const uint32_t pj = S.res_pos[j];
             const float4 a = A.sv[pj];
-            float w = kernel_m4(hk, sqrtf(__uint_as_float(S.res_d2[j])));
+            float w = kernel_w(A.gauss, hk, sqrtf(__uint_as_float(S.res_d2[j])));
             w = __fmul_rn(w, __fdiv_rn(a.w, A.pd_s[pj]));
             const double w8 = (double)w;
             acc[j] = w8;
@@ -375,6 +461,8 @@ struct DdensArgs {
     unsigned long long *fix;      // 2 words per cell: low, high
     double scale;
     float scale_f;                // the same power of two
+    unsigned long long *norm0;    // counter of NORM = 0 particles, or null
+    int gauss;                    // KERNEL_MODE = 2
 };
 
 // v < 2^62 is added as its two 32-bit halves to two 64-bit counters (low half to
@@ -384,6 +472,14 @@ struct DdensArgs {
 __device__ __forceinline__ void add128(unsigned long long *cell, unsigned long long v) {
     atomicAdd(cell, v & 0xffffffffULL);
     atomicAdd(cell + 1, v >> 32);
+}
+
+// DDENS weight: M4 of Q = SQRT(D2) * INV_H, or with KERNEL_MODE = 2 the Gaussian
+// EXP(-D2 * INV_H_SQ), INV_H_SQ = INV_H * INV_H (src/particles.f90:522-538)
+__device__ __forceinline__ float m4_q(float d2, float inv_h);
+__device__ __forceinline__ float kernel_q(bool gauss, float d2, float inv_h) {
+    if (gauss) return expf(-__fmul_rn(d2, __fmul_rn(inv_h, inv_h)));
+    return m4_q(d2, inv_h);
 }
 
 __device__ __forceinline__ float m4_q(float d2, float inv_h) {
@@ -408,8 +504,9 @@ __device__ __noinline__ void ddens_nested(const DdensArgs &A, const float4 p, in
     const float inv_h = __fdiv_rn(2.0f, h);
     const float h2max = __fmul_rn(__fmul_rn(4.0f, h), h);
     const int inc = (int)__fadd_rn(__fdiv_rn(__fmul_rn(2.0f, h), dx), 0.5f);
-    // only cells with Q <= 2 (d <= h) carry weight; rows and planes beyond h are skipped
-    const float hh = h * h * 1.00002f + 1e-30f;
+    // M4: only cells with Q <= 2 (d <= h) carry weight; rows and planes beyond h
+    // are skipped.  Gaussian: every cell with D2 <= H2_MAX (d <= 2h) does.
+    const float hh = (A.gauss ? h2max : h * h) * 1.00002f + 1e-30f;
     const float inv_dx = 1.0f / dx;
     const float *rad = A.rad - A.rad_lo;
     const float m = A.sv[i].w;
@@ -455,8 +552,8 @@ __device__ __noinline__ void ddens_nested(const DdensArgs &A, const float4 p, in
                 while (e >= a && d2_of(e) > hh) e--;
                 for (int i2 = a; i2 <= e; i2++) {
                     const float d2 = d2_of(i2);
-                    if (d2 > h2max) continue;            // never, as hh < h2max; kept as in the reference
-                    const float w = m4_q(d2, inv_h);
+                    if (d2 > h2max) continue;            // SKIP CUBE CORNERS (M4: never, as hh < h2max)
+                    const float w = kernel_q(A.gauss, d2, inv_h);
                     if (pass == 0) {
                         norm = __fadd_rn(norm, w);
                     } else if (w != 0.0f) {
@@ -504,7 +601,8 @@ __global__ void __launch_bounds__(DD_THREADS, 6) k_ddens(KnnGrid G, int64_t n, D
     const float h = A.hp_s[i];
     const float inv_h = __fdiv_rn(2.0f, h);
     const int inc = (int)__fadd_rn(__fdiv_rn(__fmul_rn(2.0f, h), dx), 0.5f);
-    const float hh = h * h * 1.00002f + 1e-30f;
+    const float h2max = __fmul_rn(__fmul_rn(4.0f, h), h);
+    const float hh = (A.gauss ? h2max : h * h) * 1.00002f + 1e-30f;
     const float inv_dx = 1.0f / dx;
     const float *rad = A.rad - A.rad_lo;
     const int k_lo = max(kz - inc, 1), k_hi = min(kz + inc, nx);
@@ -577,12 +675,14 @@ __global__ void __launch_bounds__(DD_THREADS, 6) k_ddens(KnnGrid G, int64_t n, D
         for (int t = 0; t < ncell; t++) {
             const float tx = __fsub_rn(p.x, rad[i2]);
             const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), dy2), dz2);
-            norm = __fadd_rn(norm, m4_q(d2, inv_h));
+            // listed cells beyond H2_MAX (Gaussian only: M4 lists none) add nothing
+            if (!(A.gauss && d2 > h2max)) norm = __fadd_rn(norm, kernel_q(A.gauss, d2, inv_h));
             if (++i2 > ie && t + 1 < ncell) load_row(++r);
         }
     }
     const float m = A.sv[i].w;
     if (norm == 0.0f) {
+        if (A.norm0) atomicAdd(A.norm0, 1ull);
         // the particle only contributes to its own cell
         if (ix >= 1 && ix <= nx && jy >= 1 && jy <= nx && kz >= 1 && kz <= nx) {
             const int64_t cid = (int64_t)(ix - 1) + (int64_t)nx * ((int64_t)(jy - 1) + (int64_t)nx * (kz - 1));
@@ -597,7 +697,7 @@ __global__ void __launch_bounds__(DD_THREADS, 6) k_ddens(KnnGrid G, int64_t n, D
     for (int t = 0; t < ncell; t++) {
         const float tx = __fsub_rn(p.x, rad[i2]);
         const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(tx, tx), dy2), dz2);
-        const float w = m4_q(d2, inv_h);
+        const float w = (A.gauss && d2 > h2max) ? 0.0f : kernel_q(A.gauss, d2, inv_h);
         if (w != 0.0f) {
             const float contrib = __fdiv_rn(__fmul_rn(w, m), norm);
             // contrib * 2^k is exact in f32 (below 2^62, no overflow), so
@@ -624,7 +724,7 @@ __global__ void k_fix128_to_f32(int64_t nc, const unsigned long long *__restrict
 
 // ---- TSC (DENS_INTERP_TSC / VEL_INTERP_TSC) as a gather over TSC cells -------
 // Particles are sorted by their TSC cell I (src/particles.f90:73-75); each grid
-// cell gathers from the 27 neighbouring TSC cells in a fixed order.
+// cell gathers from the 27 neighbouring TSC cells.
 struct TscArgs {
     int nx, rad_lo, periodic;
     float dx, r1, rn, leng;
@@ -664,55 +764,83 @@ __global__ void k_tsc_keys(int64_t n, const float *__restrict__ x, const float *
     vals[i] = (int32_t)i;
 }
 
-__global__ void k_tsc_gather(int64_t nc, const int64_t *__restrict__ start, const int32_t *__restrict__ order,
-                             const float *__restrict__ x, const float *__restrict__ y,
-                             const float *__restrict__ z, const float *__restrict__ m,
-                             const float *__restrict__ vx, const float *__restrict__ vy,
-                             const float *__restrict__ vz, TscArgs A, float *__restrict__ u_mass,
-                             float *__restrict__ u2, float *__restrict__ u3, float *__restrict__ u4) {
+// Each grid cell merges the 27 particle lists of the TSC cells around it (each
+// ascending by particle index: stable sort) and adds the contributions in
+// particle order: the order of the reference's serial loop, which the oracle
+// keeps (the reference's OpenMP atomics leave it open).  Density sums in
+// REAL*8, the velocity and weight sums in REAL*4 (src/particles.f90:241-248).
+__global__ void __launch_bounds__(128)
+k_tsc_gather(int64_t nc, const int64_t *__restrict__ start, const int32_t *__restrict__ order,
+             const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
+             const float *__restrict__ m, const float *__restrict__ vx, const float *__restrict__ vy,
+             const float *__restrict__ vz, TscArgs A, float *__restrict__ u_mass, float *__restrict__ u2,
+             float *__restrict__ u3, float *__restrict__ u4) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
     const int nx = A.nx;
     const int ix = (int)(c % nx) + 1, jy = (int)((c / nx) % nx) + 1, kz = (int)(c / ((int64_t)nx * nx)) + 1;
-    double dm = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0, sw = 0.0;
-    for (int oz = -1; oz <= 1; oz++) {
-        int k = kz + oz;
-        if (A.periodic) { if (k < 1) k += nx; if (k > nx) k -= nx; } else if (k < 1 || k > nx) continue;
-        for (int oy = -1; oy <= 1; oy++) {
-            int j = jy + oy;
-            if (A.periodic) { if (j < 1) j += nx; if (j > nx) j -= nx; } else if (j < 1 || j > nx) continue;
-            for (int ox = -1; ox <= 1; ox++) {
-                int i = ix + ox;
-                if (A.periodic) { if (i < 1) i += nx; if (i > nx) i -= nx; } else if (i < 1 || i > nx) continue;
-                const int64_t b = (int64_t)(i - 1) + (int64_t)nx * ((int64_t)(j - 1) + (int64_t)nx * (k - 1));
-                for (int64_t q = start[b]; q < start[b + 1]; q++) {
-                    const int32_t pidx = order[q];
-                    int ci, cj, ck;
-                    float wx[3], wy[3], wz[3];
-                    tsc_axis(A, x[pidx], ci, wx);
-                    tsc_axis(A, y[pidx], cj, wy);
-                    tsc_axis(A, z[pidx], ck, wz);
-                    // offset of this grid cell from the particle's TSC cell is -ox etc.
-                    const float fx = wx[1 - ox], fy = wy[1 - oy], fz = wz[1 - oz];
-                    if (u_mass) dm += (double)__fmul_rn(__fmul_rn(__fmul_rn(m[pidx], fx), fy), fz);
-                    if (u2) {
-                        const float w = __fmul_rn(__fmul_rn(fx, fy), fz);
-                        s2 += (double)__fmul_rn(vx[pidx], w);
-                        s3 += (double)__fmul_rn(vy[pidx], w);
-                        s4 += (double)__fmul_rn(vz[pidx], w);
-                        sw += (double)w;
-                    }
-                }
+    int64_t cur[27], end[27];
+    int32_t head[27];
+#pragma unroll
+    for (int j = 0; j < 27; j++) {
+        const int ox = j % 3 - 1, oy = (j / 3) % 3 - 1, oz = j / 9 - 1;
+        int i = ix + ox, jj = jy + oy, k = kz + oz;
+        bool ok = true;
+        if (A.periodic) {
+            if (i < 1) i += nx; else if (i > nx) i -= nx;
+            if (jj < 1) jj += nx; else if (jj > nx) jj -= nx;
+            if (k < 1) k += nx; else if (k > nx) k -= nx;
+        } else {
+            ok = i >= 1 && i <= nx && jj >= 1 && jj <= nx && k >= 1 && k <= nx;
+        }
+        cur[j] = 0;
+        end[j] = 0;
+        if (ok) {
+            const int64_t b = (int64_t)(i - 1) + (int64_t)nx * ((int64_t)(jj - 1) + (int64_t)nx * (k - 1));
+            cur[j] = start[b];
+            end[j] = start[b + 1];
+        }
+        head[j] = cur[j] < end[j] ? order[cur[j]] : INT_MAX;
+    }
+    double dm = 0.0;
+    float s2 = 0.0f, s3 = 0.0f, s4 = 0.0f, sw = 0.0f;
+    for (;;) {
+        int32_t best = INT_MAX;
+        int jb = -1;
+#pragma unroll
+        for (int j = 0; j < 27; j++)
+            if (head[j] < best) { best = head[j]; jb = j; }
+        if (jb < 0) break;
+        const int ox = jb % 3 - 1, oy = (jb / 3) % 3 - 1, oz = jb / 9 - 1;
+#pragma unroll
+        for (int j = 0; j < 27; j++)
+            if (j == jb) {
+                cur[j]++;
+                head[j] = cur[j] < end[j] ? order[cur[j]] : INT_MAX;
             }
+        const int32_t pidx = best;
+        int ci, cj, ck;
+        float wx[3], wy[3], wz[3];
+        tsc_axis(A, x[pidx], ci, wx);
+        tsc_axis(A, y[pidx], cj, wy);
+        tsc_axis(A, z[pidx], ck, wz);
+        // this cell lies at -ox, -oy, -oz from the particle's TSC cell
+        const float fx = wx[1 - ox], fy = wy[1 - oy], fz = wz[1 - oz];
+        if (u_mass) dm += (double)__fmul_rn(__fmul_rn(__fmul_rn(m[pidx], fx), fy), fz);
+        if (u2) {
+            const float w = __fmul_rn(__fmul_rn(fx, fy), fz);
+            s2 = __fadd_rn(s2, __fmul_rn(vx[pidx], w));
+            s3 = __fadd_rn(s3, __fmul_rn(vy[pidx], w));
+            s4 = __fadd_rn(s4, __fmul_rn(vz[pidx], w));
+            sw = __fadd_rn(sw, w);
         }
     }
     if (u_mass) u_mass[c] = (float)dm;
     if (u2) {
-        float wei = (float)sw;
-        if (wei == 0.0f) wei = 1.0f;
-        u2[c] = __fdiv_rn((float)s2, wei);
-        u3[c] = __fdiv_rn((float)s3, wei);
-        u4[c] = __fdiv_rn((float)s4, wei);
+        const float wei = sw == 0.0f ? 1.0f : sw;
+        u2[c] = __fdiv_rn(s2, wei);
+        u3[c] = __fdiv_rn(s3, wei);
+        u4[c] = __fdiv_rn(s4, wei);
     }
 }
 
@@ -752,6 +880,20 @@ __global__ void k_zero_f32(int64_t n, float *a) {
     if (i < n) a[i] = 0.0f;
 }
 
+// with the counters on: the ball-fallback cells and the particles left with
+// h = 0 for FILL_H_ZEROS (Ctx::path_counts[0..1])
+static void count_orphans(Ctx &c, const KnnGrid &G, int64_t n, const float *hp_s, int32_t nball) {
+    if (!G.stats) return;
+    c.path_counts[0] = nball;
+    unsigned long long *d = c.get_t<unsigned long long>(B_RED2, 1);
+    AV_CUDA(cudaMemsetAsync(d, 0, sizeof *d, c.stream));
+    if (n > 0) ++c.launches, k_count_zero<<<grid_for(n, 256), 256, 0, c.stream>>>(n, hp_s, d);
+    unsigned long long h = 0;
+    AV_CUDA(cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    c.path_counts[1] = (int64_t)h;
+}
+
 template <int KMAX, bool STATS>
 static void run_sph_kernels_ws(Ctx &c, const KnnGrid &G, const avism_params *p, const Level &L,
                               const P2G &a, const float *rad_d, bool vel_sph, bool need_h_cells,
@@ -783,6 +925,7 @@ static void run_sph_kernels_ws(Ctx &c, const KnnGrid &G, const avism_params *p, 
         A.nx = nx; A.rad_lo = L.g.rad_lo; A.K = K; A.dx = L.g.dx; A.rad = rad_d; A.smask = a.smask;
         A.sv = sv; A.pd_s = pd_s;
         A.hp_s = hp_s; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
+        A.gauss = p->kernel_mode == 2;
         A.ball_list = ball_list; A.ball_count = cnt_d;
         const int64_t nblk = (int64_t)((nx + 3) / 4) * ((nx + 3) / 4) * ((nx + 1) / 2);
         ++c.launches, k_cells_knn_w<KMAX, STATS><<<(unsigned)nblk, SPH_WARPS * 32, sm_cells, c.stream>>>(G, A);
@@ -791,9 +934,10 @@ static void run_sph_kernels_ws(Ctx &c, const KnnGrid &G, const avism_params *p, 
         int32_t nball = 0;
         AV_CUDA(cudaMemcpyAsync(&nball, cnt_d, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
         c.sync();
-        if (nball > 0) ++c.launches, k_cells_ball<<<grid_for(nball, 128), 128, 0, c.stream>>>(G, A, nball);
+        cells_ball(c, G, A, nball);
         AV_CUDA(cudaGetLastError());
         c.mark("cells_ball");
+        count_orphans(c, G, a.n, hp_s, nball);
         {
             constexpr int KC = KMAX;
             const int T = KNN_THREADS(KC);
@@ -840,6 +984,7 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
         A.nx = nx; A.rad_lo = L.g.rad_lo; A.K = K; A.dx = L.g.dx; A.rad = rad_d; A.smask = a.smask;
         A.sv = sv; A.pd_s = pd_s;
         A.hp_s = hp_s; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
+        A.gauss = p->kernel_mode == 2;
         A.ball_list = ball_list; A.ball_count = cnt_d;
         const int tx = TileDims<T>::x, ty = TileDims<T>::y, tz = TileDims<T>::z;
         const int64_t nblk = (int64_t)((nx + tx - 1) / tx) * ((nx + ty - 1) / ty) * ((nx + tz - 1) / tz);
@@ -849,9 +994,10 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
         int32_t nball = 0;
         AV_CUDA(cudaMemcpyAsync(&nball, cnt_d, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
         c.sync();
-        if (nball > 0) ++c.launches, k_cells_ball<<<grid_for(nball, 128), 128, 0, c.stream>>>(G, A, nball);
+        cells_ball(c, G, A, nball);
         AV_CUDA(cudaGetLastError());
         c.mark("cells_ball");
+        count_orphans(c, G, a.n, hp_s, nball);
         ++c.launches, k_fill_h<KCAP><<<grid_for(a.n, T), T, sm, c.stream>>>(G, a.n, K, hp_s);
         c.mark("fill_h_zeros");
         if (a.hpart) ++c.launches, k_unbin_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, G.sp, hp_s, a.hpart);
@@ -886,7 +1032,10 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
     if (a.hpart) ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.hpart);
     if (a.part_dens) ++c.launches, k_zero_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.part_dens);
     c.mark("p2g_setup");
-    const bool vel_sph = p->flag_vel_interp == 1, dens_sph = p->flag_dens_interp == 1;
+    // no velocities (FLAG_VEL_AVAILABLE = 0, src/avism.f90:1259-1306): density only,
+    // with H_DISTANCE + FILL_H_ZEROS before DDENS; u2..u4 stay zero
+    const bool no_vel = p->no_velocities != 0;
+    const bool vel_sph = p->flag_vel_interp == 1 && !no_vel, dens_sph = p->flag_dens_interp == 1;
     TscArgs TA;
     TA.nx = nx; TA.rad_lo = L.g.rad_lo; TA.periodic = p->periodic; TA.dx = L.g.dx; TA.rad = rad_d;
     TA.r1 = L.rad_at(1) - 0.5f * L.g.dx;
@@ -902,6 +1051,7 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
         BinnedParticles bp = bin_particles(c, a.n, a.x, a.y, a.z, p->lado0, p->periodic, occ, a.vx, a.vy, a.vz,
                                            a.m, sv, fine);
         KnnGrid G = make_knn_grid(bp);
+        c.path_counts[0] = c.path_counts[1] = c.path_counts[2] = 0;
         if (c.knn_stats) {
             G.stats = c.get_t<unsigned long long>(B_KNN_STATS, 8);
             AV_CUDA(cudaMemsetAsync(G.stats, 0, 8 * sizeof(unsigned long long), c.stream));
@@ -965,15 +1115,28 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
             DdensArgs D;
             D.nx = nx; D.rad_lo = L.g.rad_lo; D.dx = L.g.dx; D.rx1 = L.rad_at(1); D.rad = rad_d;
             D.hp_s = hp_s; D.sv = sv; D.fix = fix; D.scale = scale; D.scale_f = (float)scale;
+            D.norm0 = nullptr;
+            D.gauss = p->kernel_mode == 2;
+            if (G.stats) {
+                D.norm0 = c.get_t<unsigned long long>(B_RED2, 1);
+                AV_CUDA(cudaMemsetAsync(D.norm0, 0, sizeof(unsigned long long), c.stream));
+            }
             c.mark("ddens_setup");
             ++c.launches, k_ddens<<<grid_for(a.n, DD_THREADS), DD_THREADS, 0, c.stream>>>(G, a.n, D);
             AV_CUDA(cudaGetLastError());
+            if (D.norm0) {
+                unsigned long long h = 0;
+                AV_CUDA(cudaMemcpyAsync(&h, D.norm0, sizeof h, cudaMemcpyDeviceToHost, c.stream));
+                c.sync();
+                c.path_counts[2] = (int64_t)h;
+            }
             c.mark("ddens_scatter");
             ++c.launches, k_fix128_to_f32<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, fix, 1.0 / scale, a.u_mass);
             c.mark("ddens_convert");
         }
     }
-    if (!vel_sph || !dens_sph) {
+    const bool vel_tsc = !no_vel && !vel_sph;
+    if (vel_tsc || !dens_sph) {
         // TSC: sort particles by their TSC cell, then gather
         uint32_t *ka = c.get_t<uint32_t>(B_KEYS_A, a.n), *kb = c.get_t<uint32_t>(B_KEYS_B, a.n);
         int32_t *va = c.get_t<int32_t>(B_VALS_A, a.n), *vb = c.get_t<int32_t>(B_VALS_B, a.n);
@@ -992,7 +1155,7 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
                                                                 dummy, start, nc);
         ++c.launches, k_tsc_gather<<<grid_for(nc, 128), 128, 0, c.stream>>>(
             nc, start, dv.Current(), a.x, a.y, a.z, a.m, a.vx, a.vy, a.vz, TA,
-            dens_sph ? nullptr : a.u_mass, vel_sph ? nullptr : a.u2, a.u3, a.u4);
+            dens_sph ? nullptr : a.u_mass, vel_tsc ? a.u2 : nullptr, a.u3, a.u4);
         AV_CUDA(cudaGetLastError());
         c.mark("tsc");
     }

@@ -9,7 +9,14 @@ value distributions of the benchmark workloads:
                           outflow inside them (64^3, 2^18 particles, L=100);
   * ``lognormal``      -- particles Poisson-sampled from exp(G) of a Gaussian random
                           field with P(k) ~ k^n, velocities from linear theory
-                          (v ~ grad(phi), scaled to a target rms).
+                          (v ~ grad(phi), scaled to a target rms);
+  * ``weighted_cone``  -- a survey-like tracer catalogue: power-law masses
+                          dn/dM ~ M^-1.9, placed by sampling a biased lognormal
+                          field inside a cone with radial selection and a
+                          random angular mask (non-periodic);
+  * ``add_clumps``     -- dense clumps added to a particle set, to reach the
+                          reference's rare branches (ball fallback, FILL_H_ZEROS,
+                          NORM = 0).
 
 ``to_reader_units`` applies the unit conversion READ_BINARY_PART_1 performs
 (src/reader.f90:455-458) so the arrays can be passed to the C-ABI.
@@ -166,6 +173,87 @@ def lognormal_torch(n, ng, box, index, sigma_ln=1.0, vrms=350.0, ache=0.678, see
     m = torch.full((n,), float(_mean_mass(n, box, ache)), device=device)
     return dict(x=x, y=y, z=z, vx=v[:, 0].contiguous(), vy=v[:, 1].contiguous(),
                 vz=v[:, 2].contiguous(), m=m, box=box)
+
+
+def power_law_masses(n, slope=-1.9, mlo=1e11, mhi=1e15, rng=None):
+    """n masses [Msun] with dn/dM ~ M^slope on [mlo, mhi] (inverse CDF)."""
+    rng = rng or np.random.default_rng(0)
+    a = slope + 1.0
+    u = rng.random(n)
+    m = (mlo ** a + u * (mhi ** a - mlo ** a)) ** (1.0 / a)
+    return m.astype(np.float32)
+
+
+def weighted_cone(box=1200.0, ng=128, rmax=600.0, half_angle_deg=60.0, rsel=400.0, mask_frac=0.15,
+                  n_target=4_000_000, index=-1.2, sigma_ln=1.0, bias=1.5, vrms=350.0, seed=1005):
+    """Weighted tracers in a survey cone (non-periodic geometry).
+
+    Positions: a lognormal field exp(G) on ng^3 (P(k) ~ k^index, sigma_ln),
+    sampled with weight rho^bias, kept inside the cone of ``half_angle_deg``
+    about +z from the origin out to ``rmax``, with the radial selection
+    n(r) ~ exp(-(r/rsel)^2) and a seeded angular mask: the cone's sky is cut
+    into 24 x 48 (cos theta, phi) pixels and a random ``mask_frac`` of them
+    removed.  Masses: dn/dM ~ M^-1.9 on 1e11..1e15 Msun.  Velocities: linear
+    theory from the same field, ``vrms`` rms.  About ``n_target`` tracers."""
+    rng = np.random.default_rng(seed)
+    g, vel = _grf(ng, box, index, sigma_ln, rng)
+    w = np.exp(bias * g)
+    h = box / ng
+    c1 = np.arange(ng) * h - box / 2 + h / 2
+    X, Y, Z = np.meshgrid(c1, c1, c1, indexing="ij")
+    R = np.sqrt(X ** 2 + Y ** 2 + Z ** 2)
+    cost = np.where(R > 0, Z / np.maximum(R, 1e-30), 1.0)
+    cmin = np.cos(np.radians(half_angle_deg))
+    inside = (R <= rmax) & (cost >= cmin)
+    sel = np.exp(-(R / rsel) ** 2) * inside
+    dens = (w * sel).ravel()
+    p = dens / dens.sum()
+    # expected count n_target before the angular mask
+    cell = rng.choice(ng ** 3, size=rng.poisson(n_target), p=p)
+    ix, iy, iz = np.unravel_index(cell, (ng, ng, ng))
+    off = rng.random((len(cell), 3))
+    pos = np.stack([ix + off[:, 0], iy + off[:, 1], iz + off[:, 2]], 1) * h - box / 2
+    r = np.linalg.norm(pos, axis=1)
+    ct = np.where(r > 0, pos[:, 2] / np.maximum(r, 1e-30), 1.0)
+    phi = np.arctan2(pos[:, 1], pos[:, 0])
+    keep = (r <= rmax) & (ct >= cmin)
+    npc, npp = 24, 48
+    masked = rng.random(npc * npp) < mask_frac
+    pc = np.clip(((ct - cmin) / (1 - cmin) * npc).astype(int), 0, npc - 1)
+    pp = np.clip(((phi + np.pi) / (2 * np.pi) * npp).astype(int), 0, npp - 1)
+    keep &= ~masked[pc * npp + pp]
+    pos, cell = pos[keep], cell[keep]
+    v = np.stack([vf.ravel()[cell] for vf in vel], 1)
+    v *= vrms / np.sqrt((v ** 2).sum(1).mean())
+    half = box / 2
+    pos = np.clip(pos, -half, half).astype(np.float32)
+    v = v.astype(np.float32)
+    m = power_law_masses(len(pos), rng=rng)
+    return dict(x=pos[:, 0].copy(), y=pos[:, 1].copy(), z=pos[:, 2].copy(),
+                vx=v[:, 0].copy(), vy=v[:, 1].copy(), vz=v[:, 2].copy(), m=m, box=box,
+                pixel_mask=masked.reshape(npc, npp))
+
+
+def add_clumps(parts: dict, centres, radius, count, seed=0):
+    """``parts`` with a clump of ``count`` particles uniform in a ball of
+    ``radius`` around each centre (velocities of the clump's centre particle,
+    masses equal to the set's first mass)."""
+    rng = np.random.default_rng(seed)
+    out = {k: v for k, v in parts.items()}
+    add = {k: [] for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    for c in np.asarray(centres, np.float64):
+        u = rng.normal(size=(count, 3))
+        u /= np.linalg.norm(u, axis=1, keepdims=True)
+        rr = radius * rng.random(count) ** (1 / 3)
+        q = c[None] + u * rr[:, None]
+        for a, k in enumerate(("x", "y", "z")):
+            add[k].append(q[:, a].astype(np.float32))
+        for k in ("vx", "vy", "vz"):
+            add[k].append(rng.normal(0, np.std(parts[k]), count).astype(np.float32))
+        add["m"].append(np.full(count, parts["m"][0], np.float32))
+    for k in add:
+        out[k] = np.concatenate([np.asarray(parts[k], np.float32)] + add[k])
+    return out
 
 
 def to_reader_units(parts: dict) -> dict:

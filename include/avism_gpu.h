@@ -64,7 +64,13 @@ typedef struct avism_params {
     int32_t level;              /* IR                                             */
     int32_t levmin;             /* LEVMIN                                         */
     int32_t learned;            /* 0: plain search, 1: learned proposal, 2: density estimate */
-    int32_t reserved[7];
+    int32_t kernel_mode;        /* KERNEL_MODE (src/particles.f90:9): 1 (or 0) M4 cubic
+                                   spline, 2 Gaussian exp(-q^2)                    */
+    int32_t no_velocities;      /* 1: FLAG_VEL_AVAILABLE = 0, the divergence is the
+                                   linear-theory -Omega_m^0.6 a H (rho/rho_mean - 1)
+                                   (src/avism.f90:1259-1306, 1647-1650); the
+                                   velocity arrays may then be NULL               */
+    int32_t reserved[5];
 } avism_params;
 
 /* ---- level geometry (MALLA + PBC extension, src/avism.f90:780-865) ------ */
@@ -198,7 +204,12 @@ int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n,
  * off): out[0] queries, [1] radius attempts, [2] candidates scanned, [3]
  * candidates kept inside the radius, [4] queries that fell back to the shell
  * search, [5] queries (K <= 32) ranked by the exact counting select after the
- * bitonic order failed its check.  No reference counterpart (instrumentation of
+ * bitonic order failed its check; and which of the reference's rare branches
+ * the call took: [6] cells whose K-th distance is <= DX and that took the
+ * ball_search fallback (src/particles.f90:868-878), [7] particles left with
+ * h = 0 for FILL_H_ZEROS (src/particles.f90:398-430), [8] particles whose
+ * DDENS NORM is 0 and whose mass goes to their own cell
+ * (src/particles.f90:549-557).  No reference counterpart (instrumentation of
  * this library).                                                              */
 int avism_gpu_knn_counters(avism_gpu_ctx *ctx, int enable, int64_t *out, int n);
 

@@ -54,14 +54,15 @@ int orc_ppart_dens(const orc_kdtree *t, int64_t n, const float *x, const float *
 int orc_vvel_interp_sph_vw(const orc_kdtree *t, const avism_grid *g, const float *radx,
                            int k, int64_t n, const float *m, const float *vx,
                            const float *vy, const float *vz, const float *part_dens,
-                           const int8_t *smask, float *hpart, float *u2, float *u3, float *u4);
+                           const int8_t *smask, int gauss, float *hpart, float *u2, float *u3,
+                           float *u4);
 int orc_h_distance(const orc_kdtree *t, const avism_grid *g, const float *radx, int k,
                    int64_t n, const int8_t *smask, float *hpart);
 int orc_fill_h_zeros(const orc_kdtree *t, int64_t n, const float *x, const float *y,
                      const float *z, int k, float *hpart);
 int orc_ddens_interp_sph(const avism_grid *g, const float *radx, int64_t n,
                          const float *x, const float *y, const float *z,
-                         const float *hpart, const float *m, float *u);
+                         const float *hpart, const float *m, int gauss, float *u);
 int orc_dens_interp_tsc(const avism_grid *g, const float *radx, int periodic, int64_t n,
                         const float *x, const float *y, const float *z, const float *m,
                         float *u);
@@ -104,4 +105,8 @@ int orc_run_level(const avism_params *p, int64_t n, const float *x, const float 
 #ifdef __cplusplus
 }
 #endif
+/* cells on the ball fallback, FILL_H_ZEROS orphans and DDENS NORM = 0
+ * particles of the last orc_particles_to_grid call */
+void orc_path_counts(int64_t *out);
+
 #endif

@@ -19,9 +19,12 @@ import numpy as np
 from scipy.spatial import cKDTree
 
 
-def _m4(d, h):
-    """KERNEL_FUNC, M4 branch: W(d; h) with q = d / (h / 2)."""
+def _m4(d, h, gauss=False):
+    """KERNEL_FUNC: W(d; h) with q = d / (h / 2): the M4 branch, or with
+    KERNEL_MODE = 2 the Gaussian exp(-q^2) (src/particles.f90:935-963)."""
     q = d / (h / 2.0)
+    if gauss:
+        return np.exp(-q * q)
     return np.where(q <= 1.0, 1.0 - 1.5 * q * q * (1.0 - 0.5 * q),
                     np.where(q <= 2.0, 0.25 * (2.0 - q) ** 3, 0.0))
 
@@ -32,6 +35,7 @@ def particles_to_grid_fp64(p, x, y, z, vx, vy, vz, m):
     from .oracle import grid_setup
     g, radx = grid_setup(p)
     nx, K, box, per = int(p.nx), int(p.kneighbours), float(p.lado0), bool(p.periodic)
+    gauss = int(getattr(p, "kernel_mode", 1)) == 2
     dx = float(g.dx)
     rad = np.asarray(radx, np.float64)
     off = int(g.rad_lo)
@@ -58,19 +62,19 @@ def particles_to_grid_fp64(p, x, y, z, vx, vy, vz, m):
     knn = dc[:, K - 1] > dx
     ds, js = dc[knn], ic[knn]
     np.maximum.at(hpart, js.ravel(), ds.ravel())
-    w = _m4(ds, ds[:, K - 1:K]) * (mm[js] / part_dens[js])
+    w = _m4(ds, ds[:, K - 1:K], gauss) * (mm[js] / part_dens[js])
     b = w.sum(1)
     u2[knn], u3[knn], u4[knn] = (w * vx[js]).sum(1) / b, (w * vy[js]).sum(1) / b, (w * vz[js]).sum(1) / b
     for cc in np.nonzero(~knn)[0]:                      # ball of radius DX
         lst = np.asarray(tree.query_ball_point(wrap(q[cc]), r=dx), np.int64)
         dd = np.sqrt(((_min_image(pts[lst] - q[cc], box) if per else pts[lst] - q[cc]) ** 2).sum(1))
         np.maximum.at(hpart, lst, dd)
-        w = _m4(dd, dd.max()) * (mm[lst] / part_dens[lst])
+        w = _m4(dd, dd.max(), gauss) * (mm[lst] / part_dens[lst])
         u2[cc], u3[cc], u4[cc] = (w * vx[lst]).sum() / w.sum(), (w * vy[lst]).sum() / w.sum(), \
             (w * vz[lst]).sum() / w.sum()
     # FILL_H_ZEROS
     hpart = np.where(hpart > 0.0, hpart, own_rk)
-    u_mass = _ddens(x, y, z, hpart, mm, rad, off, nx, dx)
+    u_mass = _ddens(x, y, z, hpart, mm, rad, off, nx, dx, gauss=gauss)
     return dict(u_mass=u_mass, u2=u2, u3=u3, u4=u4, hpart=hpart, part_dens=part_dens)
 
 
@@ -78,9 +82,10 @@ def _min_image(dv, box):
     return dv - box * np.round(dv / box)
 
 
-def _ddens(x, y, z, h, mm, rad, off, nx, dx, chunk_cells=2 ** 24):
+def _ddens(x, y, z, h, mm, rad, off, nx, dx, chunk_cells=2 ** 24, gauss=False):
     """DDENS_INTERP_SPH: per particle, the in-grid cells of its (2 INC + 1)^3 box
-    with d^2 <= 4 h^2, M4 weights normalised to the particle's mass."""
+    with d^2 <= 4 h^2, M4 (or Gaussian exp(-4 d^2 / h^2)) weights normalised to
+    the particle's mass."""
     r1 = rad[1 - off]
     cell = lambda v: np.floor((v - r1) / dx).astype(np.int64) + 1
     ix, jy, kz = cell(x), cell(y), cell(z)
@@ -101,7 +106,7 @@ def _ddens(x, y, z, h, mm, rad, off, nx, dx, chunk_cells=2 ** 24):
                  (z[pp, None] - radin[k2c - 1]) ** 2
             hh = h[pp, None]
             ok &= d2 <= 4.0 * hh * hh
-            w = np.where(ok, _m4(np.sqrt(d2), hh), 0.0)
+            w = np.where(ok, _m4(np.sqrt(d2), hh, gauss), 0.0)
             norm = w.sum(1)
             has = norm > 0.0
             contrib = np.where(has[:, None], w * (mm[pp, None] / np.where(has, norm, 1.0)[:, None]), 0.0)

@@ -75,6 +75,8 @@ def knn(x, y, z, qx, qy, qz, k, box_l=0.0):
 
 
 def particles_to_grid(p: Params, x, y, z, vx, vy, vz, m, smask=None):
+    # without velocities (no_velocities = 1) zeros stand in for them
+    vx, vy, vz = (np.zeros(len(x), np.float32) if v is None else v for v in (vx, vy, vz))
     x, y, z, vx, vy, vz, m = map(_f32, (x, y, z, vx, vy, vz, m))
     n = len(x)
     nc = p.nx ** 3
@@ -92,8 +94,17 @@ def particles_to_grid(p: Params, x, y, z, vx, vy, vz, m, smask=None):
     return dict(u_mass=out[0], u2=out[1], u3=out[2], u4=out[3], hpart=h, part_dens=pd)
 
 
+def path_counts():
+    """(ball-fallback cells, FILL_H_ZEROS orphans, DDENS NORM = 0 particles) of
+    the last particles_to_grid call."""
+    out = np.zeros(3, np.int64)
+    lib().orc_path_counts(out.ctypes.data_as(C.POINTER(C.c_int64)))
+    return dict(ball_cells=int(out[0]), orphans=int(out[1]), norm0=int(out[2]))
+
+
 def fields(p: Params, u_mass, u2, u3, u4):
     g, _ = grid_setup(p)
+    u2, u3, u4 = (np.zeros(p.nx ** 3, np.float32) if v is None else v for v in (u2, u3, u4))
     ne3 = g.ne ** 3
     u1 = np.zeros(ne3, np.float32)
     dv = np.zeros(ne3, np.float32)
@@ -171,7 +182,7 @@ def merge_post(p: Params, nvoid, cubes: dict, u1co_ext, meandens):
 def run_level(p: Params, parts: dict):
     """particles -> catalogue on the CPU (a5-a24)."""
     g, _ = grid_setup(p)
-    pg = particles_to_grid(p, *(parts[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")))
+    pg = particles_to_grid(p, *(parts.get(k) for k in ("x", "y", "z", "vx", "vy", "vz", "m")))
     u1, dv, md = fields(p, pg["u_mass"], pg["u2"], pg["u3"], pg["u4"])
     vf = voidfind(p, u1, dv)
     cat = merge_post(p, vf["nvoid"], vf["cubes"], u1, md)
@@ -203,7 +214,7 @@ def next_level(p: Params, nvoid, marca_ext, uvoid, req):
 
 def run_sublevel(p: Params, parts: dict, marcap_ext, reqp):
     """A level below the first: particles -> catalogue with the parent map."""
-    pg = particles_to_grid(p, *(parts[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")))
+    pg = particles_to_grid(p, *(parts.get(k) for k in ("x", "y", "z", "vx", "vy", "vz", "m")))
     u1, dv, md = fields(p, pg["u_mass"], pg["u2"], pg["u3"], pg["u4"])
     vf = voidfind(p, u1, dv, marcap_ext=marcap_ext, reqp=reqp)
     cat = merge_post(p, vf["nvoid"], vf["cubes"], u1, md)

@@ -7,6 +7,8 @@
  * src/num.f90:89-133 (REAL_MAKE_PERIODIC: every ghost cell takes the value of
  * the inner cell at the wrapped coordinates).  The FP64 mean is summed in
  * K,J,I order (the reference uses an OpenMP reduction of unspecified order).
+ * Without velocities the divergence is the linear-theory one of
+ * src/avism.f90:1647-1650.
  */
 #include <math.h>
 #include <stdlib.h>
@@ -93,7 +95,13 @@ int orc_fields(const avism_params *p, const float *u_mass, const float *u2, cons
     for (int64_t c = 0; c < nc; c++) u1[c] = u1[c] / mean;
     const float ul3 = (UL_F * UL_F) * UL_F;
     *meandens = mean * (UM_F / ul3);
-    orc_diver_uniform(nx, dx, u2, u3, u4, p->periodic, dv);
+    if (p->no_velocities) {
+        /* DIVERCO = - OMEGA0**(0.6)*RETE*HTE*(U1CO(:,:,:) - 1.0), src/avism.f90:1647-1650 */
+        const float coef = (powf(p->omega0, 0.6f) * g.rete) * g.hte;
+        for (int64_t c = 0; c < nc; c++) dv[c] = -(coef * (u1[c] - 1.0f));
+    } else {
+        orc_diver_uniform(nx, dx, u2, u3, u4, p->periodic, dv);
+    }
     /* ext grids with the periodic ghost fill (src/num.f90:89-133) */
     for (int kz = 0; kz < ne; kz++)
         for (int jy = 0; jy < ne; jy++)

@@ -24,15 +24,26 @@
 
 #define RAD(i) radx[(i) - g->rad_lo]
 
+/* branch counters of the last orc_particles_to_grid: cells on the ball_search
+ * fallback, FILL_H_ZEROS orphans, DDENS particles with NORM = 0 */
+static int64_t g_path_counts[3];
+
+void orc_path_counts(int64_t *out)
+{
+    for (int i = 0; i < 3; i++) out[i] = g_path_counts[i];
+}
+
 static inline int64_t cell_id(int nx, int i, int j, int k)   /* 1-based i,j,k */
 {
     return (int64_t)(i - 1) + (int64_t)nx * ((int64_t)(j - 1) + (int64_t)nx * (int64_t)(k - 1));
 }
 
-/* KERNEL_FUNC, M4 branch (src/particles.f90:935-963): returns W(dist; h) */
-static inline float kernel_m4(float h, float dist)
+/* KERNEL_FUNC (src/particles.f90:935-963): returns W(dist; h) for KERNEL_MODE
+ * 1 (M4 cubic spline) or 2 (Gaussian EXP(-Q**2)) */
+static inline float kernel_w(int gauss, float h, float dist)
 {
     const float q = dist / (h / 2.0f);
+    if (gauss) return expf(-(q * q));
     if (q <= 1.0f) return 1.0f - (1.5f * (q * q)) * (1.0f - 0.5f * q);
     if (q <= 2.0f) { const float t = 2.0f - q; return 0.25f * ((t * t) * t); }
     return 0.0f;
@@ -78,13 +89,15 @@ static int64_t cell_neigh(const orc_kdtree *t, float tx, float ty, float tz, int
     }
     orc_kd_knn(t, tx, ty, tz, k, *idx, *d2);
     if (sqrtf((*d2)[k - 1]) > dx) return k;
+    __atomic_fetch_add(&g_path_counts[0], 1, __ATOMIC_RELAXED);
     return orc_kd_ball(t, tx, ty, tz, dx, idx, d2, cap);
 }
 
 int orc_vvel_interp_sph_vw(const orc_kdtree *t, const avism_grid *g, const float *radx,
                            int k, int64_t n, const float *m, const float *vx,
                            const float *vy, const float *vz, const float *part_dens,
-                           const int8_t *smask, float *hpart, float *u2, float *u3, float *u4)
+                           const int8_t *smask, int gauss, float *hpart, float *u2, float *u3,
+                           float *u4)
 {
     (void)n;
     const int nx = g->nx;
@@ -106,7 +119,7 @@ int orc_vvel_interp_sph_vw(const orc_kdtree *t, const avism_grid *g, const float
                         atomic_max_pos(&hpart[idx[i]], w[i]);
                     }
                     const float hk = cnt > 0 ? w[cnt - 1] : 0.0f;
-                    for (int64_t i = 0; i < cnt; i++) w[i] = kernel_m4(hk, w[i]);
+                    for (int64_t i = 0; i < cnt; i++) w[i] = kernel_w(gauss, hk, w[i]);
                     for (int64_t i = 0; i < cnt; i++) w[i] = w[i] * (m[idx[i]] / part_dens[idx[i]]);
                     double b = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
                     for (int64_t i = 0; i < cnt; i++) {
@@ -154,6 +167,7 @@ int orc_fill_h_zeros(const orc_kdtree *t, int64_t n, const float *x, const float
     #pragma omp parallel for schedule(dynamic, 256)
     for (int64_t i = 0; i < n; i++) {
         if (hpart[i] > 0.0f) continue;
+        __atomic_fetch_add(&g_path_counts[1], 1, __ATOMIC_RELAXED);
         int64_t idx[1024]; float d2[1024];
         orc_kd_knn(t, x[i], y[i], z[i], k, idx, d2);
         hpart[i] = sqrtf(d2[k - 1]);
@@ -179,7 +193,7 @@ static void slab_of(int nx, int *k0, int *k1)
 
 int orc_ddens_interp_sph(const avism_grid *g, const float *radx, int64_t n,
                          const float *x, const float *y, const float *z,
-                         const float *hpart, const float *m, float *u)
+                         const float *hpart, const float *m, int gauss, float *u)
 {
     const int nx = g->nx;
     const float dx = g->dx;
@@ -199,6 +213,7 @@ int orc_ddens_interp_sph(const avism_grid *g, const float *radx, int64_t n,
             const int inc = (int)((2.0f * h) / dx + 0.5f);
             if (kz + inc < ks0 || kz - inc > ks1) continue;
             const float inv_h = 2.0f / h;
+            const float inv_h_sq = inv_h * inv_h;
             const float h2max = (4.0f * h) * h;
             float norm = 0.0f;
             for (int pass = 0; pass < 2; pass++) {
@@ -217,17 +232,22 @@ int orc_ddens_interp_sph(const avism_grid *g, const float *radx, int64_t n,
                             const float dx2 = tx * tx;
                             const float d2 = (dx2 + dy2) + dz2;
                             if (d2 > h2max) continue;
-                            const float q = sqrtf(d2) * inv_h;
                             float w;
-                            if (q <= 1.0f) w = 1.0f - (1.5f * (q * q)) * (1.0f - 0.5f * q);
-                            else if (q <= 2.0f) { const float s = 2.0f - q; w = 0.25f * ((s * s) * s); }
-                            else w = 0.0f;
+                            if (gauss) {
+                                w = expf(-(d2 * inv_h_sq));           /* KERNEL_MODE = 2 */
+                            } else {
+                                const float q = sqrtf(d2) * inv_h;
+                                if (q <= 1.0f) w = 1.0f - (1.5f * (q * q)) * (1.0f - 0.5f * q);
+                                else if (q <= 2.0f) { const float s = 2.0f - q; w = 0.25f * ((s * s) * s); }
+                                else w = 0.0f;
+                            }
                             if (pass == 0) norm = norm + w;
                             else u8[cell_id(nx, i2, j2, k2)] += (double)((w * m[p]) / norm);
                         }
                     }
                 }
                 if (pass == 0 && norm == 0.0f) {
+                    if (kz >= ks0 && kz <= ks1) __atomic_fetch_add(&g_path_counts[2], 1, __ATOMIC_RELAXED);
                     if (ix >= 1 && ix <= nx && jy >= 1 && jy <= nx && kz >= ks0 && kz <= ks1 && kz <= nx)
                         u8[cell_id(nx, ix, jy, kz)] += (double)m[p];
                     break;
@@ -371,30 +391,33 @@ int orc_particles_to_grid(const avism_params *p, int64_t n, const float *x, cons
             free(radx);
             return AVISM_ERR_OUT_OF_BOX;
         }
+    for (int i = 0; i < 3; i++) g_path_counts[i] = 0;
     float *h = hpart ? hpart : (float *)malloc((size_t)n * sizeof(float));
     float *pd = part_dens ? part_dens : (float *)malloc((size_t)n * sizeof(float));
     for (int64_t i = 0; i < n; i++) { h[i] = 0.0f; pd[i] = 0.0f; }
     for (int64_t c = 0; c < nc; c++) { u_mass[c] = 0.0f; u2[c] = 0.0f; u3[c] = 0.0f; u4[c] = 0.0f; }
     orc_kdtree *t = NULL;
-    if (p->flag_vel_interp == 1 || p->flag_dens_interp == 1)
+    if ((p->flag_vel_interp == 1 && !p->no_velocities) || p->flag_dens_interp == 1)
         t = orc_kd_build(n, x, y, z, p->periodic ? p->lado0 : 0.0f);
-    /* velocities, src/avism.f90:1159-1194 */
-    if (p->flag_vel_interp == 0) {
+    const int gauss = p->kernel_mode == 2;
+    /* velocities, src/avism.f90:1159-1194; none without velocities (1259-1306) */
+    const int vel_sph = p->flag_vel_interp == 1 && !p->no_velocities;
+    if (!p->no_velocities && p->flag_vel_interp == 0) {
         orc_vel_interp_tsc(&g, radx, p->periodic, n, x, y, z, vx, vy, vz, u2, u3, u4);
-    } else {
+    } else if (vel_sph) {
         orc_ppart_dens(t, n, x, y, z, m, k, pd);
-        orc_vvel_interp_sph_vw(t, &g, radx, k, n, m, vx, vy, vz, pd, smask, h, u2, u3, u4);
+        orc_vvel_interp_sph_vw(t, &g, radx, k, n, m, vx, vy, vz, pd, smask, gauss, h, u2, u3, u4);
         orc_fill_h_zeros(t, n, x, y, z, k, h);
     }
-    /* density, src/avism.f90:1214-1245 */
+    /* density, src/avism.f90:1214-1245 (1270-1296 without velocities) */
     if (p->flag_dens_interp == 0) {
         orc_dens_interp_tsc(&g, radx, p->periodic, n, x, y, z, m, u_mass);
     } else {
-        if (p->flag_vel_interp == 0) {
+        if (!vel_sph) {
             orc_h_distance(t, &g, radx, k, n, smask, h);
             orc_fill_h_zeros(t, n, x, y, z, k, h);
         }
-        orc_ddens_interp_sph(&g, radx, n, x, y, z, h, m, u_mass);
+        orc_ddens_interp_sph(&g, radx, n, x, y, z, h, m, gauss, u_mass);
     }
     orc_kd_free(t);
     if (!hpart) free(h);

@@ -1,11 +1,13 @@
-"""Writes the golden fixtures of tests/test_golden.py from the CPU oracle.
+"""Writes the golden fixtures of tests/test_golden.py and
+tests/test_gpu_config2.py from the CPU oracle.
 
 The reference (Fortran, no compiler in this image) cannot produce outputs
 here, so these fixtures freeze the oracle's results on small seeded inputs:
 a change in the oracle or in the CUDA path that alters any of them shows up
 as a test failure.  Run from the repository root:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # the small fixtures
+    python tests/golden/make_golden.py config2    # the 256^3 digests (minutes)
 """
 import os
 import sys
@@ -56,7 +58,55 @@ def indexx_case():
     return {"arr": a, "indx": np.asarray(O.indexx(a))}
 
 
+def digest(a) -> str:
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def config2_input():
+    """The 256^3 scale-up workload: 2^24 particles Poisson-sampled from a
+    lognormal field (GRF on 256^3, P(k) ~ k^-1.5, sigma_ln = 1), periodic
+    L = 250 cMpc, linear-theory velocities at 350 km/s rms, seed 1002."""
+    return synth.to_reader_units(synth.lognormal(n=2 ** 24, ng=256, box=250.0, index=-1.5, sigma_ln=1.0,
+                                                 vrms=350.0, seed=1002))
+
+
+CONFIG2_CAT = ("indice", "uvoid", "ncellv", "volnew", "req", "xc", "yc", "zc", "gxc", "gyc", "gzc", "eps", "ip",
+               "umean", "mtot")
+
+
+def config2_case():
+    """Digests of the oracle's fields, cubes and catalogue at 256^3 for SPH/SPH
+    and TSC/TSC (k = 32, README thresholds), and the catalogue columns."""
+    parts = config2_input()
+    keys = ("x", "y", "z", "vx", "vy", "vz", "m")
+    out = {"input": np.array(digest(np.concatenate([parts[k] for k in keys])))}
+    for vel, dens in ((1, 1), (0, 0)):
+        tag = f"v{vel}d{dens}"
+        p = Params(nx=256, periodic=1, lado0=250.0, kneighbours=32, flag_vel_interp=vel, flag_dens_interp=dens,
+                   nvoid_max=4_000_000)
+        r = O.run_level(p, parts)
+        for k in ("u_mass", "u2", "u3", "u4", "hpart", "part_dens"):
+            out[f"{tag}_{k}"] = np.array(digest(r["grid"][k]))
+        out[f"{tag}_u1co"] = np.array(digest(r["u1co"]))
+        out[f"{tag}_diverco"] = np.array(digest(r["diverco"]))
+        out[f"{tag}_meandens"] = np.float32(r["meandens"])
+        out[f"{tag}_nvoid"] = np.int32(r["vf"]["nvoid"])
+        out[f"{tag}_cubes"] = np.array(digest(np.concatenate([np.asarray(r["vf"]["cubes"][k]).view(np.int32)
+                                                              for k in sorted(r["vf"]["cubes"])])))
+        out[f"{tag}_marca"] = np.array(digest(r["cat"]["marca"]))
+        for k in CONFIG2_CAT:
+            out[f"{tag}_cat_{k}"] = np.asarray(r["cat"][k])
+        out[f"{tag}_nvoidt"] = np.int32(r["cat"]["nvoidt"])
+        print(tag, r["vf"]["nvoid"], r["cat"]["nvoidt"], flush=True)
+    return out
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "config2":
+        np.savez_compressed(os.path.join(HERE, "config2_256.npz"), **config2_case())
+        print("written")
+        sys.exit(0)
     np.savez_compressed(os.path.join(HERE, "level_mock32.npz"), **level_case())
     np.savez_compressed(os.path.join(HERE, "knn_3000.npz"), **knn_case())
     np.savez_compressed(os.path.join(HERE, "indexx_ties.npz"), **indexx_case())
