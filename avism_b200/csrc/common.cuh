@@ -38,7 +38,7 @@ enum BufId : int {
     B_PX, B_PY, B_PZ, B_PVX, B_PVY, B_PVZ, B_PM,   // particle inputs (device copies)
     B_HPART, B_PDENS, B_NORM,
     B_UMASS, B_U2, B_U3, B_U4,                     // inner grids
-    B_FIX0, B_FIX1, B_FIX2, B_FIX3,                // int64 fixed-point accumulators
+    B_FIX0, B_FIX1, B_FIX2, B_FIX3,                // exact-sum limb counters (u64)
     B_U1CO, B_DIVER,                               // inner normalised density / divergence
     B_U1EXT, B_DVEXT,                              // ext grids (ABI outputs)
     B_FLAGS, B_SMASK, B_MARCAP,                    // ext byte flags, ext mask, ext parent ids
@@ -61,6 +61,8 @@ enum BufId : int {
     B_PX4, B_PV4,                                  // packed (x, y, z, m), (vx, vy, vz, 0) in input order
     B_FSTART,                                      // int32 offsets of quarter-bin x cells
     B_PER_CELL, B_PER_LAB, B_PER_PAIRS,            // VOID_PERIODIC: centre cells, their labels, label-map updates
+    B_LL_CELL, B_LL_CELL2, B_LL_KEY, B_LL_KEY2,    // cells of every void in K, J, I order (sorted by label)
+    B_LL_CNT, B_LL_OFF, B_LL_SUM,                  // their counts, offsets and per-void REAL*4 sums
     B_NUM
 };
 

@@ -86,53 +86,159 @@ __global__ void k_ncellv(int64_t ne3, const int32_t *marca, const int32_t *uvoid
     if (m > 0 && lane == __ffs(grp) - 1) atomicAdd(&ncell[m - 1], __popc(grp));
 }
 
-// ---- VOID_SHAPE inertia: per cell terms in REAL*4 (src/shape.f90:176-196) ----
-__global__ void k_inertia(PostGrid G, const int32_t *marca, const float *rad, int rad_lo, const float *gxc,
-                          const float *gyc, const float *gzc, double *inert /* 6 per label */) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t ne3 = (int64_t)G.ne * G.ne * G.ne;
-    int32_t m = 0;
-    float t[6] = {0, 0, 0, 0, 0, 0};
-    if (e < ne3) {
-        m = marca[e];
-        if (m > 0) {
-            const int i = (int)(e % G.ne) + G.low1, j = (int)((e / G.ne) % G.ne) + G.low1;
-            const int k = (int)(e / ((int64_t)G.ne * G.ne)) + G.low1;
-            const float r0 = __fsub_rn(rad[i - rad_lo], gxc[m - 1]);
-            const float r1 = __fsub_rn(rad[j - rad_lo], gyc[m - 1]);
-            const float r2 = __fsub_rn(rad[k - rad_lo], gzc[m - 1]);
+// ---- per-void REAL*4 sums in the reference's serial K, J, I order -------------
+// VOID_SHAPE's inertia (src/shape.f90:158-182) and the global properties UMEAN and
+// MTOT (src/avism.f90:1917-1936) are REAL*4 accumulations over a void's cells in
+// the order of the reference's serial triple loop, so their bits depend on that
+// order.  The cells of every void are listed in increasing linear index (the
+// K, J, I order: a stable sort by label of the void cells taken in grid order),
+// then one warp per void walks its list 32 cells at a time: all lanes compute
+// the cells' terms into shared memory, then one lane per accumulator adds them
+// in order.  The chains stay serial, as the reference's; voids run in parallel.
+
+// void cells of the ext grid (VOID_SHAPE: every cell LOW1..LOW2 with MARCA > 0)
+struct ExtVoidCell {
+    const int32_t *marca;
+    __host__ __device__ bool operator()(int32_t e) const { return marca[e] > 0; }
+};
+// inner cells of main voids (the global properties' loop, 1..NX)
+struct InnerMainCell {
+    PostGrid G;
+    const int32_t *marca, *uvoid;
+    __device__ bool operator()(int32_t c) const {
+        const int nx = G.nx;
+        const int i = c % nx + 1, j = (c / nx) % nx + 1, k = c / (nx * nx) + 1;
+        const int32_t m = marca[pidx(G, i, j, k)];
+        return m > 0 && uvoid[m - 1] == -1;
+    }
+};
+
+__global__ void k_cell_labels(int32_t n, const int32_t *__restrict__ cell, const int32_t *__restrict__ marca,
+                              PostGrid G, int inner, int32_t *__restrict__ key, int32_t *__restrict__ cnt) {
+    const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int32_t c = cell[t];
+    int32_t m;
+    if (inner) {
+        const int nx = G.nx;
+        m = marca[pidx(G, c % nx + 1, (c / nx) % nx + 1, c / (nx * nx) + 1)];
+    } else {
+        m = marca[c];
+    }
+    key[t] = m;
+    atomicAdd(&cnt[m - 1], 1);
+}
+
+constexpr int SEQ_WARPS = 4;
+
+// VOID_SHAPE: INERTIA(I1,I2) = INERTIA(I1,I2) + DELTA*RR*RR - RK(I1)*RK(I2), evaluated
+// left to right, per cell in order; off-diagonal DELTA*RR*RR is +0, and adding +0
+// leaves the (never -0) sum unchanged, so those chains subtract only.  Output:
+// 6 sums per label (I11, I22, I33, I12, I13, I23).
+__global__ void __launch_bounds__(SEQ_WARPS * 32)
+k_inertia_seq(int32_t nv, const int64_t *__restrict__ off, const int32_t *__restrict__ cell, PostGrid G,
+              const float *__restrict__ rad, int rad_lo, const float *__restrict__ gxc, const float *__restrict__ gyc,
+              const float *__restrict__ gzc, float *__restrict__ inert) {
+    __shared__ float term[SEQ_WARPS][7][33];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int32_t v = blockIdx.x * SEQ_WARPS + w;
+    if (v >= nv) return;
+    const int64_t a = off[v], b = off[v + 1];
+    const float cx = gxc[v], cy = gyc[v], cz = gzc[v];
+    float acc = 0.0f;                                   // lane q < 6 owns accumulator q
+    float (*T)[33] = term[w];
+    for (int64_t base = a; base < b; base += 32) {
+        const int n = (int)(b - base < 32 ? b - base : 32);
+        if (lane < n) {
+            const int32_t e = cell[base + lane];
+            const int i = e % G.ne + G.low1, j = (e / G.ne) % G.ne + G.low1, k = e / (G.ne * G.ne) + G.low1;
+            const float r0 = __fsub_rn(rad[i - rad_lo], cx);
+            const float r1 = __fsub_rn(rad[j - rad_lo], cy);
+            const float r2 = __fsub_rn(rad[k - rad_lo], cz);
             const float rr = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(r0, r0), __fmul_rn(r1, r1)), __fmul_rn(r2, r2)));
-            const float rr2 = __fmul_rn(rr, rr);
-            t[0] = __fsub_rn(rr2, __fmul_rn(r0, r0));
-            t[1] = __fsub_rn(rr2, __fmul_rn(r1, r1));
-            t[2] = __fsub_rn(rr2, __fmul_rn(r2, r2));
-            t[3] = -__fmul_rn(r0, r1);
-            t[4] = -__fmul_rn(r0, r2);
-            t[5] = -__fmul_rn(r1, r2);
+            T[0][lane] = __fmul_rn(__fmul_rn(1.0f, rr), rr);
+            T[1][lane] = __fmul_rn(r0, r0);
+            T[2][lane] = __fmul_rn(r1, r1);
+            T[3][lane] = __fmul_rn(r2, r2);
+            T[4][lane] = __fmul_rn(r0, r1);
+            T[5][lane] = __fmul_rn(r0, r2);
+            T[6][lane] = __fmul_rn(r1, r2);
         }
-    }
-    if (__all_sync(0xffffffffu, m == 0)) return;            // no void cell in this warp
-    const unsigned grp = __match_any_sync(0xffffffffu, m);
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(grp) - 1;
-    if (__all_sync(0xffffffffu, grp == 0xffffffffu)) {
-        // one label in the whole warp: a shuffle tree in FP64
-        for (int q = 0; q < 6; q++) {
-            double s = (double)t[q];
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) atomicAdd(&inert[(size_t)(m - 1) * 6 + q], s);
+        __syncwarp();
+        if (lane < 3) {
+            for (int t = 0; t < n; t++) acc = __fsub_rn(__fadd_rn(acc, T[0][t]), T[1 + lane][t]);
+        } else if (lane < 6) {
+            for (int t = 0; t < n; t++) acc = __fsub_rn(acc, T[1 + lane][t]);
         }
-        return;
+        __syncwarp();
     }
-    for (int q = 0; q < 6; q++) {
-        // sum in lane order inside the group
-        double s = 0.0;
-        for (int src = 0; src < 32; src++) {
-            const float v = __shfl_sync(0xffffffffu, t[q], src);
-            if ((grp >> src) & 1) s += (double)v;
+    if (lane < 6) inert[(size_t)v * 6 + lane] = acc;
+}
+
+// global properties: UMEAN(IND) = UMEAN(IND) + U1CO and MTOT(IND) = MTOT(IND) +
+// U1CO*MEANDENS*DXX*DYY*DZZ*RETE**3 per inner cell in order; 2 sums per label
+__global__ void __launch_bounds__(SEQ_WARPS * 32)
+k_props_seq(int32_t nv, const int64_t *__restrict__ off, const int32_t *__restrict__ cell,
+            const float *__restrict__ u1co, float meandens, float dx, float rete3, float *__restrict__ sums) {
+    __shared__ float term[SEQ_WARPS][2][33];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int32_t v = blockIdx.x * SEQ_WARPS + w;
+    if (v >= nv) return;
+    const int64_t a = off[v], b = off[v + 1];
+    float acc = 0.0f;
+    float (*T)[33] = term[w];
+    for (int64_t base = a; base < b; base += 32) {
+        const int n = (int)(b - base < 32 ? b - base : 32);
+        if (lane < n) {
+            const float u = u1co[cell[base + lane]];
+            T[0][lane] = u;
+            T[1][lane] = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(u, meandens), dx), dx), dx), rete3);
         }
-        if (m > 0 && lane == leader) atomicAdd(&inert[(size_t)(m - 1) * 6 + q], s);
+        __syncwarp();
+        if (lane < 2)
+            for (int t = 0; t < n; t++) acc = __fadd_rn(acc, T[lane][t]);
+        __syncwarp();
     }
+    if (lane < 2) sums[(size_t)v * 2 + lane] = acc;
+}
+
+// the cells passing `pick` among 0..ncells-1, grouped by their label (1..nv)
+// in increasing cell index; off[v]..off[v+1] are label v+1's
+template <class Pick>
+static void void_cell_lists(Ctx &c, int32_t ncells, Pick pick, const int32_t *marca, PostGrid G, int inner,
+                            int32_t nv, const int32_t **cell_out, const int64_t **off_out, int32_t *cnt_host) {
+    const int32_t nvs = std::max(nv, 1);
+    int32_t *cell = c.get_t<int32_t>(B_LL_CELL, (size_t)std::max(ncells, 1));
+    int32_t *nsel_d = c.get_t<int32_t>(B_SCAL, 4);
+    cub::CountingInputIterator<int32_t> it(0);
+    size_t tmp = 0;
+    AV_CUDA(cub::DeviceSelect::If(nullptr, tmp, it, cell, nsel_d, ncells, pick, c.stream));
+    AV_CUDA(cub::DeviceSelect::If(c.get(B_CUB_TMP, tmp), tmp, it, cell, nsel_d, ncells, pick, c.stream));
+    int32_t nsel = 0;
+    AV_CUDA(cudaMemcpyAsync(&nsel, nsel_d, sizeof nsel, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    const int32_t m1 = std::max(nsel, 1);
+    int32_t *key = c.get_t<int32_t>(B_LL_KEY, (size_t)m1);
+    int32_t *key2 = c.get_t<int32_t>(B_LL_KEY2, (size_t)m1);
+    int32_t *cell2 = c.get_t<int32_t>(B_LL_CELL2, (size_t)m1);
+    int32_t *cnt = c.get_t<int32_t>(B_LL_CNT, (size_t)nvs + 1);
+    int64_t *off = c.get_t<int64_t>(B_LL_OFF, (size_t)nvs + 1);
+    AV_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * ((size_t)nvs + 1), c.stream));
+    if (nsel > 0)
+        ++c.launches, k_cell_labels<<<grid_for(nsel, 256), 256, 0, c.stream>>>(nsel, cell, marca, G, inner, key, cnt);
+    AV_CUDA(cudaGetLastError());
+    cub::DoubleBuffer<int32_t> dk(key, key2), dv(cell, cell2);
+    int bits = 1;
+    while ((1LL << bits) <= (int64_t)nv) bits++;
+    tmp = 0;
+    AV_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, nsel, 0, bits, c.stream));
+    AV_CUDA(cub::DeviceRadixSort::SortPairs(c.get(B_CUB_TMP, tmp), tmp, dk, dv, nsel, 0, bits, c.stream));
+    tmp = 0;
+    AV_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt, off, nv + 1, c.stream));
+    AV_CUDA(cub::DeviceScan::ExclusiveSum(c.get(B_CUB_TMP, tmp), tmp, cnt, off, nv + 1, c.stream));
+    if (cnt_host) AV_CUDA(cudaMemcpyAsync(cnt_host, cnt, sizeof(int32_t) * (size_t)nv, cudaMemcpyDeviceToHost, c.stream));
+    *cell_out = dv.Current();
+    *off_out = off;
 }
 
 // ---- VOID_SHAPE axes: one thread per main void (src/shape.f90:198-232) -----
@@ -208,19 +314,19 @@ __device__ __forceinline__ void sort_desc3(float d[3]) {
 
 
 __global__ void k_void_axes(int32_t nv, const int32_t *__restrict__ uvoid, const int32_t *__restrict__ ncellv,
-                            const double *__restrict__ inert, float dx, double pi, float *__restrict__ eps,
+                            const float *__restrict__ inert, float dx, double pi, float *__restrict__ eps,
                             float *__restrict__ ipv) {
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nv) return;
     float e = 0.0f, ip = 0.0f;
     if (uvoid[v] == -1) {
-        const double *s = &inert[(size_t)v * 6];
+        const float *s = &inert[(size_t)v * 6];
         const float n = (float)ncellv[v];
         float a[3][3];
-        a[0][0] = (float)s[0] / n; a[1][1] = (float)s[1] / n; a[2][2] = (float)s[2] / n;
-        a[0][1] = a[1][0] = (float)s[3] / n;
-        a[0][2] = a[2][0] = (float)s[4] / n;
-        a[1][2] = a[2][1] = (float)s[5] / n;
+        a[0][0] = s[0] / n; a[1][1] = s[1] / n; a[2][2] = s[2] / n;
+        a[0][1] = a[1][0] = s[3] / n;
+        a[0][2] = a[2][0] = s[4] / n;
+        a[1][2] = a[2][1] = s[5] / n;
         float ev[3] = {0.0f, 0.0f, 0.0f}, ax[3];
         jacobi3(a, ev);
         ax[0] = sqrtf(2.5f * fabsf((ev[1] + ev[2]) - ev[0]));
@@ -450,51 +556,6 @@ __global__ void k_scatter_pairs(int32_t n, const int32_t *__restrict__ pairs, in
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[pairs[2 * i]] = pairs[2 * i + 1];
 }
-
-// ---- global properties on the inner cells (src/avism.f90:1917-1933) ------------
-__global__ void k_final_props(PostGrid G, const int32_t *marca, const int32_t *uvoid, const float *u1co,
-                              float meandens, float dx, float rete3, int32_t *ncell, double *sums /* 2 per label */) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int nx = G.nx;
-    int32_t m = 0;
-    float u = 0.0f, mt = 0.0f;
-    if (c < (int64_t)nx * nx * nx) {
-        const int i = (int)(c % nx) + 1, j = (int)((c / nx) % nx) + 1, k = (int)(c / ((int64_t)nx * nx)) + 1;
-        m = marca[pidx(G, i, j, k)];
-        if (m > 0 && uvoid[m - 1] != -1) m = 0;
-        if (m > 0) {
-            u = u1co[c];
-            mt = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(u, meandens), dx), dx), dx), rete3);
-        }
-    }
-    if (__all_sync(0xffffffffu, m == 0)) return;            // no void cell in this warp
-    const unsigned grp = __match_any_sync(0xffffffffu, m);
-    const int lane = threadIdx.x & 31;
-    if (__all_sync(0xffffffffu, grp == 0xffffffffu)) {
-        double su = (double)u, sm = (double)mt;
-        for (int o = 16; o > 0; o >>= 1) {
-            su += __shfl_xor_sync(0xffffffffu, su, o);
-            sm += __shfl_xor_sync(0xffffffffu, sm, o);
-        }
-        if (lane == 0) {
-            atomicAdd(&ncell[m - 1], 32);
-            atomicAdd(&sums[(size_t)(m - 1) * 2], su);
-            atomicAdd(&sums[(size_t)(m - 1) * 2 + 1], sm);
-        }
-        return;
-    }
-    double su = 0.0, sm = 0.0;
-    for (int src = 0; src < 32; src++) {
-        const float a = __shfl_sync(0xffffffffu, u, src), b = __shfl_sync(0xffffffffu, mt, src);
-        if ((grp >> src) & 1) { su += (double)a; sm += (double)b; }
-    }
-    if (m > 0 && lane == __ffs(grp) - 1) {
-        atomicAdd(&ncell[m - 1], __popc(grp));
-        atomicAdd(&sums[(size_t)(m - 1) * 2], su);
-        atomicAdd(&sums[(size_t)(m - 1) * 2 + 1], sm);
-    }
-}
-
 
 // ---- neighbour lists of MERGE_VOID: cubes of the same father whose 1-cell
 //      halo boxes overlap; d2 is distance() of src/kdtree.f90:1441-1465 on the
@@ -743,14 +804,21 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         AV_CUDA(cudaMemcpyAsync(gc_d, mo.gxc.data(), sizeof(float) * nv, cudaMemcpyHostToDevice, c.stream));
         AV_CUDA(cudaMemcpyAsync(gc_d + nvs, mo.gyc.data(), sizeof(float) * nv, cudaMemcpyHostToDevice, c.stream));
         AV_CUDA(cudaMemcpyAsync(gc_d + 2 * nvs, mo.gzc.data(), sizeof(float) * nv, cudaMemcpyHostToDevice, c.stream));
-        double *in_d = c.get_t<double>(B_SCAN_A, (size_t)nvs * 6);
-        AV_CUDA(cudaMemsetAsync(in_d, 0, sizeof(double) * 6 * (size_t)nvs, c.stream));
+        float *in_d = c.get_t<float>(B_LL_SUM, (size_t)nvs * 6);
         c.mark("shape_setup");
-        ++c.launches, k_inertia<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, marca, rad_d, g.rad_lo, gc_d, gc_d + nvs, gc_d + 2 * nvs, in_d);
+        const int32_t *vcell;
+        const int64_t *voff;
+        AV_CHECK(ne3 < (int64_t)INT32_MAX, AVISM_ERR_UNSUPPORTED, "VOID_SHAPE: ext grid above 2^31 cells");
+        void_cell_lists(c, (int32_t)ne3, ExtVoidCell{marca}, marca, PG, 0, nv, &vcell, &voff, nullptr);
+        c.mark("shape_lists");
+        if (nv > 0)
+            ++c.launches, k_inertia_seq<<<grid_for(nv, SEQ_WARPS), SEQ_WARPS * 32, 0, c.stream>>>(
+                nv, voff, vcell, PG, rad_d, g.rad_lo, gc_d, gc_d + nvs, gc_d + 2 * nvs, in_d);
+        AV_CUDA(cudaGetLastError());
         c.mark("shape_inertia");
         int32_t *nc_d = dev_upload<int32_t>(c, B_RED2, ncellv.data(), (size_t)nv);
         push_uvoid();
-        float *ax_d = gc_d;                          // the centres are consumed by k_inertia
+        float *ax_d = gc_d;                          // the centres are consumed by k_inertia_seq
         ++c.launches, k_void_axes<<<grid_for(nv, 128), 128, 0, c.stream>>>(nv, uv_d, nc_d, in_d, dx, pi, ax_d, ax_d + nvs);
         dev_download(c, eps.data(), ax_d, nv);
         dev_download(c, ipv.data(), ax_d + nvs, nv);
@@ -989,21 +1057,25 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
     std::vector<float> umean(nvs, 0.0f), mtot(nvs, 0.0f);
     double volt = 0.0;
     {
-        int32_t *nc_d = c.get_t<int32_t>(B_RED2, nvs);
-        double *sum_d = c.get_t<double>(B_SCAN_A, (size_t)nvs * 2);
-        AV_CUDA(cudaMemsetAsync(nc_d, 0, sizeof(int32_t) * (size_t)nvs, c.stream));
-        AV_CUDA(cudaMemsetAsync(sum_d, 0, sizeof(double) * 2 * (size_t)nvs, c.stream));
         push_uvoid();
         const float rete3 = (g.rete * g.rete) * g.rete;
-        ++c.launches, k_final_props<<<grid_for((int64_t)nx * nx * nx, 256), 256, 0, c.stream>>>(PG, marca, uv_d, u1co_inner,
-                                                                                  meandens, dx, rete3, nc_d, sum_d);
-        std::vector<double> sums((size_t)nvs * 2);
-        dev_download(c, ncellv.data(), nc_d, nv);
+        const int32_t *pcell;
+        const int64_t *poff;
+        const int64_t nc3 = (int64_t)nx * nx * nx;
+        AV_CHECK(nc3 < (int64_t)INT32_MAX, AVISM_ERR_UNSUPPORTED, "global properties: grid above 2^31 cells");
+        void_cell_lists(c, (int32_t)nc3, InnerMainCell{PG, marca, uv_d}, marca, PG, 1, nv, &pcell, &poff,
+                        ncellv.data());
+        float *sum_d = c.get_t<float>(B_LL_SUM, (size_t)nvs * 2);
+        if (nv > 0)
+            ++c.launches, k_props_seq<<<grid_for(nv, SEQ_WARPS), SEQ_WARPS * 32, 0, c.stream>>>(
+                nv, poff, pcell, u1co_inner, meandens, dx, rete3, sum_d);
+        AV_CUDA(cudaGetLastError());
+        std::vector<float> sums((size_t)nvs * 2);
         dev_download(c, sums.data(), sum_d, (size_t)nv * 2);
         int64_t ncount = 0;
         for (int32_t i = 0; i < nv; i++) {
-            umean[i] = (float)sums[(size_t)i * 2];
-            mtot[i] = (float)sums[(size_t)i * 2 + 1];
+            umean[i] = sums[(size_t)i * 2];
+            mtot[i] = sums[(size_t)i * 2 + 1];
             ncount += ncellv[i];
             if (ncellv[i] > 0) umean[i] = umean[i] / (float)ncellv[i];
         }

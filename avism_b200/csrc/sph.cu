@@ -5,8 +5,8 @@
 // (398-430) and DDENS_INTERP_SPH (434-617).  Every REAL*4 expression is
 // evaluated in the reference's order (the library is built with --fmad=false);
 // the reference's REAL*8 accumulators stay REAL*8.  DDENS's FP64 atomic
-// scatter becomes a 128-bit fixed-point scatter, which is exact and order
-// independent, so the grid does not depend on thread timing.
+// scatter becomes an exact integer scatter (add_exact), order independent, so
+// the grid does not depend on thread timing.
 #include <cub/cub.cuh>
 #include <cfloat>
 #include <climits>
@@ -15,6 +15,7 @@
 #include "knn_core.cuh"
 #include "knn_warp.cuh"
 #include "bin_kernels.cuh"
+#include "knn_group.cuh"
 
 namespace avism {
 
@@ -451,27 +452,38 @@ k_cells_knn_w(KnnGrid G, CellArgs A) {
 }
 
 // ---- DDENS_INTERP_SPH: per-particle NORM in the reference's loop order, then
-//      a 128-bit fixed-point scatter of m*w/NORM --------------------------------
+//      an exact scatter of m*w/NORM ----------------------------------------------
 struct DdensArgs {
     int nx, rad_lo;
     float dx, rx1;
     const float *rad;
     const float *hp_s;            // h in binned order
     const float4 *sv;             // (vx, vy, vz, m) in binned order
-    unsigned long long *fix;      // 2 words per cell: low, high
-    double scale;
-    float scale_f;                // the same power of two
+    unsigned long long *fix;      // nlimb counters per cell (exact sums, add_exact)
+    int nlimb;
     unsigned long long *norm0;    // counter of NORM = 0 particles, or null
     int gauss;                    // KERNEL_MODE = 2
 };
 
-// v < 2^62 is added as its two 32-bit halves to two 64-bit counters (low half to
-// word 0, high half to word 1).  Neither counter can overflow for fewer than 2^32
-// additions per cell, no result is needed, so both compile to fire-and-forget
-// reductions; the cell's exact 128-bit sum is word1 * 2^32 + word0.
-__device__ __forceinline__ void add128(unsigned long long *cell, unsigned long long v) {
-    atomicAdd(cell, v & 0xffffffffULL);
-    atomicAdd(cell + 1, v >> 32);
+// Exact REAL*4 sums.  Every finite f32 value is an integer multiple of 2^-149,
+// so a cell's sum is kept exactly as an integer in units of 2^-149, split in
+// 32-bit limbs; limb i accumulates in the cell's 64-bit counter i.  A term's
+// 24-bit significand, shifted to its place, spans at most two limbs, added as
+// two fire-and-forget reductions; a counter cannot overflow for fewer than 2^32
+// additions per cell.  The carries between limbs are resolved once, when the
+// cell is read (k_exact_to_f32).  The sum is independent of the order of the
+// additions, unlike the reference's REAL*8 atomics, and as fine as REAL*4 allows
+// at every magnitude (masses over many decades lose nothing).
+__device__ __forceinline__ void add_exact(unsigned long long *cell, float v) {
+    const uint32_t b = __float_as_uint(v);            // v >= 0
+    if (b == 0) return;
+    const uint32_t e = b >> 23;
+    const uint32_t mant = (b & 0x7fffffu) | (e ? 0x800000u : 0u);
+    const uint32_t pos = e ? e - 1 : 0;               // place of the significand's lowest bit
+    const unsigned long long w = (unsigned long long)mant << (pos & 31);
+    unsigned long long *c = cell + (pos >> 5);
+    atomicAdd(c, w & 0xffffffffULL);
+    if (w >> 32) atomicAdd(c + 1, w >> 32);
 }
 
 // DDENS weight: M4 of Q = SQRT(D2) * INV_H, or with KERNEL_MODE = 2 the Gaussian
@@ -558,9 +570,8 @@ __device__ __noinline__ void ddens_nested(const DdensArgs &A, const float4 p, in
                         norm = __fadd_rn(norm, w);
                     } else if (w != 0.0f) {
                         const float contrib = __fdiv_rn(__fmul_rn(w, m), norm);
-                        const unsigned long long v = (unsigned long long)llrint((double)contrib * A.scale);
                         const int64_t cid = (int64_t)(i2 - 1) + (int64_t)nx * ((int64_t)(j2 - 1) + (int64_t)nx * (k2 - 1));
-                        add128(A.fix + 2 * cid, v);
+                        add_exact(A.fix + (int64_t)A.nlimb * cid, contrib);
                     }
                 }
             }
@@ -569,7 +580,7 @@ __device__ __noinline__ void ddens_nested(const DdensArgs &A, const float4 p, in
             // the particle only contributes to its own cell
             if (ix >= 1 && ix <= nx && jy >= 1 && jy <= nx && kz >= 1 && kz <= nx) {
                 const int64_t cid = (int64_t)(ix - 1) + (int64_t)nx * ((int64_t)(jy - 1) + (int64_t)nx * (kz - 1));
-                add128(A.fix + 2 * cid, (unsigned long long)llrint((double)m * A.scale));
+                add_exact(A.fix + (int64_t)A.nlimb * cid, m);
             }
             break;
         }
@@ -686,11 +697,11 @@ __global__ void __launch_bounds__(DD_THREADS, 6) k_ddens(KnnGrid G, int64_t n, D
         // the particle only contributes to its own cell
         if (ix >= 1 && ix <= nx && jy >= 1 && jy <= nx && kz >= 1 && kz <= nx) {
             const int64_t cid = (int64_t)(ix - 1) + (int64_t)nx * ((int64_t)(jy - 1) + (int64_t)nx * (kz - 1));
-            add128(A.fix + 2 * cid, (unsigned long long)llrint((double)m * A.scale));
+            add_exact(A.fix + (int64_t)A.nlimb * cid, m);
         }
         return;
     }
-    // pass 1: m * w / NORM in 128-bit fixed point
+    // pass 1: m * w / NORM, exact sums per cell
     int r = 0;
     load_row(0);
     int64_t rowc = (int64_t)nx * ((int64_t)(j2 - 1) + (int64_t)nx * (k2 - 1)) - 1;
@@ -700,10 +711,7 @@ __global__ void __launch_bounds__(DD_THREADS, 6) k_ddens(KnnGrid G, int64_t n, D
         const float w = (A.gauss && d2 > h2max) ? 0.0f : kernel_q(A.gauss, d2, inv_h);
         if (w != 0.0f) {
             const float contrib = __fdiv_rn(__fmul_rn(w, m), norm);
-            // contrib * 2^k is exact in f32 (below 2^62, no overflow), so
-            // rounding it to an integer in f32 gives llrint((double)contrib * scale)
-            const unsigned long long v = __float2ull_rn(__fmul_rn(contrib, A.scale_f));
-            add128(A.fix + 2 * (rowc + i2), v);
+            add_exact(A.fix + (int64_t)A.nlimb * (rowc + i2), contrib);
         }
         if (++i2 > ie && t + 1 < ncell) {
             load_row(++r);
@@ -712,14 +720,60 @@ __global__ void __launch_bounds__(DD_THREADS, 6) k_ddens(KnnGrid G, int64_t n, D
     }
 }
 
-__global__ void k_fix128_to_f32(int64_t nc, const unsigned long long *__restrict__ fix, double inv_scale,
-                                float *__restrict__ out) {
+// A cell's exact sum, rounded to REAL*8 (nearest, ties to even) and then to
+// REAL*4, as the reference's U(...) = U8(...) conversion of its REAL*8 sum.
+constexpr int EXACT_MAX_LIMBS = 11;
+
+__global__ void k_exact_to_f32(int64_t nc, const unsigned long long *__restrict__ fix, int nlimb,
+                               float *__restrict__ out) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
-    const unsigned __int128 t = ((unsigned __int128)fix[2 * c + 1] << 32) + (unsigned __int128)fix[2 * c];
-    const unsigned long long lo = (unsigned long long)t, hi = (unsigned long long)(t >> 64);
-    const double v = ((double)hi * 18446744073709551616.0 + (double)lo) * inv_scale;
-    out[c] = (float)v;
+    uint32_t limb[EXACT_MAX_LIMBS + 1];
+    unsigned long long carry = 0;
+    int top = -1;
+#pragma unroll
+    for (int i = 0; i < EXACT_MAX_LIMBS; i++) {
+        if (i < nlimb) {
+            const unsigned long long v = fix[(int64_t)nlimb * c + i] + carry;   // < 2^64: counters < 2^63
+            limb[i] = (uint32_t)v;
+            carry = v >> 32;
+        } else {
+            limb[i] = (uint32_t)carry;
+            carry = 0;
+        }
+        if (limb[i]) top = i;
+    }
+    if (top < 0) { out[c] = 0.0f; return; }
+    // the top three limbs as one integer x; the limbs below only matter as a sticky bit
+    const int base = top >= 2 ? top - 2 : 0;
+    unsigned __int128 x = 0;
+    for (int i = top; i >= base; i--) x = (x << 32) | limb[i];
+    bool sticky = false;
+    for (int i = 0; i < base; i++) sticky |= limb[i] != 0;
+    const unsigned long long xh = (unsigned long long)(x >> 64), xl = (unsigned long long)x;
+    const int nbits = xh ? 128 - __clzll(xh) : 64 - __clzll(xl);
+    double d;
+    if (nbits <= 53) {
+        d = ldexp((double)xl, 32 * base - 149);           // exact (no limbs below: base = 0)
+    } else {
+        const int sh = nbits - 53;
+        unsigned long long m = (unsigned long long)(x >> sh);
+        const unsigned __int128 rem = x & (((unsigned __int128)1 << sh) - 1);
+        const unsigned __int128 half = (unsigned __int128)1 << (sh - 1);
+        const bool up = rem > half || (rem == half && (sticky || (m & 1)));
+        int e = sh;
+        if (up && ++m == (1ULL << 53)) { m >>= 1; e++; }
+        d = ldexp((double)m, e + 32 * base - 149);
+    }
+    out[c] = __double2float_rn(d);
+}
+
+// limbs for sums of terms up to mmax: the top term's bit place, 24 significand
+// bits and 32 bits of carries (fewer than 2^32 terms per cell)
+static int exact_limbs(float mmax) {
+    const uint32_t e = (uint32_t)(reinterpret_cast<const uint32_t &>(mmax) >> 23);
+    const int top = (int)e + 1 + 24 + 32;              // one spare place for a rounded-up term
+    return std::min(EXACT_MAX_LIMBS, top / 32 + 2);
 }
 
 // ---- TSC (DENS_INTERP_TSC / VEL_INTERP_TSC) as a gather over TSC cells -------
@@ -844,6 +898,91 @@ k_tsc_gather(int64_t nc, const int64_t *__restrict__ start, const int32_t *__res
     }
 }
 
+// ---- PPART_DENS and VVEL_INTERP_SPH_VW / H_DISTANCE on the group search -------
+// (knn_group.cuh): a warp answers 32 queries, one per lane, over shared staged
+// candidates; each lane then runs its query's REAL*8 sums itself, in neighbour
+// order.  Queries: 32 consecutive particles of the binned order, or a 4x4x2
+// tile of grid cells.
+constexpr int GK_WARPS = 2;
+
+template <int KMAX>
+constexpr size_t group_smem_bytes() { return (size_t)GK_WARPS * sizeof(GroupKnnSmem<KMAX>); }
+
+__device__ __forceinline__ float group_radius(const KnnGrid &G, float qx, float qy, float qz, int K) {
+    const float r = query_r0(G, qx, qy, qz);
+    return r > 0.0f ? r : knn_uniform_radius(G, K);
+}
+
+template <int KMAX, bool STATS>
+__global__ void __launch_bounds__(GK_WARPS * 32)
+k_ppart_dens_g(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float *__restrict__ pd_s,
+               float *__restrict__ part_dens) {
+    extern __shared__ __align__(16) unsigned char gk_smem[];
+    GroupKnnSmem<KMAX> &S = reinterpret_cast<GroupKnnSmem<KMAX> *>(gk_smem)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int64_t i = ((int64_t)blockIdx.x * GK_WARPS + (threadIdx.x >> 5)) * 32 + lane;
+    const bool active = i < n;
+    const float4 p = active ? G.sp[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float R = active ? group_radius(G, p.x, p.y, p.z, K) : 0.0f;
+    const int cnt = group_knn<KMAX, STATS>(G, active, p.x, p.y, p.z, R, K, S);
+    if (!active) return;
+    double bas8 = 0.0;
+    for (int j = 0; j < cnt; j++) bas8 = bas8 + (double)sv[S.pos[j][lane]].w;
+    const float hk = sqrtf(__uint_as_float(S.d2[K - 1][lane]));
+    const double pi = 3.141592653589793;     // DACOS(-1.D0)
+    const float rho = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(hk, hk), hk)));
+    pd_s[i] = rho;
+    if (part_dens) part_dens[__float_as_int(p.w)] = rho;
+}
+
+template <int KMAX, bool STATS>
+__global__ void __launch_bounds__(GK_WARPS * 32)
+k_cells_g(KnnGrid G, CellArgs A) {
+    extern __shared__ __align__(16) unsigned char gk_smem[];
+    GroupKnnSmem<KMAX> &S = reinterpret_cast<GroupKnnSmem<KMAX> *>(gk_smem)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int nx = A.nx;
+    const int ntx = (nx + 3) / 4, nty = (nx + 3) / 4, ntz = (nx + 1) / 2;
+    const int64_t tile = (int64_t)blockIdx.x * GK_WARPS + (threadIdx.x >> 5);
+    const int tx = (int)(tile % ntx), ty = (int)((tile / ntx) % nty), tz = (int)(tile / ((int64_t)ntx * nty));
+    const int ix = tx * 4 + (lane & 3) + 1, jy = ty * 4 + ((lane >> 2) & 3) + 1, kz = tz * 2 + (lane >> 4) + 1;
+    const int64_t c = (int64_t)(ix - 1) + (int64_t)nx * ((int64_t)(jy - 1) + (int64_t)nx * (kz - 1));
+    bool active = tz < ntz && ix <= nx && jy <= nx && kz <= nx;
+    if (active && A.smask && A.smask[c] == 0) active = false;
+    float qx = 0.0f, qy = 0.0f, qz = 0.0f, R = 0.0f;
+    if (active) {
+        qx = A.rad[ix - A.rad_lo];
+        qy = A.rad[jy - A.rad_lo];
+        qz = A.rad[kz - A.rad_lo];
+        R = group_radius(G, qx, qy, qz, A.K);
+    }
+    const int cnt = group_knn<KMAX, STATS>(G, active, qx, qy, qz, R, A.K, S);
+    if (!active) return;
+    const float hk = sqrtf(__uint_as_float(S.d2[cnt - 1][lane]));
+    if (!(hk > A.dx)) {                           // ball_search(TREE, TAR, DX) branch
+        const int slot = atomicAdd(A.ball_count, 1);
+        A.ball_list[slot] = (int32_t)c;
+        return;
+    }
+    for (int j = 0; j < cnt; j++) atomic_max_pos(&A.hp_s[S.pos[j][lane]], sqrtf(__uint_as_float(S.d2[j][lane])));
+    if (!A.do_vel) return;
+    double b = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
+    for (int j = 0; j < cnt; j++) {
+        const uint32_t pj = S.pos[j][lane];
+        const float4 a = A.sv[pj];
+        float w = kernel_w(A.gauss, hk, sqrtf(__uint_as_float(S.d2[j][lane])));
+        w = __fmul_rn(w, __fdiv_rn(a.w, A.pd_s[pj]));
+        const double w8 = (double)w;
+        b = b + w8;
+        bx = bx + w8 * (double)a.x;
+        by = by + w8 * (double)a.y;
+        bz = bz + w8 * (double)a.z;
+    }
+    A.u2[c] = (float)(bx / b);
+    A.u3[c] = (float)(by / b);
+    A.u4[c] = (float)(bz / b);
+}
+
 // ---- starting radius of the radius-guided search: the K-th neighbour distance of
 //      a uniform density equal to the particle count of the 3x3x3 bins around ----
 __global__ void k_radius_estimate(KnnGrid G, int K, float fac, float *r0) {
@@ -880,6 +1019,11 @@ __global__ void k_zero_f32(int64_t n, float *a) {
     if (i < n) a[i] = 0.0f;
 }
 
+static bool group_search_on() {
+    const char *e = getenv("AVISM_TUNE_GROUP");
+    return e ? atoi(e) != 0 : true;
+}
+
 // with the counters on: the ball-fallback cells and the particles left with
 // h = 0 for FILL_H_ZEROS (Ctx::path_counts[0..1])
 static void count_orphans(Ctx &c, const KnnGrid &G, int64_t n, const float *hp_s, int32_t nball) {
@@ -911,9 +1055,21 @@ static void run_sph_kernels_ws(Ctx &c, const KnnGrid &G, const avism_params *p, 
     const int carve = std::min(100, (int)((100 * 5 * (sm_cells + 1024) + 228 * 1024 - 1) / (228 * 1024)) + 5);
     AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cells));
     AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX, STATS>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+    // the group search (32 queries per warp over staged tiles); AVISM_TUNE_GROUP=0
+    // keeps one query per warp
+    const bool group = KMAX <= 64 && group_search_on();
+    const size_t gsm = group_smem_bytes<KMAX>();
+    if (group) {
+        AV_CUDA(cudaFuncSetAttribute(k_ppart_dens_g<KMAX, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
+        AV_CUDA(cudaFuncSetAttribute(k_cells_g<KMAX, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
+    }
     if (vel_sph) {
-        ++c.launches, k_ppart_dens_w<KMAX, STATS><<<grid_for(a.n, SPH_WARPS * PP_QPW), SPH_WARPS * 32, sm, c.stream>>>(
-            G, a.n, K, sv, pd_s, a.part_dens);
+        if (group)
+            ++c.launches, k_ppart_dens_g<KMAX, STATS><<<grid_for(a.n, GK_WARPS * 32), GK_WARPS * 32, gsm, c.stream>>>(
+                G, a.n, K, sv, pd_s, a.part_dens);
+        else
+            ++c.launches, k_ppart_dens_w<KMAX, STATS><<<grid_for(a.n, SPH_WARPS * PP_QPW), SPH_WARPS * 32, sm, c.stream>>>(
+                G, a.n, K, sv, pd_s, a.part_dens);
         AV_CUDA(cudaGetLastError());
         c.mark("ppart_dens");
     }
@@ -928,7 +1084,11 @@ static void run_sph_kernels_ws(Ctx &c, const KnnGrid &G, const avism_params *p, 
         A.gauss = p->kernel_mode == 2;
         A.ball_list = ball_list; A.ball_count = cnt_d;
         const int64_t nblk = (int64_t)((nx + 3) / 4) * ((nx + 3) / 4) * ((nx + 1) / 2);
-        ++c.launches, k_cells_knn_w<KMAX, STATS><<<(unsigned)nblk, SPH_WARPS * 32, sm_cells, c.stream>>>(G, A);
+        if (group)
+            ++c.launches, k_cells_g<KMAX, STATS><<<(unsigned)((nblk + GK_WARPS - 1) / GK_WARPS), GK_WARPS * 32, gsm,
+                                                   c.stream>>>(G, A);
+        else
+            ++c.launches, k_cells_knn_w<KMAX, STATS><<<(unsigned)nblk, SPH_WARPS * 32, sm_cells, c.stream>>>(G, A);
         AV_CUDA(cudaGetLastError());
         c.mark("cells_knn");
         int32_t nball = 0;
@@ -1078,8 +1238,9 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
                 a.wprop->box = bp.box;
             }
             c.mark("proposal");
-        } else if (p->learned == 2) {
+        } else if (p->learned == 2 || (K <= 64 && group_search_on())) {
             // hand-made proposal: a starting radius per bin from the local bin density
+            // (the group search needs a local radius: the plain start uses it too)
             const int64_t nbins = (int64_t)bp.nb * bp.nb * bp.nb;
             float *r0 = c.get_t<float>(B_KNN_R0, nbins);
             const char *fac_env = getenv("AVISM_TUNE_RFAC");
@@ -1095,7 +1256,8 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
         else if (K <= 128) run_sph_kernels_w<128>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
         else run_sph_kernels<256>(c, G, p, L, a, rad_d, vel_sph, need_h_cells, sv, pd_s, hp_s);
         if (dens_sph) {
-            // scale: the largest term m*w/NORM <= m_max stays below 2^62
+            // exact per-cell sums: the limb count follows the largest mass (every
+            // term m*w/NORM is at most about m)
             float mmax = 0.0f;
             {
                 float *d = c.get_t<float>(B_RED0, 1);
@@ -1107,14 +1269,12 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
                 c.sync();
             }
             AV_CHECK(mmax > 0.0f && std::isfinite(mmax), AVISM_ERR_ARG, "particle masses must be positive");
-            int e2;
-            std::frexp((double)mmax, &e2);              // mmax < 2^e2
-            const double scale = std::ldexp(1.0, 62 - e2);
-            unsigned long long *fix = c.get_t<unsigned long long>(B_FIX0, 2 * nc);
-            AV_CUDA(cudaMemsetAsync(fix, 0, 2 * nc * sizeof(unsigned long long), c.stream));
+            const int nlimb = exact_limbs(mmax);
+            unsigned long long *fix = c.get_t<unsigned long long>(B_FIX0, (size_t)nlimb * nc);
+            AV_CUDA(cudaMemsetAsync(fix, 0, (size_t)nlimb * nc * sizeof(unsigned long long), c.stream));
             DdensArgs D;
             D.nx = nx; D.rad_lo = L.g.rad_lo; D.dx = L.g.dx; D.rx1 = L.rad_at(1); D.rad = rad_d;
-            D.hp_s = hp_s; D.sv = sv; D.fix = fix; D.scale = scale; D.scale_f = (float)scale;
+            D.hp_s = hp_s; D.sv = sv; D.fix = fix; D.nlimb = nlimb;
             D.norm0 = nullptr;
             D.gauss = p->kernel_mode == 2;
             if (G.stats) {
@@ -1131,7 +1291,7 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
                 c.path_counts[2] = (int64_t)h;
             }
             c.mark("ddens_scatter");
-            ++c.launches, k_fix128_to_f32<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, fix, 1.0 / scale, a.u_mass);
+            ++c.launches, k_exact_to_f32<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, fix, nlimb, a.u_mass);
             c.mark("ddens_convert");
         }
     }

@@ -284,7 +284,8 @@ int orc_merge_post(const avism_params *p, int32_t nvoid, const avism_cubes *cb,
                 for (int i2 = 0; i2 < 3; i2++)
                     for (int i1 = 0; i1 < 3; i1++) {
                         const float delta = (i1 == i2) ? 1.0f : 0.0f;
-                        I3[i1 + 3 * i2] = I3[i1 + 3 * i2] + ((delta * rr) * rr - rk[i1] * rk[i2]);
+                        /* INERTIA + DELTA*RR*RR - RK(I1)*RK(I2), left to right */
+                        I3[i1 + 3 * i2] = (I3[i1 + 3 * i2] + (delta * rr) * rr) - rk[i1] * rk[i2];
                     }
             }
     for (int32_t i = 0; i < nv; i++) { out->eps[i] = 0.0f; out->ip[i] = 0.0f; }

@@ -106,7 +106,8 @@ def test_weighted_cone_level_exact(gpu):
     for k in g["cubes"]:
         assert np.array_equal(g["cubes"][k], o["vf"]["cubes"][k]), k
     assert g["meandens"] == o["meandens"]
-    for k in ("indice", "uvoid", "ncellv", "volnew", "req", "gxc", "gyc", "gzc", "xc", "yc", "zc"):
+    for k in ("indice", "uvoid", "ncellv", "volnew", "req", "gxc", "gyc", "gzc", "xc", "yc", "zc", "eps", "ip",
+              "umean", "mtot"):
         assert np.array_equal(np.asarray(g["cat"][k]), np.asarray(o["cat"][k])), k
     assert g["cat"]["nvoidt"] == o["cat"]["nvoidt"]
     # the learned and density-estimate starting radii give the same catalogue

@@ -14,7 +14,8 @@ from avism_b200._abi import Params
 pytestmark = pytest.mark.gpu
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "config2_256.npz")
-EXACT = ("indice", "uvoid", "ncellv", "volnew", "req", "xc", "yc", "zc", "gxc", "gyc", "gzc")
+EXACT = ("indice", "uvoid", "ncellv", "volnew", "req", "xc", "yc", "zc", "gxc", "gyc", "gzc", "eps", "ip", "umean",
+         "mtot")
 
 
 def digest(a) -> str:
@@ -53,13 +54,3 @@ def test_config2_level_matches_oracle(gpu, case, vel, dens):
     assert r["cat"]["nvoidt"] == int(gold[f"{tag}_nvoidt"]) > 0
     for k in EXACT:
         assert np.array_equal(np.asarray(r["cat"][k]), gold[f"{tag}_cat_{k}"]), k
-    main = gold[f"{tag}_cat_uvoid"] == -1
-    n = np.maximum(gold[f"{tag}_cat_ncellv"][main], 1).astype(np.float64)
-    tol = 2e-6 * np.sqrt(n) + 1e-6
-    for k in ("umean", "mtot"):
-        a, b = gold[f"{tag}_cat_{k}"][main].astype(np.float64), np.asarray(r["cat"][k])[main].astype(np.float64)
-        assert np.all(np.abs(a - b) <= tol * np.abs(a)), k
-    for k in ("eps", "ip"):
-        a, b = gold[f"{tag}_cat_{k}"][main].astype(np.float64), np.asarray(r["cat"][k])[main].astype(np.float64)
-        ok = (np.abs(a - b) <= 1e-4 * np.maximum(1.0, np.abs(a))) | (a == -99) | (b == -99)
-        assert np.all(ok), k

@@ -1,10 +1,8 @@
 """GPU parity: the CUDA path (through the C-ABI) against the CPU oracle.
 
-Bit-exact: kNN lists, INDEXX permutations, the SPH fields, normalised density,
-divergence, flag grids, the grown cubes and all integer catalogue columns.
-Floating-point reductions whose order the reference itself leaves open (the
-REAL*4 inertia, mean-density and mass sums over a void) agree to the stated
-tolerances."""
+Bit-exact: kNN lists, INDEXX permutations, the SPH and TSC fields, normalised
+density, divergence, flag grids, the grown cubes and every catalogue column
+(the REAL*4 inertia, UMEAN and MTOT sums in the reference's serial order)."""
 import numpy as np
 import pytest
 
@@ -126,20 +124,12 @@ def test_merge_post_parity(gpu, fields_pair):
         vo = O.voidfind(p, o[0], o[1])
         co = O.merge_post(p, vo["nvoid"], vo["cubes"], o[0], o[2])
         cg = gpu.merge_post(p, vo["nvoid"], vo["cubes"], o[0], o[2])
-        for k in ("indice", "uvoid", "ncellv", "marca", "volnew", "req", "xc", "yc", "zc", "gxc", "gyc", "gzc"):
+        # every column bit-exact: the REAL*4 inertia, UMEAN and MTOT sums run in
+        # the reference's serial K, J, I order per void on the GPU too
+        for k in ("indice", "uvoid", "ncellv", "marca", "volnew", "req", "xc", "yc", "zc", "gxc", "gyc", "gzc",
+                  "eps", "ip", "umean", "mtot"):
             assert np.array_equal(co[k], cg[k]), k
         assert (co["nvoid2"], co["nvoidt"], co["volt_clean"]) == (cg["nvoid2"], cg["nvoidt"], cg["volt_clean"])
-        main = co["uvoid"] == -1
-        # REAL*4 sums in K,J,I order (reference) vs FP64 sums (GPU)
-        n = np.maximum(co["ncellv"][main], 1).astype(np.float64)
-        tol = 2e-6 * np.sqrt(n) + 1e-6
-        for k in ("umean", "mtot"):
-            a, b = co[k][main].astype(np.float64), cg[k][main].astype(np.float64)
-            assert np.all(np.abs(a - b) <= tol * np.abs(a)), k
-        for k in ("eps", "ip"):
-            a, b = co[k][main].astype(np.float64), cg[k][main].astype(np.float64)
-            ok = (np.abs(a - b) <= 1e-4 * np.maximum(1.0, np.abs(a))) | (a == -99) | (b == -99)
-            assert np.all(ok), k
 
 
 def test_run_level_matches_oracle(gpu, mock1, oracle_mock1):
@@ -151,7 +141,8 @@ def test_run_level_matches_oracle(gpu, mock1, oracle_mock1):
         for k in r["cubes"]:
             assert np.array_equal(r["cubes"][k], o["vf"]["cubes"][k]), k
         assert r["meandens"] == o["meandens"]
-        for k in ("indice", "uvoid", "ncellv", "marca", "volnew", "req", "gxc", "gyc", "gzc"):
+        for k in ("indice", "uvoid", "ncellv", "marca", "volnew", "req", "gxc", "gyc", "gzc", "eps", "ip",
+                  "umean", "mtot"):
             assert np.array_equal(r["cat"][k], o["cat"][k]), k
         assert r["cat"]["nvoidt"] == o["cat"]["nvoidt"] and r["cat"]["nvoidt"] > 0
 
