@@ -15,7 +15,6 @@
 #include "knn_core.cuh"
 #include "knn_warp.cuh"
 #include "bin_kernels.cuh"
-#include "knn_group.cuh"
 
 namespace avism {
 
@@ -898,91 +897,6 @@ k_tsc_gather(int64_t nc, const int64_t *__restrict__ start, const int32_t *__res
     }
 }
 
-// ---- PPART_DENS and VVEL_INTERP_SPH_VW / H_DISTANCE on the group search -------
-// (knn_group.cuh): a warp answers 32 queries, one per lane, over shared staged
-// candidates; each lane then runs its query's REAL*8 sums itself, in neighbour
-// order.  Queries: 32 consecutive particles of the binned order, or a 4x4x2
-// tile of grid cells.
-constexpr int GK_WARPS = 2;
-
-template <int KMAX>
-constexpr size_t group_smem_bytes() { return (size_t)GK_WARPS * sizeof(GroupKnnSmem<KMAX>); }
-
-__device__ __forceinline__ float group_radius(const KnnGrid &G, float qx, float qy, float qz, int K) {
-    const float r = query_r0(G, qx, qy, qz);
-    return r > 0.0f ? r : knn_uniform_radius(G, K);
-}
-
-template <int KMAX, bool STATS>
-__global__ void __launch_bounds__(GK_WARPS * 32)
-k_ppart_dens_g(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float *__restrict__ pd_s,
-               float *__restrict__ part_dens) {
-    extern __shared__ __align__(16) unsigned char gk_smem[];
-    GroupKnnSmem<KMAX> &S = reinterpret_cast<GroupKnnSmem<KMAX> *>(gk_smem)[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    const int64_t i = ((int64_t)blockIdx.x * GK_WARPS + (threadIdx.x >> 5)) * 32 + lane;
-    const bool active = i < n;
-    const float4 p = active ? G.sp[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const float R = active ? group_radius(G, p.x, p.y, p.z, K) : 0.0f;
-    const int cnt = group_knn<KMAX, STATS>(G, active, p.x, p.y, p.z, R, K, S);
-    if (!active) return;
-    double bas8 = 0.0;
-    for (int j = 0; j < cnt; j++) bas8 = bas8 + (double)sv[S.pos[j][lane]].w;
-    const float hk = sqrtf(__uint_as_float(S.d2[K - 1][lane]));
-    const double pi = 3.141592653589793;     // DACOS(-1.D0)
-    const float rho = (float)(bas8 / ((4.0 / 3.0) * pi * (double)__fmul_rn(__fmul_rn(hk, hk), hk)));
-    pd_s[i] = rho;
-    if (part_dens) part_dens[__float_as_int(p.w)] = rho;
-}
-
-template <int KMAX, bool STATS>
-__global__ void __launch_bounds__(GK_WARPS * 32)
-k_cells_g(KnnGrid G, CellArgs A) {
-    extern __shared__ __align__(16) unsigned char gk_smem[];
-    GroupKnnSmem<KMAX> &S = reinterpret_cast<GroupKnnSmem<KMAX> *>(gk_smem)[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    const int nx = A.nx;
-    const int ntx = (nx + 3) / 4, nty = (nx + 3) / 4, ntz = (nx + 1) / 2;
-    const int64_t tile = (int64_t)blockIdx.x * GK_WARPS + (threadIdx.x >> 5);
-    const int tx = (int)(tile % ntx), ty = (int)((tile / ntx) % nty), tz = (int)(tile / ((int64_t)ntx * nty));
-    const int ix = tx * 4 + (lane & 3) + 1, jy = ty * 4 + ((lane >> 2) & 3) + 1, kz = tz * 2 + (lane >> 4) + 1;
-    const int64_t c = (int64_t)(ix - 1) + (int64_t)nx * ((int64_t)(jy - 1) + (int64_t)nx * (kz - 1));
-    bool active = tz < ntz && ix <= nx && jy <= nx && kz <= nx;
-    if (active && A.smask && A.smask[c] == 0) active = false;
-    float qx = 0.0f, qy = 0.0f, qz = 0.0f, R = 0.0f;
-    if (active) {
-        qx = A.rad[ix - A.rad_lo];
-        qy = A.rad[jy - A.rad_lo];
-        qz = A.rad[kz - A.rad_lo];
-        R = group_radius(G, qx, qy, qz, A.K);
-    }
-    const int cnt = group_knn<KMAX, STATS>(G, active, qx, qy, qz, R, A.K, S);
-    if (!active) return;
-    const float hk = sqrtf(__uint_as_float(S.d2[cnt - 1][lane]));
-    if (!(hk > A.dx)) {                           // ball_search(TREE, TAR, DX) branch
-        const int slot = atomicAdd(A.ball_count, 1);
-        A.ball_list[slot] = (int32_t)c;
-        return;
-    }
-    for (int j = 0; j < cnt; j++) atomic_max_pos(&A.hp_s[S.pos[j][lane]], sqrtf(__uint_as_float(S.d2[j][lane])));
-    if (!A.do_vel) return;
-    double b = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
-    for (int j = 0; j < cnt; j++) {
-        const uint32_t pj = S.pos[j][lane];
-        const float4 a = A.sv[pj];
-        float w = kernel_w(A.gauss, hk, sqrtf(__uint_as_float(S.d2[j][lane])));
-        w = __fmul_rn(w, __fdiv_rn(a.w, A.pd_s[pj]));
-        const double w8 = (double)w;
-        b = b + w8;
-        bx = bx + w8 * (double)a.x;
-        by = by + w8 * (double)a.y;
-        bz = bz + w8 * (double)a.z;
-    }
-    A.u2[c] = (float)(bx / b);
-    A.u3[c] = (float)(by / b);
-    A.u4[c] = (float)(bz / b);
-}
-
 // ---- starting radius of the radius-guided search: the K-th neighbour distance of
 //      a uniform density equal to the particle count of the 3x3x3 bins around ----
 __global__ void k_radius_estimate(KnnGrid G, int K, float fac, float *r0) {
@@ -1019,11 +933,6 @@ __global__ void k_zero_f32(int64_t n, float *a) {
     if (i < n) a[i] = 0.0f;
 }
 
-static bool group_search_on() {
-    const char *e = getenv("AVISM_TUNE_GROUP");
-    return e ? atoi(e) != 0 : true;
-}
-
 // with the counters on: the ball-fallback cells and the particles left with
 // h = 0 for FILL_H_ZEROS (Ctx::path_counts[0..1])
 static void count_orphans(Ctx &c, const KnnGrid &G, int64_t n, const float *hp_s, int32_t nball) {
@@ -1055,21 +964,9 @@ static void run_sph_kernels_ws(Ctx &c, const KnnGrid &G, const avism_params *p, 
     const int carve = std::min(100, (int)((100 * 5 * (sm_cells + 1024) + 228 * 1024 - 1) / (228 * 1024)) + 5);
     AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cells));
     AV_CUDA(cudaFuncSetAttribute(k_cells_knn_w<KMAX, STATS>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
-    // the group search (32 queries per warp over staged tiles); AVISM_TUNE_GROUP=0
-    // keeps one query per warp
-    const bool group = KMAX <= 64 && group_search_on();
-    const size_t gsm = group_smem_bytes<KMAX>();
-    if (group) {
-        AV_CUDA(cudaFuncSetAttribute(k_ppart_dens_g<KMAX, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
-        AV_CUDA(cudaFuncSetAttribute(k_cells_g<KMAX, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
-    }
     if (vel_sph) {
-        if (group)
-            ++c.launches, k_ppart_dens_g<KMAX, STATS><<<grid_for(a.n, GK_WARPS * 32), GK_WARPS * 32, gsm, c.stream>>>(
-                G, a.n, K, sv, pd_s, a.part_dens);
-        else
-            ++c.launches, k_ppart_dens_w<KMAX, STATS><<<grid_for(a.n, SPH_WARPS * PP_QPW), SPH_WARPS * 32, sm, c.stream>>>(
-                G, a.n, K, sv, pd_s, a.part_dens);
+        ++c.launches, k_ppart_dens_w<KMAX, STATS><<<grid_for(a.n, SPH_WARPS * PP_QPW), SPH_WARPS * 32, sm, c.stream>>>(
+            G, a.n, K, sv, pd_s, a.part_dens);
         AV_CUDA(cudaGetLastError());
         c.mark("ppart_dens");
     }
@@ -1084,11 +981,7 @@ static void run_sph_kernels_ws(Ctx &c, const KnnGrid &G, const avism_params *p, 
         A.gauss = p->kernel_mode == 2;
         A.ball_list = ball_list; A.ball_count = cnt_d;
         const int64_t nblk = (int64_t)((nx + 3) / 4) * ((nx + 3) / 4) * ((nx + 1) / 2);
-        if (group)
-            ++c.launches, k_cells_g<KMAX, STATS><<<(unsigned)((nblk + GK_WARPS - 1) / GK_WARPS), GK_WARPS * 32, gsm,
-                                                   c.stream>>>(G, A);
-        else
-            ++c.launches, k_cells_knn_w<KMAX, STATS><<<(unsigned)nblk, SPH_WARPS * 32, sm_cells, c.stream>>>(G, A);
+        ++c.launches, k_cells_knn_w<KMAX, STATS><<<(unsigned)nblk, SPH_WARPS * 32, sm_cells, c.stream>>>(G, A);
         AV_CUDA(cudaGetLastError());
         c.mark("cells_knn");
         int32_t nball = 0;
@@ -1238,9 +1131,8 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
                 a.wprop->box = bp.box;
             }
             c.mark("proposal");
-        } else if (p->learned == 2 || (K <= 64 && group_search_on())) {
+        } else if (p->learned == 2) {
             // hand-made proposal: a starting radius per bin from the local bin density
-            // (the group search needs a local radius: the plain start uses it too)
             const int64_t nbins = (int64_t)bp.nb * bp.nb * bp.nb;
             float *r0 = c.get_t<float>(B_KNN_R0, nbins);
             const char *fac_env = getenv("AVISM_TUNE_RFAC");
