@@ -361,6 +361,41 @@ class AvismGPU:
             C.byref(vo.c), C.byref(md)))
         return dict(cubes=cubes.view(nv.value), nvoid=nv.value, cat=vo.view(nv.value), meandens=md.value)
 
+    # ---- survey mode (src/avism.f90:1420-1596) -------------------------------------
+    def _survey_args(self, parts, rands, smask):
+        a = {k: (_f32(parts[k]) if parts.get(k) is not None else None)
+             for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        r = {k: _f32(rands[k]) for k in ("x", "y", "z", "w")}
+        sm = np.ascontiguousarray(smask, np.int8)
+        return (len(a["x"]), *(_vp(a[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")), len(r["x"]),
+                *(_vp(r[k]) for k in ("x", "y", "z", "w")), _vp(sm)), sm
+
+    def survey_fields(self, p: Params, parts: dict, rands: dict, smask):
+        """(U1CO ext, DIVERCO ext, MEANDENS, the randoms' grid) in survey mode."""
+        g, _ = grid_setup(p)
+        u1 = np.zeros(g.ne ** 3, np.float32)
+        dv = np.zeros(g.ne ** 3, np.float32)
+        ur = np.zeros(p.nx ** 3, np.float32)
+        md = C.c_float()
+        args, _keep = self._survey_args(parts, rands, smask)
+        pc = p.to_c()
+        self._chk(self.lib.avism_gpu_survey_fields(self.h, C.byref(pc), *args, _vp(u1), _vp(dv), C.byref(md),
+                                                   _vp(ur)))
+        return u1, dv, md.value, ur
+
+    def run_level_survey(self, p: Params, parts: dict, rands: dict, smask, want_marca=False, capacity=None):
+        g, _ = grid_setup(p)
+        cap = int(capacity or p.nvoid_max)
+        cubes = Cubes(cap)
+        vo = Voids(cap, g.ne if want_marca else None)
+        nv, md = C.c_int32(), C.c_float()
+        pc = p.to_c()
+        pc.nvoid_max = min(p.nvoid_max, cap)
+        args, _keep = self._survey_args(parts, rands, smask)
+        self._chk(self.lib.avism_gpu_run_level_survey(self.h, C.byref(pc), *args, C.byref(cubes.c), C.byref(nv),
+                                                      C.byref(vo.c), C.byref(md)))
+        return dict(cubes=cubes.view(nv.value), nvoid=nv.value, cat=vo.view(nv.value), meandens=md.value)
+
     # ---- whole level ------------------------------------------------------------
     def run_level(self, p: Params, parts: dict, want_marca=False, want_cubes=True, capacity=None):
         g, _ = grid_setup(p)

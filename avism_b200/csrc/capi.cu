@@ -588,6 +588,109 @@ int avism_gpu_run_sublevel(avism_gpu_ctx *ctx, const avism_params *p, int64_t n,
     });
 }
 
+// ---- survey mode (FLAG_SURVEY = 1, src/avism.f90:1420-1596) ------------------
+// the survey mask on the ext grid: the inner cells' values, 0 on the ghost shell
+// (SMASK = 0 before the inner cells are set, src/avism.f90:867-869)
+__global__ void k_smask_ext(int nx, int low1, int ne, const int8_t *__restrict__ inner, int8_t *__restrict__ ext) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)ne * ne * ne) return;
+    const int i = (int)(e % ne) + low1, j = (int)((e / ne) % ne) + low1, k = (int)(e / ((int64_t)ne * ne)) + low1;
+    const bool in = i >= 1 && i <= nx && j >= 1 && j <= nx && k >= 1 && k <= nx;
+    ext[e] = in ? inner[(int64_t)(i - 1) + (int64_t)nx * ((int64_t)(j - 1) + (int64_t)nx * (k - 1))] : (int8_t)0;
+}
+
+namespace {
+
+// tracers and randoms to the grid, the D/(alpha R) contrast and the divergence,
+// into the inner U1CO / DIVER buffers; returns MEANDENS
+float survey_fields_dev(Ctx &c, const avism_params *p, const Level &L, int64_t n, const float *x, const float *y,
+                        const float *z, const float *vx, const float *vy, const float *vz, const float *m,
+                        int64_t nrand, const float *rx, const float *ry, const float *rz, const float *rw,
+                        const int8_t *smask, float **u1_out, float **dv_out, const int8_t **smask_out) {
+    const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
+    AV_CHECK(smask && nrand >= 1 && rx && ry && rz && rw, AVISM_ERR_ARG, "survey: mask and randoms required");
+    const int8_t *sm = (const int8_t *)to_device(c, B_SMASK_IN, smask, (size_t)nc);
+    // tracers (with the mask)
+    P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, sm, false);
+    particles_to_grid(c, p, L, a);
+    float *u1 = c.get_t<float>(B_U1CO, nc), *dv = c.get_t<float>(B_DIVER, nc);
+    rho_inner(c, L, a.u_mass, u1);
+    if (!p->no_velocities) divergence_inner(c, p, L, u1, a.u2, a.u3, a.u4, dv);
+    c.mark("survey_tracers");
+    // randoms: no velocities; H_DISTANCE and FILL_H_ZEROS with
+    // KNEIGHBOURS2 = MIN(8*KNEIGHBOURS, 256) (src/avism.f90:1516), or TSC
+    avism_params pr = *p;
+    pr.no_velocities = 1;
+    pr.kneighbours = std::min(8 * p->kneighbours, 256);
+    pr.learned = p->learned == 1 ? 2 : p->learned;     // the network predicts K = KNEIGHBOURS radii
+    P2G ar = p2g_args(c, &pr, L, nrand, rx, ry, rz, nullptr, nullptr, nullptr, rw, sm, false);
+    ar.u_mass = c.get_t<float>(B_U1RAND, nc);
+    particles_to_grid(c, &pr, L, ar);
+    c.mark("survey_randoms");
+    const float meandens = survey_contrast(c, L, sm, ar.u_mass, u1);
+    if (p->no_velocities) divergence_inner(c, p, L, u1, nullptr, nullptr, nullptr, dv);
+    c.mark("survey_contrast");
+    *u1_out = u1;
+    *dv_out = dv;
+    *smask_out = sm;
+    return meandens;
+}
+
+}  // namespace
+
+int avism_gpu_survey_fields(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x, const float *y,
+                            const float *z, const float *vx, const float *vy, const float *vz, const float *m,
+                            int64_t nrand, const float *rx, const float *ry, const float *rz, const float *rw,
+                            const int8_t *smask, float *u1co_ext, float *diverco_ext, float *meandens,
+                            float *u1rand) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        Level L = make_level(p);
+        const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
+        const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
+        float *u1, *dv;
+        const int8_t *sm;
+        const float md = survey_fields_dev(c, p, L, n, x, y, z, vx, vy, vz, m, nrand, rx, ry, rz, rw, smask, &u1, &dv,
+                                           &sm);
+        float *e1 = is_device_ptr(u1co_ext) ? u1co_ext : c.get_t<float>(B_U1EXT, ne3);
+        float *e2 = is_device_ptr(diverco_ext) ? diverco_ext : c.get_t<float>(B_DVEXT, ne3);
+        if (u1co_ext) { ext_copy(c, L, u1, e1); from_device(c, u1co_ext, e1, sizeof(float) * (size_t)ne3); }
+        if (diverco_ext) { ext_copy(c, L, dv, e2); from_device(c, diverco_ext, e2, sizeof(float) * (size_t)ne3); }
+        from_device(c, u1rand, c.buf[B_U1RAND], sizeof(float) * (size_t)nc);
+        c.sync();
+        if (meandens) *meandens = md;
+    });
+}
+
+int avism_gpu_run_level_survey(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x, const float *y,
+                               const float *z, const float *vx, const float *vy, const float *vz, const float *m,
+                               int64_t nrand, const float *rx, const float *ry, const float *rz, const float *rw,
+                               const int8_t *smask, avism_cubes *cubes, int32_t *nvoid, avism_voids *voids,
+                               float *meandens) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        AV_CHECK(nvoid && voids, AVISM_ERR_ARG, "run_level_survey: null argument");
+        Level L = make_level(p);
+        const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
+        float *u1, *dv;
+        const int8_t *sm;
+        const float md = survey_fields_dev(c, p, L, n, x, y, z, vx, vy, vz, m, nrand, rx, ry, rz, rw, smask, &u1, &dv,
+                                           &sm);
+        int8_t *sme = c.get_t<int8_t>(B_SMASK, (size_t)ne3);
+        ++c.launches, k_smask_ext<<<grid_for(ne3, 256), 256, 0, c.stream>>>(L.g.nx, L.g.low1, L.g.ne, sm, sme);
+        AV_CUDA(cudaGetLastError());
+        CubesDev cd{};
+        const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, sme, nullptr, nullptr, 0, cd, nullptr);
+        HostCubes hc(c, cd, nv);
+        if (cubes) cubes_out(c, cd, nv, cubes);
+        c.mark("cubes_d2h");
+        merge_post(c, p, L, nv, &hc.v, u1, md, voids, voids->marca);
+        c.mark("catalogue_d2h");
+        *nvoid = nv;
+        if (meandens) *meandens = md;
+    });
+}
+
 int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x, const float *y,
                         const float *z, const float *vx, const float *vy, const float *vz, const float *m,
                         avism_cubes *cubes, int32_t *nvoid, avism_voids *voids, float *meandens) {

@@ -63,6 +63,7 @@ enum BufId : int {
     B_PER_CELL, B_PER_LAB, B_PER_PAIRS,            // VOID_PERIODIC: centre cells, their labels, label-map updates
     B_LL_CELL, B_LL_CELL2, B_LL_KEY, B_LL_KEY2,    // cells of every void in K, J, I order (sorted by label)
     B_LL_CNT, B_LL_OFF, B_LL_SUM,                  // their counts, offsets and per-void REAL*4 sums
+    B_U1RAND, B_SMASK_IN,                          // survey: the randoms' grid, the inner mask
     B_NUM
 };
 
@@ -228,6 +229,12 @@ FieldsOut fields_inner(Ctx &c, const avism_params *p, const Level &L, const floa
                        const float *u2, const float *u3, const float *u4, float *u1co_in,
                        float *diver_in);
 void ext_copy(Ctx &c, const Level &L, const float *inner, float *ext);
+// the pieces of fields_inner: U1CO = U1DMCO*ROTE on the inner grid, the divergence
+// (velocities or the linear theory), and survey mode's D/(alpha R) contrast
+void rho_inner(Ctx &c, const Level &L, const float *u_mass, float *u1co_in);
+void divergence_inner(Ctx &c, const avism_params *p, const Level &L, const float *u1co_in, const float *u2,
+                      const float *u3, const float *u4, float *diver_in);
+float survey_contrast(Ctx &c, const Level &L, const int8_t *smask, const float *u1rand, float *u1co_in);
 
 // flags on the ext grid from inner (wrapped) fields, or from given ext fields.
 void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, const float *dv,

@@ -204,29 +204,24 @@ static bool diver_tma_ok(int nx, const float *a, const float *b, const float *c)
     return nx % DV_TX == 0 && nx % DV_TY == 0 && nx % DV_TZ == 0 && al(a) && al(b) && al(c);
 }
 
-FieldsOut fields_inner(Ctx &c, const avism_params *p, const Level &L, const float *u_mass,
-                       const float *u2, const float *u3, const float *u4, float *u1co_in,
-                       float *diver_in) {
-    const int nx = L.g.nx;
-    const int64_t nc = (int64_t)nx * nx * nx;
+// U1CO = (U1DMCO / (DXX*DYY*DZZ*RETE**3) / ROTE) * ROTE (src/avism.f90:1249-1250, 1386)
+void rho_inner(Ctx &c, const Level &L, const float *u_mass, float *u1co_in) {
+    const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
     const float dx = L.g.dx;
     const float vol = ((dx * dx) * dx) * ((L.g.rete * L.g.rete) * L.g.rete);
     ++c.launches, k_rho<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u_mass, vol, L.g.rote, u1co_in);
-    double *sum_d = c.get_t<double>(B_RED1, 1);
-    cub::TransformInputIterator<double, ToDouble, const float *> it(u1co_in, ToDouble());
-    size_t tmp = 0;
-    AV_CUDA(cub::DeviceReduce::Sum(nullptr, tmp, it, sum_d, (int)nc, c.stream));
-    void *t = c.get(B_CUB_TMP, tmp);
-    AV_CUDA(cub::DeviceReduce::Sum(t, tmp, it, sum_d, (int)nc, c.stream));
-    double sum = 0.0;
-    AV_CUDA(cudaMemcpyAsync(&sum, sum_d, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    c.sync();
-    const float mean = (float)(sum / (double)nc);
-    ++c.launches, k_div_scalar<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u1co_in, mean);
-    c.mark("normalise");
+    AV_CUDA(cudaGetLastError());
+}
+
+// DIVERCO from the velocity grids (DIVER_UNIFORM), or without velocities the
+// linear-theory -OMEGA0**(0.6)*RETE*HTE*(U1CO - 1.0) (src/avism.f90:1647-1650),
+// the REAL*4 coefficient with the host libm's powf, as the reference's
+void divergence_inner(Ctx &c, const avism_params *p, const Level &L, const float *u1co_in, const float *u2,
+                      const float *u3, const float *u4, float *diver_in) {
+    const int nx = L.g.nx;
+    const int64_t nc = (int64_t)nx * nx * nx;
+    const float dx = L.g.dx;
     if (p->no_velocities) {
-        // DIVERCO = -OMEGA0**(0.6)*RETE*HTE*(U1CO - 1.0) (src/avism.f90:1647-1650),
-        // the REAL*4 coefficient with the host libm's powf, as the reference's
         const float coef = (::powf(p->omega0, 0.6f) * L.g.rete) * L.g.hte;
         ++c.launches, k_lin_div<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u1co_in, coef, diver_in);
     } else if (diver_tma_ok(nx, u2, u3, u4)) {
@@ -247,10 +242,122 @@ FieldsOut fields_inner(Ctx &c, const avism_params *p, const Level &L, const floa
         ++c.launches, k_diver<<<grid_for(nc, 256), 256, 0, c.stream>>>(nx, dx, p->periodic, u2, u3, u4, diver_in);
     }
     AV_CUDA(cudaGetLastError());
+}
+
+FieldsOut fields_inner(Ctx &c, const avism_params *p, const Level &L, const float *u_mass,
+                       const float *u2, const float *u3, const float *u4, float *u1co_in,
+                       float *diver_in) {
+    const int nx = L.g.nx;
+    const int64_t nc = (int64_t)nx * nx * nx;
+    rho_inner(c, L, u_mass, u1co_in);
+    double *sum_d = c.get_t<double>(B_RED1, 1);
+    cub::TransformInputIterator<double, ToDouble, const float *> it(u1co_in, ToDouble());
+    size_t tmp = 0;
+    AV_CUDA(cub::DeviceReduce::Sum(nullptr, tmp, it, sum_d, (int)nc, c.stream));
+    void *t = c.get(B_CUB_TMP, tmp);
+    AV_CUDA(cub::DeviceReduce::Sum(t, tmp, it, sum_d, (int)nc, c.stream));
+    double sum = 0.0;
+    AV_CUDA(cudaMemcpyAsync(&sum, sum_d, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    const float mean = (float)(sum / (double)nc);
+    ++c.launches, k_div_scalar<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u1co_in, mean);
+    c.mark("normalise");
+    divergence_inner(c, p, L, u1co_in, u2, u3, u4, diver_in);
     FieldsOut o;
     const float ul3 = (UL_F * UL_F) * UL_F;
     o.meandens = mean * (UM_F / ul3);
     return o;
+}
+
+// ---- survey mode: the D/(alpha R) contrast (src/avism.f90:1527-1578) ----------
+// DSUM, RSUM and the MEANRATIO sum are REAL*8 sums per x-row (sequential in i),
+// the rows of a plane summed in j order, the planes in k order: fixed, so ALPHA
+// and the ratios do not depend on thread timing (the reference's DSUM / RSUM
+// are an OpenMP reduction; its MEANRATIO a serial SUM).
+__global__ void k_row_sums(int nx, const float *__restrict__ a, const int8_t *__restrict__ smask, int positive,
+                           double *__restrict__ rows) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= (int64_t)nx * nx) return;
+    const float *ar = a + r * nx;
+    const int8_t *sr = smask + r * nx;
+    double s = 0.0;
+    for (int i = 0; i < nx; i++) {
+        const int8_t m = sr[i];
+        if (positive ? m > 0 : m != 0) s = s + (double)ar[i];
+    }
+    rows[r] = s;
+}
+__global__ void k_plane_sums(int nx, const double *__restrict__ rows, double *__restrict__ planes) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nx) return;
+    double s = 0.0;
+    for (int j = 0; j < nx; j++) s = s + rows[(int64_t)k * nx + j];
+    planes[k] = s;
+}
+__global__ void k_total_sum(int nx, const double *__restrict__ planes, double *__restrict__ out) {
+    double s = 0.0;
+    for (int k = 0; k < nx; k++) s = s + planes[k];
+    *out = s;
+}
+// BASS8 = U1CO/(ALPHA*U1RAND) (or the floor where U1RAND = 0), floored at 1e-4,
+// clamped at 1000, in REAL*8; stored as REAL*4 (src/avism.f90:1543-1566)
+__global__ void k_survey_ratio(int64_t nc, float *__restrict__ u1, const float *__restrict__ ur,
+                               const int8_t *__restrict__ smask, double alpha) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc || smask[c] == 0) return;
+    const double floor8 = (double)1e-4f, max8 = (double)1000.0f;
+    double b = (double)ur[c] > 0.0 ? __ddiv_rn((double)u1[c], __dmul_rn(alpha, (double)ur[c])) : floor8;
+    b = fmax(floor8, b);
+    b = fmin(max8, b);
+    u1[c] = (float)b;
+}
+// WHERE (SMASK > 0) U1CO = U1CO / MEANRATIO
+__global__ void k_survey_scale(int64_t nc, float *__restrict__ u1, const int8_t *__restrict__ smask, float meanratio) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nc && smask[c] > 0) u1[c] = __fdiv_rn(u1[c], meanratio);
+}
+// COUNT(SMASK > 0)
+__global__ void k_count_positive(int64_t nc, const int8_t *__restrict__ smask, unsigned long long *__restrict__ count) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned b = __ballot_sync(0xffffffffu, c < nc && smask[c] > 0);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(count, (unsigned long long)__popc(b));
+}
+
+static double blocked_sum(Ctx &c, int nx, const float *a, const int8_t *smask, int positive) {
+    double *rows = c.get_t<double>(B_RED0, (size_t)nx * nx + nx + 1);
+    double *planes = rows + (size_t)nx * nx, *tot = planes + nx;
+    ++c.launches, k_row_sums<<<grid_for((int64_t)nx * nx, 128), 128, 0, c.stream>>>(nx, a, smask, positive, rows);
+    ++c.launches, k_plane_sums<<<grid_for(nx, 128), 128, 0, c.stream>>>(nx, rows, planes);
+    ++c.launches, k_total_sum<<<1, 1, 0, c.stream>>>(nx, planes, tot);
+    AV_CUDA(cudaGetLastError());
+    double h = 0.0;
+    AV_CUDA(cudaMemcpyAsync(&h, tot, sizeof h, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    return h;
+}
+
+// the inner U1CO (rho/rho_B * ROTE) becomes D/(alpha R), mean 1 over SMASK > 0;
+// returns MEANDENS = ROTE * (UM / UL**3)
+float survey_contrast(Ctx &c, const Level &L, const int8_t *smask, const float *u1rand, float *u1co_in) {
+    const int nx = L.g.nx;
+    const int64_t nc = (int64_t)nx * nx * nx;
+    const double dsum = blocked_sum(c, nx, u1co_in, smask, 0);
+    const double rsum = blocked_sum(c, nx, u1rand, smask, 0);
+    const double alpha = dsum / rsum;
+    ++c.launches, k_survey_ratio<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u1co_in, u1rand, smask, alpha);
+    AV_CUDA(cudaGetLastError());
+    unsigned long long *cnt = c.get_t<unsigned long long>(B_RED2, 1);
+    AV_CUDA(cudaMemsetAsync(cnt, 0, sizeof *cnt, c.stream));
+    ++c.launches, k_count_positive<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, smask, cnt);
+    unsigned long long count = 0;
+    AV_CUDA(cudaMemcpyAsync(&count, cnt, sizeof count, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    AV_CHECK(count > 0, AVISM_ERR_ARG, "survey: the mask has no observed cell (SMASK > 0)");
+    const float meanratio = (float)(blocked_sum(c, nx, u1co_in, smask, 1) / (double)count);
+    ++c.launches, k_survey_scale<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u1co_in, smask, meanratio);
+    AV_CUDA(cudaGetLastError());
+    const float ul3 = (UL_F * UL_F) * UL_F;
+    return L.g.rote * (UM_F / ul3);
 }
 
 __global__ void k_ext_copy(int nx, int low1, int ne, const float *__restrict__ inner, float *__restrict__ ext) {

@@ -234,6 +234,53 @@ def weighted_cone(box=1200.0, ng=128, rmax=600.0, half_angle_deg=60.0, rsel=400.
                 pixel_mask=masked.reshape(npc, npp))
 
 
+def _cone_pixels(pos, cmin, npc, npp):
+    r = np.linalg.norm(pos, axis=1)
+    ct = np.where(r > 0, pos[:, 2] / np.maximum(r, 1e-30), 1.0)
+    phi = np.arctan2(pos[:, 1], pos[:, 0])
+    pc = np.clip(((ct - cmin) / (1 - cmin) * npc).astype(int), 0, npc - 1)
+    pp = np.clip(((phi + np.pi) / (2 * np.pi) * npp).astype(int), 0, npp - 1)
+    return r, ct, pc * npp + pp
+
+
+def cone_randoms(n, pixel_mask, box=1200.0, rmax=600.0, half_angle_deg=60.0, rsel=400.0, weight=1e12, seed=2005):
+    """Randoms of the survey geometry of ``weighted_cone``: uniform in volume
+    inside the cone, thinned by the same radial selection exp(-(r/rsel)^2) and
+    angular mask (``pixel_mask`` of weighted_cone), all with the same weight
+    [Msun].  Returns x, y, z, w."""
+    rng = np.random.default_rng(seed)
+    cmin = np.cos(np.radians(half_angle_deg))
+    npc, npp = pixel_mask.shape
+    out = np.empty((0, 3))
+    while len(out) < n:
+        m = 4 * (n - len(out)) + 1024
+        u = rng.random(m)
+        r = rmax * u ** (1 / 3)
+        ct = cmin + (1 - cmin) * rng.random(m)
+        phi = rng.uniform(-np.pi, np.pi, m)
+        st = np.sqrt(1 - ct ** 2)
+        q = np.stack([r * st * np.cos(phi), r * st * np.sin(phi), r * ct], 1)
+        keep = rng.random(m) < np.exp(-(r / rsel) ** 2)
+        _, _, pix = _cone_pixels(q, cmin, npc, npp)
+        keep &= ~pixel_mask.ravel()[pix]
+        out = np.concatenate([out, q[keep]])
+    out = np.clip(out[:n], -box / 2, box / 2).astype(np.float32)
+    return dict(x=out[:, 0].copy(), y=out[:, 1].copy(), z=out[:, 2].copy(), w=np.full(n, weight, np.float32))
+
+
+def cone_mask(nx, pixel_mask, box=1200.0, rmax=600.0, half_angle_deg=60.0):
+    """The survey mask on an nx^3 grid (column-major, x fastest): 1 for cells
+    whose centre lies inside the cone, within rmax and in an unmasked pixel."""
+    h = box / nx
+    c1 = -box / 2 + h / 2 + np.arange(nx) * h
+    Z, Y, X = np.meshgrid(c1, c1, c1, indexing="ij")
+    pos = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    cmin = np.cos(np.radians(half_angle_deg))
+    r, ct, pix = _cone_pixels(pos, cmin, *pixel_mask.shape)
+    inside = (r <= rmax) & (ct >= cmin) & ~pixel_mask.ravel()[pix]
+    return inside.astype(np.int8)
+
+
 def add_clumps(parts: dict, centres, radius, count, seed=0):
     """``parts`` with a clump of ``count`` particles uniform in a ball of
     ``radius`` around each centre (velocities of the clump's centre particle,

@@ -267,6 +267,35 @@ int avism_gpu_run_sublevel(avism_gpu_ctx *ctx, const avism_params *p, int64_t n,
                            const int32_t *marcap_ext, const float *reqp, int32_t nreqp, avism_cubes *cubes,
                            int32_t *nvoid, avism_voids *voids, float *meandens);
 
+/* ---- survey mode (FLAG_SURVEY = 1): replaces src/avism.f90:1420-1596.  The
+ *      tracers (x..m, masses as weights; velocities nullable with
+ *      no_velocities = 1) and the randoms (rx, ry, rz, weights rw, in the units
+ *      READ_BINARY_PART_1 leaves: weights / UM) go to the grid with the survey
+ *      mask smask (inner NX^3 int8: 0 unobserved; avism_io_read_mask).  The
+ *      randoms use the same interpolation, SPH with their own kNN of
+ *      KNEIGHBOURS2 = MIN(8*KNEIGHBOURS, 256) neighbours (H_DISTANCE,
+ *      FILL_H_ZEROS, DDENS_INTERP_SPH) or TSC.  The contrast is D/(alpha R):
+ *      alpha = DSUM/RSUM over the observed cells, the ratio floored at 1e-4 and
+ *      clamped at 1000, divided by its mean over SMASK > 0; MEANDENS is the
+ *      background density.  Without velocities the divergence is the linear
+ *      theory one.  DSUM, RSUM and the mean ratio are REAL*8 sums per x-row,
+ *      rows in j order, planes in k order (the reference's OpenMP reduction
+ *      leaves the order open).
+ *      avism_gpu_survey_fields returns the ext grids U1CO and DIVERCO (as
+ *      avism_gpu_fields) and the randoms' mass grid u1rand (inner, nullable);
+ *      avism_gpu_run_level_survey runs the whole level with the mask on the ext
+ *      grid (0 on the ghost shell) for MARK_ALL and the growth.                  */
+int avism_gpu_survey_fields(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x, const float *y,
+                            const float *z, const float *vx, const float *vy, const float *vz, const float *m,
+                            int64_t nrand, const float *rx, const float *ry, const float *rz, const float *rw,
+                            const int8_t *smask, float *u1co_ext, float *diverco_ext, float *meandens,
+                            float *u1rand);
+int avism_gpu_run_level_survey(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x, const float *y,
+                               const float *z, const float *vx, const float *vy, const float *vz, const float *m,
+                               int64_t nrand, const float *rx, const float *ry, const float *rz, const float *rw,
+                               const int8_t *smask, avism_cubes *cubes, int32_t *nvoid, avism_voids *voids,
+                               float *meandens);
+
 /* ---- kNN without allocation.  No reference counterpart: an extra form of
  *      avism_gpu_knn (same neighbours, same distances, bit for bit) for callers
  *      that cannot allocate device memory -- a host whose device memory is

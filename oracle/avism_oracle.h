@@ -102,6 +102,16 @@ int orc_run_level(const avism_params *p, int64_t n, const float *x, const float 
                   const float *m, avism_cubes *cubes, int32_t *nvoid, avism_voids *voids,
                   float *meandens, float *u1co_ext, float *diverco_ext);
 
+/* survey mode (src/avism.f90:1420-1596): the D/(alpha R) contrast of the
+ * inner U1CO (rho/rho_B * ROTE on entry) from the randoms' grid u1rand, and
+ * the whole fields stage with tracers, randoms and the mask */
+int orc_survey_contrast(const avism_params *p, const avism_grid *g, const int8_t *smask, const float *u1rand,
+                        float *u1, float *meandens);
+int orc_survey_fields(const avism_params *p, int64_t n, const float *x, const float *y, const float *z,
+                      const float *vx, const float *vy, const float *vz, const float *m, int64_t nrand,
+                      const float *rx, const float *ry, const float *rz, const float *rw, const int8_t *smask,
+                      float *u1co_ext, float *diverco_ext, float *meandens, float *u1rand_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -117,6 +117,50 @@ def fields(p: Params, u_mass, u2, u3, u4):
     return u1, dv, md.value
 
 
+def survey_fields(p: Params, parts: dict, rands: dict, smask):
+    """Survey mode (src/avism.f90:1420-1596): tracers and randoms to the grid,
+    the D/(alpha R) contrast and the divergence; (U1CO ext, DIVERCO ext,
+    MEANDENS, the randoms' grid)."""
+    g, _ = grid_setup(p)
+    n = len(parts["x"])
+    zero = np.zeros(n, np.float32)
+    a = [_f32(parts[k]) if parts.get(k) is not None else zero for k in ("x", "y", "z", "vx", "vy", "vz", "m")]
+    r = [_f32(rands[k]) for k in ("x", "y", "z", "w")]
+    sm = np.ascontiguousarray(smask, np.int8)
+    ne3 = g.ne ** 3
+    u1 = np.zeros(ne3, np.float32)
+    dv = np.zeros(ne3, np.float32)
+    ur = np.zeros(p.nx ** 3, np.float32)
+    md = C.c_float()
+    f = lib().orc_survey_fields
+    f.argtypes = [C.c_void_p, C.c_int64] + [C.POINTER(C.c_float)] * 7 + [C.c_int64] + \
+        [C.POINTER(C.c_float)] * 4 + [C.c_void_p] + [C.POINTER(C.c_float)] * 3 + [C.POINTER(C.c_float)]
+    pc = p.to_c()
+    _chk(f(C.byref(pc), n, *(ptr(v, C.c_float) for v in a), len(r[0]), *(ptr(v, C.c_float) for v in r),
+           sm.ctypes.data, ptr(u1, C.c_float), ptr(dv, C.c_float), C.byref(md), ptr(ur, C.c_float)))
+    return u1, dv, md.value, ur
+
+
+def smask_ext(p: Params, smask):
+    """The survey mask on the ext grid: the inner cells' values, 0 on the ghost
+    shell (SMASK = 0 before the inner cells are set, src/avism.f90:867-869)."""
+    g, _ = grid_setup(p)
+    ne, nx = g.ne, g.nx
+    out = np.zeros((ne, ne, ne), np.int8)
+    o = 1 - g.low1
+    out[o:o + nx, o:o + nx, o:o + nx] = np.asarray(smask, np.int8).reshape(nx, nx, nx)
+    return out.ravel()
+
+
+def run_level_survey(p: Params, parts: dict, rands: dict, smask):
+    """particles + randoms -> catalogue in survey mode on the CPU."""
+    u1, dv, md, ur = survey_fields(p, parts, rands, smask)
+    se = smask_ext(p, smask)
+    vf = voidfind(p, u1, dv, smask_ext=se)
+    cat = merge_post(p, vf["nvoid"], vf["cubes"], u1, md)
+    return dict(u1co=u1, diverco=dv, meandens=md, u1rand=ur, vf=vf, cat=cat, smask_ext=se)
+
+
 def diver_uniform(nx, dx, v2, v3, v4, periodic):
     out = np.zeros(nx ** 3, np.float32)
     f = lib().orc_diver_uniform
