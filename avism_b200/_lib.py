@@ -40,6 +40,8 @@ SIGNATURES = {
                                            C.c_uint32, _c_void, _c_void]),
     "avism_gpu_next_level": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 5),
     "avism_gpu_run_sublevel": (C.c_int, [_c_void, _c_void, _i64] + [_c_void] * 9 + [_i32] + [_c_void] * 4),
+    "avism_gpu_grid_fields": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 7),
+    "avism_gpu_run_level_grid": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 8),
     "avism_gpu_survey_fields": (C.c_int, [_c_void, _c_void, _i64] + [_c_void] * 7 + [_i64] + [_c_void] * 9),
     "avism_gpu_run_level_survey": (C.c_int, [_c_void, _c_void, _i64] + [_c_void] * 7 + [_i64] + [_c_void] * 9),
     "avism_gpu_knn_noalloc": (C.c_int, [C.c_int, _c_void, _i64, _c_void, _c_void, _c_void, _f32, _i64,

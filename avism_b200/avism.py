@@ -361,6 +361,33 @@ class AvismGPU:
             C.byref(vo.c), C.byref(md)))
         return dict(cubes=cubes.view(nv.value), nvoid=nv.value, cat=vo.view(nv.value), meandens=md.value)
 
+    # ---- grid input (FLAG_DATA = 2, src/avism.f90:1316-1362) --------------------------
+    def grid_fields(self, p: Params, nhy, u1g, u2g, u3g, u4g):
+        """(U1CO ext, DIVERCO ext, MEANDENS) of the level from the input grids
+        (U1G = delta + 1, velocities / UV, nhy^3)."""
+        g, _ = grid_setup(p)
+        u1 = np.zeros(g.ne ** 3, np.float32)
+        dv = np.zeros(g.ne ** 3, np.float32)
+        md = C.c_float()
+        pc = p.to_c()
+        self._chk(self.lib.avism_gpu_grid_fields(self.h, C.byref(pc), int(nhy),
+                                                 *(_vp(_f32(a)) for a in (u1g, u2g, u3g, u4g)), _vp(u1), _vp(dv),
+                                                 C.byref(md)))
+        return u1, dv, md.value
+
+    def run_level_grid(self, p: Params, nhy, u1g, u2g, u3g, u4g, want_marca=False, capacity=None):
+        g, _ = grid_setup(p)
+        cap = int(capacity or p.nvoid_max)
+        cubes = Cubes(cap)
+        vo = Voids(cap, g.ne if want_marca else None)
+        nv, md = C.c_int32(), C.c_float()
+        pc = p.to_c()
+        pc.nvoid_max = min(p.nvoid_max, cap)
+        self._chk(self.lib.avism_gpu_run_level_grid(self.h, C.byref(pc), int(nhy),
+                                                    *(_vp(_f32(a)) for a in (u1g, u2g, u3g, u4g)),
+                                                    C.byref(cubes.c), C.byref(nv), C.byref(vo.c), C.byref(md)))
+        return dict(cubes=cubes.view(nv.value), nvoid=nv.value, cat=vo.view(nv.value), meandens=md.value)
+
     # ---- survey mode (src/avism.f90:1420-1596) -------------------------------------
     def _survey_args(self, parts, rands, smask):
         a = {k: (_f32(parts[k]) if parts.get(k) is not None else None)

@@ -691,6 +691,72 @@ int avism_gpu_run_level_survey(avism_gpu_ctx *ctx, const avism_params *p, int64_
     });
 }
 
+// ---- grid input (FLAG_DATA = 2, READ_BINARY_GRID): src/avism.f90:1316-1362 --------
+namespace {
+float grid_fields_dev(Ctx &c, const avism_params *p, const Level &L, int32_t nhy, const float *u1g,
+                      const float *u2g, const float *u3g, const float *u4g, float **u1_out, float **dv_out) {
+    AV_CHECK(u1g && u2g && u3g && u4g && nhy >= 4, AVISM_ERR_ARG, "grid input: four grids of nhy >= 4 required");
+    AV_CHECK(p->level <= 0, AVISM_ERR_UNSUPPORTED, "LEVEL > 0 FOR BIN_GRID NOT IMPLEMENTED YET");
+    AV_CHECK((int64_t)p->nx << (-p->level) == (int64_t)nhy, AVISM_ERR_ARG,
+             "grid input: params.nx must be nhy * 2^level (level <= 0)");
+    const int64_t n0 = (int64_t)nhy * nhy * nhy;
+    const float *g[4];
+    const float *src[4] = {u1g, u2g, u3g, u4g};
+    float *buf = nullptr;
+    for (int q = 0; q < 4; q++) {
+        if (is_device_ptr(src[q])) { g[q] = src[q]; continue; }
+        if (!buf) buf = c.get_t<float>(B_GRID_IN, 4 * (size_t)n0);
+        AV_CUDA(cudaMemcpyAsync(buf + q * n0, src[q], sizeof(float) * (size_t)n0, cudaMemcpyHostToDevice, c.stream));
+        g[q] = buf + q * n0;
+    }
+    const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
+    float *u1 = c.get_t<float>(B_U1CO, nc), *dv = c.get_t<float>(B_DIVER, nc);
+    const float md = grid_fields_inner(c, p, L, nhy, g[0], g[1], g[2], g[3], u1, dv);
+    *u1_out = u1;
+    *dv_out = dv;
+    return md;
+}
+}  // namespace
+
+int avism_gpu_grid_fields(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g, const float *u2g,
+                          const float *u3g, const float *u4g, float *u1co_ext, float *diverco_ext, float *meandens) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        Level L = make_level(p);
+        const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
+        float *u1, *dv;
+        const float md = grid_fields_dev(c, p, L, nhy, u1g, u2g, u3g, u4g, &u1, &dv);
+        float *e1 = is_device_ptr(u1co_ext) ? u1co_ext : c.get_t<float>(B_U1EXT, ne3);
+        float *e2 = is_device_ptr(diverco_ext) ? diverco_ext : c.get_t<float>(B_DVEXT, ne3);
+        if (u1co_ext) { ext_copy(c, L, u1, e1); from_device(c, u1co_ext, e1, sizeof(float) * (size_t)ne3); }
+        if (diverco_ext) { ext_copy(c, L, dv, e2); from_device(c, diverco_ext, e2, sizeof(float) * (size_t)ne3); }
+        c.sync();
+        if (meandens) *meandens = md;
+    });
+}
+
+int avism_gpu_run_level_grid(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g,
+                             const float *u2g, const float *u3g, const float *u4g, avism_cubes *cubes,
+                             int32_t *nvoid, avism_voids *voids, float *meandens) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        AV_CHECK(nvoid && voids, AVISM_ERR_ARG, "run_level_grid: null argument");
+        Level L = make_level(p);
+        float *u1, *dv;
+        const float md = grid_fields_dev(c, p, L, nhy, u1g, u2g, u3g, u4g, &u1, &dv);
+        c.mark("divergence");
+        CubesDev cd{};
+        const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, nullptr, nullptr, 0, cd, nullptr);
+        HostCubes hc(c, cd, nv);
+        if (cubes) cubes_out(c, cd, nv, cubes);
+        c.mark("cubes_d2h");
+        merge_post(c, p, L, nv, &hc.v, u1, md, voids, voids->marca);
+        c.mark("catalogue_d2h");
+        *nvoid = nv;
+        if (meandens) *meandens = md;
+    });
+}
+
 int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x, const float *y,
                         const float *z, const float *vx, const float *vy, const float *vz, const float *m,
                         avism_cubes *cubes, int32_t *nvoid, avism_voids *voids, float *meandens) {

@@ -64,6 +64,7 @@ enum BufId : int {
     B_LL_CELL, B_LL_CELL2, B_LL_KEY, B_LL_KEY2,    // cells of every void in K, J, I order (sorted by label)
     B_LL_CNT, B_LL_OFF, B_LL_SUM,                  // their counts, offsets and per-void REAL*4 sums
     B_U1RAND, B_SMASK_IN,                          // survey: the randoms' grid, the inner mask
+    B_GRID_IN,                                     // grid input: the four input grids
     B_NUM
 };
 
@@ -235,6 +236,9 @@ void rho_inner(Ctx &c, const Level &L, const float *u_mass, float *u1co_in);
 void divergence_inner(Ctx &c, const avism_params *p, const Level &L, const float *u1co_in, const float *u2,
                       const float *u3, const float *u4, float *diver_in);
 float survey_contrast(Ctx &c, const Level &L, const int8_t *smask, const float *u1rand, float *u1co_in);
+// grid input: U1CO, DIVER and MEANDENS of the level from the input grids (NHY^3)
+float grid_fields_inner(Ctx &c, const avism_params *p, const Level &L, int nhy, const float *u1g, const float *u2g,
+                        const float *u3g, const float *u4g, float *u1co_in, float *diver_in);
 
 // flags on the ext grid from inner (wrapped) fields, or from given ext fields.
 void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, const float *dv,

@@ -360,6 +360,65 @@ float survey_contrast(Ctx &c, const Level &L, const int8_t *smask, const float *
     return L.g.rote * (UM_F / ul3);
 }
 
+// ---- grid input (FLAG_DATA = 2, src/avism.f90:1316-1362) ----------------------
+// SMOOTH_2 (src/amr2uniform.f90:65-120) for levels below 0: every cell of the
+// input grid (NHY^3) adds its value times WEI = (DX0*DY0*DZ0)/(DX*DY*DZ) to the
+// coarse cell INT(((RX-RADX(1))/DX)+0.5)+1.  Here each coarse cell gathers its
+// input cells (a contiguous range per axis, [lo, hi], from the host's map) in
+// the reference's serial K, J, I order, so the REAL*4 sums match.
+__global__ void k_smooth2(int nx, int nhy, const int32_t *__restrict__ lo, const int32_t *__restrict__ hi,
+                          float wei, const float *__restrict__ a, float *__restrict__ out) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int64_t)nx * nx * nx) return;
+    const int i = (int)(c % nx), j = (int)((c / nx) % nx), k = (int)(c / ((int64_t)nx * nx));
+    float s = 0.0f;
+    for (int kk = lo[k]; kk <= hi[k]; kk++)
+        for (int jj = lo[j]; jj <= hi[j]; jj++)
+            for (int ii = lo[i]; ii <= hi[i]; ii++)
+                s = __fadd_rn(s, __fmul_rn(a[(int64_t)ii + (int64_t)nhy * ((int64_t)jj + (int64_t)nhy * kk)], wei));
+    out[c] = s;
+}
+
+// U1CO = U1GCO, the divergence of (U2GCO, U3GCO, U4GCO), MEANDENS = ROTE*(UM/UL**3);
+// u1g..u4g: the input grid (NHY^3, device), the level's grid is p->nx = NHY * 2^IR
+float grid_fields_inner(Ctx &c, const avism_params *p, const Level &L, int nhy, const float *u1g, const float *u2g,
+                        const float *u3g, const float *u4g, float *u1co_in, float *diver_in) {
+    const int nx = L.g.nx;
+    const int64_t nc = (int64_t)nx * nx * nx;
+    const float *g[4] = {u1g, u2g, u3g, u4g};
+    float *co[4] = {u1co_in, c.get_t<float>(B_U2, nc), c.get_t<float>(B_U3, nc), c.get_t<float>(B_U4, nc)};
+    if (nx == nhy) {                                   // IR = 0: U1GCO = U1G, ...
+        for (int q = 0; q < 4; q++)
+            AV_CUDA(cudaMemcpyAsync(co[q], g[q], sizeof(float) * (size_t)nc, cudaMemcpyDeviceToDevice, c.stream));
+    } else {
+        // the input grid's coordinates (MALLA at NHY, src/avism.f90:366-382) and
+        // each input cell's coarse cell on this level
+        avism_params p0 = *p;
+        p0.nx = nhy;
+        const Level L0 = make_level(&p0);
+        const float dx = L.g.dx, dx0 = L0.g.dx, r1 = L.rad_at(1);
+        std::vector<int32_t> lo(nx, INT32_MAX), hi(nx, -1);
+        for (int ii = 1; ii <= nhy; ii++) {
+            const int I = (int)(((L0.rad_at(ii) - r1) / dx) + 0.5f) + 1;
+            AV_CHECK(I >= 1 && I <= nx, AVISM_ERR_ARG, "grid input: an input cell falls outside the level's grid");
+            lo[I - 1] = std::min(lo[I - 1], ii - 1);
+            hi[I - 1] = std::max(hi[I - 1], ii - 1);
+        }
+        const float wei = ((dx0 * dx0) * dx0) / ((dx * dx) * dx);
+        int32_t *d = c.get_t<int32_t>(B_LABMAP, 2 * (size_t)nx);
+        AV_CUDA(cudaMemcpyAsync(d, lo.data(), sizeof(int32_t) * nx, cudaMemcpyHostToDevice, c.stream));
+        AV_CUDA(cudaMemcpyAsync(d + nx, hi.data(), sizeof(int32_t) * nx, cudaMemcpyHostToDevice, c.stream));
+        for (int q = 0; q < 4; q++)
+            ++c.launches, k_smooth2<<<grid_for(nc, 256), 256, 0, c.stream>>>(nx, nhy, d, d + nx, wei, g[q], co[q]);
+        AV_CUDA(cudaGetLastError());
+        c.sync();                                      // lo / hi are host vectors
+    }
+    c.mark("grid_input");
+    divergence_inner(c, p, L, u1co_in, co[1], co[2], co[3], diver_in);
+    const float ul3 = (UL_F * UL_F) * UL_F;
+    return L.g.rote * (UM_F / ul3);
+}
+
 __global__ void k_ext_copy(int nx, int low1, int ne, const float *__restrict__ inner, float *__restrict__ ext) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t ne3 = (int64_t)ne * ne * ne;

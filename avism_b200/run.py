@@ -11,6 +11,13 @@ input, with the particle arrays kept across levels::
 
 Masses and velocities are divided by UM and UV after reading, as
 src/reader.f90:455-458 does.  The work runs on the GPU through the C-ABI.
+
+The reference's other inputs, one level each:
+  * --grid NHY: a READ_BINARY_GRID file (delta and velocities on NHY^3 cells,
+    src/reader.f90:523-552) at the level with --nx = NHY * 2^level, level <= 0;
+  * --mask FILE --randoms FILE: survey mode (FLAG_SURVEY = 1) with the mask and
+    randoms files (src/avism.f90:403-418, 1425-1444); --novel reads the
+    particle file as READ_BINARY_PART_2 (no velocities).
 """
 from __future__ import annotations
 
@@ -67,6 +74,40 @@ def run_iteration(particle_path, p: Params, out_dir, it: int = 1, nlev: int = 1,
     return dict(voids=vp, cubes=cp, map=mp, levels=results)
 
 
+def run_single(path, p: Params, out_dir, it: int = 1, grid_nhy: int = 0, mask=None, randoms=None,
+               novel: bool = False, ncox: int = 0, cubes: bool = False, engine=None) -> dict:
+    """One level from a grid file (grid_nhy > 0) or a survey (mask and randoms
+    files), written as run_iteration writes its levels."""
+    import numpy as np
+    from . import synth
+    from ._abi import UM, UV
+    from .avism import read_grid_file, read_mask_file, read_particle_file_novel, read_randoms_file
+    if engine is None:
+        from .avism import AvismGPU
+        engine = AvismGPU(0)
+    if grid_nhy:
+        g = read_grid_file(path, grid_nhy)
+        p = Params(**{**p.__dict__, "zeta": float(g["zeta"])})
+        # delta -> rho / rho_B, km/s -> c (src/reader.f90:546-550)
+        u1 = (g["u1"] + np.float32(1.0)).astype(np.float32)
+        vs = [(g[k] / np.float32(UV)).astype(np.float32) for k in ("u2", "u3", "u4")]
+        res = engine.run_level_grid(p, grid_nhy, u1, *vs)
+    else:
+        parts = read_particle_file_novel(path) if novel else read_particle_file(path)
+        p = Params(**{**p.__dict__, "zeta": float(parts.pop("zeta")), "no_velocities": int(novel)})
+        parts = synth.to_reader_units(parts) if not novel else {**parts, "m": (parts["m"] / UM).astype(np.float32)}
+        sm, _ = read_mask_file(mask, ncox or p.nx, p.nx)
+        rr = read_randoms_file(randoms)
+        rr["w"] = (rr["w"] / UM).astype(np.float32)            # MASSRAND / UM (src/avism.f90:1440)
+        res = engine.run_level_survey(p, parts, rr, sm)
+    os.makedirs(out_dir, exist_ok=True)
+    vp = os.path.join(out_dir, f"voids{it:05d}")
+    cp = os.path.join(out_dir, f"cubes{it:05d}") if cubes else None
+    write_catalogue_headers(vp, cp, 1, p.level, p.level, p.nx, p.nx, p.nx, p.lado0)
+    append_catalogue_level(vp, p, res, cubes_path=cp)
+    return dict(voids=vp, cubes=cp, levels=[res])
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("particles")
@@ -81,13 +122,24 @@ def main(argv=None):
     ap.add_argument("--iter", type=int, default=1)
     ap.add_argument("--cubes", action="store_true")
     ap.add_argument("--map", action="store_true")
+    ap.add_argument("--grid", type=int, default=0, metavar="NHY", help="the input is a grid file of NHY^3 cells")
+    ap.add_argument("--level", type=int, default=0, help="the level of a grid input (<= 0)")
+    ap.add_argument("--mask", help="survey mask file (survey mode)")
+    ap.add_argument("--randoms", help="survey randoms file (survey mode)")
+    ap.add_argument("--ncox", type=int, default=0, help="the survey mask's coarse grid (default --nx)")
+    ap.add_argument("--novel", action="store_true", help="particle file without velocities (READ_BINARY_PART_2)")
     a = ap.parse_args(argv)
     p = Params(nx=a.nx, lado0=a.lado0, periodic=a.periodic, kneighbours=a.kneighbours, learned=a.learned,
-               nvoid_max=a.nvoid_max)
-    r = run_iteration(a.particles, p, a.out, it=a.iter, nlev=a.levels, cubes=a.cubes, maps=a.map)
+               nvoid_max=a.nvoid_max, level=a.level, levmin=a.level)
+    if a.grid or a.mask:
+        r = run_single(a.particles, p, a.out, it=a.iter, grid_nhy=a.grid, mask=a.mask, randoms=a.randoms,
+                       novel=a.novel, ncox=a.ncox, cubes=a.cubes)
+    else:
+        r = run_iteration(a.particles, p, a.out, it=a.iter, nlev=a.levels, cubes=a.cubes, maps=a.map)
     for lev in r["levels"]:
         print(f"level: {lev['nvoid']} cubes, {lev['cat']['nvoidt']} voids")
-    print(f"wrote {r['voids']}" + (f", {r['cubes']}" if r["cubes"] else "") + (f", {r['map']}" if r["map"] else ""))
+    print(f"wrote {r['voids']}" + (f", {r['cubes']}" if r["cubes"] else "") +
+          (f", {r['map']}" if r.get("map") else ""))
 
 
 if __name__ == "__main__":

@@ -267,6 +267,24 @@ int avism_gpu_run_sublevel(avism_gpu_ctx *ctx, const avism_params *p, int64_t n,
                            const int32_t *marcap_ext, const float *reqp, int32_t nreqp, avism_cubes *cubes,
                            int32_t *nvoid, avism_voids *voids, float *meandens);
 
+/* ---- grid input (FLAG_DATA = 2): replaces src/avism.f90:1316-1362 for the
+ *      grids of READ_BINARY_GRID (src/reader.f90:523-552).  u1g..u4g: the input
+ *      grid, nhy^3 cells, column-major, as the reference holds it after
+ *      reading: U1G = delta + 1 (rho / rho_B) and the velocities / UV.  The
+ *      level's grid is params.nx = nhy * 2^level; level 0 takes the grids as
+ *      they are, a level below 0 smooths them onto the coarser grid
+ *      (SMOOTH_2, src/amr2uniform.f90:65-120), a level above 0 is the
+ *      reference's 'LEVEL > 0 FOR BIN_GRID NOT IMPLEMENTED YET' stop
+ *      (AVISM_ERR_UNSUPPORTED).  U1CO = U1GCO (no mean normalisation),
+ *      DIVERCO = DIVER_UNIFORM of the velocities, MEANDENS the background
+ *      density ROTE*UM/UL^3.  avism_gpu_grid_fields returns the ext grids (as
+ *      avism_gpu_fields), avism_gpu_run_level_grid the level's catalogue.      */
+int avism_gpu_grid_fields(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g, const float *u2g,
+                          const float *u3g, const float *u4g, float *u1co_ext, float *diverco_ext, float *meandens);
+int avism_gpu_run_level_grid(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g,
+                             const float *u2g, const float *u3g, const float *u4g, avism_cubes *cubes,
+                             int32_t *nvoid, avism_voids *voids, float *meandens);
+
 /* ---- survey mode (FLAG_SURVEY = 1): replaces src/avism.f90:1420-1596.  The
  *      tracers (x..m, masses as weights; velocities nullable with
  *      no_velocities = 1) and the randoms (rx, ry, rz, weights rw, in the units

@@ -112,6 +112,10 @@ int orc_survey_fields(const avism_params *p, int64_t n, const float *x, const fl
                       const float *rx, const float *ry, const float *rz, const float *rw, const int8_t *smask,
                       float *u1co_ext, float *diverco_ext, float *meandens, float *u1rand_out);
 
+/* grid input (FLAG_DATA = 2, src/avism.f90:1316-1362; SMOOTH_2 below level 0) */
+int orc_grid_fields(const avism_params *p, int32_t nhy, const float *u1g, const float *u2g, const float *u3g,
+                    const float *u4g, float *u1co_ext, float *diverco_ext, float *meandens);
+
 #ifdef __cplusplus
 }
 #endif

@@ -141,6 +141,28 @@ def survey_fields(p: Params, parts: dict, rands: dict, smask):
     return u1, dv, md.value, ur
 
 
+def grid_fields(p: Params, nhy, u1g, u2g, u3g, u4g):
+    """Grid input (src/avism.f90:1316-1362): (U1CO ext, DIVERCO ext, MEANDENS)."""
+    g, _ = grid_setup(p)
+    u1 = np.zeros(g.ne ** 3, np.float32)
+    dv = np.zeros(g.ne ** 3, np.float32)
+    md = C.c_float()
+    f = lib().orc_grid_fields
+    f.argtypes = [C.c_void_p, C.c_int32] + [C.POINTER(C.c_float)] * 6 + [C.POINTER(C.c_float)]
+    pc = p.to_c()
+    _chk(f(C.byref(pc), int(nhy), *(ptr(_f32(a), C.c_float) for a in (u1g, u2g, u3g, u4g)),
+           ptr(u1, C.c_float), ptr(dv, C.c_float), C.byref(md)))
+    return u1, dv, md.value
+
+
+def run_level_grid(p: Params, nhy, u1g, u2g, u3g, u4g):
+    """grids -> catalogue on the CPU (grid input)."""
+    u1, dv, md = grid_fields(p, nhy, u1g, u2g, u3g, u4g)
+    vf = voidfind(p, u1, dv)
+    cat = merge_post(p, vf["nvoid"], vf["cubes"], u1, md)
+    return dict(u1co=u1, diverco=dv, meandens=md, vf=vf, cat=cat)
+
+
 def smask_ext(p: Params, smask):
     """The survey mask on the ext grid: the inner cells' values, 0 on the ghost
     shell (SMASK = 0 before the inner cells are set, src/avism.f90:867-869)."""

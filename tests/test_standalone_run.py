@@ -63,3 +63,48 @@ def test_two_level_iteration_files(tmp_path):
     assert np.array_equal(l1["rows"][:, 13], reqp[l1["rows"][:, 12].astype(int) - 1])
     # the map holds both levels: 3 arrays of 32^3 then of 64^3 cells, 4 bytes each
     assert os.path.getsize(out["map"]) == 3 * 4 * (32 ** 3 + 64 ** 3)
+
+
+class OracleModes(OracleEngine):
+    def run_level_grid(self, p, nhy, u1, u2, u3, u4):
+        return self._res(O.run_level_grid(p, nhy, u1, u2, u3, u4))
+
+    def run_level_survey(self, p, parts, rands, smask):
+        return self._res(O.run_level_survey(p, parts, rands, smask))
+
+
+def test_grid_file_level(tmp_path):
+    """A READ_BINARY_GRID file through the runner's grid mode (level -1)."""
+    from avism_b200.run import run_single
+    from test_grid_input import grid_case
+    from avism_b200._abi import UV
+    u1, vs = grid_case(32)
+    path = tmp_path / "bin_file_grid00001"
+    _fortran_records(path, [np.float32(0.0).tobytes(), (u1 - np.float32(1)).astype(np.float32)] +
+                     [(v * np.float32(UV)).astype(np.float32) for v in vs])
+    p = Params(nx=16, periodic=1, lado0=100.0, level=-1, levmin=-1, rmin=2.0)
+    r = run_single(path, p, tmp_path / "out", grid_nhy=32, cubes=True, engine=OracleModes())
+    head, levels = _read_voids_file(r["voids"])
+    assert levels[0]["level"] == -1 and len(levels[0]["rows"]) == r["levels"][0]["cat"]["nvoidt"] > 0
+
+
+def test_survey_files_level(tmp_path):
+    """A particle file without velocities, mask.dat and rands.dat through the
+    runner's survey mode."""
+    from avism_b200.run import run_single
+    c = synth.weighted_cone(box=150.0, ng=64, rmax=75.0, rsel=50.0, n_target=20000, seed=1005)
+    rr = synth.cone_randoms(60000, c["pixel_mask"], box=150.0, rmax=75.0, rsel=50.0, seed=2005)
+    sm = synth.cone_mask(64, c["pixel_mask"], box=150.0, rmax=75.0)
+    pp = tmp_path / "bin_file_part00001"
+    n = len(c["x"])
+    _fortran_records(pp, [np.int64(n).tobytes() + np.float32(0.0).tobytes()] +
+                     [c[k] for k in ("x", "y", "z", "m")])
+    mp = tmp_path / "mask.dat"
+    with open(mp, "wb") as f:
+        f.write(np.int32(64).tobytes() + np.zeros(3, np.float32).tobytes() + sm.tobytes())
+    rp = tmp_path / "rands.dat"
+    _fortran_records(rp, [np.int32(len(rr["x"])).tobytes()] + [rr[k] for k in ("x", "y", "z", "w")])
+    p = Params(nx=64, periodic=0, lado0=150.0, kneighbours=16, flag_vel_interp=0, flag_dens_interp=0, rmin=3.0)
+    r = run_single(pp, p, tmp_path / "out", mask=mp, randoms=rp, novel=True, engine=OracleModes())
+    head, levels = _read_voids_file(r["voids"])
+    assert len(levels[0]["rows"]) == r["levels"][0]["cat"]["nvoidt"] > 0
