@@ -597,11 +597,15 @@ __device__ __noinline__ void ddens_nested(const DdensArgs &A, const float4 p, in
 // occupancy pays more than the particles whose longer lists go to ddens_nested
 constexpr int DD_THREADS = 256, DD_RMAX = 28;
 
-__global__ void __launch_bounds__(DD_THREADS, 6) k_ddens(KnnGrid G, int64_t n, DdensArgs A) {
+// order: the particles (binned positions) in the order the threads take them, or
+// null for the binned order itself
+__global__ void __launch_bounds__(DD_THREADS, 6) k_ddens(KnnGrid G, int64_t n, DdensArgs A,
+                                                        const int32_t *__restrict__ order) {
     __shared__ uint32_t rows[DD_RMAX * DD_THREADS];
     uint32_t *my = rows + threadIdx.x;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int64_t i = order ? (int64_t)order[t] : t;
     const float4 p = G.sp[i];
     const int nx = A.nx;
     const float dx = A.dx;
@@ -722,6 +726,21 @@ __global__ void __launch_bounds__(DD_THREADS, 6) k_ddens(KnnGrid G, int64_t n, D
 // A cell's exact sum, rounded to REAL*8 (nearest, ties to even) and then to
 // REAL*4, as the reference's U(...) = U8(...) conversion of its REAL*8 sum.
 constexpr int EXACT_MAX_LIMBS = 11;
+
+// the support class of every particle for the scatter's thread order: larger
+// smoothing lengths first, in steps of a quarter cell (the scatter's sums are
+// exact, so the order leaves the grid unchanged; it only gives the threads of a
+// warp supports of similar size)
+constexpr int DD_CLASSES = 32;
+__global__ void k_ddens_class(int64_t n, const float *__restrict__ hp_s, float inv_dx, uint32_t *__restrict__ key,
+                              int32_t *__restrict__ val) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float q = hp_s[i] * inv_dx * 4.0f;
+    const int c = q < (float)(DD_CLASSES - 1) ? (int)q : DD_CLASSES - 1;
+    key[i] = (uint32_t)(DD_CLASSES - 1 - c);
+    val[i] = (int32_t)i;
+}
 
 __global__ void k_exact_to_f32(int64_t nc, const unsigned long long *__restrict__ fix, int nlimb,
                                float *__restrict__ out) {
@@ -1173,8 +1192,22 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
                 D.norm0 = c.get_t<unsigned long long>(B_RED2, 1);
                 AV_CUDA(cudaMemsetAsync(D.norm0, 0, sizeof(unsigned long long), c.stream));
             }
+            // the threads take the particles by support size (AVISM_TUNE_DDORDER=0: binned order)
+            const int32_t *order = nullptr;
+            const char *ord_env = getenv("AVISM_TUNE_DDORDER");
+            if ((ord_env ? atoi(ord_env) : 1) != 0 && a.n > 0) {
+                uint32_t *ka = c.get_t<uint32_t>(B_KEYS_A, a.n), *kb = c.get_t<uint32_t>(B_KEYS_B, a.n);
+                int32_t *va = c.get_t<int32_t>(B_VALS_A, a.n), *vb = c.get_t<int32_t>(B_VALS_B, a.n);
+                ++c.launches, k_ddens_class<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, hp_s, 1.0f / L.g.dx, ka, va);
+                cub::DoubleBuffer<uint32_t> dk(ka, kb);
+                cub::DoubleBuffer<int32_t> dv(va, vb);
+                size_t tmp = 0;
+                AV_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, (int)a.n, 0, 5, c.stream));
+                AV_CUDA(cub::DeviceRadixSort::SortPairs(c.get(B_CUB_TMP, tmp), tmp, dk, dv, (int)a.n, 0, 5, c.stream));
+                order = dv.Current();
+            }
             c.mark("ddens_setup");
-            ++c.launches, k_ddens<<<grid_for(a.n, DD_THREADS), DD_THREADS, 0, c.stream>>>(G, a.n, D);
+            ++c.launches, k_ddens<<<grid_for(a.n, DD_THREADS), DD_THREADS, 0, c.stream>>>(G, a.n, D, order);
             AV_CUDA(cudaGetLastError());
             if (D.norm0) {
                 unsigned long long h = 0;
