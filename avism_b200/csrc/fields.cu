@@ -627,25 +627,44 @@ k_flags_inner(FlagArgs A, uint8_t *__restrict__ fin) {
     }
 }
 
+// 16 consecutive ext cells of one row per thread, stored as one 16-byte word when
+// the row pitch allows (NE a multiple of 16); the inner bytes they wrap to are
+// contiguous except across the periodic seam
 __global__ void k_flags_spread(FlagArgs A, const uint8_t *__restrict__ fin, uint8_t *__restrict__ flags) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int ne = A.ne, nx = A.nx;
-    if (i >= ne) return;
-    const int c[3] = {i + A.low1, (int)blockIdx.y + A.low1, (int)blockIdx.z + A.low1};
-    const int64_t e = (int64_t)i + (int64_t)ne * (blockIdx.y + (int64_t)ne * blockIdx.z);
-    bool inside = true;
+    const int nch = (ne + 15) / 16;
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (int64_t)nch * ne * ne) return;
+    const int ch = (int)(g % nch), y = (int)((g / nch) % ne), z = (int)(g / ((int64_t)nch * ne));
+    const int i0 = ch * 16;
+    const int cy = y + A.low1, cz = z + A.low1;
+    const int64_t e0 = (int64_t)ne * (y + (int64_t)ne * z) + i0;
+    const bool row_in = cy >= A.low1 + 4 && cy <= A.low2 - 4 && cz >= A.low1 + 4 && cz <= A.low2 - 4;
+    int wy = cy, wz = cz;
+    if (wy < 1) wy += nx; else if (wy > nx) wy -= nx;
+    if (wz < 1) wz += nx; else if (wz > nx) wz -= nx;
+    const uint8_t *frow = fin + (int64_t)nx * ((wy - 1) + (int64_t)nx * (wz - 1));
+    uint32_t w[4] = {0, 0, 0, 0};
+    const int m = min(16, ne - i0);
 #pragma unroll
-    for (int a = 0; a < 3; a++) inside &= c[a] >= A.low1 + 4 && c[a] <= A.low2 - 4;
-    if (inside) {
-        int w[3];
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            w[a] = c[a];
-            if (w[a] < 1) w[a] += nx; else if (w[a] > nx) w[a] -= nx;
+    for (int t = 0; t < 16; t++) {
+        if (t >= m) break;
+        const int cx = i0 + t + A.low1;
+        uint8_t f;
+        if (row_in && cx >= A.low1 + 4 && cx <= A.low2 - 4) {
+            int wx = cx;
+            if (wx < 1) wx += nx; else if (wx > nx) wx -= nx;
+            f = frow[wx - 1];
+        } else {
+            const int c[3] = {cx, cy, cz};
+            f = flag_byte(A, e0 + t, c);
         }
-        flags[e] = fin[(int64_t)(w[0] - 1) + (int64_t)nx * ((w[1] - 1) + (int64_t)nx * (w[2] - 1))];
+        w[t >> 2] |= (uint32_t)f << (8 * (t & 3));
+    }
+    if (m == 16 && (reinterpret_cast<uintptr_t>(flags + e0) & 15) == 0) {
+        *reinterpret_cast<uint4 *>(flags + e0) = make_uint4(w[0], w[1], w[2], w[3]);
     } else {
-        flags[e] = flag_byte(A, e, c);
+        for (int t = 0; t < m; t++) flags[e0 + t] = (uint8_t)(w[t >> 2] >> (8 * (t & 3)));
     }
 }
 
@@ -666,8 +685,8 @@ void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, 
         uint8_t *fin = c.get_t<uint8_t>(B_FLAGS_IN, (size_t)nx * nx * nx);
         const unsigned ntiles = (unsigned)((nx / FL_TX) * (nx / FL_TY) * (nx / FL_TZ));
         ++c.launches, k_flags_inner<<<ntiles, FL_TX * FL_TY, 0, c.stream>>>(A, fin);
-        const dim3 g((unsigned)((L.g.ne + 127) / 128), (unsigned)L.g.ne, (unsigned)L.g.ne);
-        ++c.launches, k_flags_spread<<<g, 128, 0, c.stream>>>(A, fin, flags);
+        const int64_t nth = (int64_t)((L.g.ne + 15) / 16) * L.g.ne * L.g.ne;
+        ++c.launches, k_flags_spread<<<grid_for(nth, 256), 256, 0, c.stream>>>(A, fin, flags);
     } else {
         ++c.launches, k_flags<<<grid_for(ne3, 256), 256, 0, c.stream>>>(A, flags);
     }
