@@ -627,9 +627,21 @@ k_flags_inner(FlagArgs A, uint8_t *__restrict__ fin) {
     }
 }
 
-// 16 consecutive ext cells of one row per thread, stored as one 16-byte word when
-// the row pitch allows (NE a multiple of 16); the inner bytes they wrap to are
-// contiguous except across the periodic seam
+// 16 consecutive ext cells of one row per thread.  A chunk whose cells all lie
+// inside the face shell and wrap to 16 contiguous, 16-byte aligned inner bytes
+// (the common case) is one 16-byte load and one 16-byte store; any other chunk
+// goes byte by byte, computing the shell's bytes directly.
+static __device__ __noinline__ uint8_t spread_byte(const FlagArgs &A, const uint8_t *__restrict__ frow, bool row_in,
+                                                  int64_t e, int cx, int cy, int cz) {
+    if (row_in && cx >= A.low1 + 4 && cx <= A.low2 - 4) {
+        int wx = cx;
+        if (wx < 1) wx += A.nx; else if (wx > A.nx) wx -= A.nx;
+        return frow[wx - 1];
+    }
+    const int c[3] = {cx, cy, cz};
+    return flag_byte(A, e, c);
+}
+
 __global__ void k_flags_spread(FlagArgs A, const uint8_t *__restrict__ fin, uint8_t *__restrict__ flags) {
     const int ne = A.ne, nx = A.nx;
     const int nch = (ne + 15) / 16;
@@ -644,28 +656,18 @@ __global__ void k_flags_spread(FlagArgs A, const uint8_t *__restrict__ fin, uint
     if (wy < 1) wy += nx; else if (wy > nx) wy -= nx;
     if (wz < 1) wz += nx; else if (wz > nx) wz -= nx;
     const uint8_t *frow = fin + (int64_t)nx * ((wy - 1) + (int64_t)nx * (wz - 1));
-    uint32_t w[4] = {0, 0, 0, 0};
+    const int cx0 = i0 + A.low1;
+    int w0 = cx0;
+    if (w0 < 1) w0 += nx; else if (w0 > nx) w0 -= nx;
+    const bool fast = row_in && i0 + 16 <= ne && cx0 >= A.low1 + 4 && cx0 + 15 <= A.low2 - 4 && w0 + 15 <= nx &&
+                      (reinterpret_cast<uintptr_t>(frow + w0 - 1) & 15) == 0 &&
+                      (reinterpret_cast<uintptr_t>(flags + e0) & 15) == 0;
+    if (fast) {
+        *reinterpret_cast<uint4 *>(flags + e0) = *reinterpret_cast<const uint4 *>(frow + w0 - 1);
+        return;
+    }
     const int m = min(16, ne - i0);
-#pragma unroll
-    for (int t = 0; t < 16; t++) {
-        if (t >= m) break;
-        const int cx = i0 + t + A.low1;
-        uint8_t f;
-        if (row_in && cx >= A.low1 + 4 && cx <= A.low2 - 4) {
-            int wx = cx;
-            if (wx < 1) wx += nx; else if (wx > nx) wx -= nx;
-            f = frow[wx - 1];
-        } else {
-            const int c[3] = {cx, cy, cz};
-            f = flag_byte(A, e0 + t, c);
-        }
-        w[t >> 2] |= (uint32_t)f << (8 * (t & 3));
-    }
-    if (m == 16 && (reinterpret_cast<uintptr_t>(flags + e0) & 15) == 0) {
-        *reinterpret_cast<uint4 *>(flags + e0) = make_uint4(w[0], w[1], w[2], w[3]);
-    } else {
-        for (int t = 0; t < m; t++) flags[e0 + t] = (uint8_t)(w[t >> 2] >> (8 * (t & 3)));
-    }
+    for (int t = 0; t < m; t++) flags[e0 + t] = spread_byte(A, frow, row_in, e0 + t, cx0 + t, cy, cz);
 }
 
 void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, const float *dv,
