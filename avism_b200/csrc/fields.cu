@@ -550,7 +550,7 @@ __global__ void k_flags(FlagArgs A, uint8_t *__restrict__ flags) {
 // parent map).  k_flags_inner computes those inner bytes once: a CTA holds a
 // 32 x 8 column of cells and marches it along z, with a ring of 7 U1CO planes
 // (+-3 halo) and 3 DIVERCO planes (+-1 halo) in shared memory.  k_flags_spread
-// then writes the ext grid, computing the face shell directly.
+// and k_flags_shell then write the ext grid.
 constexpr int FL_TX = 32, FL_TY = 8, FL_TZ = 32, FL_H = 3;
 constexpr int FL_UX = FL_TX + 2 * FL_H, FL_UY = FL_TY + 2 * FL_H;
 constexpr int FL_DX = FL_TX + 2, FL_DY = FL_TY + 2;
@@ -627,47 +627,67 @@ k_flags_inner(FlagArgs A, uint8_t *__restrict__ fin) {
     }
 }
 
-// 16 consecutive ext cells of one row per thread.  A chunk whose cells all lie
-// inside the face shell and wrap to 16 contiguous, 16-byte aligned inner bytes
-// (the common case) is one 16-byte load and one 16-byte store; any other chunk
-// goes byte by byte, computing the shell's bytes directly.
-static __device__ __noinline__ uint8_t spread_byte(const FlagArgs &A, const uint8_t *__restrict__ frow, bool row_in,
-                                                  int64_t e, int cx, int cy, int cz) {
-    if (row_in && cx >= A.low1 + 4 && cx <= A.low2 - 4) {
-        int wx = cx;
-        if (wx < 1) wx += A.nx; else if (wx > A.nx) wx -= A.nx;
-        return frow[wx - 1];
-    }
-    const int c[3] = {cx, cy, cz};
-    return flag_byte(A, e, c);
-}
-
+// The ext grid in two launches.  k_flags_spread writes every cell at least 4
+// cells inside the faces from the inner byte it wraps to, 16 consecutive cells
+// of a row per thread (one 16-byte load and store when both sides are aligned);
+// k_flags_shell computes the faces' 4-cell shell directly, one cell per thread,
+// so the heavier shell bytes do not hold up the copies.
 __global__ void k_flags_spread(FlagArgs A, const uint8_t *__restrict__ fin, uint8_t *__restrict__ flags) {
     const int ne = A.ne, nx = A.nx;
     const int nch = (ne + 15) / 16;
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= (int64_t)nch * ne * ne) return;
-    const int ch = (int)(g % nch), y = (int)((g / nch) % ne), z = (int)(g / ((int64_t)nch * ne));
+    if (g >= (int64_t)nch * (ne - 8) * (ne - 8)) return;
+    const int ch = (int)(g % nch), y = 4 + (int)((g / nch) % (ne - 8)), z = 4 + (int)(g / ((int64_t)nch * (ne - 8)));
     const int i0 = ch * 16;
     const int cy = y + A.low1, cz = z + A.low1;
-    const int64_t e0 = (int64_t)ne * (y + (int64_t)ne * z) + i0;
-    const bool row_in = cy >= A.low1 + 4 && cy <= A.low2 - 4 && cz >= A.low1 + 4 && cz <= A.low2 - 4;
     int wy = cy, wz = cz;
     if (wy < 1) wy += nx; else if (wy > nx) wy -= nx;
     if (wz < 1) wz += nx; else if (wz > nx) wz -= nx;
     const uint8_t *frow = fin + (int64_t)nx * ((wy - 1) + (int64_t)nx * (wz - 1));
+    uint8_t *erow = flags + (int64_t)ne * (y + (int64_t)ne * z);
     const int cx0 = i0 + A.low1;
     int w0 = cx0;
     if (w0 < 1) w0 += nx; else if (w0 > nx) w0 -= nx;
-    const bool fast = row_in && i0 + 16 <= ne && cx0 >= A.low1 + 4 && cx0 + 15 <= A.low2 - 4 && w0 + 15 <= nx &&
-                      (reinterpret_cast<uintptr_t>(frow + w0 - 1) & 15) == 0 &&
-                      (reinterpret_cast<uintptr_t>(flags + e0) & 15) == 0;
-    if (fast) {
-        *reinterpret_cast<uint4 *>(flags + e0) = *reinterpret_cast<const uint4 *>(frow + w0 - 1);
+    if (i0 >= 4 && i0 + 16 <= ne - 4 && w0 + 15 <= nx && (reinterpret_cast<uintptr_t>(frow + w0 - 1) & 15) == 0 &&
+        (reinterpret_cast<uintptr_t>(erow + i0) & 15) == 0) {
+        *reinterpret_cast<uint4 *>(erow + i0) = *reinterpret_cast<const uint4 *>(frow + w0 - 1);
         return;
     }
-    const int m = min(16, ne - i0);
-    for (int t = 0; t < m; t++) flags[e0 + t] = spread_byte(A, frow, row_in, e0 + t, cx0 + t, cy, cz);
+    const int a = max(i0, 4), b = min(i0 + 16, ne - 4);
+    for (int i = a; i < b; i++) {
+        int wx = i + A.low1;
+        if (wx < 1) wx += nx; else if (wx > nx) wx -= nx;
+        erow[i] = frow[wx - 1];
+    }
+}
+
+// the cells within 4 of a face: z slabs, then y slabs of the remaining planes,
+// then x slabs of the remaining rows
+__global__ void k_flags_shell(FlagArgs A, uint8_t *__restrict__ flags) {
+    const int ne = A.ne, m = ne - 8;
+    const int64_t nzs = 8 * (int64_t)ne * ne, nys = 8 * (int64_t)ne * m, nxs = 8 * (int64_t)m * m;
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int x, y, z;
+    if (g < nzs) {
+        x = (int)(g % ne); y = (int)((g / ne) % ne);
+        const int s = (int)(g / ((int64_t)ne * ne));
+        z = s < 4 ? s : ne - 8 + s;
+    } else if ((g -= nzs) < nys) {
+        x = (int)(g % ne);
+        const int s = (int)((g / ne) % 8);
+        y = s < 4 ? s : ne - 8 + s;
+        z = 4 + (int)(g / (8 * (int64_t)ne));
+    } else if ((g -= nys) < nxs) {
+        const int s = (int)(g % 8);
+        x = s < 4 ? s : ne - 8 + s;
+        y = 4 + (int)((g / 8) % m);
+        z = 4 + (int)(g / (8 * (int64_t)m));
+    } else {
+        return;
+    }
+    const int c[3] = {x + A.low1, y + A.low1, z + A.low1};
+    const int64_t e = (int64_t)x + (int64_t)ne * (y + (int64_t)ne * z);
+    flags[e] = flag_byte(A, e, c);
 }
 
 void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, const float *dv,
@@ -687,8 +707,11 @@ void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, 
         uint8_t *fin = c.get_t<uint8_t>(B_FLAGS_IN, (size_t)nx * nx * nx);
         const unsigned ntiles = (unsigned)((nx / FL_TX) * (nx / FL_TY) * (nx / FL_TZ));
         ++c.launches, k_flags_inner<<<ntiles, FL_TX * FL_TY, 0, c.stream>>>(A, fin);
-        const int64_t nth = (int64_t)((L.g.ne + 15) / 16) * L.g.ne * L.g.ne;
+        const int64_t ne = L.g.ne, m = ne - 8;
+        const int64_t nth = ((ne + 15) / 16) * m * m;
         ++c.launches, k_flags_spread<<<grid_for(nth, 256), 256, 0, c.stream>>>(A, fin, flags);
+        const int64_t nshell = 8 * ne * ne + 8 * ne * m + 8 * m * m;
+        ++c.launches, k_flags_shell<<<grid_for(nshell, 256), 256, 0, c.stream>>>(A, flags);
     } else {
         ++c.launches, k_flags<<<grid_for(ne3, 256), 256, 0, c.stream>>>(A, flags);
     }
