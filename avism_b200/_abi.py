@@ -96,8 +96,8 @@ class Cubes:
         self.c = AvismCubesC(**{k: ptr(self.arr[k], C.c_int32) for k in CUBE_INT},
                              **{k: ptr(self.arr[k], C.c_float) for k in CUBE_FLT})
 
-    def view(self, nvoid: int) -> dict:
-        return {k: v[:nvoid].copy() for k, v in self.arr.items()}
+    def view(self, nvoid: int, copy: bool = True) -> dict:
+        return {k: (v[:nvoid].copy() if copy else v[:nvoid]) for k, v in self.arr.items()}
 
     @classmethod
     def from_dict(cls, d: dict, nvoid: int) -> "Cubes":
@@ -120,13 +120,13 @@ class Voids:
         kw["marca"] = ptr(self.marca, C.c_int32) if self.marca is not None else _I32P()
         self.c = AvismVoidsC(**kw)
 
-    def view(self, nvoid: int) -> dict:
-        d = {k: v[:nvoid].copy() for k, v in self.arr.items()}
+    def view(self, nvoid: int, copy: bool = True) -> dict:
+        d = {k: (v[:nvoid].copy() if copy else v[:nvoid]) for k, v in self.arr.items()}
         d["nvoid2"] = int(self.c.nvoid2)
         d["nvoidt"] = int(self.c.nvoidt)
         d["volt_clean"] = float(self.c.volt_clean)
         if self.marca is not None:
-            d["marca"] = self.marca.copy()
+            d["marca"] = self.marca.copy() if copy else self.marca
         return d
 
 

@@ -424,13 +424,29 @@ class AvismGPU:
         return dict(cubes=cubes.view(nv.value), nvoid=nv.value, cat=vo.view(nv.value), meandens=md.value)
 
     # ---- whole level ------------------------------------------------------------
-    def run_level(self, p: Params, parts: dict, want_marca=False, want_cubes=True, capacity=None):
+    @staticmethod
+    def level_buffers(p: Params, capacity=None, want_marca=False):
+        """Caller-owned cube and catalogue arrays for run_level(bufs=...), reused
+        across calls the way the Fortran driver keeps its COMMONDATA arrays."""
         g, _ = grid_setup(p)
         cap = int(capacity or p.nvoid_max)
+        return Cubes(cap), Voids(cap, g.ne if want_marca else None)
+
+    def run_level(self, p: Params, parts: dict, want_marca=False, want_cubes=True, capacity=None, bufs=None):
+        """One level, particles -> catalogue.  With bufs (from level_buffers) the
+        results are views of those arrays, valid until their next use."""
+        g, _ = grid_setup(p)
         a = {k: (_f32(parts[k]) if parts.get(k) is not None else None) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
         n = len(a["x"])
-        cubes = Cubes(cap) if want_cubes else None
-        vo = Voids(cap, g.ne if want_marca else None)
+        if bufs is not None:
+            cubes, vo = bufs
+            cap = min(cubes.cap, len(vo.arr["indice"]))
+            if want_marca and vo.marca is None:
+                raise ValueError("run_level: want_marca needs buffers made with want_marca=True")
+        else:
+            cap = int(capacity or p.nvoid_max)
+            cubes = Cubes(cap) if want_cubes else None
+            vo = Voids(cap, g.ne if want_marca else None)
         nv = C.c_int32()
         md = C.c_float()
         pc = p.to_c()
@@ -438,5 +454,6 @@ class AvismGPU:
         self._chk(self.lib.avism_gpu_run_level(
             self.h, C.byref(pc), n, *(_vp(a[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")),
             C.byref(cubes.c) if cubes else None, C.byref(nv), C.byref(vo.c), C.byref(md)))
-        return dict(cubes=cubes.view(nv.value) if cubes else None, nvoid=nv.value,
-                    cat=vo.view(nv.value), meandens=md.value)
+        cp = bufs is None
+        return dict(cubes=cubes.view(nv.value, cp) if cubes else None, nvoid=nv.value,
+                    cat=vo.view(nv.value, cp), meandens=md.value)

