@@ -76,6 +76,13 @@ struct Ctx {
     std::string last_error;
     std::vector<double> stage_ms;
     int num_sms = 148;
+    // host->device copies of the particle attributes (m, vx, vy, vz) run on a
+    // second stream after the positions' copies, so that binning's keys and sort
+    // overlap them; ev_attr marks their end, attrs_ready() orders the main
+    // stream after it
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_pos = nullptr, ev_attr = nullptr;
+    bool attr_pending = false;
     // scratch pinned host memory for small readbacks
     void *hpin = nullptr;
     size_t hpin_cap = 0;
@@ -155,6 +162,11 @@ struct Ctx {
         return hpin;
     }
     void sync() { AV_CUDA(cudaStreamSynchronize(stream)); }
+    void attrs_ready() {
+        if (!attr_pending) return;
+        attr_pending = false;
+        AV_CUDA(cudaStreamWaitEvent(stream, ev_attr, 0));
+    }
 };
 
 // pointer classification: true if p is device (or managed) memory
@@ -162,6 +174,8 @@ bool is_device_ptr(const void *p);
 
 // copies a caller array into a device buffer (no copy if it is already device memory)
 const void *to_device(Ctx &c, BufId id, const void *src, size_t bytes);
+// as to_device, the copy issued on stream st
+const void *to_device_on(Ctx &c, cudaStream_t st, BufId id, const void *src, size_t bytes);
 // copies a device result to the caller's array (device-to-device if it is device memory)
 void from_device(Ctx &c, void *dst, const void *src_dev, size_t bytes);
 

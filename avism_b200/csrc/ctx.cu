@@ -25,6 +25,14 @@ const void *to_device(Ctx &c, BufId id, const void *src, size_t bytes) {
     return d;
 }
 
+const void *to_device_on(Ctx &c, cudaStream_t st, BufId id, const void *src, size_t bytes) {
+    if (!src) return nullptr;
+    if (is_device_ptr(src)) return src;
+    void *d = c.get(id, bytes);
+    AV_CUDA(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, st));
+    return d;
+}
+
 void from_device(Ctx &c, void *dst, const void *src_dev, size_t bytes) {
     if (!dst || bytes == 0) return;
     if (dst == src_dev) return;

@@ -64,6 +64,7 @@ BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y,
     if (sv) {
         pa = c.get_t<float4>(B_PX4, n);
         pb = c.get_t<float4>(B_PV4, n);
+        c.attrs_ready();
         ++c.launches, k_pack_particles<<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, y, z, m, vx, vy, vz, pa, pb);
     }
     if (fine) {

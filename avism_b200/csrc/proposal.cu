@@ -815,6 +815,7 @@ void proposal_features(Ctx &c, const avism_params *p, const P2G &a, float *feat_
     *bw_out = bp.bw;
     if (!feat_dev) return;
     float4 *sv = c.get_t<float4>(B_SV, std::max<int64_t>(a.n, 1));
+    c.attrs_ready();
     if (a.n > 0)
         ++c.launches, k_sorted_attrs<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, G.sp, a.vx, a.vy, a.vz, a.m, sv);
     Pyramid P = build_pyramid(c, G, sv, a.n);

@@ -1173,6 +1173,7 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
             {
                 float *d = c.get_t<float>(B_RED0, 1);
                 size_t tmp = 0;
+                c.attrs_ready();
                 AV_CUDA(cub::DeviceReduce::Max(nullptr, tmp, a.m, d, (int)a.n, c.stream));
                 void *t = c.get(B_CUB_TMP, tmp);
                 AV_CUDA(cub::DeviceReduce::Max(t, tmp, a.m, d, (int)a.n, c.stream));
@@ -1238,6 +1239,7 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
         float4 *dummy = c.get_t<float4>(B_SP, std::max<int64_t>(a.n, 1));
         ++c.launches, k_bin_gather<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, dk.Current(), dv.Current(), a.x, a.y, a.z,
                                                                 dummy, start, nc);
+        c.attrs_ready();
         ++c.launches, k_tsc_gather<<<grid_for(nc, 128), 128, 0, c.stream>>>(
             nc, start, dv.Current(), a.x, a.y, a.z, a.m, a.vx, a.vy, a.vz, TA,
             dens_sph ? nullptr : a.u_mass, vel_tsc ? a.u2 : nullptr, a.u3, a.u4);
