@@ -57,7 +57,7 @@ enum BufId : int {
     B_KNN_STATS,                                   // warp kNN counters
     B_FLAGS_IN,                                    // flag bytes of the periodic inner grid
     B_PR_CNT, B_PR_BOX1, B_PR_BOX2, B_PR_BOX4,     // centred box counts of the bins
-    B_PR_TMPA, B_PR_TMPB,
+    B_PR_TMPA, B_PR_TMPB, B_PR_TMPC,
     B_PX4, B_PV4,                                  // packed (x, y, z, m), (vx, vy, vz, 0) in input order
     B_FSTART,                                      // int32 offsets of quarter-bin x cells
     B_PER_CELL, B_PER_LAB, B_PER_PAIRS,            // VOID_PERIODIC: centre cells, their labels, label-map updates

@@ -107,25 +107,34 @@ __global__ void k_counts(int64_t nb3, const float4 *__restrict__ lev0, float *__
     if (b < nb3) cnt[b] = lev0[b].x;
 }
 
-// one separable pass of a (2w+1)-wide box sum along `axis` (wrapped or
-// clamped); grid (ceil(nb / blockDim), nb, nb), x along threads
-__global__ void k_box_pass(int nb, int w, int axis, int periodic, const float *__restrict__ in,
-                           float *__restrict__ out) {
+// one separable pass of the (2w+1)-wide box sums along `axis` (wrapped or
+// clamped) for the three half-widths w = 1, 2, 4 at once (in[s] -> out[s]);
+// grid (ceil(nb / blockDim), nb, nb), x along threads
+struct Box3 {
+    const float *in[3];
+    float *out[3];
+};
+__global__ void k_box_pass3(int nb, int axis, int periodic, Box3 B) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= nb) return;
     const int c[3] = {x, (int)blockIdx.y, (int)blockIdx.z};
     const int64_t b = (int64_t)x + (int64_t)nb * (blockIdx.y + (int64_t)nb * blockIdx.z);
     const int64_t stride = axis == 0 ? 1 : (axis == 1 ? nb : (int64_t)nb * nb);
-    float s = 0.f;
-    for (int d = -w; d <= w; d++) {
-        int q = c[axis] + d;
-        if (q < 0 || q >= nb) {
-            if (!periodic) continue;
-            q = q < 0 ? q + nb : q - nb;
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+        const int w = box_w(s + 1);
+        float acc = 0.f;
+#pragma unroll
+        for (int d = -w; d <= w; d++) {
+            int q = c[axis] + d;
+            if (q < 0 || q >= nb) {
+                if (!periodic) continue;
+                q = q < 0 ? q + nb : q - nb;
+            }
+            acc += B.in[s][b + (int64_t)(q - c[axis]) * stride];
         }
-        s += in[b + (int64_t)(q - c[axis]) * stride];
+        B.out[s][b] = acc;
     }
-    out[b] = s;
 }
 
 __device__ __forceinline__ float cbox_at(const Pyramid &P, int s, int nb, int x, int y, int z) {
@@ -766,20 +775,24 @@ Pyramid build_pyramid(Ctx &c, const KnnGrid &G, const float4 *sv, int64_t n) {
         const int64_t n3 = (int64_t)P.nbl[l] * P.nbl[l] * P.nbl[l];
         ++c.launches, k_pyr_down<<<grid_for(n3, 256), 256, 0, c.stream>>>(P.lev[l - 1], P.nbl[l - 1], P.lev[l], P.nbl[l]);
     }
-    // centred box counts: three separable passes per half-width
+    // centred box counts: three separable passes, each for all half-widths
     float *cnt = c.get_t<float>(B_PR_CNT, (size_t)nb3);
     float *ta = c.get_t<float>(B_PR_TMPA, (size_t)nb3), *tb = c.get_t<float>(B_PR_TMPB, (size_t)nb3);
     ++c.launches, k_counts<<<grid_for(nb3, 256), 256, 0, c.stream>>>(nb3, P.lev[0], cnt);
     P.cbox[0] = cnt;
     const BufId bid[3] = {B_PR_BOX1, B_PR_BOX2, B_PR_BOX4};
-    for (int s = 1; s < 4; s++) {
-        float *out = c.get_t<float>(bid[s - 1], (size_t)nb3);
-        const int w = box_w(s);
-        const dim3 bg((unsigned)((G.nb + 127) / 128), (unsigned)G.nb, (unsigned)G.nb);
-        ++c.launches, k_box_pass<<<bg, 128, 0, c.stream>>>(G.nb, w, 0, G.periodic, cnt, ta);
-        ++c.launches, k_box_pass<<<bg, 128, 0, c.stream>>>(G.nb, w, 1, G.periodic, ta, tb);
-        ++c.launches, k_box_pass<<<bg, 128, 0, c.stream>>>(G.nb, w, 2, G.periodic, tb, out);
-        P.cbox[s] = out;
+    const dim3 bg((unsigned)((G.nb + 127) / 128), (unsigned)G.nb, (unsigned)G.nb);
+    {
+        // x: counts -> the three outputs; y: outputs -> temporaries; z: back
+        float *out[3], *tmp[3] = {ta, tb, c.get_t<float>(B_PR_TMPC, (size_t)nb3)};
+        for (int s = 0; s < 3; s++) out[s] = c.get_t<float>(bid[s], (size_t)nb3);
+        Box3 bx{{cnt, cnt, cnt}, {out[0], out[1], out[2]}};
+        Box3 by{{out[0], out[1], out[2]}, {tmp[0], tmp[1], tmp[2]}};
+        Box3 bz{{tmp[0], tmp[1], tmp[2]}, {out[0], out[1], out[2]}};
+        ++c.launches, k_box_pass3<<<bg, 128, 0, c.stream>>>(G.nb, 0, G.periodic, bx);
+        ++c.launches, k_box_pass3<<<bg, 128, 0, c.stream>>>(G.nb, 1, G.periodic, by);
+        ++c.launches, k_box_pass3<<<bg, 128, 0, c.stream>>>(G.nb, 2, G.periodic, bz);
+        for (int s = 1; s < 4; s++) P.cbox[s] = out[s - 1];
     }
     // velocity scale of the divergence features: v_rms of the particles
     {
