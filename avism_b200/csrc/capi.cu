@@ -72,12 +72,22 @@ struct Timer {
 };
 
 // copies packed device cube arrays into the caller's avism_cubes
-void cubes_out(Ctx &c, const CubesDev &d, int32_t nvoid, avism_cubes *o) {
+// the caller's cube arrays: device ones from the device records, host ones from
+// the host copy (h, a HostCubes view of the same records)
+void cubes_out(Ctx &c, const CubesDev &d, const avism_cubes &h, int32_t nvoid, avism_cubes *o) {
     int32_t *ints[10] = {o->inicio_x, o->final_x, o->inicio_y, o->final_y, o->inicio_z, o->final_z,
                          o->icx, o->icy, o->icz, o->father};
     float *flts[7] = {o->vol, o->rini_x, o->rfin_x, o->rini_y, o->rfin_y, o->rini_z, o->rfin_z};
-    for (int k = 0; k < 10; k++) from_device(c, ints[k], d.i32 + (size_t)k * d.cap, sizeof(int32_t) * (size_t)nvoid);
-    for (int k = 0; k < 7; k++) from_device(c, flts[k], d.f32 + (size_t)k * d.cap, sizeof(float) * (size_t)nvoid);
+    const int32_t *hi[10] = {h.inicio_x, h.final_x, h.inicio_y, h.final_y, h.inicio_z, h.final_z,
+                             h.icx, h.icy, h.icz, h.father};
+    const float *hf[7] = {h.vol, h.rini_x, h.rfin_x, h.rini_y, h.rfin_y, h.rini_z, h.rfin_z};
+    auto one = [&](void *dst, const void *dev, const void *host, size_t bytes) {
+        if (!dst || bytes == 0) return;
+        if (is_device_ptr(dst)) AV_CUDA(cudaMemcpyAsync(dst, dev, bytes, cudaMemcpyDeviceToDevice, c.stream));
+        else std::memcpy(dst, host, bytes);
+    };
+    for (int k = 0; k < 10; k++) one(ints[k], d.i32 + (size_t)k * d.cap, hi[k], sizeof(int32_t) * (size_t)nvoid);
+    for (int k = 0; k < 7; k++) one(flts[k], d.f32 + (size_t)k * d.cap, hf[k], sizeof(float) * (size_t)nvoid);
     c.sync();
 }
 
@@ -107,21 +117,23 @@ struct HostCubes {
         for (int k = 0; k < 10; k++) *vi[k] = i[k].data();
         for (int k = 0; k < 7; k++) *vf[k] = f[k].data();
     }
+    // the device cube records (17 columns at stride cap) in two strided copies
+    // into the context's pinned buffer, which the view then points into
     HostCubes(Ctx &c, const CubesDev &d, int32_t n) {
-        for (int k = 0; k < 10; k++) {
-            i[k].resize(std::max(n, 1));
-            if (n) AV_CUDA(cudaMemcpyAsync(i[k].data(), d.i32 + (size_t)k * d.cap, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c.stream));
+        const size_t cb = sizeof(int32_t) * (size_t)std::max(n, 1);
+        char *h = (char *)c.host_pinned(17 * cb);
+        if (n) {
+            AV_CUDA(cudaMemcpy2DAsync(h, cb, d.i32, sizeof(int32_t) * (size_t)d.cap, cb, 10, cudaMemcpyDeviceToHost,
+                                      c.stream));
+            AV_CUDA(cudaMemcpy2DAsync(h + 10 * cb, cb, d.f32, sizeof(float) * (size_t)d.cap, cb, 7,
+                                      cudaMemcpyDeviceToHost, c.stream));
+            c.sync();
         }
-        for (int k = 0; k < 7; k++) {
-            f[k].resize(std::max(n, 1));
-            if (n) AV_CUDA(cudaMemcpyAsync(f[k].data(), d.f32 + (size_t)k * d.cap, sizeof(float) * n, cudaMemcpyDeviceToHost, c.stream));
-        }
-        c.sync();
         int32_t **vi[10] = {&v.inicio_x, &v.final_x, &v.inicio_y, &v.final_y, &v.inicio_z, &v.final_z,
                             &v.icx, &v.icy, &v.icz, &v.father};
         float **vf[7] = {&v.vol, &v.rini_x, &v.rfin_x, &v.rini_y, &v.rfin_y, &v.rini_z, &v.rfin_z};
-        for (int k = 0; k < 10; k++) *vi[k] = i[k].data();
-        for (int k = 0; k < 7; k++) *vf[k] = f[k].data();
+        for (int k = 0; k < 10; k++) *vi[k] = reinterpret_cast<int32_t *>(h + k * cb);
+        for (int k = 0; k < 7; k++) *vf[k] = reinterpret_cast<float *>(h + (10 + k) * cb);
     }
 };
 
@@ -478,7 +490,8 @@ int avism_gpu_voidfind(avism_gpu_ctx *ctx, const avism_params *p, const float *u
         }
         CubesDev cd{};
         const int32_t nv = voidfind_device(c, p, L, u1, dv, 1, sm, mp, rq, nreqp, cd);
-        cubes_out(c, cd, nv, cubes);
+        HostCubes hc(c, cd, nv);
+        cubes_out(c, cd, hc.v, nv, cubes);
         *nvoid = nv;
     });
 }
@@ -607,7 +620,7 @@ int avism_gpu_run_sublevel(avism_gpu_ctx *ctx, const avism_params *p, int64_t n,
         CubesDev cd{};
         const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, mp, rq, nreqp, cd, &wp);
         HostCubes hc(c, cd, nv);
-        if (cubes) cubes_out(c, cd, nv, cubes);
+        if (cubes) cubes_out(c, cd, hc.v, nv, cubes);
         c.mark("cubes_d2h");
         merge_post(c, p, L, nv, &hc.v, u1, fo.meandens, voids, voids->marca);
         c.mark("catalogue_d2h");
@@ -710,7 +723,7 @@ int avism_gpu_run_level_survey(avism_gpu_ctx *ctx, const avism_params *p, int64_
         CubesDev cd{};
         const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, sme, nullptr, nullptr, 0, cd, nullptr);
         HostCubes hc(c, cd, nv);
-        if (cubes) cubes_out(c, cd, nv, cubes);
+        if (cubes) cubes_out(c, cd, hc.v, nv, cubes);
         c.mark("cubes_d2h");
         merge_post(c, p, L, nv, &hc.v, u1, md, voids, voids->marca);
         c.mark("catalogue_d2h");
@@ -776,7 +789,7 @@ int avism_gpu_run_level_grid(avism_gpu_ctx *ctx, const avism_params *p, int32_t 
         CubesDev cd{};
         const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, nullptr, nullptr, 0, cd, nullptr);
         HostCubes hc(c, cd, nv);
-        if (cubes) cubes_out(c, cd, nv, cubes);
+        if (cubes) cubes_out(c, cd, hc.v, nv, cubes);
         c.mark("cubes_d2h");
         merge_post(c, p, L, nv, &hc.v, u1, md, voids, voids->marca);
         c.mark("catalogue_d2h");
@@ -804,7 +817,7 @@ int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, co
         CubesDev cd{};
         const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, nullptr, nullptr, 0, cd, &wp);
         HostCubes hc(c, cd, nv);
-        if (cubes) cubes_out(c, cd, nv, cubes);
+        if (cubes) cubes_out(c, cd, hc.v, nv, cubes);
         c.mark("cubes_d2h");
         merge_post(c, p, L, nv, &hc.v, u1, fo.meandens, voids, voids->marca);
         c.mark("catalogue_d2h");

@@ -1097,8 +1097,14 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
     }
 
     // ---- outputs
-    auto put_i = [&](int32_t *dst, const std::vector<int32_t> &v) { if (dst) from_device(c, dst, v.data(), sizeof(int32_t) * (size_t)nv); };
-    auto put_f = [&](float *dst, const std::vector<float> &v) { if (dst) from_device(c, dst, v.data(), sizeof(float) * (size_t)nv); };
+    // host columns: a plain copy into host arrays, an upload into device ones
+    auto put = [&](void *dst, const void *src, size_t bytes) {
+        if (!dst || bytes == 0) return;
+        if (is_device_ptr(dst)) AV_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c.stream));
+        else std::memcpy(dst, src, bytes);
+    };
+    auto put_i = [&](int32_t *dst, const std::vector<int32_t> &v) { put(dst, v.data(), sizeof(int32_t) * (size_t)nv); };
+    auto put_f = [&](float *dst, const std::vector<float> &v) { put(dst, v.data(), sizeof(float) * (size_t)nv); };
     put_i(out->indice, indice);
     put_i(out->uvoid, uvoid);
     put_i(out->ncellv, ncellv);
