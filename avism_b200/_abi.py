@@ -41,7 +41,8 @@ class AvismParams(C.Structure):
         ("flag_vel_interp", C.c_int32), ("flag_dens_interp", C.c_int32),
         ("level", C.c_int32), ("levmin", C.c_int32), ("learned", C.c_int32),
         ("kernel_mode", C.c_int32), ("no_velocities", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("flag_dens", C.c_int32), ("flag_div", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -155,6 +156,8 @@ class Params:
     learned: int = 0
     kernel_mode: int = 1
     no_velocities: int = 0
+    flag_dens: int = 0
+    flag_div: int = 0
     extra: dict = field(default_factory=dict)
 
     def to_c(self) -> AvismParams:

@@ -105,6 +105,27 @@ def read_grid_file(path, nx) -> dict:
     return out
 
 
+def read_masclet_files(grid_path, gas_path, dm_path, nhy) -> dict:
+    """A MASCLET snapshot (READ_MASCLET, src/reader.f90:86-405): the level-0 gas
+    grids (u1g = delta + 1, u2g..u4g; nhy^3), every level's DM particles (x..m,
+    level 0 first with mass MAP), and the header (nl, ndxyz0, zeta, map)."""
+    lib = _lib.load()
+    nl, nd0, zeta, mp = C.c_int32(), C.c_int32(), C.c_float(), C.c_float()
+    n = C.c_int64()
+    _io_chk(lib.avism_io_masclet_header(_path(grid_path), C.byref(nl), C.byref(nd0), C.byref(n), C.byref(zeta),
+                                        C.byref(mp)), f"MASCLET grid file {grid_path}")
+    nc = int(nhy) ** 3
+    gas = {k: np.zeros(nc, np.float32) for k in ("u1g", "u2g", "u3g", "u4g")}
+    parts = {k: np.zeros(max(n.value, 1), np.float32) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    got = C.c_int64()
+    _io_chk(lib.avism_io_read_masclet(_path(grid_path), _path(gas_path), _path(dm_path), int(nhy),
+                                      *(_vp(gas[k]) for k in ("u1g", "u2g", "u3g", "u4g")), n.value,
+                                      *(_vp(parts[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")),
+                                      C.byref(got)), f"MASCLET files {gas_path}, {dm_path}")
+    parts = {k: v[:got.value] for k, v in parts.items()}
+    return dict(gas=gas, parts=parts, nl=nl.value, ndxyz0=nd0.value, zeta=zeta.value, map=mp.value)
+
+
 def read_mask_file(path, ncox, nx):
     """The survey mask (src/avism.f90:403-418, 873-901) on the level's nx^3
     inner cells (int8) and (MASKLOW, MASKUPPER, MASKSIDE)."""
@@ -386,6 +407,45 @@ class AvismGPU:
         self._chk(self.lib.avism_gpu_run_level_grid(self.h, C.byref(pc), int(nhy),
                                                     *(_vp(_f32(a)) for a in (u1g, u2g, u3g, u4g)),
                                                     C.byref(cubes.c), C.byref(nv), C.byref(vo.c), C.byref(md)))
+        return dict(cubes=cubes.view(nv.value), nvoid=nv.value, cat=vo.view(nv.value), meandens=md.value)
+
+    # ---- MASCLET input (FLAG_DATA = 0) at levels <= 0 (src/avism.f90:980-1156) ------
+    def _masclet_args(self, nhy, gas, parts):
+        """gas: (u1g = 1 + delta, u2g, u3g, u4g) at nhy^3 (velocity grids may be
+        None when params.flag_div is 1 or -1); parts: the DM particles or None."""
+        g = tuple(None if a is None else _f32(a) for a in gas)
+        if parts is None:
+            a = {k: None for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+            n = 0
+        else:
+            a = {k: (_f32(parts[k]) if parts.get(k) is not None else None)
+                 for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+            n = len(a["x"])
+        args = (int(nhy), *(_vp(x) for x in g), n, *(_vp(a[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")))
+        return args, (g, a)
+
+    def masclet_fields(self, p: Params, nhy, gas, parts=None):
+        """(U1CO ext, DIVERCO ext, MEANDENS) of a MASCLET snapshot's level."""
+        gr, _ = grid_setup(p)
+        u1 = np.zeros(gr.ne ** 3, np.float32)
+        dv = np.zeros(gr.ne ** 3, np.float32)
+        md = C.c_float()
+        pc = p.to_c()
+        args, _keep = self._masclet_args(nhy, gas, parts)
+        self._chk(self.lib.avism_gpu_masclet_fields(self.h, C.byref(pc), *args, _vp(u1), _vp(dv), C.byref(md)))
+        return u1, dv, md.value
+
+    def run_level_masclet(self, p: Params, nhy, gas, parts=None, want_marca=False, capacity=None):
+        gr, _ = grid_setup(p)
+        cap = int(capacity or p.nvoid_max)
+        cubes = Cubes(cap)
+        vo = Voids(cap, gr.ne if want_marca else None)
+        nv, md = C.c_int32(), C.c_float()
+        pc = p.to_c()
+        pc.nvoid_max = min(p.nvoid_max, cap)
+        args, _keep = self._masclet_args(nhy, gas, parts)
+        self._chk(self.lib.avism_gpu_run_level_masclet(self.h, C.byref(pc), *args, C.byref(cubes.c), C.byref(nv),
+                                                       C.byref(vo.c), C.byref(md)))
         return dict(cubes=cubes.view(nv.value), nvoid=nv.value, cat=vo.view(nv.value), meandens=md.value)
 
     # ---- survey mode (src/avism.f90:1420-1596) -------------------------------------

@@ -198,6 +198,8 @@ void check_params(const avism_params *p) {
     AV_CHECK(p->nvoid_max >= 1, AVISM_ERR_ARG, "NVOID_MAX must be positive");
     AV_CHECK(p->kernel_mode >= 0 && p->kernel_mode <= 2, AVISM_ERR_ARG, "KERNEL_MODE must be 1 (M4) or 2 (Gaussian)");
     AV_CHECK(p->no_velocities == 0 || p->no_velocities == 1, AVISM_ERR_ARG, "no_velocities must be 0 or 1");
+    AV_CHECK(p->flag_dens >= 0 && p->flag_dens <= 2, AVISM_ERR_ARG, "FLAG_DENS must be 0, 1 or 2");
+    AV_CHECK(p->flag_div >= -1 && p->flag_div <= 2, AVISM_ERR_ARG, "FLAG_DIV must be 0, 1 or 2 (or -1)");
 }
 
 }  // namespace
@@ -785,6 +787,88 @@ int avism_gpu_run_level_grid(avism_gpu_ctx *ctx, const avism_params *p, int32_t 
         Level L = make_level(p);
         float *u1, *dv;
         const float md = grid_fields_dev(c, p, L, nhy, u1g, u2g, u3g, u4g, &u1, &dv);
+        c.mark("divergence");
+        CubesDev cd{};
+        const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, nullptr, nullptr, 0, cd, nullptr);
+        HostCubes hc(c, cd, nv);
+        if (cubes) cubes_out(c, cd, hc.v, nv, cubes);
+        c.mark("cubes_d2h");
+        merge_post(c, p, L, nv, &hc.v, u1, md, voids, voids->marca);
+        c.mark("catalogue_d2h");
+        *nvoid = nv;
+        if (meandens) *meandens = md;
+    });
+}
+
+// ---- MASCLET input (FLAG_DATA = 0) at levels <= 0 ------------------------------
+namespace {
+float masclet_fields_dev(Ctx &c, const avism_params *p, const Level &L, int32_t nhy, const float *u1g,
+                         const float *u2g, const float *u3g, const float *u4g, int64_t n, const float *x,
+                         const float *y, const float *z, const float *vx, const float *vy, const float *vz,
+                         const float *m, float **u1_out, float **dv_out) {
+    AV_CHECK(p->level <= 0, AVISM_ERR_UNSUPPORTED,
+             "MASCLET input: levels above 0 (AMR patches: VMESH, DIVER_FINA_GAS) are not implemented");
+    AV_CHECK(nhy >= 4 && (int64_t)p->nx << (-p->level) == (int64_t)nhy, AVISM_ERR_ARG,
+             "MASCLET input: params.nx must be nhy * 2^level (level <= 0)");
+    const bool need_dm = p->flag_dens <= 1 || p->flag_div == 0 || p->flag_div == 1;
+    const bool need_gas_v = p->flag_div == 0 || p->flag_div == 2;
+    AV_CHECK(u1g && (!need_gas_v || (u2g && u3g && u4g)), AVISM_ERR_ARG, "MASCLET input: null gas grid");
+    const int64_t n0 = (int64_t)nhy * nhy * nhy;
+    const float *g[4] = {nullptr, nullptr, nullptr, nullptr};
+    const float *src[4] = {u1g, u2g, u3g, u4g};
+    float *buf = nullptr;
+    for (int q = 0; q < (need_gas_v ? 4 : 1); q++) {
+        if (is_device_ptr(src[q])) { g[q] = src[q]; continue; }
+        if (!buf) buf = c.get_t<float>(B_GRID_IN, 4 * (size_t)n0);
+        AV_CUDA(cudaMemcpyAsync(buf + q * n0, src[q], sizeof(float) * (size_t)n0, cudaMemcpyHostToDevice, c.stream));
+        g[q] = buf + q * n0;
+    }
+    const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
+    const float *um = nullptr, *d2 = nullptr, *d3 = nullptr, *d4 = nullptr;
+    if (need_dm) {
+        // the DM particles as in the particle path (src/avism.f90:984-1061)
+        P2G a = p2g_args(c, p, L, n, x, y, z, vx, vy, vz, m, nullptr, false);
+        particles_to_grid(c, p, L, a);
+        um = a.u_mass; d2 = a.u2; d3 = a.u3; d4 = a.u4;
+    }
+    float *u1 = c.get_t<float>(B_U1CO, nc), *dv = c.get_t<float>(B_DIVER, nc);
+    const float md = masclet_fields_inner(c, p, L, nhy, g, um, d2, d3, d4, u1, dv);
+    *u1_out = u1;
+    *dv_out = dv;
+    return md;
+}
+}  // namespace
+
+int avism_gpu_masclet_fields(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g,
+                             const float *u2g, const float *u3g, const float *u4g, int64_t n, const float *x,
+                             const float *y, const float *z, const float *vx, const float *vy, const float *vz,
+                             const float *m, float *u1co_ext, float *diverco_ext, float *meandens) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        Level L = make_level(p);
+        const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
+        float *u1, *dv;
+        const float md = masclet_fields_dev(c, p, L, nhy, u1g, u2g, u3g, u4g, n, x, y, z, vx, vy, vz, m, &u1, &dv);
+        float *e1 = is_device_ptr(u1co_ext) ? u1co_ext : c.get_t<float>(B_U1EXT, ne3);
+        float *e2 = is_device_ptr(diverco_ext) ? diverco_ext : c.get_t<float>(B_DVEXT, ne3);
+        if (u1co_ext) { ext_copy(c, L, u1, e1); from_device(c, u1co_ext, e1, sizeof(float) * (size_t)ne3); }
+        if (diverco_ext) { ext_copy(c, L, dv, e2); from_device(c, diverco_ext, e2, sizeof(float) * (size_t)ne3); }
+        c.sync();
+        if (meandens) *meandens = md;
+    });
+}
+
+int avism_gpu_run_level_masclet(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g,
+                                const float *u2g, const float *u3g, const float *u4g, int64_t n, const float *x,
+                                const float *y, const float *z, const float *vx, const float *vy,
+                                const float *vz, const float *m, avism_cubes *cubes, int32_t *nvoid,
+                                avism_voids *voids, float *meandens) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        AV_CHECK(nvoid && voids, AVISM_ERR_ARG, "run_level_masclet: null argument");
+        Level L = make_level(p);
+        float *u1, *dv;
+        const float md = masclet_fields_dev(c, p, L, nhy, u1g, u2g, u3g, u4g, n, x, y, z, vx, vy, vz, m, &u1, &dv);
         c.mark("divergence");
         CubesDev cd{};
         const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, nullptr, nullptr, 0, cd, nullptr);

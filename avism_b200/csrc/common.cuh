@@ -65,6 +65,7 @@ enum BufId : int {
     B_LL_CNT, B_LL_OFF, B_LL_SUM,                  // their counts, offsets and per-void REAL*4 sums
     B_U1RAND, B_SMASK_IN,                          // survey: the randoms' grid, the inner mask
     B_GRID_IN,                                     // grid input: the four input grids
+    B_GAS1, B_GAS2, B_GAS3, B_GAS4, B_DIVER2,      // MASCLET input: the level's gas grids, the DM divergence
     B_NUM
 };
 
@@ -253,6 +254,15 @@ float survey_contrast(Ctx &c, const Level &L, const int8_t *smask, const float *
 // grid input: U1CO, DIVER and MEANDENS of the level from the input grids (NHY^3)
 float grid_fields_inner(Ctx &c, const avism_params *p, const Level &L, int nhy, const float *u1g, const float *u2g,
                         const float *u3g, const float *u4g, float *u1co_in, float *diver_in);
+// input grids given at NHY^3 on this level (copied, or SMOOTH_2-averaged below level 0)
+void level_grids(Ctx &c, const Level &L, const avism_params *p, int nhy, int ngrids, const float *const *g,
+                 float *const *co);
+// MASCLET input at levels <= 0: U1CO and DIVERCO (inner) from the gas grids and
+// the DM grids of particles_to_grid (u_mass and du* may be null when the flags
+// do not use them); returns MEANDENS
+float masclet_fields_inner(Ctx &c, const avism_params *p, const Level &L, int nhy, const float *const *gas,
+                           const float *u_mass, const float *du2, const float *du3, const float *du4, float *u1co_in,
+                           float *diver_in);
 
 // flags on the ext grid from inner (wrapped) fields, or from given ext fields.
 void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, const float *dv,

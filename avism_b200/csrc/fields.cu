@@ -381,42 +381,121 @@ __global__ void k_smooth2(int nx, int nhy, const int32_t *__restrict__ lo, const
 
 // U1CO = U1GCO, the divergence of (U2GCO, U3GCO, U4GCO), MEANDENS = ROTE*(UM/UL**3);
 // u1g..u4g: the input grid (NHY^3, device), the level's grid is p->nx = NHY * 2^IR
-float grid_fields_inner(Ctx &c, const avism_params *p, const Level &L, int nhy, const float *u1g, const float *u2g,
-                        const float *u3g, const float *u4g, float *u1co_in, float *diver_in) {
+// The level's copies of input grids given at NHY^3 (level 0): copied at
+// level 0, SMOOTH_2-averaged below it (src/amr2uniform.f90:65-120).
+void level_grids(Ctx &c, const Level &L, const avism_params *p, int nhy, int ngrids, const float *const *g,
+                 float *const *co) {
     const int nx = L.g.nx;
     const int64_t nc = (int64_t)nx * nx * nx;
+    if (nx == nhy) {                                   // IR = 0: U1GCO = U1G, ...
+        for (int q = 0; q < ngrids; q++)
+            AV_CUDA(cudaMemcpyAsync(co[q], g[q], sizeof(float) * (size_t)nc, cudaMemcpyDeviceToDevice, c.stream));
+        return;
+    }
+    // the input grid's coordinates (MALLA at NHY, src/avism.f90:366-382) and
+    // each input cell's coarse cell on this level
+    avism_params p0 = *p;
+    p0.nx = nhy;
+    const Level L0 = make_level(&p0);
+    const float dx = L.g.dx, dx0 = L0.g.dx, r1 = L.rad_at(1);
+    std::vector<int32_t> lo(nx, INT32_MAX), hi(nx, -1);
+    for (int ii = 1; ii <= nhy; ii++) {
+        const int I = (int)(((L0.rad_at(ii) - r1) / dx) + 0.5f) + 1;
+        AV_CHECK(I >= 1 && I <= nx, AVISM_ERR_ARG, "grid input: an input cell falls outside the level's grid");
+        lo[I - 1] = std::min(lo[I - 1], ii - 1);
+        hi[I - 1] = std::max(hi[I - 1], ii - 1);
+    }
+    const float wei = ((dx0 * dx0) * dx0) / ((dx * dx) * dx);
+    int32_t *d = c.get_t<int32_t>(B_LABMAP, 2 * (size_t)nx);
+    AV_CUDA(cudaMemcpyAsync(d, lo.data(), sizeof(int32_t) * nx, cudaMemcpyHostToDevice, c.stream));
+    AV_CUDA(cudaMemcpyAsync(d + nx, hi.data(), sizeof(int32_t) * nx, cudaMemcpyHostToDevice, c.stream));
+    for (int q = 0; q < ngrids; q++)
+        ++c.launches, k_smooth2<<<grid_for(nc, 256), 256, 0, c.stream>>>(nx, nhy, d, d + nx, wei, g[q], co[q]);
+    AV_CUDA(cudaGetLastError());
+    c.sync();                                          // lo / hi are host vectors
+}
+
+float grid_fields_inner(Ctx &c, const avism_params *p, const Level &L, int nhy, const float *u1g, const float *u2g,
+                        const float *u3g, const float *u4g, float *u1co_in, float *diver_in) {
+    const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
     const float *g[4] = {u1g, u2g, u3g, u4g};
     float *co[4] = {u1co_in, c.get_t<float>(B_U2, nc), c.get_t<float>(B_U3, nc), c.get_t<float>(B_U4, nc)};
-    if (nx == nhy) {                                   // IR = 0: U1GCO = U1G, ...
-        for (int q = 0; q < 4; q++)
-            AV_CUDA(cudaMemcpyAsync(co[q], g[q], sizeof(float) * (size_t)nc, cudaMemcpyDeviceToDevice, c.stream));
-    } else {
-        // the input grid's coordinates (MALLA at NHY, src/avism.f90:366-382) and
-        // each input cell's coarse cell on this level
-        avism_params p0 = *p;
-        p0.nx = nhy;
-        const Level L0 = make_level(&p0);
-        const float dx = L.g.dx, dx0 = L0.g.dx, r1 = L.rad_at(1);
-        std::vector<int32_t> lo(nx, INT32_MAX), hi(nx, -1);
-        for (int ii = 1; ii <= nhy; ii++) {
-            const int I = (int)(((L0.rad_at(ii) - r1) / dx) + 0.5f) + 1;
-            AV_CHECK(I >= 1 && I <= nx, AVISM_ERR_ARG, "grid input: an input cell falls outside the level's grid");
-            lo[I - 1] = std::min(lo[I - 1], ii - 1);
-            hi[I - 1] = std::max(hi[I - 1], ii - 1);
-        }
-        const float wei = ((dx0 * dx0) * dx0) / ((dx * dx) * dx);
-        int32_t *d = c.get_t<int32_t>(B_LABMAP, 2 * (size_t)nx);
-        AV_CUDA(cudaMemcpyAsync(d, lo.data(), sizeof(int32_t) * nx, cudaMemcpyHostToDevice, c.stream));
-        AV_CUDA(cudaMemcpyAsync(d + nx, hi.data(), sizeof(int32_t) * nx, cudaMemcpyHostToDevice, c.stream));
-        for (int q = 0; q < 4; q++)
-            ++c.launches, k_smooth2<<<grid_for(nc, 256), 256, 0, c.stream>>>(nx, nhy, d, d + nx, wei, g[q], co[q]);
-        AV_CUDA(cudaGetLastError());
-        c.sync();                                      // lo / hi are host vectors
-    }
+    level_grids(c, L, p, nhy, 4, g, co);
     c.mark("grid_input");
     divergence_inner(c, p, L, u1co_in, co[1], co[2], co[3], diver_in);
     const float ul3 = (UL_F * UL_F) * UL_F;
     return L.g.rote * (UM_F / ul3);
+}
+
+// ---- MASCLET input (FLAG_DATA = 0) at levels <= 0 -----------------------------
+// U1DMCO = (mass / (DXX*DYY*DZZ*RETE**3)) / ROTE (src/avism.f90:1065-1066), then
+// U1CO by FLAG_DENS (1371-1373): U1DMCO + U1GCO, U1DMCO or U1GCO, times ROTE
+// (1386)
+__global__ void k_masclet_rho(int64_t nc, const float *__restrict__ u_mass, const float *__restrict__ u1g, float vol,
+                              float rote, int flag_dens, float *__restrict__ u1) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    float dm = 0.0f;
+    if (flag_dens <= 1) {
+        dm = __fdiv_rn(u_mass[c], vol);
+        dm = __fdiv_rn(dm, rote);
+    }
+    const float u = flag_dens == 0 ? __fadd_rn(dm, u1g[c]) : (flag_dens == 1 ? dm : u1g[c]);
+    u1[c] = __fmul_rn(u, rote);
+}
+// DIVERCO = MIN(DIVERGCO, DIVERDMCO) (src/avism.f90:1636-1642)
+__global__ void k_min_into(int64_t nc, float *__restrict__ a, const float *__restrict__ b) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nc) a[c] = b[c] < a[c] ? b[c] : a[c];
+}
+
+float masclet_fields_inner(Ctx &c, const avism_params *p, const Level &L, int nhy, const float *const *gas,
+                           const float *u_mass, const float *du2, const float *du3, const float *du4, float *u1co_in,
+                           float *diver_in) {
+    const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
+    const bool need_gas_v = p->flag_div == 0 || p->flag_div == 2;
+    const int ng = need_gas_v ? 4 : 1;
+    float *co[4] = {c.get_t<float>(B_GAS1, nc), nullptr, nullptr, nullptr};
+    if (need_gas_v) {
+        co[1] = c.get_t<float>(B_GAS2, nc);
+        co[2] = c.get_t<float>(B_GAS3, nc);
+        co[3] = c.get_t<float>(B_GAS4, nc);
+    }
+    if (p->flag_dens != 1 || need_gas_v) level_grids(c, L, p, nhy, ng, gas, co);
+    const float dx = L.g.dx;
+    const float vol = ((dx * dx) * dx) * ((L.g.rete * L.g.rete) * L.g.rete);
+    ++c.launches, k_masclet_rho<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u_mass, co[0], vol, L.g.rote,
+                                                                        p->flag_dens, u1co_in);
+    AV_CUDA(cudaGetLastError());
+    // MEANDENS8: the REAL*8 sum over the cells (1389-1405), U1CO / MEANDENS
+    double *sum_d = c.get_t<double>(B_RED1, 1);
+    cub::TransformInputIterator<double, ToDouble, const float *> it(u1co_in, ToDouble());
+    size_t tmp = 0;
+    AV_CUDA(cub::DeviceReduce::Sum(nullptr, tmp, it, sum_d, (int)nc, c.stream));
+    AV_CUDA(cub::DeviceReduce::Sum(c.get(B_CUB_TMP, tmp), tmp, it, sum_d, (int)nc, c.stream));
+    double sum = 0.0;
+    AV_CUDA(cudaMemcpyAsync(&sum, sum_d, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    const float mean = (float)(sum / (double)nc);
+    ++c.launches, k_div_scalar<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u1co_in, mean);
+    c.mark("normalise");
+    // DIVERCO by FLAG_DIV (1633-1650)
+    avism_params pv = *p;
+    pv.no_velocities = p->flag_div == -1 ? 1 : 0;
+    if (p->flag_div == -1) {
+        divergence_inner(c, &pv, L, u1co_in, nullptr, nullptr, nullptr, diver_in);
+    } else {
+        if (need_gas_v) divergence_inner(c, &pv, L, u1co_in, co[1], co[2], co[3], diver_in);
+        if (p->flag_div == 1) divergence_inner(c, &pv, L, u1co_in, du2, du3, du4, diver_in);
+        if (p->flag_div == 0) {
+            float *dd = c.get_t<float>(B_DIVER2, nc);
+            divergence_inner(c, &pv, L, u1co_in, du2, du3, du4, dd);
+            ++c.launches, k_min_into<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, diver_in, dd);
+        }
+    }
+    AV_CUDA(cudaGetLastError());
+    const float ul3 = (UL_F * UL_F) * UL_F;
+    return mean * (UM_F / ul3);
 }
 
 __global__ void k_ext_copy(int nx, int low1, int ne, const float *__restrict__ inner, float *__restrict__ ext) {

@@ -10,6 +10,9 @@
 //  * survey inputs: the stream mask file (src/avism.f90:403-418, mapped onto
 //    the level's grid as src/avism.f90:873-901) and the randoms file
 //    (src/avism.f90:1425-1444);
+//  * MASCLET snapshots (READ_MASCLET, src/reader.f90:86-405): the grid file
+//    (text), the gas file and the dark-matter file (sequential unformatted);
+//    the level-0 gas grids and every level's particles are read;
 //  * the vel_cube.dat side dump of the SPH velocity grids
 //    (src/avism.f90:1198-1202, STREAM access);
 //  * the voids / cubes catalogues and the map of one iteration
@@ -21,6 +24,7 @@
 //    readers split on whitespace.
 #include <climits>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -71,6 +75,78 @@ bool read_particle_head(FILE *f, int64_t *n, float *zeta) {
 
 // 9 significant digits read back as the same REAL*4
 void put_f(FILE *f, float v) { std::fprintf(f, " %.9g", (double)v); }
+
+// one record of any length (or chain of subrecords), skipped
+bool skip_record(FILE *f) {
+    for (;;) {
+        int32_t head = 0, tail = 0;
+        if (std::fread(&head, 4, 1, f) != 1 || head == INT32_MIN) return false;
+        const int64_t len = head < 0 ? -(int64_t)head : head;
+        if (std::fseek(f, (long)len, SEEK_CUR) != 0) return false;
+        if (std::fread(&tail, 4, 1, f) != 1 || tail == INT32_MIN) return false;
+        if ((tail < 0 ? -(int64_t)tail : tail) != len) return false;
+        if (head >= 0) return true;
+    }
+}
+
+// list-directed input of a text file: the next `count` numbers (blank- or
+// comma-separated), starting on a new line and going on over the following
+// lines if one holds fewer (a READ(u,*) statement); count 0 skips one line
+bool read_values(FILE *f, int count, double *out) {
+    char line[4096];
+    int got = 0;
+    do {
+        if (!std::fgets(line, sizeof line, f)) return false;
+        char *s = line;
+        while (got < count) {
+            while (*s == ' ' || *s == '\t' || *s == ',' || *s == '\r' || *s == '\n') s++;
+            if (!*s) break;
+            char *e = nullptr;
+            const double v = std::strtod(s, &e);
+            if (e == s) return false;
+            out[got++] = v;
+            s = e;
+        }
+    } while (got < count);
+    return true;
+}
+
+// the MASCLET grid file (src/reader.f90:153-175): IRR, T, NL, MAP / ZETA /
+// IR, NDXYZ0, NST0, then per level IRR, NPATCH, NPART, NPARTST, a skipped line
+// and four lines per patch (sizes, cell offsets, corner, parent)
+struct MascletGrid {
+    int nl = 0, ndxyz0 = 0;
+    float t = 0.0f, map = 0.0f, zeta = 0.0f;
+    std::vector<int64_t> npatch, npart;           // levels 1..NL at [1..NL]
+};
+bool read_masclet_grid(const char *path, MascletGrid &g) {
+    File in(path, "r");
+    if (!in.f) return false;
+    double v[4];
+    if (!read_values(in.f, 4, v)) return false;
+    g.t = (float)v[1];
+    g.nl = (int)v[2];
+    g.map = (float)v[3];
+    if (!read_values(in.f, 1, v)) return false;
+    g.zeta = (float)v[0];
+    if (!read_values(in.f, 3, v)) return false;
+    g.ndxyz0 = (int)v[1];
+    if (g.nl < 0 || g.ndxyz0 < 0) return false;
+    g.npatch.assign(g.nl + 1, 0);
+    g.npart.assign(g.nl + 1, 0);
+    for (int ir = 1; ir <= g.nl; ir++) {
+        if (!read_values(in.f, 4, v)) return false;
+        g.npatch[ir] = (int64_t)v[1];
+        g.npart[ir] = (int64_t)v[2];
+        if (g.npatch[ir] < 0 || g.npart[ir] < 0) return false;
+        if (!read_values(in.f, 0, v)) return false;
+        for (int64_t i = 0; i < g.npatch[ir]; i++)
+            if (!read_values(in.f, 3, v) || !read_values(in.f, 3, v) || !read_values(in.f, 3, v) ||
+                !read_values(in.f, 1, v))
+                return false;
+    }
+    return true;
+}
 
 }  // namespace
 
@@ -126,6 +202,72 @@ int avism_io_read_grid(const char *path, int32_t nx, float *zeta, float *u1, flo
     const uint64_t bytes = (uint64_t)nx * (uint64_t)nx * (uint64_t)nx * 4;
     for (float *d : dst)
         if (!read_record(in.f, d, bytes)) return AVISM_ERR_IO;
+    return AVISM_OK;
+}
+
+int avism_io_masclet_header(const char *grid_path, int32_t *nl, int32_t *ndxyz0, int64_t *npartt, float *zeta,
+                            float *map) {
+    if (!grid_path) return AVISM_ERR_ARG;
+    MascletGrid g;
+    if (!read_masclet_grid(grid_path, g)) return AVISM_ERR_IO;
+    int64_t n = g.ndxyz0;
+    for (int ir = 1; ir <= g.nl; ir++) n += g.npart[ir];
+    if (nl) *nl = g.nl;
+    if (ndxyz0) *ndxyz0 = g.ndxyz0;
+    if (npartt) *npartt = n;
+    if (zeta) *zeta = g.zeta;
+    if (map) *map = g.map;
+    return AVISM_OK;
+}
+
+int avism_io_read_masclet(const char *grid_path, const char *gas_path, const char *dm_path, int32_t nhy,
+                          float *u1g, float *u2g, float *u3g, float *u4g, int64_t capacity, float *x, float *y,
+                          float *z, float *vx, float *vy, float *vz, float *m, int64_t *npartt) {
+    if (!grid_path || !gas_path || !dm_path || nhy < 1) return AVISM_ERR_ARG;
+    float *const gas[4] = {u1g, u2g, u3g, u4g};
+    float *const part[7] = {x, y, z, vx, vy, vz, m};
+    for (float *d : gas)
+        if (!d) return AVISM_ERR_ARG;
+    for (float *d : part)
+        if (!d) return AVISM_ERR_ARG;
+    MascletGrid g;
+    if (!read_masclet_grid(grid_path, g)) return AVISM_ERR_IO;
+    int64_t n = g.ndxyz0;
+    for (int ir = 1; ir <= g.nl; ir++) n += g.npart[ir];
+    if (n > capacity) return AVISM_ERR_ARG;                              // 'ERROR: NPARTT > PARTIRED'
+    const uint64_t cells = (uint64_t)nhy * (uint64_t)nhy * (uint64_t)nhy * 4;
+    // gas (src/reader.f90:259-273): a header record, then U1G, U2G, U3G, U4G at level 0
+    {
+        File in(gas_path, "rb");
+        if (!in.f || !skip_record(in.f)) return AVISM_ERR_IO;
+        for (float *d : gas)
+            if (!read_record(in.f, d, cells)) return AVISM_ERR_IO;
+    }
+    // dark matter (src/reader.f90:315-385): a header record, U1DM, the level-0
+    // particles' x, y, z, vx, vy, vz (mass MAP) and one more record; then per
+    // level one record per patch (U11DM) and the particles' seven columns with
+    // their masses, and one more record
+    {
+        File in(dm_path, "rb");
+        if (!in.f || !skip_record(in.f) || !skip_record(in.f)) return AVISM_ERR_IO;
+        int64_t conta = g.ndxyz0;
+        for (int q = 0; q < 6; q++)
+            if (!read_record(in.f, part[q], (uint64_t)g.ndxyz0 * 4)) return AVISM_ERR_IO;
+        if (!skip_record(in.f)) return AVISM_ERR_IO;
+        for (int64_t i = 0; i < g.ndxyz0; i++) m[i] = g.map;
+        for (int ir = 1; ir <= g.nl; ir++) {
+            for (int64_t i = 0; i < g.npatch[ir]; i++)
+                if (!skip_record(in.f)) return AVISM_ERR_IO;
+            for (int q = 0; q < 7; q++)
+                if (!read_record(in.f, part[q] + conta, (uint64_t)g.npart[ir] * 4)) return AVISM_ERR_IO;
+            if (!skip_record(in.f)) return AVISM_ERR_IO;
+            conta += g.npart[ir];
+        }
+    }
+    // delta to density (src/reader.f90:389-394)
+    const uint64_t nc = (uint64_t)nhy * (uint64_t)nhy * (uint64_t)nhy;
+    for (uint64_t c = 0; c < nc; c++) u1g[c] = u1g[c] + 1.0f;
+    if (npartt) *npartt = n;
     return AVISM_OK;
 }
 

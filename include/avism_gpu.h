@@ -70,7 +70,12 @@ typedef struct avism_params {
                                    linear-theory -Omega_m^0.6 a H (rho/rho_mean - 1)
                                    (src/avism.f90:1259-1306, 1647-1650); the
                                    velocity arrays may then be NULL               */
-    int32_t reserved[5];
+    int32_t flag_dens;          /* MASCLET input (FLAG_DATA = 0): FLAG_DENS, the density
+                                   components: 0 DM + gas, 1 DM, 2 gas            */
+    int32_t flag_div;           /* MASCLET input: FLAG_DIV, the divergence: 0 the
+                                   minimum of gas and DM, 1 DM, 2 gas, -1 linear
+                                   theory of the density (src/avism.f90:1633-1650) */
+    int32_t reserved[3];
 } avism_params;
 
 /* ---- level geometry (MALLA + PBC extension, src/avism.f90:780-865) ------ */
@@ -285,6 +290,34 @@ int avism_gpu_run_level_grid(avism_gpu_ctx *ctx, const avism_params *p, int32_t 
                              const float *u2g, const float *u3g, const float *u4g, avism_cubes *cubes,
                              int32_t *nvoid, avism_voids *voids, float *meandens);
 
+/* ---- MASCLET input (FLAG_DATA = 0) at levels <= 0: replaces the MASCLET branch
+ *      of the level loop (src/avism.f90:980-1156) with the density and
+ *      divergence choices of 1366-1405 and 1633-1650.  The dark-matter particles
+ *      (every level's particles as READ_MASCLET fills them, src/reader.f90:86-405:
+ *      positions [cMpc], velocities and masses in MASCLET units) go to the grid
+ *      as in the particle path (SPH or TSC by flag_vel_interp / flag_dens_interp),
+ *      U1DMCO = mass / (DX^3 a^3) / ROTE.  The gas grids u1g = 1 + delta and the
+ *      velocities u2g..u4g (nhy^3, level 0) are copied at level 0 and averaged by
+ *      SMOOTH_2 (src/amr2uniform.f90:65-120) below it.  U1CO = (U1DMCO + U1GCO,
+ *      U1DMCO or U1GCO by flag_dens) * ROTE / its REAL*8 mean; DIVERCO by
+ *      flag_div: the minimum of the DIVER_UNIFORM of the gas and of the DM
+ *      velocities (0), DM (1), gas (2), or the linear theory of U1CO (-1).  The
+ *      particle arrays may be NULL (n = 0) when neither flag uses the dark
+ *      matter (flag_dens = 2 and flag_div = 2 or -1); u2g..u4g may be NULL when
+ *      flag_div is 1 or -1.  Levels above 0 (the AMR patches: VMESH and
+ *      DIVER_FINA_GAS) return AVISM_ERR_UNSUPPORTED.
+ *      avism_gpu_masclet_fields returns the ext grids (as avism_gpu_fields),
+ *      avism_gpu_run_level_masclet the level's catalogue.                       */
+int avism_gpu_masclet_fields(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g,
+                             const float *u2g, const float *u3g, const float *u4g, int64_t n, const float *x,
+                             const float *y, const float *z, const float *vx, const float *vy, const float *vz,
+                             const float *m, float *u1co_ext, float *diverco_ext, float *meandens);
+int avism_gpu_run_level_masclet(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g,
+                                const float *u2g, const float *u3g, const float *u4g, int64_t n, const float *x,
+                                const float *y, const float *z, const float *vx, const float *vy,
+                                const float *vz, const float *m, avism_cubes *cubes, int32_t *nvoid,
+                                avism_voids *voids, float *meandens);
+
 /* ---- survey mode (FLAG_SURVEY = 1): replaces src/avism.f90:1420-1596.  The
  *      tracers (x..m, masses as weights; velocities nullable with
  *      no_velocities = 1) and the randoms (rx, ry, rz, weights rw, in the units
@@ -375,6 +408,22 @@ int avism_io_read_particles_novel(const char *path, int64_t capacity, float *x, 
  * velocities by UV (src/reader.f90:546-550); avism_gpu_run_level_grid expects
  * those converted values.                                                     */
 int avism_io_read_grid(const char *path, int32_t nx, float *zeta, float *u1, float *u2, float *u3, float *u4);
+/* MASCLET snapshot (READ_MASCLET, src/reader.f90:86-405): the grid file (text:
+ * IRR T NL MAP / ZETA / IR NDXYZ0 NST0, then per level IRR NPATCH NPART NPARTST,
+ * a skipped line and four lines per patch), the gas file and the dark-matter
+ * file (sequential unformatted).  avism_io_masclet_header gives the number of
+ * levels, the level-0 particle count, NPARTT (all levels), ZETA and MAP (the
+ * level-0 particle mass).  avism_io_read_masclet reads the level-0 gas grids
+ * u1g..u4g (nhy^3; u1g = the stored delta + 1, as src/reader.f90:389-394) and
+ * every level's DM particles into x..m (level 0 first, masses MAP; then each
+ * level's particles with their stored masses); the AMR patches' grids are
+ * skipped.  AVISM_ERR_ARG when NPARTT > capacity, AVISM_ERR_IO on a record
+ * that is missing or of the wrong length.                                     */
+int avism_io_masclet_header(const char *grid_path, int32_t *nl, int32_t *ndxyz0, int64_t *npartt, float *zeta,
+                            float *map);
+int avism_io_read_masclet(const char *grid_path, const char *gas_path, const char *dm_path, int32_t nhy,
+                          float *u1g, float *u2g, float *u3g, float *u4g, int64_t capacity, float *x, float *y,
+                          float *z, float *vx, float *vy, float *vz, float *m, int64_t *npartt);
 /* Survey mask (src/avism.f90:403-418): a stream file [int32 NMASK, REAL*4
  * MASKLOW, MASKUPPER, MASKSIDE, INTEGER*1 SMASK2(NMASK^3)].  NMASK must equal
  * ncox (the coarse grid, else AVISM_ERR_ARG as the reference's stop); the mask

@@ -115,6 +115,17 @@ int orc_survey_fields(const avism_params *p, int64_t n, const float *x, const fl
 /* grid input (FLAG_DATA = 2, src/avism.f90:1316-1362; SMOOTH_2 below level 0) */
 int orc_grid_fields(const avism_params *p, int32_t nhy, const float *u1g, const float *u2g, const float *u3g,
                     const float *u4g, float *u1co_ext, float *diverco_ext, float *meandens);
+/* the level's copies (level 0) or SMOOTH_2 averages (below it) of NHY^3 grids;
+ * co[q] must hold zeros */
+void orc_level_grids(const avism_params *p, int32_t nhy, int ngrids, const float *const *in, float *const *co);
+
+/* MASCLET input (FLAG_DATA = 0) at levels <= 0 (src/avism.f90:980-1156,
+ * 1366-1405, 1633-1650): DM particles and gas grids, combined by FLAG_DENS /
+ * FLAG_DIV; the particle arrays may be NULL when the flags do not use them */
+int orc_masclet_fields(const avism_params *p, int32_t nhy, const float *u1g, const float *u2g, const float *u3g,
+                       const float *u4g, int64_t n, const float *x, const float *y, const float *z,
+                       const float *vx, const float *vy, const float *vz, const float *m, float *u1co_ext,
+                       float *diverco_ext, float *meandens);
 
 #ifdef __cplusplus
 }

@@ -138,6 +138,42 @@ int orc_survey_fields(const avism_params *p, int64_t n, const float *x, const fl
     return st;
 }
 
+/* The level's copies of grids given at NHY^3 (level 0): copied at level 0;
+ * below it SMOOTH_2 (src/amr2uniform.f90:65-120): a serial scatter of U*WEI
+ * into the coarse cell of every input cell, K, J, I order.  co[q] hold zeros. */
+void orc_level_grids(const avism_params *p, int32_t nhy, int ngrids, const float *const *in, float *const *co)
+{
+    avism_grid g, g0;
+    orc_grid_setup(p, &g, NULL);
+    const int nx = g.nx;
+    const int64_t nc = (int64_t)nx * nx * nx;
+    if (nx == nhy) {
+        for (int q = 0; q < ngrids; q++) memcpy(co[q], in[q], (size_t)nc * sizeof(float));
+        return;
+    }
+    float *radx = (float *)malloc((size_t)(g.rad_hi - g.rad_lo + 1) * sizeof(float));
+    orc_grid_setup(p, &g, radx);
+    avism_params p0 = *p;
+    p0.nx = nhy;
+    orc_grid_setup(&p0, &g0, NULL);
+    float *rad0 = (float *)malloc((size_t)(g0.rad_hi - g0.rad_lo + 1) * sizeof(float));
+    orc_grid_setup(&p0, &g0, rad0);
+    const float dx = g.dx, dx0 = g0.dx, r1 = radx[1 - g.rad_lo];
+    const float wei = ((dx0 * dx0) * dx0) / ((dx * dx) * dx);
+    for (int kk = 1; kk <= nhy; kk++)
+        for (int jj = 1; jj <= nhy; jj++)
+            for (int ii = 1; ii <= nhy; ii++) {
+                const int i = (int)(((rad0[ii - g0.rad_lo] - r1) / dx) + 0.5f) + 1;
+                const int j = (int)(((rad0[jj - g0.rad_lo] - r1) / dx) + 0.5f) + 1;
+                const int k = (int)(((rad0[kk - g0.rad_lo] - r1) / dx) + 0.5f) + 1;
+                const int64_t c = (int64_t)(i - 1) + (int64_t)nx * ((int64_t)(j - 1) + (int64_t)nx * (k - 1));
+                const int64_t f = (int64_t)(ii - 1) + (int64_t)nhy * ((int64_t)(jj - 1) + (int64_t)nhy * (kk - 1));
+                for (int q = 0; q < ngrids; q++) co[q][c] = co[q][c] + in[q][f] * wei;
+            }
+    free(rad0);
+    free(radx);
+}
+
 /* Grid input (FLAG_DATA = 2, src/avism.f90:1316-1362): U1CO = U1GCO, MEANDENS =
  * ROTE*(UM/UL**3), DIVERCO = DIVER_UNIFORM of the velocities.  Levels below 0
  * take SMOOTH_2 (src/amr2uniform.f90:65-120) of the NHY^3 input grids: a serial
@@ -145,7 +181,7 @@ int orc_survey_fields(const avism_params *p, int64_t n, const float *x, const fl
 int orc_grid_fields(const avism_params *p, int32_t nhy, const float *u1g, const float *u2g, const float *u3g,
                     const float *u4g, float *u1co_ext, float *diverco_ext, float *meandens)
 {
-    avism_grid g, g0;
+    avism_grid g;
     int st = orc_grid_setup(p, &g, NULL);
     if (st) return st;
     if (p->level > 0) return AVISM_ERR_UNSUPPORTED;          /* 'LEVEL > 0 FOR BIN_GRID NOT IMPLEMENTED YET' */
@@ -156,30 +192,7 @@ int orc_grid_fields(const avism_params *p, int32_t nhy, const float *u1g, const 
     for (int q = 0; q < 4; q++) co[q] = (float *)calloc((size_t)nc, sizeof(float));
     float *d = (float *)malloc((size_t)nc * sizeof(float));
     const float *in[4] = {u1g, u2g, u3g, u4g};
-    float *radx = (float *)malloc((size_t)(g.rad_hi - g.rad_lo + 1) * sizeof(float));
-    orc_grid_setup(p, &g, radx);
-    if (nx == nhy) {
-        for (int q = 0; q < 4; q++) memcpy(co[q], in[q], (size_t)nc * sizeof(float));
-    } else {
-        avism_params p0 = *p;
-        p0.nx = nhy;
-        orc_grid_setup(&p0, &g0, NULL);
-        float *rad0 = (float *)malloc((size_t)(g0.rad_hi - g0.rad_lo + 1) * sizeof(float));
-        orc_grid_setup(&p0, &g0, rad0);
-        const float dx = g.dx, dx0 = g0.dx, r1 = radx[1 - g.rad_lo];
-        const float wei = ((dx0 * dx0) * dx0) / ((dx * dx) * dx);
-        for (int kk = 1; kk <= nhy; kk++)
-            for (int jj = 1; jj <= nhy; jj++)
-                for (int ii = 1; ii <= nhy; ii++) {
-                    const int i = (int)(((rad0[ii - g0.rad_lo] - r1) / dx) + 0.5f) + 1;
-                    const int j = (int)(((rad0[jj - g0.rad_lo] - r1) / dx) + 0.5f) + 1;
-                    const int k = (int)(((rad0[kk - g0.rad_lo] - r1) / dx) + 0.5f) + 1;
-                    const int64_t c = (int64_t)(i - 1) + (int64_t)nx * ((int64_t)(j - 1) + (int64_t)nx * (k - 1));
-                    const int64_t f = (int64_t)(ii - 1) + (int64_t)nhy * ((int64_t)(jj - 1) + (int64_t)nhy * (kk - 1));
-                    for (int q = 0; q < 4; q++) co[q][c] = co[q][c] + in[q][f] * wei;
-                }
-        free(rad0);
-    }
+    orc_level_grids(p, nhy, 4, in, co);
     orc_diver_uniform(nx, g.dx, co[1], co[2], co[3], p->periodic, d);
     for (int kz = 0; kz < ne; kz++)
         for (int jy = 0; jy < ne; jy++)
@@ -197,6 +210,5 @@ int orc_grid_fields(const avism_params *p, int32_t nhy, const float *u1g, const 
     *meandens = g.rote * (UM_F / ul3);
     for (int q = 0; q < 4; q++) free(co[q]);
     free(d);
-    free(radx);
     return AVISM_OK;
 }
