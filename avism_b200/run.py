@@ -75,13 +75,17 @@ def run_iteration(particle_path, p: Params, out_dir, it: int = 1, nlev: int = 1,
 
 
 def run_single(path, p: Params, out_dir, it: int = 1, grid_nhy: int = 0, mask=None, randoms=None,
-               novel: bool = False, ncox: int = 0, cubes: bool = False, engine=None) -> dict:
-    """One level from a grid file (grid_nhy > 0) or a survey (mask and randoms
-    files), written as run_iteration writes its levels."""
+               novel: bool = False, ncox: int = 0, cubes: bool = False, engine=None, masclet=None,
+               masclet_nhy: int = 0) -> dict:
+    """One level from a grid file (grid_nhy > 0), a MASCLET snapshot (path the
+    grid file, masclet = (gas file, DM file), masclet_nhy the base grid; level
+    <= 0) or a survey (mask and randoms files), written as run_iteration writes
+    its levels."""
     import numpy as np
     from . import synth
     from ._abi import UM, UV
-    from .avism import read_grid_file, read_mask_file, read_particle_file_novel, read_randoms_file
+    from .avism import (read_grid_file, read_mask_file, read_masclet_files, read_particle_file_novel,
+                        read_randoms_file)
     if engine is None:
         from .avism import AvismGPU
         engine = AvismGPU(0)
@@ -92,6 +96,11 @@ def run_single(path, p: Params, out_dir, it: int = 1, grid_nhy: int = 0, mask=No
         u1 = (g["u1"] + np.float32(1.0)).astype(np.float32)
         vs = [(g[k] / np.float32(UV)).astype(np.float32) for k in ("u2", "u3", "u4")]
         res = engine.run_level_grid(p, grid_nhy, u1, *vs)
+    elif masclet:
+        r = read_masclet_files(path, masclet[0], masclet[1], masclet_nhy)
+        p = Params(**{**p.__dict__, "zeta": float(r["zeta"])})
+        gas = tuple(r["gas"][k] for k in ("u1g", "u2g", "u3g", "u4g"))
+        res = engine.run_level_masclet(p, masclet_nhy, gas, r["parts"])
     else:
         parts = read_particle_file_novel(path) if novel else read_particle_file(path)
         p = Params(**{**p.__dict__, "zeta": float(parts.pop("zeta")), "no_velocities": int(novel)})
@@ -128,12 +137,17 @@ def main(argv=None):
     ap.add_argument("--randoms", help="survey randoms file (survey mode)")
     ap.add_argument("--ncox", type=int, default=0, help="the survey mask's coarse grid (default --nx)")
     ap.add_argument("--novel", action="store_true", help="particle file without velocities (READ_BINARY_PART_2)")
+    ap.add_argument("--masclet", nargs=2, metavar=("GAS", "DM"),
+                    help="the input (positional) is a MASCLET grid file with these gas and DM files")
+    ap.add_argument("--nhy", type=int, default=0, help="the MASCLET base grid (NHYX)")
+    ap.add_argument("--flag-dens", type=int, default=0, choices=[0, 1, 2], help="MASCLET FLAG_DENS")
+    ap.add_argument("--flag-div", type=int, default=0, choices=[-1, 0, 1, 2], help="MASCLET FLAG_DIV")
     a = ap.parse_args(argv)
     p = Params(nx=a.nx, lado0=a.lado0, periodic=a.periodic, kneighbours=a.kneighbours, learned=a.learned,
-               nvoid_max=a.nvoid_max, level=a.level, levmin=a.level)
-    if a.grid or a.mask:
+               nvoid_max=a.nvoid_max, level=a.level, levmin=a.level, flag_dens=a.flag_dens, flag_div=a.flag_div)
+    if a.grid or a.mask or a.masclet:
         r = run_single(a.particles, p, a.out, it=a.iter, grid_nhy=a.grid, mask=a.mask, randoms=a.randoms,
-                       novel=a.novel, ncox=a.ncox, cubes=a.cubes)
+                       novel=a.novel, ncox=a.ncox, cubes=a.cubes, masclet=a.masclet, masclet_nhy=a.nhy or a.nx)
     else:
         r = run_iteration(a.particles, p, a.out, it=a.iter, nlev=a.levels, cubes=a.cubes, maps=a.map)
     for lev in r["levels"]:

@@ -35,7 +35,9 @@ def test_fields_and_level_exact(gpu, snap, fd, fv, lev):
     assert np.array_equal(u1o, u1g) and np.array_equal(dvo, dvg) and mdo == mdg
     o = O.run_level_masclet(p, snap["ng"], mc.gas(snap), parts)
     g = gpu.run_level_masclet(p, snap["ng"], mc.gas(snap), parts, capacity=200000)
-    assert g["nvoid"] == o["vf"]["nvoid"] > 0
+    assert g["nvoid"] == o["vf"]["nvoid"]
+    if lev == 0:
+        assert g["nvoid"] > 0                    # (at 16^3 the mock's voids fall below NCELL_MIN)
     for k in g["cubes"]:
         assert np.array_equal(g["cubes"][k], o["vf"]["cubes"][k]), k
     for k in ("indice", "uvoid", "ncellv", "volnew", "req", "gxc", "gyc", "gzc", "eps", "ip", "umean", "mtot"):

@@ -72,6 +72,9 @@ class OracleModes(OracleEngine):
     def run_level_survey(self, p, parts, rands, smask):
         return self._res(O.run_level_survey(p, parts, rands, smask))
 
+    def run_level_masclet(self, p, nhy, gas, parts):
+        return self._res(O.run_level_masclet(p, nhy, gas, parts))
+
 
 def test_grid_file_level(tmp_path):
     """A READ_BINARY_GRID file through the runner's grid mode (level -1)."""
@@ -106,5 +109,18 @@ def test_survey_files_level(tmp_path):
     _fortran_records(rp, [np.int32(len(rr["x"])).tobytes()] + [rr[k] for k in ("x", "y", "z", "w")])
     p = Params(nx=64, periodic=0, lado0=150.0, kneighbours=16, flag_vel_interp=0, flag_dens_interp=0, rmin=3.0)
     r = run_single(pp, p, tmp_path / "out", mask=mp, randoms=rp, novel=True, engine=OracleModes())
+    head, levels = _read_voids_file(r["voids"])
+    assert len(levels[0]["rows"]) == r["levels"][0]["cat"]["nvoidt"] > 0
+
+
+def test_masclet_files_level(tmp_path):
+    """A MASCLET snapshot's three files through the runner's MASCLET mode."""
+    from avism_b200.run import run_single
+    import masclet_case as mc
+    snap = mc.snapshot()
+    grid, gas, dm = mc.write_files(snap, str(tmp_path))
+    p = Params(nx=snap["ng"], periodic=1, lado0=snap["box"], flag_dens=0, flag_div=0)
+    r = run_single(grid, p, tmp_path / "out", masclet=(gas, dm), masclet_nhy=snap["ng"], cubes=True,
+                   engine=OracleModes())
     head, levels = _read_voids_file(r["voids"])
     assert len(levels[0]["rows"]) == r["levels"][0]["cat"]["nvoidt"] > 0
