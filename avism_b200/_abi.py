@@ -46,6 +46,32 @@ class AvismParams(C.Structure):
     ]
 
 
+class AvismPatchesC(C.Structure):
+    """avism_patches: a MASCLET snapshot's level-1 patches."""
+    _fields_ = ([("npatch", C.c_int32)] +
+                [(n, C.POINTER(C.c_int32)) for n in ("nx", "ny", "nz", "ix", "iy", "iz")] +
+                [(n, C.POINTER(C.c_float)) for n in ("rx", "ry", "rz")] +
+                [("offset", C.POINTER(C.c_int64))] +
+                [(n, C.POINTER(C.c_float)) for n in ("u11g", "u12g", "u13g", "u14g")])
+
+
+def patches_c(amr: dict):
+    """(AvismPatchesC, arrays to keep alive) of a dict with the patch sizes
+    nx..nz, first base cells ix..iz, corners rx..rz, offsets (npatch + 1) and
+    the cells u11g..u14g."""
+    keep = {}
+    for k in ("nx", "ny", "nz", "ix", "iy", "iz"):
+        keep[k] = np.ascontiguousarray(amr[k], np.int32)
+    for k in ("rx", "ry", "rz", "u11g", "u12g", "u13g", "u14g"):
+        keep[k] = np.ascontiguousarray(amr[k], np.float32)
+    keep["offset"] = np.ascontiguousarray(amr["offset"], np.int64)
+    s = AvismPatchesC(npatch=len(keep["nx"]))
+    for k, v in keep.items():
+        ct = C.c_int32 if v.dtype == np.int32 else (C.c_int64 if v.dtype == np.int64 else C.c_float)
+        setattr(s, k, v.ctypes.data_as(C.POINTER(ct)))
+    return s, keep
+
+
 class AvismGrid(C.Structure):
     _fields_ = [
         ("nx", C.c_int32), ("nplus", C.c_int32), ("low1", C.c_int32), ("low2", C.c_int32),

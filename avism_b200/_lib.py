@@ -42,8 +42,8 @@ SIGNATURES = {
     "avism_gpu_run_sublevel": (C.c_int, [_c_void, _c_void, _i64] + [_c_void] * 9 + [_i32] + [_c_void] * 4),
     "avism_gpu_grid_fields": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 7),
     "avism_gpu_run_level_grid": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 8),
-    "avism_gpu_masclet_fields": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 4 + [_i64] + [_c_void] * 10),
-    "avism_gpu_run_level_masclet": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 4 + [_i64] + [_c_void] * 11),
+    "avism_gpu_masclet_fields": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 5 + [_i64] + [_c_void] * 10),
+    "avism_gpu_run_level_masclet": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 5 + [_i64] + [_c_void] * 11),
     "avism_gpu_survey_fields": (C.c_int, [_c_void, _c_void, _i64] + [_c_void] * 7 + [_i64] + [_c_void] * 9),
     "avism_gpu_run_level_survey": (C.c_int, [_c_void, _c_void, _i64] + [_c_void] * 7 + [_i64] + [_c_void] * 9),
     "avism_gpu_knn_noalloc": (C.c_int, [C.c_int, _c_void, _i64, _c_void, _c_void, _c_void, _f32, _i64,
@@ -56,6 +56,8 @@ SIGNATURES = {
     "avism_io_masclet_header": (C.c_int, [C.c_char_p, _c_void, _c_void, _c_void, _c_void, _c_void]),
     "avism_io_read_masclet": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, _i32] + [_c_void] * 4 + [_i64] +
                               [_c_void] * 8),
+    "avism_io_masclet_patches_size": (C.c_int, [C.c_char_p, _c_void, _c_void]),
+    "avism_io_read_masclet_patches": (C.c_int, [C.c_char_p, C.c_char_p, _i32, _i32, _i64] + [_c_void] * 14),
     "avism_io_read_mask": (C.c_int, [C.c_char_p, _i32, _i32, _c_void, _c_void]),
     "avism_io_randoms_header": (C.c_int, [C.c_char_p, _c_void]),
     "avism_io_read_randoms": (C.c_int, [C.c_char_p, _i32] + [_c_void] * 4),

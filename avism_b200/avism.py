@@ -123,7 +123,34 @@ def read_masclet_files(grid_path, gas_path, dm_path, nhy) -> dict:
                                       *(_vp(parts[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")),
                                       C.byref(got)), f"MASCLET files {gas_path}, {dm_path}")
     parts = {k: v[:got.value] for k, v in parts.items()}
-    return dict(gas=gas, parts=parts, nl=nl.value, ndxyz0=nd0.value, zeta=zeta.value, map=mp.value)
+    out = dict(gas=gas, parts=parts, nl=nl.value, ndxyz0=nd0.value, zeta=zeta.value, map=mp.value)
+    out["amr"] = read_masclet_patches(grid_path, gas_path, nhy) if nl.value >= 1 else None
+    return out
+
+
+def read_masclet_patches(grid_path, gas_path, nhy) -> dict:
+    """The level-1 patches of a MASCLET snapshot (src/reader.f90:168-174,
+    285-312, 393) as the `amr` argument of masclet_fields / run_level_masclet:
+    nx..nz, ix..iz, rx..rz per patch, offset (npatch + 1) and the cells
+    u11g (delta + 1), u12g, u13g, u14g."""
+    lib = _lib.load()
+    np_, nc = C.c_int32(), C.c_int64()
+    _io_chk(lib.avism_io_masclet_patches_size(_path(grid_path), C.byref(np_), C.byref(nc)),
+            f"MASCLET grid file {grid_path}")
+    npatch, ncells = np_.value, nc.value
+    out = {k: np.zeros(max(npatch, 1), np.int32) for k in ("nx", "ny", "nz", "ix", "iy", "iz")}
+    out.update({k: np.zeros(max(npatch, 1), np.float32) for k in ("rx", "ry", "rz")})
+    out["offset"] = np.zeros(npatch + 1, np.int64)
+    out.update({k: np.zeros(max(ncells, 1), np.float32) for k in ("u11g", "u12g", "u13g", "u14g")})
+    _io_chk(lib.avism_io_read_masclet_patches(
+        _path(grid_path), _path(gas_path), int(nhy), npatch, ncells,
+        *(_vp(out[k]) for k in ("nx", "ny", "nz", "ix", "iy", "iz", "rx", "ry", "rz", "offset",
+                                "u11g", "u12g", "u13g", "u14g"))), f"MASCLET gas file {gas_path}")
+    for k in ("nx", "ny", "nz", "ix", "iy", "iz", "rx", "ry", "rz"):
+        out[k] = out[k][:npatch]
+    for k in ("u11g", "u12g", "u13g", "u14g"):
+        out[k] = out[k][:ncells]
+    return out
 
 
 def read_mask_file(path, ncox, nx):
@@ -410,9 +437,12 @@ class AvismGPU:
         return dict(cubes=cubes.view(nv.value), nvoid=nv.value, cat=vo.view(nv.value), meandens=md.value)
 
     # ---- MASCLET input (FLAG_DATA = 0) at levels <= 0 (src/avism.f90:980-1156) ------
-    def _masclet_args(self, nhy, gas, parts):
+    def _masclet_args(self, nhy, gas, parts, amr=None):
         """gas: (u1g = 1 + delta, u2g, u3g, u4g) at nhy^3 (velocity grids may be
-        None when params.flag_div is 1 or -1); parts: the DM particles or None."""
+        None when params.flag_div is 1 or -1 below level 1); parts: the DM
+        particles or None; amr: the level-1 patches (a dict, see patches_c)."""
+        from ._abi import patches_c
+        pc_amr, keep_amr = patches_c(amr) if amr is not None else (None, None)
         g = tuple(None if a is None else _f32(a) for a in gas)
         if parts is None:
             a = {k: None for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
@@ -421,21 +451,22 @@ class AvismGPU:
             a = {k: (_f32(parts[k]) if parts.get(k) is not None else None)
                  for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
             n = len(a["x"])
-        args = (int(nhy), *(_vp(x) for x in g), n, *(_vp(a[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")))
-        return args, (g, a)
+        args = (int(nhy), *(_vp(x) for x in g), C.byref(pc_amr) if pc_amr is not None else None, n,
+                *(_vp(a[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")))
+        return args, (g, a, pc_amr, keep_amr)
 
-    def masclet_fields(self, p: Params, nhy, gas, parts=None):
+    def masclet_fields(self, p: Params, nhy, gas, parts=None, amr=None):
         """(U1CO ext, DIVERCO ext, MEANDENS) of a MASCLET snapshot's level."""
         gr, _ = grid_setup(p)
         u1 = np.zeros(gr.ne ** 3, np.float32)
         dv = np.zeros(gr.ne ** 3, np.float32)
         md = C.c_float()
         pc = p.to_c()
-        args, _keep = self._masclet_args(nhy, gas, parts)
+        args, _keep = self._masclet_args(nhy, gas, parts, amr)
         self._chk(self.lib.avism_gpu_masclet_fields(self.h, C.byref(pc), *args, _vp(u1), _vp(dv), C.byref(md)))
         return u1, dv, md.value
 
-    def run_level_masclet(self, p: Params, nhy, gas, parts=None, want_marca=False, capacity=None):
+    def run_level_masclet(self, p: Params, nhy, gas, parts=None, amr=None, want_marca=False, capacity=None):
         gr, _ = grid_setup(p)
         cap = int(capacity or p.nvoid_max)
         cubes = Cubes(cap)
@@ -443,7 +474,7 @@ class AvismGPU:
         nv, md = C.c_int32(), C.c_float()
         pc = p.to_c()
         pc.nvoid_max = min(p.nvoid_max, cap)
-        args, _keep = self._masclet_args(nhy, gas, parts)
+        args, _keep = self._masclet_args(nhy, gas, parts, amr)
         self._chk(self.lib.avism_gpu_run_level_masclet(self.h, C.byref(pc), *args, C.byref(cubes.c), C.byref(nv),
                                                        C.byref(vo.c), C.byref(md)))
         return dict(cubes=cubes.view(nv.value), nvoid=nv.value, cat=vo.view(nv.value), meandens=md.value)

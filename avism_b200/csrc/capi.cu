@@ -802,17 +802,61 @@ int avism_gpu_run_level_grid(avism_gpu_ctx *ctx, const avism_params *p, int32_t 
 
 // ---- MASCLET input (FLAG_DATA = 0) at levels <= 0 ------------------------------
 namespace {
+// the level-1 patches: geometry to host vectors, cells to the device
+void host_bytes(void *dst, const void *src, size_t bytes) {
+    if (bytes) AV_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDefault));
+}
+void host_i32(std::vector<int32_t> &dst, const int32_t *src, size_t n) {
+    dst.resize(n);
+    host_bytes(dst.data(), src, sizeof(int32_t) * n);
+}
+void host_f32(std::vector<float> &dst, const float *src, size_t n) {
+    dst.resize(n);
+    host_bytes(dst.data(), src, sizeof(float) * n);
+}
+void host_i64(std::vector<int64_t> &dst, const int64_t *src, size_t n) {
+    dst.resize(n);
+    host_bytes(dst.data(), src, sizeof(int64_t) * n);
+}
+AmrPatches amr_patches(Ctx &c, const avism_patches *a) {
+    AV_CHECK(a && a->npatch >= 0 && a->offset, AVISM_ERR_ARG, "MASCLET level 1: the patches are required");
+    AmrPatches r;
+    const size_t np = (size_t)a->npatch;
+    r.npatch = a->npatch;
+    AV_CHECK(np == 0 || (a->nx && a->ny && a->nz && a->ix && a->iy && a->iz && a->rx && a->ry && a->rz),
+             AVISM_ERR_ARG, "MASCLET level 1: null patch geometry");
+    host_i32(r.nx, a->nx, np); host_i32(r.ny, a->ny, np); host_i32(r.nz, a->nz, np);
+    host_i32(r.ix, a->ix, np); host_i32(r.iy, a->iy, np); host_i32(r.iz, a->iz, np);
+    host_f32(r.rx, a->rx, np); host_f32(r.ry, a->ry, np); host_f32(r.rz, a->rz, np);
+    host_i64(r.offset, a->offset, np + 1);
+    AV_CHECK(r.offset[0] >= 0, AVISM_ERR_ARG, "MASCLET level 1: negative patch offset");
+    for (size_t q = 0; q < np; q++)
+        AV_CHECK(r.nx[q] >= 1 && r.ny[q] >= 1 && r.nz[q] >= 1 &&
+                     r.offset[q + 1] - r.offset[q] == (int64_t)r.nx[q] * r.ny[q] * r.nz[q],
+                 AVISM_ERR_ARG, "MASCLET level 1: patch sizes and offsets disagree");
+    const size_t cells = sizeof(float) * (size_t)std::max<int64_t>(r.offset[np], 1);
+    AV_CHECK(a->u11g && a->u12g && a->u13g && a->u14g, AVISM_ERR_ARG, "MASCLET level 1: null patch cells");
+    r.u11g = (const float *)to_device(c, B_AMR1, a->u11g, cells);
+    r.u12g = (const float *)to_device(c, B_AMR2, a->u12g, cells);
+    r.u13g = (const float *)to_device(c, B_AMR3, a->u13g, cells);
+    r.u14g = (const float *)to_device(c, B_AMR4, a->u14g, cells);
+    return r;
+}
+
 float masclet_fields_dev(Ctx &c, const avism_params *p, const Level &L, int32_t nhy, const float *u1g,
-                         const float *u2g, const float *u3g, const float *u4g, int64_t n, const float *x,
-                         const float *y, const float *z, const float *vx, const float *vy, const float *vz,
-                         const float *m, float **u1_out, float **dv_out) {
-    AV_CHECK(p->level <= 0, AVISM_ERR_UNSUPPORTED,
-             "MASCLET input: levels above 0 (AMR patches: VMESH, DIVER_FINA_GAS) are not implemented");
-    AV_CHECK(nhy >= 4 && (int64_t)p->nx << (-p->level) == (int64_t)nhy, AVISM_ERR_ARG,
-             "MASCLET input: params.nx must be nhy * 2^level (level <= 0)");
+                         const float *u2g, const float *u3g, const float *u4g, const avism_patches *amr, int64_t n,
+                         const float *x, const float *y, const float *z, const float *vx, const float *vy,
+                         const float *vz, const float *m, float **u1_out, float **dv_out) {
+    AV_CHECK(p->level <= 1, AVISM_ERR_UNSUPPORTED,
+             "MASCLET input: levels above 1 are not implemented (the reference's VMESH indexes its base-size "
+             "refinement flags beyond them there)");
+    AV_CHECK(nhy >= 4 && (p->level == 1 ? p->nx == 2 * nhy : (int64_t)p->nx << (-p->level) == (int64_t)nhy),
+             AVISM_ERR_ARG, "MASCLET input: params.nx must be nhy * 2^level");
     const bool need_dm = p->flag_dens <= 1 || p->flag_div == 0 || p->flag_div == 1;
-    const bool need_gas_v = p->flag_div == 0 || p->flag_div == 2;
+    const bool need_gas_v = p->level == 1 || p->flag_div == 0 || p->flag_div == 2;
     AV_CHECK(u1g && (!need_gas_v || (u2g && u3g && u4g)), AVISM_ERR_ARG, "MASCLET input: null gas grid");
+    AmrPatches ap;
+    if (p->level == 1) ap = amr_patches(c, amr);
     const int64_t n0 = (int64_t)nhy * nhy * nhy;
     const float *g[4] = {nullptr, nullptr, nullptr, nullptr};
     const float *src[4] = {u1g, u2g, u3g, u4g};
@@ -832,7 +876,7 @@ float masclet_fields_dev(Ctx &c, const avism_params *p, const Level &L, int32_t 
         um = a.u_mass; d2 = a.u2; d3 = a.u3; d4 = a.u4;
     }
     float *u1 = c.get_t<float>(B_U1CO, nc), *dv = c.get_t<float>(B_DIVER, nc);
-    const float md = masclet_fields_inner(c, p, L, nhy, g, um, d2, d3, d4, u1, dv);
+    const float md = masclet_fields_inner(c, p, L, nhy, g, p->level == 1 ? &ap : nullptr, um, d2, d3, d4, u1, dv);
     *u1_out = u1;
     *dv_out = dv;
     return md;
@@ -840,15 +884,16 @@ float masclet_fields_dev(Ctx &c, const avism_params *p, const Level &L, int32_t 
 }  // namespace
 
 int avism_gpu_masclet_fields(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g,
-                             const float *u2g, const float *u3g, const float *u4g, int64_t n, const float *x,
-                             const float *y, const float *z, const float *vx, const float *vy, const float *vz,
-                             const float *m, float *u1co_ext, float *diverco_ext, float *meandens) {
+                             const float *u2g, const float *u3g, const float *u4g, const avism_patches *amr,
+                             int64_t n, const float *x, const float *y, const float *z, const float *vx,
+                             const float *vy, const float *vz, const float *m, float *u1co_ext,
+                             float *diverco_ext, float *meandens) {
     return guarded(ctx, [&](Ctx &c) {
         check_params(p);
         Level L = make_level(p);
         const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
         float *u1, *dv;
-        const float md = masclet_fields_dev(c, p, L, nhy, u1g, u2g, u3g, u4g, n, x, y, z, vx, vy, vz, m, &u1, &dv);
+        const float md = masclet_fields_dev(c, p, L, nhy, u1g, u2g, u3g, u4g, amr, n, x, y, z, vx, vy, vz, m, &u1, &dv);
         float *e1 = is_device_ptr(u1co_ext) ? u1co_ext : c.get_t<float>(B_U1EXT, ne3);
         float *e2 = is_device_ptr(diverco_ext) ? diverco_ext : c.get_t<float>(B_DVEXT, ne3);
         if (u1co_ext) { ext_copy(c, L, u1, e1); from_device(c, u1co_ext, e1, sizeof(float) * (size_t)ne3); }
@@ -859,16 +904,16 @@ int avism_gpu_masclet_fields(avism_gpu_ctx *ctx, const avism_params *p, int32_t 
 }
 
 int avism_gpu_run_level_masclet(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g,
-                                const float *u2g, const float *u3g, const float *u4g, int64_t n, const float *x,
-                                const float *y, const float *z, const float *vx, const float *vy,
-                                const float *vz, const float *m, avism_cubes *cubes, int32_t *nvoid,
-                                avism_voids *voids, float *meandens) {
+                                const float *u2g, const float *u3g, const float *u4g, const avism_patches *amr,
+                                int64_t n, const float *x, const float *y, const float *z, const float *vx,
+                                const float *vy, const float *vz, const float *m, avism_cubes *cubes,
+                                int32_t *nvoid, avism_voids *voids, float *meandens) {
     return guarded(ctx, [&](Ctx &c) {
         check_params(p);
         AV_CHECK(nvoid && voids, AVISM_ERR_ARG, "run_level_masclet: null argument");
         Level L = make_level(p);
         float *u1, *dv;
-        const float md = masclet_fields_dev(c, p, L, nhy, u1g, u2g, u3g, u4g, n, x, y, z, vx, vy, vz, m, &u1, &dv);
+        const float md = masclet_fields_dev(c, p, L, nhy, u1g, u2g, u3g, u4g, amr, n, x, y, z, vx, vy, vz, m, &u1, &dv);
         c.mark("divergence");
         CubesDev cd{};
         const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, nullptr, nullptr, 0, cd, nullptr);

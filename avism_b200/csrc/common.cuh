@@ -66,6 +66,7 @@ enum BufId : int {
     B_U1RAND, B_SMASK_IN,                          // survey: the randoms' grid, the inner mask
     B_GRID_IN,                                     // grid input: the four input grids
     B_GAS1, B_GAS2, B_GAS3, B_GAS4, B_DIVER2,      // MASCLET input: the level's gas grids, the DM divergence
+    B_AMR1, B_AMR2, B_AMR3, B_AMR4,                // MASCLET level 1: the patches' cells
     B_NUM
 };
 
@@ -257,12 +258,20 @@ float grid_fields_inner(Ctx &c, const avism_params *p, const Level &L, int nhy, 
 // input grids given at NHY^3 on this level (copied, or SMOOTH_2-averaged below level 0)
 void level_grids(Ctx &c, const Level &L, const avism_params *p, int nhy, int ngrids, const float *const *g,
                  float *const *co);
-// MASCLET input at levels <= 0: U1CO and DIVERCO (inner) from the gas grids and
-// the DM grids of particles_to_grid (u_mass and du* may be null when the flags
-// do not use them); returns MEANDENS
+// MASCLET level-1 patches: geometry on the host, cells on the device
+struct AmrPatches {
+    int32_t npatch = 0;
+    std::vector<int32_t> nx, ny, nz, ix, iy, iz;
+    std::vector<float> rx, ry, rz;
+    std::vector<int64_t> offset;
+    const float *u11g = nullptr, *u12g = nullptr, *u13g = nullptr, *u14g = nullptr;
+};
+// MASCLET input at levels <= 1: U1CO and DIVERCO (inner) from the gas grids (at
+// level 1 the patches amr) and the DM grids of particles_to_grid (u_mass and
+// du* may be null when the flags do not use them); returns MEANDENS
 float masclet_fields_inner(Ctx &c, const avism_params *p, const Level &L, int nhy, const float *const *gas,
-                           const float *u_mass, const float *du2, const float *du3, const float *du4, float *u1co_in,
-                           float *diver_in);
+                           const AmrPatches *amr, const float *u_mass, const float *du2, const float *du3,
+                           const float *du4, float *u1co_in, float *diver_in);
 
 // flags on the ext grid from inner (wrapped) fields, or from given ext fields.
 void make_flags(Ctx &c, const avism_params *p, const Level &L, const float *u1, const float *dv,

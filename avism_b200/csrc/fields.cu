@@ -444,16 +444,188 @@ __global__ void k_masclet_rho(int64_t nc, const float *__restrict__ u_mass, cons
     u1[c] = __fmul_rn(u, rote);
 }
 // DIVERCO = MIN(DIVERGCO, DIVERDMCO) (src/avism.f90:1636-1642)
+__global__ void k_fill_i32_1(int64_t n, int32_t *__restrict__ a) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = 1;
+}
 __global__ void k_min_into(int64_t nc, float *__restrict__ a, const float *__restrict__ b) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c < nc) a[c] = b[c] < a[c] ? b[c] : a[c];
 }
 
+// ---- MASCLET level 1: DIVER_FINA_GAS (src/divergence.f90:55-340) and VMESH
+//      (src/amr2uniform.f90:127-248) on the level-1 patches ----------------------
+// DIVER0 inside the base grid: central differences over 2*DX0
+__global__ void k_diver0(int nh, float dx0, const float *__restrict__ u2, const float *__restrict__ u3,
+                         const float *__restrict__ u4, float *__restrict__ d) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = nh - 2;
+    if (t >= (int64_t)m * m * m) return;
+    const int i = (int)(t % m) + 1, j = (int)((t / m) % m) + 1, k = (int)(t / ((int64_t)m * m)) + 1;   // 0-based 1..nh-2
+    auto B = [&](int a, int b, int cc) { return (int64_t)a + (int64_t)nh * ((int64_t)b + (int64_t)nh * cc); };
+    const float h = __fmul_rn(2.0f, dx0);
+    const float b21 = __fdiv_rn(__fsub_rn(u2[B(i + 1, j, k)], u2[B(i - 1, j, k)]), h);
+    const float b32 = __fdiv_rn(__fsub_rn(u3[B(i, j + 1, k)], u3[B(i, j - 1, k)]), h);
+    const float b43 = __fdiv_rn(__fsub_rn(u4[B(i, j, k + 1)], u4[B(i, j, k - 1)]), h);
+    d[B(i, j, k)] = __fadd_rn(__fadd_rn(b21, b32), b43);
+}
+// one face of DIVER0 copied from the plane inside it (axis a, side 0: index 1, 1: NHY)
+__global__ void k_diver0_face(int nh, int a, int side, float *__restrict__ d) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nh * nh) return;
+    const int u = (int)(t % nh), v = (int)(t / nh);
+    const int to = side ? nh - 1 : 0, from = side ? nh - 2 : 1;
+    auto B = [&](int q) {
+        const int i = a == 0 ? q : u, j = a == 1 ? q : (a == 0 ? u : v), k = a == 2 ? q : v;
+        return (int64_t)i + (int64_t)nh * ((int64_t)j + (int64_t)nh * k);
+    };
+    d[B(to)] = d[B(from)];
+}
+// one patch's divergence: its own central differences inside (2..N-1 over
+// 2*DXR), the 2-cell rim from its parent base cells' differences (over 2*DX0),
+// averaged with its own at index 2 and N-1 and in their place at 1 and N
+struct PatchGeom {
+    int n1, n2, n3, l1, l2, l3;
+    int64_t off;
+};
+__global__ void k_patch_div(PatchGeom P, int nh, float dxr, float dx0, const float *__restrict__ v2,
+                            const float *__restrict__ v3, const float *__restrict__ v4, const float *__restrict__ u2,
+                            const float *__restrict__ u3, const float *__restrict__ u4, float *__restrict__ dv,
+                            int *__restrict__ err) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
+    if (t >= (int64_t)n1 * n2 * n3) return;
+    const int i = (int)(t % n1) + 1, j = (int)((t / n1) % n2) + 1, k = (int)(t / ((int64_t)n1 * n2)) + 1;
+    auto Q = [&](int a, int b, int cc) {
+        return P.off + (int64_t)(a - 1) + (int64_t)n1 * ((int64_t)(b - 1) + (int64_t)n2 * (cc - 1));
+    };
+    float own = 0.0f;
+    if (i >= 2 && i <= n1 - 1 && j >= 2 && j <= n2 - 1 && k >= 2 && k <= n3 - 1) {
+        const float h = __fmul_rn(2.0f, dxr);
+        const float b21 = __fdiv_rn(__fsub_rn(v2[Q(i + 1, j, k)], v2[Q(i - 1, j, k)]), h);
+        const float b32 = __fdiv_rn(__fsub_rn(v3[Q(i, j + 1, k)], v3[Q(i, j - 1, k)]), h);
+        const float b43 = __fdiv_rn(__fsub_rn(v4[Q(i, j, k + 1)], v4[Q(i, j, k - 1)]), h);
+        own = __fadd_rn(__fadd_rn(b21, b32), b43);
+    }
+    float aux = 0.0f;
+    if (i < 3 || i > n1 - 2 || j < 3 || j > n2 - 2 || k < 3 || k > n3 - 2) {
+        const int c1 = (i + 1) / 2 + P.l1 - 1, c2 = (j + 1) / 2 + P.l2 - 1, c3 = (k + 1) / 2 + P.l3 - 1;
+        if (c1 < 2 || c1 > nh - 1 || c2 < 2 || c2 > nh - 1 || c3 < 2 || c3 > nh - 1) {
+            atomicOr(err, 1);                              // outside the base grid's differences
+            return;
+        }
+        auto B = [&](int a, int b, int cc) {
+            return (int64_t)(a - 1) + (int64_t)nh * ((int64_t)(b - 1) + (int64_t)nh * (cc - 1));
+        };
+        const float h = __fmul_rn(2.0f, dx0);
+        const float b21 = __fdiv_rn(__fsub_rn(u2[B(c1 + 1, c2, c3)], u2[B(c1 - 1, c2, c3)]), h);
+        const float b32 = __fdiv_rn(__fsub_rn(u3[B(c1, c2 + 1, c3)], u3[B(c1, c2 - 1, c3)]), h);
+        const float b43 = __fdiv_rn(__fsub_rn(u4[B(c1, c2, c3 + 1)], u4[B(c1, c2, c3 - 1)]), h);
+        aux = __fadd_rn(__fadd_rn(b21, b32), b43);
+    }
+    float v = own;
+    if (i == 2 || i == n1 - 1 || j == 2 || j == n2 - 1 || k == 2 || k == n3 - 1) v = __fmul_rn(0.5f, __fadd_rn(aux, v));
+    if (i == 1 || i == n1 || j == 1 || j == n2 || k == 1 || k == n3) v = aux;
+    dv[t] = v;
+}
+// VMESH for one patch: its cells added into the level grid (patches in order)
+__global__ void k_vmesh_add(PatchGeom P, int nx, int nh, int xr1, int yr1, int zr1, const float *__restrict__ u11,
+                            const float *__restrict__ dv, int32_t *__restrict__ flagamr, float *__restrict__ ugr,
+                            float *__restrict__ divr, uint8_t *__restrict__ flagr, int *__restrict__ err) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n1 = P.n1, n2 = P.n2;
+    if (t >= (int64_t)n1 * n2 * P.n3) return;
+    const int xr = xr1 + (int)(t % n1) + 1, yr = yr1 + (int)((t / n1) % n2) + 1, zr = zr1 + (int)(t / ((int64_t)n1 * n2)) + 1;
+    if (xr < 1 || xr > nx || yr < 1 || yr > nx || zr < 1 || zr > nx) {
+        atomicOr(err, 2);                                  // outside the level grid
+        return;
+    }
+    const int64_t c = (int64_t)(xr - 1) + (int64_t)nx * ((int64_t)(yr - 1) + (int64_t)nx * (zr - 1));
+    flagamr[c] += 1;
+    ugr[c] = __fadd_rn(ugr[c], u11[P.off + t]);
+    divr[c] = __fadd_rn(divr[c], dv[t]);
+    flagr[(int64_t)((xr - 1) / 2) + (int64_t)nh * ((int64_t)((yr - 1) / 2) + (int64_t)nh * ((zr - 1) / 2))] = 1;
+}
+// the sums over FLAGAMR; the children of unrefined base cells take the base values
+__global__ void k_vmesh_finish(int nx, int nh, const int32_t *__restrict__ flagamr, const uint8_t *__restrict__ flagr,
+                               const float *__restrict__ u1g, const float *__restrict__ d0, float *__restrict__ ugr,
+                               float *__restrict__ divr) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int64_t)nx * nx * nx) return;
+    const int i = (int)(c % nx), j = (int)((c / nx) % nx), k = (int)(c / ((int64_t)nx * nx));
+    const int64_t b = (int64_t)(i / 2) + (int64_t)nh * ((int64_t)(j / 2) + (int64_t)nh * (k / 2));
+    if (!flagr[b]) {
+        ugr[c] = u1g[b];
+        divr[c] = d0[b];
+    } else {
+        const float f = (float)flagamr[c];
+        ugr[c] = __fdiv_rn(ugr[c], f);
+        divr[c] = __fdiv_rn(divr[c], f);
+    }
+}
+
+static void amr_level1(Ctx &c, const Level &L, const avism_params *p, int nhy, const float *const *gas,
+                       const AmrPatches &a, float *ugr, float *divr) {
+    const int nx = L.g.nx, nh = nhy;
+    const int64_t nc = (int64_t)nx * nx * nx, n0 = (int64_t)nh * nh * nh;
+    avism_params p0 = *p;
+    p0.nx = nhy;
+    const Level L0 = make_level(&p0);
+    const float dx0 = L0.g.dx, dxr_div = dx0 / 2.0f, dxr = L.g.dx, rx1 = L.rad_at(1);
+    float *d0 = c.get_t<float>(B_DIVER2, n0);
+    AV_CUDA(cudaMemsetAsync(d0, 0, sizeof(float) * (size_t)n0, c.stream));
+    if (nh > 2)
+        ++c.launches, k_diver0<<<grid_for((int64_t)(nh - 2) * (nh - 2) * (nh - 2), 256), 256, 0, c.stream>>>(
+            nh, dx0, gas[1], gas[2], gas[3], d0);
+    for (int ax = 0; ax < 3; ax++)
+        for (int side = 0; side < 2; side++)
+            ++c.launches, k_diver0_face<<<grid_for((int64_t)nh * nh, 256), 256, 0, c.stream>>>(nh, ax, side, d0);
+    int32_t *flagamr = c.get_t<int32_t>(B_LABEL_AUX, nc);
+    uint8_t *flagr = c.get_t<uint8_t>(B_GAS4, n0);
+    int *err = c.get_t<int>(B_SCAL, 4);
+    AV_CUDA(cudaMemsetAsync(flagr, 0, (size_t)n0, c.stream));
+    AV_CUDA(cudaMemsetAsync(ugr, 0, sizeof(float) * (size_t)nc, c.stream));
+    AV_CUDA(cudaMemsetAsync(divr, 0, sizeof(float) * (size_t)nc, c.stream));
+    AV_CUDA(cudaMemsetAsync(err, 0, sizeof(int), c.stream));
+    ++c.launches, k_fill_i32_1<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, flagamr);
+    int64_t maxcells = 1;
+    for (int q = 0; q < a.npatch; q++) maxcells = std::max(maxcells, (int64_t)a.nx[q] * a.ny[q] * a.nz[q]);
+    float *dv = c.get_t<float>(B_GAS3, maxcells);
+    for (int q = 0; q < a.npatch; q++) {
+        PatchGeom P{a.nx[q], a.ny[q], a.nz[q], a.ix[q], a.iy[q], a.iz[q], a.offset[q]};
+        const int64_t np = (int64_t)P.n1 * P.n2 * P.n3;
+        if (np <= 0) continue;
+        ++c.launches, k_patch_div<<<grid_for(np, 256), 256, 0, c.stream>>>(P, nh, dxr_div, dx0, a.u12g, a.u13g, a.u14g,
+                                                                          gas[1], gas[2], gas[3], dv, err);
+        // IXR1 = INT(((PATCHRX - 0.5*DXR) - RX1)/DXR + 0.5) (src/amr2uniform.f90:170-172)
+        const int xr1 = (int)((((a.rx[q] - 0.5f * dxr) - rx1) / dxr) + 0.5f);
+        const int yr1 = (int)((((a.ry[q] - 0.5f * dxr) - rx1) / dxr) + 0.5f);
+        const int zr1 = (int)((((a.rz[q] - 0.5f * dxr) - rx1) / dxr) + 0.5f);
+        ++c.launches, k_vmesh_add<<<grid_for(np, 256), 256, 0, c.stream>>>(P, nx, nh, xr1, yr1, zr1, a.u11g, dv,
+                                                                          flagamr, ugr, divr, flagr, err);
+    }
+    ++c.launches, k_vmesh_finish<<<grid_for(nc, 256), 256, 0, c.stream>>>(nx, nh, flagamr, flagr, gas[0], d0, ugr,
+                                                                         divr);
+    AV_CUDA(cudaGetLastError());
+    int herr = 0;
+    AV_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    AV_CHECK(herr == 0, AVISM_ERR_ARG, "MASCLET level 1: a patch reaches outside the base grid's differences or "
+                                       "the level grid (the reference reads or writes outside its arrays there)");
+}
+
+// DIVERCO = MIN(DIVERGCO, DIVERDMCO) with DIVERDMCO = 0 (levels above 0)
+__global__ void k_min_zero(int64_t nc, float *__restrict__ a) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nc) a[c] = 0.0f < a[c] ? 0.0f : a[c];
+}
+
 float masclet_fields_inner(Ctx &c, const avism_params *p, const Level &L, int nhy, const float *const *gas,
-                           const float *u_mass, const float *du2, const float *du3, const float *du4, float *u1co_in,
-                           float *diver_in) {
+                           const AmrPatches *amr, const float *u_mass, const float *du2, const float *du3,
+                           const float *du4, float *u1co_in, float *diver_in) {
     const int64_t nc = (int64_t)L.g.nx * L.g.nx * L.g.nx;
-    const bool need_gas_v = p->flag_div == 0 || p->flag_div == 2;
+    const bool amr1 = p->level == 1;
+    const bool need_gas_v = !amr1 && (p->flag_div == 0 || p->flag_div == 2);
     const int ng = need_gas_v ? 4 : 1;
     float *co[4] = {c.get_t<float>(B_GAS1, nc), nullptr, nullptr, nullptr};
     if (need_gas_v) {
@@ -461,7 +633,8 @@ float masclet_fields_inner(Ctx &c, const avism_params *p, const Level &L, int nh
         co[2] = c.get_t<float>(B_GAS3, nc);
         co[3] = c.get_t<float>(B_GAS4, nc);
     }
-    if (p->flag_dens != 1 || need_gas_v) level_grids(c, L, p, nhy, ng, gas, co);
+    if (amr1) amr_level1(c, L, p, nhy, gas, *amr, co[0], diver_in);      // UGR, DIVR
+    else if (p->flag_dens != 1 || need_gas_v) level_grids(c, L, p, nhy, ng, gas, co);
     const float dx = L.g.dx;
     const float vol = ((dx * dx) * dx) * ((L.g.rete * L.g.rete) * L.g.rete);
     ++c.launches, k_masclet_rho<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, u_mass, co[0], vol, L.g.rote,
@@ -484,6 +657,10 @@ float masclet_fields_inner(Ctx &c, const avism_params *p, const Level &L, int nh
     pv.no_velocities = p->flag_div == -1 ? 1 : 0;
     if (p->flag_div == -1) {
         divergence_inner(c, &pv, L, u1co_in, nullptr, nullptr, nullptr, diver_in);
+    } else if (amr1) {
+        // DIVERGCO = DIVR (in diver_in), DIVERDMCO = 0
+        if (p->flag_div == 1) AV_CUDA(cudaMemsetAsync(diver_in, 0, sizeof(float) * (size_t)nc, c.stream));
+        if (p->flag_div == 0) ++c.launches, k_min_zero<<<grid_for(nc, 256), 256, 0, c.stream>>>(nc, diver_in);
     } else {
         if (need_gas_v) divergence_inner(c, &pv, L, u1co_in, co[1], co[2], co[3], diver_in);
         if (p->flag_div == 1) divergence_inner(c, &pv, L, u1co_in, du2, du3, du4, diver_in);

@@ -76,8 +76,10 @@ bool read_particle_head(FILE *f, int64_t *n, float *zeta) {
 // 9 significant digits read back as the same REAL*4
 void put_f(FILE *f, float v) { std::fprintf(f, " %.9g", (double)v); }
 
-// one record of any length (or chain of subrecords), skipped
-bool skip_record(FILE *f) {
+// one record of any length (or chain of subrecords), skipped; its payload
+// length in *total when given
+bool skip_record(FILE *f, uint64_t *total = nullptr) {
+    uint64_t sum = 0;
     for (;;) {
         int32_t head = 0, tail = 0;
         if (std::fread(&head, 4, 1, f) != 1 || head == INT32_MIN) return false;
@@ -85,7 +87,11 @@ bool skip_record(FILE *f) {
         if (std::fseek(f, (long)len, SEEK_CUR) != 0) return false;
         if (std::fread(&tail, 4, 1, f) != 1 || tail == INT32_MIN) return false;
         if ((tail < 0 ? -(int64_t)tail : tail) != len) return false;
-        if (head >= 0) return true;
+        sum += (uint64_t)len;
+        if (head >= 0) {
+            if (total) *total = sum;
+            return true;
+        }
     }
 }
 
@@ -118,6 +124,9 @@ struct MascletGrid {
     int nl = 0, ndxyz0 = 0;
     float t = 0.0f, map = 0.0f, zeta = 0.0f;
     std::vector<int64_t> npatch, npart;           // levels 1..NL at [1..NL]
+    // every patch, levels in order: PATCHNX..NZ, PATCHX..Z, PATCHRX..RZ
+    std::vector<int32_t> pn[3], pl[3];
+    std::vector<float> pr[3];
 };
 bool read_masclet_grid(const char *path, MascletGrid &g) {
     File in(path, "r");
@@ -140,10 +149,15 @@ bool read_masclet_grid(const char *path, MascletGrid &g) {
         g.npart[ir] = (int64_t)v[2];
         if (g.npatch[ir] < 0 || g.npart[ir] < 0) return false;
         if (!read_values(in.f, 0, v)) return false;
-        for (int64_t i = 0; i < g.npatch[ir]; i++)
-            if (!read_values(in.f, 3, v) || !read_values(in.f, 3, v) || !read_values(in.f, 3, v) ||
-                !read_values(in.f, 1, v))
-                return false;
+        for (int64_t i = 0; i < g.npatch[ir]; i++) {
+            if (!read_values(in.f, 3, v)) return false;
+            for (int a = 0; a < 3; a++) g.pn[a].push_back((int32_t)v[a]);
+            if (!read_values(in.f, 3, v)) return false;
+            for (int a = 0; a < 3; a++) g.pl[a].push_back((int32_t)v[a]);
+            if (!read_values(in.f, 3, v)) return false;
+            for (int a = 0; a < 3; a++) g.pr[a].push_back((float)v[a]);       // READ(33,*) AAA,BBB,CCC
+            if (!read_values(in.f, 1, v)) return false;
+        }
     }
     return true;
 }
@@ -268,6 +282,75 @@ int avism_io_read_masclet(const char *grid_path, const char *gas_path, const cha
     const uint64_t nc = (uint64_t)nhy * (uint64_t)nhy * (uint64_t)nhy;
     for (uint64_t c = 0; c < nc; c++) u1g[c] = u1g[c] + 1.0f;
     if (npartt) *npartt = n;
+    return AVISM_OK;
+}
+
+int avism_io_masclet_patches_size(const char *grid_path, int32_t *npatch, int64_t *ncells) {
+    if (!grid_path) return AVISM_ERR_ARG;
+    MascletGrid g;
+    if (!read_masclet_grid(grid_path, g)) return AVISM_ERR_IO;
+    const int64_t np = g.nl >= 1 ? g.npatch[1] : 0;
+    int64_t cells = 0;
+    for (int64_t i = 0; i < np; i++) {
+        if (g.pn[0][i] < 1 || g.pn[1][i] < 1 || g.pn[2][i] < 1) return AVISM_ERR_IO;
+        cells += (int64_t)g.pn[0][i] * g.pn[1][i] * g.pn[2][i];
+    }
+    if (npatch) *npatch = (int32_t)np;
+    if (ncells) *ncells = cells;
+    return AVISM_OK;
+}
+
+int avism_io_read_masclet_patches(const char *grid_path, const char *gas_path, int32_t nhy, int32_t capacity,
+                                  int64_t capacity_cells, int32_t *nx, int32_t *ny, int32_t *nz, int32_t *ix,
+                                  int32_t *iy, int32_t *iz, float *rx, float *ry, float *rz, int64_t *offset,
+                                  float *u11g, float *u12g, float *u13g, float *u14g) {
+    int32_t *const geom[6] = {nx, ny, nz, ix, iy, iz};
+    float *const corner[3] = {rx, ry, rz};
+    float *const cells_out[4] = {u11g, u12g, u13g, u14g};
+    if (!grid_path || !gas_path || nhy < 1 || !offset) return AVISM_ERR_ARG;
+    for (int32_t *d : geom)
+        if (!d) return AVISM_ERR_ARG;
+    for (float *d : corner)
+        if (!d) return AVISM_ERR_ARG;
+    for (float *d : cells_out)
+        if (!d) return AVISM_ERR_ARG;
+    int32_t np = 0;
+    int64_t ncells = 0;
+    const int st = avism_io_masclet_patches_size(grid_path, &np, &ncells);
+    if (st) return st;
+    if (np > capacity || ncells > capacity_cells) return AVISM_ERR_ARG;
+    MascletGrid g;
+    if (!read_masclet_grid(grid_path, g)) return AVISM_ERR_IO;
+    offset[0] = 0;
+    for (int32_t i = 0; i < np; i++) {
+        for (int a = 0; a < 3; a++) {
+            geom[a][i] = g.pn[a][i];
+            geom[3 + a][i] = g.pl[a][i];
+            corner[a][i] = g.pr[a][i];
+        }
+        offset[i + 1] = offset[i] + (int64_t)g.pn[0][i] * g.pn[1][i] * g.pn[2][i];
+    }
+    // gas (src/reader.f90:259-312): the header, the four level-0 grids and six
+    // more records; then per level-1 patch U11G, U12G, U13G, U14G and seven
+    // more records
+    File in(gas_path, "rb");
+    if (!in.f || !skip_record(in.f)) return AVISM_ERR_IO;
+    const uint64_t base = (uint64_t)nhy * (uint64_t)nhy * (uint64_t)nhy * 4;
+    for (int q = 0; q < 4; q++) {
+        uint64_t len = 0;
+        if (!skip_record(in.f, &len) || len != base) return AVISM_ERR_IO;
+    }
+    for (int q = 0; q < 6; q++)
+        if (!skip_record(in.f)) return AVISM_ERR_IO;
+    for (int32_t i = 0; i < np; i++) {
+        const uint64_t bytes = (uint64_t)(offset[i + 1] - offset[i]) * 4;
+        for (float *d : cells_out)
+            if (!read_record(in.f, d + offset[i], bytes)) return AVISM_ERR_IO;
+        for (int q = 0; q < 7; q++)
+            if (!skip_record(in.f)) return AVISM_ERR_IO;
+    }
+    // delta to density (src/reader.f90:393)
+    for (int64_t c = 0; c < ncells; c++) u11g[c] = u11g[c] + 1.0f;
     return AVISM_OK;
 }
 

@@ -79,7 +79,7 @@ def run_single(path, p: Params, out_dir, it: int = 1, grid_nhy: int = 0, mask=No
                masclet_nhy: int = 0) -> dict:
     """One level from a grid file (grid_nhy > 0), a MASCLET snapshot (path the
     grid file, masclet = (gas file, DM file), masclet_nhy the base grid; level
-    <= 0) or a survey (mask and randoms files), written as run_iteration writes
+    <= 1, level 1 from the snapshot's level-1 patches) or a survey (mask and randoms files), written as run_iteration writes
     its levels."""
     import numpy as np
     from . import synth
@@ -100,7 +100,7 @@ def run_single(path, p: Params, out_dir, it: int = 1, grid_nhy: int = 0, mask=No
         r = read_masclet_files(path, masclet[0], masclet[1], masclet_nhy)
         p = Params(**{**p.__dict__, "zeta": float(r["zeta"])})
         gas = tuple(r["gas"][k] for k in ("u1g", "u2g", "u3g", "u4g"))
-        res = engine.run_level_masclet(p, masclet_nhy, gas, r["parts"])
+        res = engine.run_level_masclet(p, masclet_nhy, gas, r["parts"], r["amr"] if p.level == 1 else None)
     else:
         parts = read_particle_file_novel(path) if novel else read_particle_file(path)
         p = Params(**{**p.__dict__, "zeta": float(parts.pop("zeta")), "no_velocities": int(novel)})

@@ -85,12 +85,12 @@ def _grf(ng, box, index, sigma, rng):
     amp[0, 0, 0] = 0.0
     noise = rng.normal(size=(ng, ng, ng))
     dk = np.fft.rfftn(noise) * amp
-    g = np.fft.irfftn(dk, s=(ng, ng, ng))
+    g = np.fft.irfftn(dk, s=(ng, ng, ng), axes=(0, 1, 2))
     scale = sigma / g.std()
     g *= scale
     dk *= scale
     # linear theory: div v ~ -delta  =>  v_k = i k delta_k / k^2
-    vel = [np.fft.irfftn(1j * K * dk / k2, s=(ng, ng, ng)) for K in (KX, KY, KZ)]
+    vel = [np.fft.irfftn(1j * K * dk / k2, s=(ng, ng, ng), axes=(0, 1, 2)) for K in (KX, KY, KZ)]
     return g, vel
 
 

@@ -304,19 +304,39 @@ int avism_gpu_run_level_grid(avism_gpu_ctx *ctx, const avism_params *p, int32_t 
  *      velocities (0), DM (1), gas (2), or the linear theory of U1CO (-1).  The
  *      particle arrays may be NULL (n = 0) when neither flag uses the dark
  *      matter (flag_dens = 2 and flag_div = 2 or -1); u2g..u4g may be NULL when
- *      flag_div is 1 or -1.  Levels above 0 (the AMR patches: VMESH and
- *      DIVER_FINA_GAS) return AVISM_ERR_UNSUPPORTED.
+ *      flag_div is 1 or -1.  At level 1 the gas fields come from the level-1
+ *      patches amr (DIVER_FINA_GAS, src/divergence.f90:55-340, and VMESH,
+ *      src/amr2uniform.f90:127-248, as the reference computes them: a cell
+ *      under k patch cells takes their sum over k + 1, the children of a
+ *      refined base cell that no patch covers take 0, the others their base
+ *      cell's values) and the DM divergence is 0 (the reference computes
+ *      DIVER_UNIFORM of the DM only at levels <= 0).  amr is ignored below
+ *      level 1.  Levels above 1 return AVISM_ERR_UNSUPPORTED: the reference's
+ *      VMESH indexes its base-size refinement flags with coordinates beyond
+ *      them there.
  *      avism_gpu_masclet_fields returns the ext grids (as avism_gpu_fields),
  *      avism_gpu_run_level_masclet the level's catalogue.                       */
+/* the level-1 refinement patches of a MASCLET snapshot (host or device arrays):
+ * sizes PATCHNX..Z, first base cells PATCHX..Z (1-based), corners PATCHRX..Z,
+ * the start of each patch's cells in the cell arrays (offset[npatch] = total),
+ * and the cells (x fastest): U11G = 1 + delta, U12G..U14G the velocities      */
+typedef struct avism_patches {
+    int32_t npatch;
+    const int32_t *nx, *ny, *nz, *ix, *iy, *iz;
+    const float *rx, *ry, *rz;
+    const int64_t *offset;
+    const float *u11g, *u12g, *u13g, *u14g;
+} avism_patches;
 int avism_gpu_masclet_fields(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g,
-                             const float *u2g, const float *u3g, const float *u4g, int64_t n, const float *x,
-                             const float *y, const float *z, const float *vx, const float *vy, const float *vz,
-                             const float *m, float *u1co_ext, float *diverco_ext, float *meandens);
+                             const float *u2g, const float *u3g, const float *u4g, const avism_patches *amr,
+                             int64_t n, const float *x, const float *y, const float *z, const float *vx,
+                             const float *vy, const float *vz, const float *m, float *u1co_ext,
+                             float *diverco_ext, float *meandens);
 int avism_gpu_run_level_masclet(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g,
-                                const float *u2g, const float *u3g, const float *u4g, int64_t n, const float *x,
-                                const float *y, const float *z, const float *vx, const float *vy,
-                                const float *vz, const float *m, avism_cubes *cubes, int32_t *nvoid,
-                                avism_voids *voids, float *meandens);
+                                const float *u2g, const float *u3g, const float *u4g, const avism_patches *amr,
+                                int64_t n, const float *x, const float *y, const float *z, const float *vx,
+                                const float *vy, const float *vz, const float *m, avism_cubes *cubes,
+                                int32_t *nvoid, avism_voids *voids, float *meandens);
 
 /* ---- survey mode (FLAG_SURVEY = 1): replaces src/avism.f90:1420-1596.  The
  *      tracers (x..m, masses as weights; velocities nullable with
@@ -424,6 +444,20 @@ int avism_io_masclet_header(const char *grid_path, int32_t *nl, int32_t *ndxyz0,
 int avism_io_read_masclet(const char *grid_path, const char *gas_path, const char *dm_path, int32_t nhy,
                           float *u1g, float *u2g, float *u3g, float *u4g, int64_t capacity, float *x, float *y,
                           float *z, float *vx, float *vy, float *vz, float *m, int64_t *npartt);
+/* The level-1 patches of a MASCLET snapshot, for avism_gpu_*_masclet at level
+ * 1 (an avism_patches over these arrays).  avism_io_masclet_patches_size gives
+ * NPATCH(1) and the patches' cells in total.  avism_io_read_masclet_patches
+ * reads their geometry from the grid file (PATCHNX..NZ, PATCHX..Z, PATCHRX..RZ;
+ * src/reader.f90:168-174), offset[npatch + 1] (the first cell of each patch in
+ * the cell arrays, offset[0] = 0) and, from the gas file, U11G (the stored
+ * delta + 1, src/reader.f90:393), U12G, U13G, U14G of each patch, column-major
+ * at its own size (src/reader.f90:285-312).  AVISM_ERR_ARG when the patches or
+ * cells exceed the capacities.                                                */
+int avism_io_masclet_patches_size(const char *grid_path, int32_t *npatch, int64_t *ncells);
+int avism_io_read_masclet_patches(const char *grid_path, const char *gas_path, int32_t nhy, int32_t capacity,
+                                  int64_t capacity_cells, int32_t *nx, int32_t *ny, int32_t *nz, int32_t *ix,
+                                  int32_t *iy, int32_t *iz, float *rx, float *ry, float *rz, int64_t *offset,
+                                  float *u11g, float *u12g, float *u13g, float *u14g);
 /* Survey mask (src/avism.f90:403-418): a stream file [int32 NMASK, REAL*4
  * MASKLOW, MASKUPPER, MASKSIDE, INTEGER*1 SMASK2(NMASK^3)].  NMASK must equal
  * ncox (the coarse grid, else AVISM_ERR_ARG as the reference's stop); the mask

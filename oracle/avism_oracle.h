@@ -121,11 +121,12 @@ void orc_level_grids(const avism_params *p, int32_t nhy, int ngrids, const float
 
 /* MASCLET input (FLAG_DATA = 0) at levels <= 0 (src/avism.f90:980-1156,
  * 1366-1405, 1633-1650): DM particles and gas grids, combined by FLAG_DENS /
- * FLAG_DIV; the particle arrays may be NULL when the flags do not use them */
+ * FLAG_DIV; the particle arrays may be NULL when the flags do not use them;
+ * level 1 takes the gas fields from the level-1 patches (VMESH, DIVER_FINA_GAS) */
 int orc_masclet_fields(const avism_params *p, int32_t nhy, const float *u1g, const float *u2g, const float *u3g,
-                       const float *u4g, int64_t n, const float *x, const float *y, const float *z,
-                       const float *vx, const float *vy, const float *vz, const float *m, float *u1co_ext,
-                       float *diverco_ext, float *meandens);
+                       const float *u4g, const avism_patches *amr, int64_t n, const float *x, const float *y,
+                       const float *z, const float *vx, const float *vy, const float *vz, const float *m,
+                       float *u1co_ext, float *diverco_ext, float *meandens);
 
 #ifdef __cplusplus
 }

@@ -163,7 +163,7 @@ def run_level_grid(p: Params, nhy, u1g, u2g, u3g, u4g):
     return dict(u1co=u1, diverco=dv, meandens=md, vf=vf, cat=cat)
 
 
-def masclet_fields(p: Params, nhy, gas, parts=None):
+def masclet_fields(p: Params, nhy, gas, parts=None, amr=None):
     """MASCLET input at levels <= 0 (src/avism.f90:980-1156, 1366-1405,
     1633-1650): (U1CO ext, DIVERCO ext, MEANDENS) from the gas grids
     (u1g = 1 + delta, u2g, u3g, u4g at nhy^3) and the DM particles."""
@@ -172,8 +172,10 @@ def masclet_fields(p: Params, nhy, gas, parts=None):
     dv = np.zeros(g.ne ** 3, np.float32)
     md = C.c_float()
     f = lib().orc_masclet_fields
-    f.argtypes = [C.c_void_p, C.c_int32] + [C.POINTER(C.c_float)] * 4 + [C.c_int64] + \
+    f.argtypes = [C.c_void_p, C.c_int32] + [C.POINTER(C.c_float)] * 4 + [C.c_void_p, C.c_int64] + \
         [C.POINTER(C.c_float)] * 7 + [C.POINTER(C.c_float)] * 3
+    from avism_b200._abi import patches_c
+    pa, keep_amr = patches_c(amr) if amr is not None else (None, None)
     keep = [None if a is None else _f32(a) for a in gas]
     gp = [ptr(a, C.c_float) if a is not None else None for a in keep]
     if parts is None:
@@ -182,13 +184,14 @@ def masclet_fields(p: Params, nhy, gas, parts=None):
         pk = [_f32(parts[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")]
         n, pp = len(pk[0]), [ptr(a, C.c_float) for a in pk]
     pc = p.to_c()
-    _chk(f(C.byref(pc), int(nhy), *gp, n, *pp, ptr(u1, C.c_float), ptr(dv, C.c_float), C.byref(md)))
+    _chk(f(C.byref(pc), int(nhy), *gp, C.byref(pa) if pa is not None else None, n, *pp, ptr(u1, C.c_float),
+           ptr(dv, C.c_float), C.byref(md)))
     return u1, dv, md.value
 
 
-def run_level_masclet(p: Params, nhy, gas, parts=None):
+def run_level_masclet(p: Params, nhy, gas, parts=None, amr=None):
     """MASCLET snapshot level -> catalogue on the CPU."""
-    u1, dv, md = masclet_fields(p, nhy, gas, parts)
+    u1, dv, md = masclet_fields(p, nhy, gas, parts, amr)
     vf = voidfind(p, u1, dv)
     cat = merge_post(p, vf["nvoid"], vf["cubes"], u1, md)
     return dict(u1co=u1, diverco=dv, meandens=md, vf=vf, cat=cat)

@@ -1,7 +1,9 @@
-"""GPU parity for MASCLET input (FLAG_DATA = 0) at levels 0 and -1: the level's
-U1CO / DIVERCO and whole catalogue through the C-ABI against the oracle, bit
-for bit, for the FLAG_DENS / FLAG_DIV choices (src/avism.f90:1366-1405,
-1633-1650); a snapshot read from its three files; levels above 0 refused."""
+"""GPU parity for MASCLET input (FLAG_DATA = 0) at levels 1, 0 and -1: the
+level's U1CO / DIVERCO and whole catalogue through the C-ABI against the oracle,
+bit for bit, for the FLAG_DENS / FLAG_DIV choices (src/avism.f90:1094-1124,
+1366-1405, 1633-1650); level 1 from the AMR patches (DIVER_FINA_GAS, VMESH); a
+snapshot read from its three files; patches outside the reference's arrays and
+levels above 1 refused."""
 import numpy as np
 import pytest
 
@@ -12,7 +14,8 @@ import masclet_case as mc
 
 pytestmark = pytest.mark.gpu
 
-CASES = [(0, 0, 0), (1, 1, 0), (2, 2, 0), (0, -1, 0), (0, 0, -1), (2, 2, -1), (2, 1, -1)]
+CASES = [(0, 0, 0), (1, 1, 0), (2, 2, 0), (0, -1, 0), (0, 0, -1), (2, 2, -1), (2, 1, -1),
+         (0, 0, 1), (2, 2, 1), (1, 1, 1), (2, -1, 1), (0, 2, 1)]
 
 
 @pytest.fixture(scope="module")
@@ -21,8 +24,8 @@ def snap():
 
 
 def params(s, fd, fv, lev, periodic=1):
-    return Params(nx=s["ng"] >> (-lev), periodic=periodic, lado0=s["box"], level=lev, levmin=lev, flag_dens=fd,
-                  flag_div=fv)
+    nx = 2 * s["ng"] if lev == 1 else s["ng"] >> (-lev)
+    return Params(nx=nx, periodic=periodic, lado0=s["box"], level=lev, levmin=lev, flag_dens=fd, flag_div=fv)
 
 
 @pytest.mark.parametrize("fd,fv,lev", CASES)
@@ -30,13 +33,14 @@ def test_fields_and_level_exact(gpu, snap, fd, fv, lev):
     p = params(snap, fd, fv, lev)
     needs_dm = fd <= 1 or fv in (0, 1)
     parts = mc.particles(snap) if needs_dm else None
-    u1o, dvo, mdo = O.masclet_fields(p, snap["ng"], mc.gas(snap), parts)
-    u1g, dvg, mdg = gpu.masclet_fields(p, snap["ng"], mc.gas(snap), parts)
+    amr = mc.amr(snap) if lev == 1 else None
+    u1o, dvo, mdo = O.masclet_fields(p, snap["ng"], mc.gas(snap), parts, amr)
+    u1g, dvg, mdg = gpu.masclet_fields(p, snap["ng"], mc.gas(snap), parts, amr)
     assert np.array_equal(u1o, u1g) and np.array_equal(dvo, dvg) and mdo == mdg
-    o = O.run_level_masclet(p, snap["ng"], mc.gas(snap), parts)
-    g = gpu.run_level_masclet(p, snap["ng"], mc.gas(snap), parts, capacity=200000)
+    o = O.run_level_masclet(p, snap["ng"], mc.gas(snap), parts, amr)
+    g = gpu.run_level_masclet(p, snap["ng"], mc.gas(snap), parts, amr, capacity=200000)
     assert g["nvoid"] == o["vf"]["nvoid"]
-    if lev == 0:
+    if lev >= 0:
         assert g["nvoid"] > 0                    # (at 16^3 the mock's voids fall below NCELL_MIN)
     for k in g["cubes"]:
         assert np.array_equal(g["cubes"][k], o["vf"]["cubes"][k]), k
@@ -67,9 +71,43 @@ def test_from_files(gpu, snap, tmp_path):
         assert np.array_equal(np.asarray(a["cat"][k]), np.asarray(b["cat"][k])), k
 
 
-def test_level_above_zero_is_unsupported(gpu, snap):
+def test_level1_from_files(gpu, snap, tmp_path):
+    from avism_b200.avism import read_masclet_files
+    r = read_masclet_files(*mc.write_files(snap, str(tmp_path)), snap["ng"])
+    p = params(snap, 0, 0, 1)
+    gas = tuple(r["gas"][k] for k in ("u1g", "u2g", "u3g", "u4g"))
+    a = gpu.run_level_masclet(p, snap["ng"], gas, r["parts"], r["amr"], capacity=200000)
+    o = O.run_level_masclet(p, snap["ng"], mc.gas(snap), mc.particles(snap), mc.amr(snap))
+    assert a["nvoid"] == o["vf"]["nvoid"]
+    for k in ("indice", "uvoid", "ncellv", "volnew", "umean", "mtot"):
+        assert np.array_equal(a["cat"][k], o["cat"][k]), k
+
+
+@pytest.mark.parametrize("bad", ["rim", "vmesh", "missing"])
+def test_level1_refuses_patches_outside(gpu, snap, bad):
+    """A patch whose rim needs base differences outside 2..NHY-1, or whose cells
+    land outside the level grid, is refused (the kernels check every index
+    before the access and report it); level 1 without patches too."""
     from avism_b200.avism import AvismError
-    p = Params(nx=2 * snap["ng"], periodic=1, lado0=snap["box"], level=1)
+    p = params(snap, 2, 2, 1)
+    a = {k: np.array(v, copy=True) for k, v in mc.amr(snap).items()}
+    if bad == "rim":
+        a["ix"][0] = 1
+    elif bad == "vmesh":
+        a["rz"][2] = a["rz"][2] + np.float32(80.0)
+    else:
+        a = None
+    with pytest.raises(AvismError):
+        gpu.masclet_fields(p, snap["ng"], mc.gas(snap), None, a)
+    # the context stays usable
+    u1, dv, _ = gpu.masclet_fields(p, snap["ng"], mc.gas(snap), None, mc.amr(snap))
+    u1o, dvo, _ = O.masclet_fields(p, snap["ng"], mc.gas(snap), None, mc.amr(snap))
+    assert np.array_equal(u1, u1o) and np.array_equal(dv, dvo)
+
+
+def test_level_above_one_is_unsupported(gpu, snap):
+    from avism_b200.avism import AvismError
+    p = Params(nx=4 * snap["ng"], periodic=1, lado0=snap["box"], level=2)
     with pytest.raises(AvismError) as e:
         gpu.masclet_fields(p, snap["ng"], mc.gas(snap), mc.particles(snap))
     assert "not implemented" in str(e.value)

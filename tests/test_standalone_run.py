@@ -72,8 +72,8 @@ class OracleModes(OracleEngine):
     def run_level_survey(self, p, parts, rands, smask):
         return self._res(O.run_level_survey(p, parts, rands, smask))
 
-    def run_level_masclet(self, p, nhy, gas, parts):
-        return self._res(O.run_level_masclet(p, nhy, gas, parts))
+    def run_level_masclet(self, p, nhy, gas, parts, amr=None):
+        return self._res(O.run_level_masclet(p, nhy, gas, parts, amr))
 
 
 def test_grid_file_level(tmp_path):
@@ -124,3 +124,18 @@ def test_masclet_files_level(tmp_path):
                    engine=OracleModes())
     head, levels = _read_voids_file(r["voids"])
     assert len(levels[0]["rows"]) == r["levels"][0]["cat"]["nvoidt"] > 0
+
+
+def test_masclet_files_level1(tmp_path):
+    """Level 1 of a MASCLET snapshot through the runner: the gas from the
+    level-1 patches the reader takes from the grid and gas files."""
+    from avism_b200.run import run_single
+    import masclet_case as mc
+    snap = mc.snapshot()
+    grid, gas, dm = mc.write_files(snap, str(tmp_path))
+    p = Params(nx=2 * snap["ng"], periodic=1, lado0=snap["box"], level=1, levmin=1, flag_dens=2, flag_div=2)
+    r = run_single(grid, p, tmp_path / "out", masclet=(gas, dm), masclet_nhy=snap["ng"], cubes=True,
+                   engine=OracleModes())
+    o = O.run_level_masclet(p, snap["ng"], mc.gas(snap), None, mc.amr(snap))
+    head, levels = _read_voids_file(r["voids"])
+    assert len(levels[0]["rows"]) == r["levels"][0]["cat"]["nvoidt"] == o["cat"]["nvoidt"] > 0
