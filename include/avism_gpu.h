@@ -290,7 +290,7 @@ int avism_gpu_run_level_grid(avism_gpu_ctx *ctx, const avism_params *p, int32_t 
                              const float *u2g, const float *u3g, const float *u4g, avism_cubes *cubes,
                              int32_t *nvoid, avism_voids *voids, float *meandens);
 
-/* ---- MASCLET input (FLAG_DATA = 0) at levels <= 0: replaces the MASCLET branch
+/* ---- MASCLET input (FLAG_DATA = 0) at levels <= 1: replaces the MASCLET branch
  *      of the level loop (src/avism.f90:980-1156) with the density and
  *      divergence choices of 1366-1405 and 1633-1650.  The dark-matter particles
  *      (every level's particles as READ_MASCLET fills them, src/reader.f90:86-405:
@@ -311,7 +311,10 @@ int avism_gpu_run_level_grid(avism_gpu_ctx *ctx, const avism_params *p, int32_t 
  *      refined base cell that no patch covers take 0, the others their base
  *      cell's values) and the DM divergence is 0 (the reference computes
  *      DIVER_UNIFORM of the DM only at levels <= 0).  amr is ignored below
- *      level 1.  Levels above 1 return AVISM_ERR_UNSUPPORTED: the reference's
+ *      level 1.  A patch whose 2-cell rim needs base-cell differences outside
+ *      2..nhy-1, or whose cells fall outside the level grid, returns
+ *      AVISM_ERR_ARG (the reference reads or writes outside its arrays there);
+ *      so do sizes that disagree with the offsets.  Levels above 1 return AVISM_ERR_UNSUPPORTED: the reference's
  *      VMESH indexes its base-size refinement flags with coordinates beyond
  *      them there.
  *      avism_gpu_masclet_fields returns the ext grids (as avism_gpu_fields),
