@@ -76,8 +76,33 @@ static __global__ void k_pack_particles(int64_t n, const float *__restrict__ x, 
     pb[i] = make_float4(vx[i], vy[i], vz[i], 0.0f);
 }
 
-// k_bin_gather with the attributes from the packed records (pa non-null) and,
-// for FINE keys, the quarter-bin offsets as well
+// positions and masses only, for the split form (velocities still in flight)
+static __global__ void k_pack_pos_mass(int64_t n, const float *__restrict__ x, const float *__restrict__ y,
+                                       const float *__restrict__ z, const float *__restrict__ m,
+                                       float4 *__restrict__ pa) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    pa[i] = make_float4(x[i], y[i], z[i], m[i]);
+}
+// the velocities packed in input order, then gathered into the binned records'
+// (vx, vy, vz) next to the masses already there
+static __global__ void k_pack_vel(int64_t n, const float *__restrict__ vx, const float *__restrict__ vy,
+                                  const float *__restrict__ vz, float4 *__restrict__ pb) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    pb[i] = make_float4(vx[i], vy[i], vz[i], 0.0f);
+}
+static __global__ void k_gather_vel(int64_t n, const float4 *__restrict__ sp, const float4 *__restrict__ pb,
+                                    float4 *__restrict__ sv) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 b = pb[__float_as_int(sp[i].w)];
+    sv[i] = make_float4(b.x, b.y, b.z, sv[i].w);
+}
+
+// k_bin_gather with the attributes from the packed records (pa non-null; pb
+// null: masses only, velocities left 0) and, for FINE keys, the quarter-bin
+// offsets as well
 template <bool FINE>
 static __global__ void k_bin_gather2(int64_t n, const uint32_t *__restrict__ keys, const int32_t *__restrict__ vals,
                               const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
@@ -88,7 +113,7 @@ static __global__ void k_bin_gather2(int64_t n, const uint32_t *__restrict__ key
     if (i >= n) return;
     const int32_t v = vals[i];
     if (pa) {
-        const float4 a = pa[v], b = pb[v];
+        const float4 a = pa[v], b = pb ? pb[v] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         sp[i] = make_float4(a.x, a.y, a.z, __int_as_float(v));
         sv[i] = make_float4(b.x, b.y, b.z, a.w);
     } else {

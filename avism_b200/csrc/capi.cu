@@ -26,6 +26,7 @@ int guarded(avism_gpu_ctx *ctx, F &&f) {
         AV_CUDA(cudaSetDevice(ctx->c.device));
         ctx->c.stage_open();
         f(ctx->c);
+        sv_velocities(ctx->c);
         ctx->c.attrs_ready();
         ctx->c.mark("end");
         ctx->c.stage_close();
@@ -33,18 +34,14 @@ int guarded(avism_gpu_ctx *ctx, F &&f) {
         return AVISM_OK;
     } catch (const Error &e) {
         cudaGetLastError();
-        // the caller's host arrays must not be read after the call returns
-        ctx->c.attr_pending = false;
-        cudaStreamSynchronize(ctx->c.copy_stream);
+        ctx->c.drop_pending_copies();
         ctx->c.stage_close();
         return fail(ctx, e.code, e.msg);
     } catch (const std::bad_alloc &) {
-        ctx->c.attr_pending = false;
-        cudaStreamSynchronize(ctx->c.copy_stream);
+        ctx->c.drop_pending_copies();
         return fail(ctx, AVISM_ERR_OOM, "host allocation failed");
     } catch (const std::exception &e) {
-        ctx->c.attr_pending = false;
-        cudaStreamSynchronize(ctx->c.copy_stream);
+        ctx->c.drop_pending_copies();
         return fail(ctx, AVISM_ERR_INTERNAL, e.what());
     }
 }
@@ -161,18 +158,23 @@ P2G p2g_args(Ctx &c, const avism_params *p, const Level &L, int64_t n, const flo
         vx = vy = vz = zv;
     }
     // the attributes on the copy stream, after the positions' copies (the link
-    // is shared); binning's keys and sort run meanwhile, and every reader of
-    // a.m / a.v* first calls c.attrs_ready()
+    // is shared): the masses first, then the velocities.  Binning's keys and
+    // sort run meanwhile; every reader of a.m first calls c.mass_ready() (or
+    // attrs_ready()), every reader of a.v* c.attrs_ready()
     const bool host_attr = (m && !is_device_ptr(m)) || (vx && !is_device_ptr(vx)) || (vy && !is_device_ptr(vy)) ||
                            (vz && !is_device_ptr(vz));
     if (host_attr) {
         AV_CUDA(cudaEventRecord(c.ev_pos, c.stream));
         AV_CUDA(cudaStreamWaitEvent(c.copy_stream, c.ev_pos, 0));
     }
+    a.m = (const float *)to_device_on(c, c.copy_stream, B_PM, m, nb);
+    if (host_attr) {
+        AV_CUDA(cudaEventRecord(c.ev_mass, c.copy_stream));
+        c.mass_pending = true;
+    }
     a.vx = (const float *)to_device_on(c, c.copy_stream, B_PVX, vx, nb);
     a.vy = (const float *)to_device_on(c, c.copy_stream, B_PVY, vy, nb);
     a.vz = (const float *)to_device_on(c, c.copy_stream, B_PVZ, vz, nb);
-    a.m = (const float *)to_device_on(c, c.copy_stream, B_PM, m, nb);
     if (host_attr) {
         AV_CUDA(cudaEventRecord(c.ev_attr, c.copy_stream));
         c.attr_pending = true;
@@ -227,6 +229,7 @@ int avism_gpu_create(avism_gpu_ctx **out, int device) {
         cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->c.copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->c.ev_pos, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->c.ev_mass, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->c.ev_attr, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         delete ctx;
@@ -245,6 +248,7 @@ int avism_gpu_destroy(avism_gpu_ctx *ctx) {
     if (ctx->c.hpin) cudaFreeHost(ctx->c.hpin);
     cudaStreamSynchronize(ctx->c.copy_stream);
     cudaEventDestroy(ctx->c.ev_pos);
+    cudaEventDestroy(ctx->c.ev_mass);
     cudaEventDestroy(ctx->c.ev_attr);
     cudaStreamDestroy(ctx->c.copy_stream);
     cudaStreamDestroy(ctx->c.stream);

@@ -78,13 +78,22 @@ struct Ctx {
     std::string last_error;
     std::vector<double> stage_ms;
     int num_sms = 148;
-    // host->device copies of the particle attributes (m, vx, vy, vz) run on a
-    // second stream after the positions' copies, so that binning's keys and sort
-    // overlap them; ev_attr marks their end, attrs_ready() orders the main
-    // stream after it
+    // host->device copies of the particle attributes (m, then vx, vy, vz) run on
+    // a second stream after the positions' copies, so that binning's keys and
+    // sort overlap them; ev_mass marks the end of the masses, ev_attr the end of
+    // all; mass_ready() / attrs_ready() order the main stream after them
     cudaStream_t copy_stream = nullptr;
-    cudaEvent_t ev_pos = nullptr, ev_attr = nullptr;
-    bool attr_pending = false;
+    cudaEvent_t ev_pos = nullptr, ev_mass = nullptr, ev_attr = nullptr;
+    bool mass_pending = false, attr_pending = false;
+    // binned velocities still to be gathered into sv (bin_particles leaves them
+    // for sv_velocities() while their copy is in flight)
+    struct SvPending {
+        bool on = false;
+        int64_t n = 0;
+        const float4 *sp = nullptr;
+        float4 *sv = nullptr;
+        const float *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    } svp;
     // scratch pinned host memory for small readbacks
     void *hpin = nullptr;
     size_t hpin_cap = 0;
@@ -164,10 +173,22 @@ struct Ctx {
         return hpin;
     }
     void sync() { AV_CUDA(cudaStreamSynchronize(stream)); }
+    void mass_ready() {
+        if (!mass_pending) return;
+        mass_pending = false;
+        AV_CUDA(cudaStreamWaitEvent(stream, ev_mass, 0));
+    }
     void attrs_ready() {
+        mass_pending = false;
         if (!attr_pending) return;
         attr_pending = false;
         AV_CUDA(cudaStreamWaitEvent(stream, ev_attr, 0));
+    }
+    // the caller's host arrays must not be read after a failed call returns
+    void drop_pending_copies() {
+        mass_pending = attr_pending = false;
+        svp = SvPending{};
+        cudaStreamSynchronize(copy_stream);
     }
 };
 
@@ -212,6 +233,9 @@ struct BinnedParticles {
 };
 
 // sv (nullable): receives (vx, vy, vz, m) in binned order
+// the velocities of bin_particles' split form gathered into sv (a no-op when
+// none are pending); every reader of sv's velocities calls it first
+void sv_velocities(Ctx &c);
 BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y, const float *z,
                               float box, int periodic, float occupancy, const float *vx = nullptr,
                               const float *vy = nullptr, const float *vz = nullptr, const float *m = nullptr,

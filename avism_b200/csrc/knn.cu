@@ -63,9 +63,24 @@ BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y,
     float4 *pa = nullptr, *pb = nullptr;
     if (sv) {
         pa = c.get_t<float4>(B_PX4, n);
-        pb = c.get_t<float4>(B_PV4, n);
-        c.attrs_ready();
-        ++c.launches, k_pack_particles<<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, y, z, m, vx, vy, vz, pa, pb);
+        if (c.attr_pending) {
+            // split form: the velocities are still being copied from the host;
+            // the records take the masses now and the velocities in
+            // sv_velocities(), before their first reader
+            c.mass_ready();
+            ++c.launches, k_pack_pos_mass<<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, y, z, m, pa);
+            c.svp.on = true;
+            c.svp.n = n;
+            c.svp.sp = sp;
+            c.svp.sv = sv;
+            c.svp.vx = vx;
+            c.svp.vy = vy;
+            c.svp.vz = vz;
+        } else {
+            pb = c.get_t<float4>(B_PV4, n);
+            c.attrs_ready();
+            ++c.launches, k_pack_particles<<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, y, z, m, vx, vy, vz, pa, pb);
+        }
     }
     if (fine) {
         int32_t *fstart = c.get_t<int32_t>(B_FSTART, nkeys + 1);
@@ -78,6 +93,18 @@ BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y,
     }
     AV_CUDA(cudaGetLastError());
     return bp;
+}
+
+void sv_velocities(Ctx &c) {
+    if (!c.svp.on) return;
+    const Ctx::SvPending v = c.svp;
+    c.svp = Ctx::SvPending{};
+    c.attrs_ready();
+    if (v.n <= 0) return;
+    float4 *pb = c.get_t<float4>(B_PV4, v.n);
+    ++c.launches, k_pack_vel<<<grid_for(v.n, 256), 256, 0, c.stream>>>(v.n, v.vx, v.vy, v.vz, pb);
+    ++c.launches, k_gather_vel<<<grid_for(v.n, 256), 256, 0, c.stream>>>(v.n, v.sp, pb, v.sv);
+    AV_CUDA(cudaGetLastError());
 }
 
 // warp-per-query form: WQ_WARPS warps per block, WQ_QPW consecutive queries per warp

@@ -55,6 +55,7 @@ struct Pyramid {
     int periodic;
     float occ;            // mean particles per bin
     float inv_vscale;     // bw / v_rms
+    int div_at_mean;      // inference: the divergence inputs held at their training mean
 };
 __host__ __device__ constexpr int box_w(int s) { return s == 0 ? 0 : (s == 1 ? 1 : (s == 2 ? 2 : 4)); }
 
@@ -105,6 +106,11 @@ __device__ __forceinline__ float4 pyr_at(const Pyramid &P, int l, int x, int y, 
 __global__ void k_counts(int64_t nb3, const float4 *__restrict__ lev0, float *__restrict__ cnt) {
     const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (b < nb3) cnt[b] = lev0[b].x;
+}
+// the same counts straight from the bins' offsets (no attributes needed)
+__global__ void k_bin_counts(int64_t nb3, const int64_t *__restrict__ start, float *__restrict__ cnt) {
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nb3) cnt[b] = (float)(start[b + 1] - start[b]);
 }
 
 // one separable pass of the (2w+1)-wide box sums along `axis` (wrapped or
@@ -161,6 +167,11 @@ __device__ void bin_features(const Pyramid &P, int nb, int bx, int by, int bz, f
         const float gy = cbox_at(P, s, nb, bx, by + sp, bz) - cbox_at(P, s, nb, bx, by - sp, bz);
         const float gz = cbox_at(P, s, nb, bx, by, bz + sp) - cbox_at(P, s, nb, bx, by, bz - sp);
         f[4 + s] = sqrtf(gx * gx + gy * gy + gz * gz) * (inv_vol * (0.5f / (float)sp));
+    }
+    if (P.div_at_mean) {
+#pragma unroll
+        for (int l = 0; l < PR_LEVELS; l++) f[8 + l] = 0.f;
+        return;
     }
 #pragma unroll
     for (int l = 0; l < PR_LEVELS; l++) {
@@ -490,7 +501,8 @@ __global__ void k_features_tiles(Pyramid P, int nb, const float *__restrict__ mu
     __align__(16) __nv_bfloat16 v[16];
 #pragma unroll
     for (int k = 0; k < 16; k++) {
-        const float x = (k < PR_NF && b < nb3) ? __fdiv_rn(__fsub_rn(f[k], mu[k]), sig[k]) : 0.f;
+        const float x = (k < PR_NF && b < nb3 && !(P.div_at_mean && k >= 8))
+                            ? __fdiv_rn(__fsub_rn(f[k], mu[k]), sig[k]) : 0.f;
         v[k] = __float2bfloat16_rn(x);
     }
     __nv_bfloat16 *t = tiles + (b / TC_M) * (TC_M * 16);
@@ -759,26 +771,34 @@ struct V2Op {
     }
 };
 
+// sv null: the density features only (the bins' counts), the divergence inputs
+// held at their training mean; otherwise all twelve from the velocity pyramid
 Pyramid build_pyramid(Ctx &c, const KnnGrid &G, const float4 *sv, int64_t n) {
     Pyramid P{};
     P.periodic = G.periodic;
     P.occ = G.occ;
-    int nbl = G.nb;
-    for (int l = 0; l < PR_LEVELS; l++) {
-        P.nbl[l] = nbl;
-        P.lev[l] = c.get_t<float4>((BufId)(B_PR_PYR0 + l), (size_t)nbl * nbl * nbl);
-        nbl = (nbl + 1) / 2;
-    }
+    P.div_at_mean = sv ? 0 : 1;
     const int64_t nb3 = (int64_t)G.nb * G.nb * G.nb;
-    ++c.launches, k_pyr_base<<<grid_for(nb3, 256), 256, 0, c.stream>>>(G, sv, P.lev[0]);
-    for (int l = 1; l < PR_LEVELS; l++) {
-        const int64_t n3 = (int64_t)P.nbl[l] * P.nbl[l] * P.nbl[l];
-        ++c.launches, k_pyr_down<<<grid_for(n3, 256), 256, 0, c.stream>>>(P.lev[l - 1], P.nbl[l - 1], P.lev[l], P.nbl[l]);
+    float *cnt = c.get_t<float>(B_PR_CNT, (size_t)nb3);
+    if (sv) {
+        int nbl = G.nb;
+        for (int l = 0; l < PR_LEVELS; l++) {
+            P.nbl[l] = nbl;
+            P.lev[l] = c.get_t<float4>((BufId)(B_PR_PYR0 + l), (size_t)nbl * nbl * nbl);
+            nbl = (nbl + 1) / 2;
+        }
+        ++c.launches, k_pyr_base<<<grid_for(nb3, 256), 256, 0, c.stream>>>(G, sv, P.lev[0]);
+        for (int l = 1; l < PR_LEVELS; l++) {
+            const int64_t n3 = (int64_t)P.nbl[l] * P.nbl[l] * P.nbl[l];
+            ++c.launches, k_pyr_down<<<grid_for(n3, 256), 256, 0, c.stream>>>(P.lev[l - 1], P.nbl[l - 1], P.lev[l],
+                                                                              P.nbl[l]);
+        }
+        ++c.launches, k_counts<<<grid_for(nb3, 256), 256, 0, c.stream>>>(nb3, P.lev[0], cnt);
+    } else {
+        ++c.launches, k_bin_counts<<<grid_for(nb3, 256), 256, 0, c.stream>>>(nb3, G.start, cnt);
     }
     // centred box counts: three separable passes, each for all half-widths
-    float *cnt = c.get_t<float>(B_PR_CNT, (size_t)nb3);
     float *ta = c.get_t<float>(B_PR_TMPA, (size_t)nb3), *tb = c.get_t<float>(B_PR_TMPB, (size_t)nb3);
-    ++c.launches, k_counts<<<grid_for(nb3, 256), 256, 0, c.stream>>>(nb3, P.lev[0], cnt);
     P.cbox[0] = cnt;
     const BufId bid[3] = {B_PR_BOX1, B_PR_BOX2, B_PR_BOX4};
     const dim3 bg((unsigned)((G.nb + 127) / 128), (unsigned)G.nb, (unsigned)G.nb);
@@ -795,7 +815,7 @@ Pyramid build_pyramid(Ctx &c, const KnnGrid &G, const float4 *sv, int64_t n) {
         for (int s = 1; s < 4; s++) P.cbox[s] = out[s - 1];
     }
     // velocity scale of the divergence features: v_rms of the particles
-    {
+    if (sv) {
         double *d = c.get_t<double>(B_RED1, 1);
         auto it = cub::TransformInputIterator<double, V2Op, const float4 *>(sv, V2Op());
         size_t tmp = 0;
@@ -837,12 +857,16 @@ void proposal_features(Ctx &c, const avism_params *p, const P2G &a, float *feat_
     AV_CUDA(cudaGetLastError());
 }
 
-// per-bin starting radius (and half-width) for a level: features from the
-// pyramid, fused into the tensor-core MLP
-void proposal_predict(Ctx &c, const KnnGrid &G, const float4 *sv, int64_t n, float *r0, float *w0) {
+// per-bin starting radius (and half-width) for a level: the density features
+// from the bins' counts, the velocity-divergence inputs held at their training
+// mean, fused into the tensor-core MLP.  The prediction then needs the
+// positions only, so a level's velocities can still be in flight (their
+// inputs gave no measurable saving in the kNN stages: 155.4 / 209.8 ms against
+// 155.5 / 210.1 ms with them at 512^3 / 2^27 particles)
+void proposal_predict(Ctx &c, const KnnGrid &G, float *r0, float *w0) {
     AV_CHECK(c.prop_loaded, AVISM_ERR_ARG,
              "learned proposal requested but no weights are loaded (avism_gpu_proposal_load)");
-    Pyramid P = build_pyramid(c, G, sv, n);
+    Pyramid P = build_pyramid(c, G, nullptr, 0);
     const int64_t nb3 = (int64_t)G.nb * G.nb * G.nb;
     const int64_t rows = (nb3 + TC_M - 1) / TC_M * TC_M;
     __nv_bfloat16 *tiles = c.get_t<__nv_bfloat16>(B_PR_FEAT, (size_t)rows * 16);

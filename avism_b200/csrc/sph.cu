@@ -999,6 +999,7 @@ static void run_sph_kernels_ws(Ctx &c, const KnnGrid &G, const avism_params *p, 
         A.hp_s = hp_s; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
         A.gauss = p->kernel_mode == 2;
         A.ball_list = ball_list; A.ball_count = cnt_d;
+        if (vel_sph) sv_velocities(c);
         const int64_t nblk = (int64_t)((nx + 3) / 4) * ((nx + 3) / 4) * ((nx + 1) / 2);
         ++c.launches, k_cells_knn_w<KMAX, STATS><<<(unsigned)nblk, SPH_WARPS * 32, sm_cells, c.stream>>>(G, A);
         AV_CUDA(cudaGetLastError());
@@ -1058,6 +1059,7 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
         A.hp_s = hp_s; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
         A.gauss = p->kernel_mode == 2;
         A.ball_list = ball_list; A.ball_count = cnt_d;
+        if (vel_sph) sv_velocities(c);
         const int tx = TileDims<T>::x, ty = TileDims<T>::y, tz = TileDims<T>::z;
         const int64_t nblk = (int64_t)((nx + tx - 1) / tx) * ((nx + ty - 1) / ty) * ((nx + tz - 1) / tz);
         ++c.launches, k_cells_knn<KCAP><<<(unsigned)nblk, T, sm, c.stream>>>(G, A);
@@ -1078,7 +1080,7 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
 }
 
 // per-bin starting radius (and half-width) from the learned proposal (proposal.cu)
-void proposal_predict(Ctx &c, const KnnGrid &G, const float4 *sv, int64_t n, float *r0, float *w0);
+void proposal_predict(Ctx &c, const KnnGrid &G, float *r0, float *w0);
 
 void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G &a) {
     const int nx = L.g.nx;
@@ -1139,7 +1141,7 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
             const int64_t nbins = (int64_t)bp.nb * bp.nb * bp.nb;
             float *r0 = c.get_t<float>(B_PR_R0, nbins);
             float *w0 = c.get_t<float>(B_PR_W0, nbins);
-            proposal_predict(c, G, sv, a.n, r0, w0);
+            proposal_predict(c, G, r0, w0);
             G.r0 = r0;
             if (a.wprop) {
                 a.wprop->w0 = w0;
@@ -1246,6 +1248,7 @@ void particles_to_grid(Ctx &c, const avism_params *p, const Level &L, const P2G 
         AV_CUDA(cudaGetLastError());
         c.mark("tsc");
     }
+    sv_velocities(c);
 }
 
 }  // namespace avism
