@@ -366,12 +366,17 @@ __device__ __forceinline__ void uf_union(int32_t *P, int32_t a, int32_t b) {
         a = old;
     }
 }
-// Union-find in shared memory over one CL_TX x CL_TY x CL_TZ tile, then every
-// non-void cell points at its tile component's smallest cell (global index);
-// k_ccl_border joins components across the tiles' low faces.  Local and
-// global indices are both (z, y, x)-lexicographic, so the local minimum is the
-// global minimum and parents keep pointing to smaller indices.
-constexpr int CL_TX = 16, CL_TY = 8, CL_TZ = 8, CL_N = CL_TX * CL_TY * CL_TZ, CL_THREADS = 256;
+// Union-find in shared memory over one CL_TX x CL_TY x CL_TZ tile of the
+// non-void cells (MARCA <= 0), then every such cell points at its tile
+// component's smallest cell (global index); k_ccl_faces joins components
+// across the tiles' low faces.  Local and global indices are both (z, y,
+// x)-lexicographic, so the local minimum is the global minimum and parents
+// keep pointing to smaller indices.  A warp takes whole x-rows of 32 cells: the
+// x-runs come from one ballot, and a cell joins the row below (y - 1, z - 1)
+// only where its left neighbour's pair is not already joined, so a run
+// overlapping another costs one union, not one per cell.
+constexpr int CL_TX = 32, CL_TY = 8, CL_TZ = 8, CL_N = CL_TX * CL_TY * CL_TZ, CL_THREADS = 256;
+constexpr int CL_ROWS = CL_TY * CL_TZ, CL_WARPS = CL_THREADS / 32;
 
 __device__ __forceinline__ int32_t luf_find(int32_t *L, int32_t x) {
     volatile int32_t *V = L;
@@ -399,71 +404,67 @@ __global__ void __launch_bounds__(CL_THREADS) k_ccl_local(PostGrid G, const int3
                                                           int32_t *__restrict__ P) {
     __shared__ int32_t L[CL_N];
     const int ne = G.ne;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ntx = (ne + CL_TX - 1) / CL_TX, nty = (ne + CL_TY - 1) / CL_TY;
     const int bx = (int)(blockIdx.x % ntx), by = (int)((blockIdx.x / ntx) % nty), bz = (int)(blockIdx.x / (ntx * nty));
-    const int X0 = bx * CL_TX, Y0 = by * CL_TY, Z0 = bz * CL_TZ;
-    auto gidx = [&](int li) -> int64_t {
-        const int x = X0 + li % CL_TX, y = Y0 + (li / CL_TX) % CL_TY, z = Z0 + li / (CL_TX * CL_TY);
-        if (x >= ne || y >= ne || z >= ne) return -1;
-        return (int64_t)x + (int64_t)ne * (y + (int64_t)ne * z);
-    };
-    for (int li = threadIdx.x; li < CL_N; li += CL_THREADS) {
-        const int64_t e = gidx(li);
-        L[li] = (e >= 0 && marca[e] <= 0) ? li : -1;
+    const int x = bx * CL_TX + lane, Y0 = by * CL_TY, Z0 = bz * CL_TZ;
+    const uint32_t below = (1u << lane) - 1u;
+    for (int r = warp; r < CL_ROWS; r += CL_WARPS) {
+        const int y = Y0 + r % CL_TY, z = Z0 + r / CL_TY;
+        const bool in = x < ne && y < ne && z < ne;
+        const bool nv = in && marca[(int64_t)x + (int64_t)ne * (y + (int64_t)ne * z)] <= 0;
+        const uint32_t gaps = ~__ballot_sync(0xffffffffu, nv) & below;      // void lanes to the left
+        const int start = gaps ? 32 - __clz(gaps) : 0;                        // first lane of this run
+        L[r * CL_TX + lane] = nv ? r * CL_TX + start : -1;
     }
     __syncthreads();
-    // x-runs of non-void cells point at their first cell
-    int32_t start[CL_N / CL_THREADS];
-#pragma unroll
-    for (int q = 0; q < CL_N / CL_THREADS; q++) {
-        const int li = threadIdx.x + q * CL_THREADS;
-        int r = li;
-        if (L[li] >= 0)
-            while (r % CL_TX > 0 && L[r - 1] >= 0) r--;
-        start[q] = r;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < CL_N / CL_THREADS; q++) {
-        const int li = threadIdx.x + q * CL_THREADS;
-        if (L[li] >= 0) L[li] = start[q];
-    }
-    __syncthreads();
-    for (int li = threadIdx.x; li < CL_N; li += CL_THREADS) {
+    for (int r = warp; r < CL_ROWS; r += CL_WARPS) {
+        const int li = r * CL_TX + lane;
         if (L[li] < 0) continue;
-        const int ly = (li / CL_TX) % CL_TY, lz = li / (CL_TX * CL_TY);
-        if (ly > 0 && L[li - CL_TX] >= 0) luf_union(L, li, li - CL_TX);
-        if (lz > 0 && L[li - CL_TX * CL_TY] >= 0) luf_union(L, li, li - CL_TX * CL_TY);
+        const bool left = lane > 0 && L[li - 1] >= 0;
+        if (r % CL_TY > 0 && L[li - CL_TX] >= 0 && !(left && L[li - CL_TX - 1] >= 0)) luf_union(L, li, li - CL_TX);
+        if (r >= CL_TY && L[li - CL_TX * CL_TY] >= 0 && !(left && L[li - CL_TX * CL_TY - 1] >= 0))
+            luf_union(L, li, li - CL_TX * CL_TY);
     }
     __syncthreads();
-    for (int li = threadIdx.x; li < CL_N; li += CL_THREADS) {
-        const int64_t e = gidx(li);
-        if (e < 0) continue;
-        int32_t r = li;
-        if (L[li] < 0) {
-            P[e] = -1;
-            continue;
-        }
-        while (L[r] != r) r = L[r];
-        P[e] = (int32_t)gidx(r);
+    for (int r = warp; r < CL_ROWS; r += CL_WARPS) {
+        const int y = Y0 + r % CL_TY, z = Z0 + r / CL_TY;
+        if (x >= ne || y >= ne || z >= ne) continue;
+        const int li = r * CL_TX + lane;
+        int32_t q = L[li];
+        if (q >= 0)
+            while (L[q] != q) q = L[q];
+        const int32_t gq = q < 0 ? -1
+                                 : (int32_t)((int64_t)(bx * CL_TX + q % CL_TX) +
+                                             (int64_t)ne * ((Y0 + (q / CL_TX) % CL_TY) + (int64_t)ne * (Z0 + q / (CL_TX * CL_TY))));
+        P[(int64_t)x + (int64_t)ne * (y + (int64_t)ne * z)] = gq;
     }
 }
 
-__global__ void k_ccl_border(PostGrid G, int32_t *P) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// the unions across the tiles' low faces: axis 0 over the planes x = 32a,
+// axis 1 over y = 8a, axis 2 over z = 8a (a >= 1), x fastest in every launch;
+// on the y and z faces a cell skips the union its left neighbour's pair
+// already made (inside one x-tile)
+__global__ void k_ccl_faces(PostGrid G, int axis, int32_t *P) {
     const int ne = G.ne;
-    const int64_t ne3 = (int64_t)ne * ne * ne;
-    if (e >= ne3) return;
-    const int i = (int)(e % ne), j = (int)((e / ne) % ne), k = (int)(e / ((int64_t)ne * ne));
-    const bool fx = i > 0 && i % CL_TX == 0, fy = j > 0 && j % CL_TY == 0, fz = k > 0 && k % CL_TZ == 0;
-    if (!(fx || fy || fz) || P[e] < 0) return;
-    if (fx && P[e - 1] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - 1));
-    if (fy && P[e - ne] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - ne));
-    if (fz && P[e - (int64_t)ne * ne] >= 0) uf_union(P, (int32_t)e, (int32_t)(e - (int64_t)ne * ne));
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nf = (ne - 1) / (axis == 0 ? CL_TX : axis == 1 ? CL_TY : CL_TZ);   // faces at a = 1..nf
+    const int64_t plane = (int64_t)ne * ne;
+    if (t >= (int64_t)nf * plane) return;
+    const int a = (int)(t / plane) + 1;
+    const int u = (int)(t % ne), v = (int)((t / ne) % ne);
+    int x, y, z;
+    int64_t step;
+    if (axis == 0) { x = a * CL_TX; y = u; z = v; step = 1; }
+    else if (axis == 1) { x = u; y = a * CL_TY; z = v; step = ne; }
+    else { x = u; y = v; z = a * CL_TZ; step = plane; }
+    const int64_t e = (int64_t)x + (int64_t)ne * (y + (int64_t)ne * z);
+    if (P[e] < 0 || P[e - step] < 0) return;
+    if (axis != 0 && x % CL_TX > 0 && P[e - 1] >= 0 && P[e - step - 1] >= 0) return;
+    uf_union(P, (int32_t)e, (int32_t)(e - step));
 }
 
-// root of x without path compression: a compressing find racing with another
-// thread's final store could leave that cell pointing at a non-root ancestor
+// root of x without path compression (read-only: the unions are done)
 __device__ __forceinline__ int32_t uf_root(const int32_t *P, int32_t x) {
     while (true) {
         const int32_t px = P[x];
@@ -471,26 +472,22 @@ __device__ __forceinline__ int32_t uf_root(const int32_t *P, int32_t x) {
         x = px;
     }
 }
-__global__ void k_ccl_flatten(int64_t ne3, int32_t *P) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < ne3 && P[e] >= 0) P[e] = uf_root(P, (int32_t)e);
-}
-// a hole takes the id of the first non-hole cell in +x (src/voidfinding.f90:1142-1158)
-__global__ void k_fill_holes(PostGrid G, const int32_t *P, const int32_t *marca_in, int32_t *marca_out) {
+// A hole is a non-void cell outside the component of the first cell; it takes
+// the id of the first non-hole cell in +x (src/voidfinding.f90:1142-1158).
+// In place: only holes are written and only non-holes are read.  Parents point
+// to smaller indices, so cell 0, when non-void, is its component's root.
+__global__ void k_fill_holes(PostGrid G, const int32_t *__restrict__ P, int32_t *marca) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int ne = G.ne;
     const int64_t ne3 = (int64_t)ne * ne * ne;
     if (e >= ne3) return;
-    const int32_t root = P[0];
-    auto hole = [&](int64_t f) { const int32_t r = P[f]; return r >= 0 && r != root; };
-    if (!hole(e)) {
-        marca_out[e] = marca_in[e];
-        return;
-    }
+    const int32_t root0 = P[0] >= 0 ? 0 : -1;
+    auto hole = [&](int64_t f) { return P[f] >= 0 && uf_root(P, (int32_t)f) != root0; };
+    if (!hole(e)) return;
     const int64_t rowend = e - (e % ne) + ne;
-    int64_t f = e;
+    int64_t f = e + 1;
     while (f < rowend && hole(f)) f++;
-    marca_out[e] = f < rowend ? marca_in[f] : 0;
+    marca[e] = f < rowend ? marca[f] : 0;
 }
 
 // ---- VOID_PERIODIC helpers ----------------------------------------------------
@@ -859,13 +856,13 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
     // ---- SIMPLE_CONNECTION_FAST
     {
         int32_t *P = c.get_t<int32_t>(B_CCL, ne3);
-        int32_t *m2 = c.get_t<int32_t>(B_PAINT, ne3);
         const int64_t ntl = (int64_t)((ne + CL_TX - 1) / CL_TX) * ((ne + CL_TY - 1) / CL_TY) * ((ne + CL_TZ - 1) / CL_TZ);
         ++c.launches, k_ccl_local<<<(unsigned)ntl, CL_THREADS, 0, c.stream>>>(PG, marca, P);
-        ++c.launches, k_ccl_border<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, P);
-        ++c.launches, k_ccl_flatten<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, P);
-        ++c.launches, k_fill_holes<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, P, marca, m2);
-        AV_CUDA(cudaMemcpyAsync(marca, m2, (size_t)ne3 * 4, cudaMemcpyDeviceToDevice, c.stream));
+        for (int axis = 0; axis < 3; axis++) {
+            const int64_t nface = (int64_t)((ne - 1) / (axis == 0 ? CL_TX : axis == 1 ? CL_TY : CL_TZ)) * ne * ne;
+            if (nface > 0) ++c.launches, k_ccl_faces<<<grid_for(nface, 256), 256, 0, c.stream>>>(PG, axis, P);
+        }
+        ++c.launches, k_fill_holes<<<grid_for(ne3, 256), 256, 0, c.stream>>>(PG, P, marca);
         AV_CUDA(cudaGetLastError());
     }
     c.mark("simple_connection");
