@@ -408,8 +408,8 @@ constexpr uint32_t TC_WAIT_LIMIT = 1u << 22;      // mbarrier polls before givin
 
 struct __align__(1024) TcSmem {
     __nv_bfloat16 a0[2][TC_M * 16];     // input tiles, K = 16 (double buffered)
-    __nv_bfloat16 a1[TC_M * PR_H];      // hidden activations (ping)
-    __nv_bfloat16 a2[TC_M * PR_H];      // hidden activations (pong)
+    __nv_bfloat16 a1[TC_M * PR_H];      // hidden activations: each epilogue overwrites the
+                                        // layer input its MMA has finished reading
     __nv_bfloat16 w1[PR_H * 16];        // W1, N = 64 rows, K = 16
     __nv_bfloat16 w2[PR_H * PR_H];
     __nv_bfloat16 w3[PR_H * PR_H];
@@ -558,15 +558,28 @@ struct TcIO {
     int *err;                  // set to 1 when a bounded wait gave up
 };
 
-// hidden layer epilogue: D (this thread's row, 64 columns) + bias -> relu -> bf16 tile
+// 16 consecutive f32 columns of this thread's TMEM lane, without the wait
+__device__ __forceinline__ void tc_ld16_issue(uint32_t taddr, uint32_t r[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+// hidden layer epilogue: D (this thread's row, 64 columns, read from TMEM in
+// four loads and one wait) + bias -> relu -> bf16 tile
 __device__ __forceinline__ void tc_hidden(uint32_t taddr, const float *bias, __nv_bfloat16 *dst, int row) {
+    uint32_t r[PR_H];
+#pragma unroll
+    for (int c0 = 0; c0 < PR_H; c0 += 16) tc_ld16_issue(taddr + c0, r + c0);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int c0 = 0; c0 < PR_H; c0 += 16) {
-        float v[16];
-        tc_ld16(taddr + c0, v);
         __align__(16) __nv_bfloat16 o[16];
 #pragma unroll
-        for (int i = 0; i < 16; i++) o[i] = __float2bfloat16_rn(fmaxf(__fadd_rn(v[i], bias[c0 + i]), 0.f));
+        for (int i = 0; i < 16; i++)
+            o[i] = __float2bfloat16_rn(fmaxf(__fadd_rn(__uint_as_float(r[c0 + i]), bias[c0 + i]), 0.f));
         *reinterpret_cast<uint4 *>(dst + tc_off(row, c0, PR_H)) = *reinterpret_cast<const uint4 *>(&o[0]);
         *reinterpret_cast<uint4 *>(dst + tc_off(row, c0 + 8, PR_H)) = *reinterpret_cast<const uint4 *>(&o[8]);
     }
@@ -676,14 +689,14 @@ k_mlp_tc(TcIO io, const TcWeights *__restrict__ Wg) {
         phase ^= 1;
         tc_fence_after();
         if (!ok) break;
-        tc_hidden(lane_addr, S.b2, S.a2, tid);
+        tc_hidden(lane_addr, S.b2, S.a1, tid);
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
         if (tid == 0) {
             for (int s = 0; s < 4; s++)
-                tc_mma(tmem, tc_desc(S.a2 + s * 128, 128, 8 * 128), tc_desc(S.w3 + s * 128, 128, 8 * 128),
+                tc_mma(tmem, tc_desc(S.a1 + s * 128, 128, 8 * 128), tc_desc(S.w3 + s * 128, 128, 8 * 128),
                        tc_idesc(TC_M, PR_H), s > 0);
             tc_commit(&S.mbar);
         }
