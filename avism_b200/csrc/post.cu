@@ -68,11 +68,27 @@ __global__ void k_time_to_label(int64_t ne3, const int32_t *tgrid, const int32_t
     marca[e] = t == INT_MAX ? 0 : owner_by_time[t];
 }
 
+// MARCA = map[MARCA] for the void cells, four cells per thread (16-byte loads:
+// MARCA is the context's own B_MARCA buffer, 256-byte aligned by cudaMalloc),
+// stores only where a label changes
 __global__ void k_relabel(int64_t ne3, int32_t *marca, const int32_t *map) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t e = q * 4;
     if (e >= ne3) return;
-    const int32_t m = marca[e];
-    if (m > 0) marca[e] = map[m];
+    if (e + 4 <= ne3) {
+        int4 v = *reinterpret_cast<const int4 *>(marca + e);
+        const int4 o = v;
+        if (v.x > 0) v.x = map[v.x];
+        if (v.y > 0) v.y = map[v.y];
+        if (v.z > 0) v.z = map[v.z];
+        if (v.w > 0) v.w = map[v.w];
+        if (v.x != o.x || v.y != o.y || v.z != o.z || v.w != o.w) *reinterpret_cast<int4 *>(marca + e) = v;
+        return;
+    }
+    for (int64_t f = e; f < ne3; f++) {
+        const int32_t m = marca[f];
+        if (m > 0 && map[m] != m) marca[f] = map[m];
+    }
 }
 
 // warp-aggregated count per main-void label (uvoid == -1) over the ext grid
@@ -772,7 +788,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
         std::vector<int32_t> map(nvs + 1);
         for (int32_t i = 0; i <= nv; i++) map[i] = rm[i] ? 0 : i;
         AV_CUDA(cudaMemcpyAsync(map_d, map.data(), sizeof(int32_t) * (size_t)(nv + 1), cudaMemcpyHostToDevice, c.stream));
-        ++c.launches, k_relabel<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, map_d);
+        ++c.launches, k_relabel<<<grid_for((ne3 + 3) / 4, 256), 256, 0, c.stream>>>(ne3, marca, map_d);
         for (int32_t i = 0; i < nv; i++)
             if (uvoid[i] > 0 && rm[uvoid[i]]) uvoid[i] = 0;
         for (int32_t i = 1; i <= nv; i++)
@@ -1046,7 +1062,7 @@ void merge_post(Ctx &c, const avism_params *p, const Level &L, int32_t nv, const
             std::vector<int32_t> flat(nvs + 1);
             for (int32_t i = 0; i <= nv; i++) flat[i] = i == 0 ? 0 : find(i);
             AV_CUDA(cudaMemcpyAsync(map_d, flat.data(), sizeof(int32_t) * (size_t)(nv + 1), cudaMemcpyHostToDevice, c.stream));
-            ++c.launches, k_relabel<<<grid_for(ne3, 256), 256, 0, c.stream>>>(ne3, marca, map_d);
+            ++c.launches, k_relabel<<<grid_for((ne3 + 3) / 4, 256), 256, 0, c.stream>>>(ne3, marca, map_d);
             c.sync();
         }
     }
