@@ -44,6 +44,8 @@ SIGNATURES = {
     "avism_gpu_run_level_grid": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 8),
     "avism_gpu_masclet_fields": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 5 + [_i64] + [_c_void] * 10),
     "avism_gpu_run_level_masclet": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 5 + [_i64] + [_c_void] * 11),
+    "avism_gpu_run_sublevel_masclet": (C.c_int, [_c_void, _c_void, _i32] + [_c_void] * 5 + [_i64] + [_c_void] * 9 +
+                                       [_i32] + [_c_void] * 4),
     "avism_gpu_survey_fields": (C.c_int, [_c_void, _c_void, _i64] + [_c_void] * 7 + [_i64] + [_c_void] * 9),
     "avism_gpu_run_level_survey": (C.c_int, [_c_void, _c_void, _i64] + [_c_void] * 7 + [_i64] + [_c_void] * 9),
     "avism_gpu_knn_noalloc": (C.c_int, [C.c_int, _c_void, _i64, _c_void, _c_void, _c_void, _f32, _i64,

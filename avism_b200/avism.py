@@ -479,6 +479,24 @@ class AvismGPU:
                                                        C.byref(vo.c), C.byref(md)))
         return dict(cubes=cubes.view(nv.value), nvoid=nv.value, cat=vo.view(nv.value), meandens=md.value)
 
+    def run_sublevel_masclet(self, p: Params, nhy, gas, marcap_ext, reqp, parts=None, amr=None, want_marca=False,
+                             capacity=None):
+        """A MASCLET level inside the parent voids (MARCAP2 and REQP of next_level)."""
+        gr, _ = grid_setup(p)
+        cap = int(capacity or p.nvoid_max)
+        cubes = Cubes(cap)
+        vo = Voids(cap, gr.ne if want_marca else None)
+        nv, md = C.c_int32(), C.c_float()
+        pc = p.to_c()
+        pc.nvoid_max = min(p.nvoid_max, cap)
+        args, _keep = self._masclet_args(nhy, gas, parts, amr)
+        mp = np.ascontiguousarray(marcap_ext, np.int32)
+        rq = _f32(reqp)
+        self._chk(self.lib.avism_gpu_run_sublevel_masclet(self.h, C.byref(pc), *args, _vp(mp), _vp(rq), len(rq),
+                                                          C.byref(cubes.c), C.byref(nv), C.byref(vo.c),
+                                                          C.byref(md)))
+        return dict(cubes=cubes.view(nv.value), nvoid=nv.value, cat=vo.view(nv.value), meandens=md.value)
+
     # ---- survey mode (src/avism.f90:1420-1596) -------------------------------------
     def _survey_args(self, parts, rands, smask):
         a = {k: (_f32(parts[k]) if parts.get(k) is not None else None)

@@ -931,6 +931,35 @@ int avism_gpu_run_level_masclet(avism_gpu_ctx *ctx, const avism_params *p, int32
     });
 }
 
+int avism_gpu_run_sublevel_masclet(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g,
+                                   const float *u2g, const float *u3g, const float *u4g, const avism_patches *amr,
+                                   int64_t n, const float *x, const float *y, const float *z, const float *vx,
+                                   const float *vy, const float *vz, const float *m, const int32_t *marcap_ext,
+                                   const float *reqp, int32_t nreqp, avism_cubes *cubes, int32_t *nvoid,
+                                   avism_voids *voids, float *meandens) {
+    return guarded(ctx, [&](Ctx &c) {
+        check_params(p);
+        AV_CHECK(nvoid && voids && marcap_ext && nreqp >= 0 && (nreqp == 0 || reqp), AVISM_ERR_ARG,
+                 "run_sublevel_masclet: null argument");
+        Level L = make_level(p);
+        const int64_t ne3 = (int64_t)L.g.ne * L.g.ne * L.g.ne;
+        float *u1, *dv;
+        const float md = masclet_fields_dev(c, p, L, nhy, u1g, u2g, u3g, u4g, amr, n, x, y, z, vx, vy, vz, m, &u1, &dv);
+        const int32_t *mp = (const int32_t *)to_device(c, B_MARCAP, marcap_ext, sizeof(int32_t) * (size_t)ne3);
+        const float *rq = nreqp > 0 ? (const float *)to_device(c, B_REQP, reqp, sizeof(float) * (size_t)nreqp) : nullptr;
+        c.mark("divergence");
+        CubesDev cd{};
+        const int32_t nv = voidfind_device(c, p, L, u1, dv, 0, nullptr, mp, rq, nreqp, cd, nullptr);
+        HostCubes hc(c, cd, nv);
+        if (cubes) cubes_out(c, cd, hc.v, nv, cubes);
+        c.mark("cubes_d2h");
+        merge_post(c, p, L, nv, &hc.v, u1, md, voids, voids->marca);
+        c.mark("catalogue_d2h");
+        *nvoid = nv;
+        if (meandens) *meandens = md;
+    });
+}
+
 int avism_gpu_run_level(avism_gpu_ctx *ctx, const avism_params *p, int64_t n, const float *x, const float *y,
                         const float *z, const float *vx, const float *vy, const float *vz, const float *m,
                         avism_cubes *cubes, int32_t *nvoid, avism_voids *voids, float *meandens) {

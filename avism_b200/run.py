@@ -17,7 +17,10 @@ The reference's other inputs, one level each:
     src/reader.f90:523-552) at the level with --nx = NHY * 2^level, level <= 0;
   * --mask FILE --randoms FILE: survey mode (FLAG_SURVEY = 1) with the mask and
     randoms files (src/avism.f90:403-418, 1425-1444); --novel reads the
-    particle file as READ_BINARY_PART_2 (no velocities).
+    particle file as READ_BINARY_PART_2 (no velocities);
+  * --masclet GAS DM --nhy NHYX: a MASCLET snapshot (the positional file is its
+    grid file); with --levels 2 and --level 0, level 1 runs inside the level-0
+    voids from the snapshot's level-1 patches.
 """
 from __future__ import annotations
 
@@ -71,6 +74,51 @@ def run_iteration(particle_path, p: Params, out_dir, it: int = 1, nlev: int = 1,
             cat = res["cat"]
             marcap, reqp = engine.next_level(q, res["nvoid"], cat["marca"], cat["uvoid"], cat["req"])
             req_parent, nvoidp = reqp, res["nvoid"]          # REQP and NVOIDP = NVOID (avism.f90:2139-2146)
+    return dict(voids=vp, cubes=cp, map=mp, levels=results)
+
+
+def run_masclet_iteration(grid_path, gas_path, dm_path, nhy, p: Params, out_dir, it: int = 1, nlev: int = 1,
+                          cubes: bool = False, maps: bool = False, engine=None) -> dict:
+    """A MASCLET snapshot's levels p.levmin .. p.levmin + nlev - 1 (at most level
+    1; p.nx is the first level's grid, nhy * 2^levmin): the first with
+    run_level_masclet, each next one inside the previous level's voids with
+    run_sublevel_masclet, level 1 from the snapshot's level-1 patches, as the
+    reference's level loop runs MASCLET input (src/avism.f90:742-2181)."""
+    from .avism import read_masclet_files
+    r = read_masclet_files(grid_path, gas_path, dm_path, nhy)
+    p = Params(**{**p.__dict__, "zeta": float(r["zeta"]), "level": p.levmin})
+    gas = tuple(r["gas"][k] for k in ("u1g", "u2g", "u3g", "u4g"))
+    parts = r["parts"] if p.flag_dens <= 1 or p.flag_div in (0, 1) else None
+    if engine is None:
+        from .avism import AvismGPU
+        engine = AvismGPU(0)
+    os.makedirs(out_dir, exist_ok=True)
+    vp = os.path.join(out_dir, f"voids{it:05d}")
+    cp = os.path.join(out_dir, f"cubes{it:05d}") if cubes else None
+    mp = os.path.join(out_dir, f"map{it:05d}") if maps else None
+    write_catalogue_headers(vp, cp, nlev, p.levmin, p.levmin + nlev - 1, p.nx, p.nx, p.nx, p.lado0)
+    if mp:
+        open(mp, "wb").close()
+    results = []
+    req_parent, nvoidp, marcap, reqp = None, 0, None, None
+    for lev in range(nlev):
+        q = Params(**{**p.__dict__, "nx": p.nx * 2 ** lev, "level": p.levmin + lev})
+        amr = r["amr"] if q.level == 1 else None
+        keep_marca = maps or lev + 1 < nlev
+        if lev == 0:
+            res = engine.run_level_masclet(q, nhy, gas, parts, amr, want_marca=keep_marca)
+        else:
+            res = engine.run_sublevel_masclet(q, nhy, gas, marcap, reqp, parts, amr, want_marca=keep_marca)
+        u1 = dv = None
+        if maps:
+            u1, dv, _ = engine.masclet_fields(q, nhy, gas, parts, amr)
+        append_catalogue_level(vp, q, res, nvoidp=nvoidp, req_parent=req_parent, cubes_path=cp, map_path=mp,
+                               u1co_ext=u1, diverco_ext=dv)
+        results.append(res)
+        if lev + 1 < nlev:
+            cat = res["cat"]
+            marcap, reqp = engine.next_level(q, res["nvoid"], cat["marca"], cat["uvoid"], cat["req"])
+            req_parent, nvoidp = reqp, res["nvoid"]
     return dict(voids=vp, cubes=cp, map=mp, levels=results)
 
 
@@ -145,7 +193,10 @@ def main(argv=None):
     a = ap.parse_args(argv)
     p = Params(nx=a.nx, lado0=a.lado0, periodic=a.periodic, kneighbours=a.kneighbours, learned=a.learned,
                nvoid_max=a.nvoid_max, level=a.level, levmin=a.level, flag_dens=a.flag_dens, flag_div=a.flag_div)
-    if a.grid or a.mask or a.masclet:
+    if a.masclet and a.levels > 1:
+        r = run_masclet_iteration(a.particles, a.masclet[0], a.masclet[1], a.nhy or a.nx, p, a.out, it=a.iter,
+                                  nlev=a.levels, cubes=a.cubes, maps=a.map)
+    elif a.grid or a.mask or a.masclet:
         r = run_single(a.particles, p, a.out, it=a.iter, grid_nhy=a.grid, mask=a.mask, randoms=a.randoms,
                        novel=a.novel, ncox=a.ncox, cubes=a.cubes, masclet=a.masclet, masclet_nhy=a.nhy or a.nx)
     else:

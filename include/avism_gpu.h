@@ -340,6 +340,16 @@ int avism_gpu_run_level_masclet(avism_gpu_ctx *ctx, const avism_params *p, int32
                                 int64_t n, const float *x, const float *y, const float *z, const float *vx,
                                 const float *vy, const float *vz, const float *m, avism_cubes *cubes,
                                 int32_t *nvoid, avism_voids *voids, float *meandens);
+/* A MASCLET level below LEVMIN (voids-in-voids, src/avism.f90:1159-1973 at IR >
+ * LEVMIN): the fields as avism_gpu_run_level_masclet, the void stage as
+ * avism_gpu_run_sublevel with the parent map MARCAP2 (marcap_ext, the ext grid
+ * of this level) and the parent radii REQP of avism_gpu_next_level.         */
+int avism_gpu_run_sublevel_masclet(avism_gpu_ctx *ctx, const avism_params *p, int32_t nhy, const float *u1g,
+                                   const float *u2g, const float *u3g, const float *u4g, const avism_patches *amr,
+                                   int64_t n, const float *x, const float *y, const float *z, const float *vx,
+                                   const float *vy, const float *vz, const float *m, const int32_t *marcap_ext,
+                                   const float *reqp, int32_t nreqp, avism_cubes *cubes, int32_t *nvoid,
+                                   avism_voids *voids, float *meandens);
 
 /* ---- survey mode (FLAG_SURVEY = 1): replaces src/avism.f90:1420-1596.  The
  *      tracers (x..m, masses as weights; velocities nullable with

@@ -197,6 +197,14 @@ def run_level_masclet(p: Params, nhy, gas, parts=None, amr=None):
     return dict(u1co=u1, diverco=dv, meandens=md, vf=vf, cat=cat)
 
 
+def run_sublevel_masclet(p: Params, nhy, gas, marcap_ext, reqp, parts=None, amr=None):
+    """A MASCLET level inside the parent voids on the CPU."""
+    u1, dv, md = masclet_fields(p, nhy, gas, parts, amr)
+    vf = voidfind(p, u1, dv, marcap_ext=marcap_ext, reqp=reqp)
+    cat = merge_post(p, vf["nvoid"], vf["cubes"], u1, md)
+    return dict(u1co=u1, diverco=dv, meandens=md, vf=vf, cat=cat)
+
+
 def smask_ext(p: Params, smask):
     """The survey mask on the ext grid: the inner cells' values, 0 on the ghost
     shell (SMASK = 0 before the inner cells are set, src/avism.f90:867-869)."""

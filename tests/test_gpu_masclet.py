@@ -107,6 +107,34 @@ def test_level1_refuses_patches_outside(gpu, snap, bad):
     assert np.array_equal(u1, u1o) and np.array_equal(dv, dvo)
 
 
+@pytest.mark.parametrize("fd,fv", [(2, 2), (0, -1)])
+def test_level1_inside_level0_voids(gpu, snap, fd, fv):
+    """Voids-in-voids on MASCLET input, GPU against the oracle's same sequence:
+    level 0, the parent map of next_level, level 1 from the patches inside the
+    level-0 voids (cubes and catalogue bit-exact)."""
+    ng = snap["ng"]
+    parts = mc.particles(snap) if fd <= 1 else None
+    p0 = params(snap, fd, fv, 0)
+    o0 = O.run_level_masclet(p0, ng, mc.gas(snap), parts)
+    g0 = gpu.run_level_masclet(p0, ng, mc.gas(snap), parts, want_marca=True, capacity=200000)
+    assert np.array_equal(g0["cat"]["marca"], o0["cat"]["marca"])
+    nv = o0["vf"]["nvoid"]
+    mp, rq = O.next_level(p0, nv, o0["cat"]["marca"], o0["cat"]["uvoid"], o0["cat"]["req"])
+    gmp, grq = gpu.next_level(p0, nv, g0["cat"]["marca"], g0["cat"]["uvoid"], g0["cat"]["req"])
+    assert np.array_equal(mp, gmp) and np.array_equal(rq, grq)
+    p1 = Params(nx=2 * ng, periodic=1, lado0=snap["box"], level=1, levmin=0, flag_dens=fd, flag_div=fv)
+    o1 = O.run_sublevel_masclet(p1, ng, mc.gas(snap), mp, rq, parts, mc.amr(snap))
+    g1 = gpu.run_sublevel_masclet(p1, ng, mc.gas(snap), mp, rq, parts, mc.amr(snap), want_marca=True,
+                                  capacity=200000)
+    assert g1["nvoid"] == o1["vf"]["nvoid"] > 0
+    for k in g1["cubes"]:
+        assert np.array_equal(g1["cubes"][k], o1["vf"]["cubes"][k]), k
+    for k in ("indice", "uvoid", "ncellv", "marca", "volnew", "req", "gxc", "gyc", "gzc", "eps", "ip", "umean",
+              "mtot"):
+        assert np.array_equal(g1["cat"][k], o1["cat"][k]), k
+    assert np.all(np.asarray(g1["cubes"]["father"]) > 0)
+
+
 def test_level_above_one_is_unsupported(gpu, snap):
     from avism_b200.avism import AvismError
     p = Params(nx=4 * snap["ng"], periodic=1, lado0=snap["box"], level=2)

@@ -208,3 +208,19 @@ def test_oracle_gas_only_needs_no_particles(snap):
     p = Params(nx=snap["ng"] // 2, periodic=0, lado0=snap["box"], level=-1, levmin=-1, flag_dens=2, flag_div=2)
     u1, dv, md = O.masclet_fields(p, snap["ng"], mc.gas(snap), None)
     assert np.isfinite(u1).all() and np.isfinite(dv).all() and md > 0
+
+
+def test_oracle_level1_inside_level0_voids(snap):
+    """Voids-in-voids on MASCLET input: level 0, its parent map (next_level),
+    then level 1 from the patches inside the level-0 voids; every level-1 cube
+    has a level-0 father."""
+    ng = snap["ng"]
+    p0 = Params(nx=ng, periodic=1, lado0=snap["box"], level=0, levmin=0, flag_dens=2, flag_div=2)
+    o0 = O.run_level_masclet(p0, ng, mc.gas(snap), None)
+    mp, rq = O.next_level(p0, o0["vf"]["nvoid"], o0["cat"]["marca"], o0["cat"]["uvoid"], o0["cat"]["req"])
+    assert 0 < np.mean(mp > 0) < 1
+    p1 = Params(nx=2 * ng, periodic=1, lado0=snap["box"], level=1, levmin=0, flag_dens=2, flag_div=2)
+    o1 = O.run_sublevel_masclet(p1, ng, mc.gas(snap), mp, rq, None, mc.amr(snap))
+    assert o1["vf"]["nvoid"] > 0 and o1["cat"]["nvoidt"] > 0
+    assert np.all(np.asarray(o1["vf"]["cubes"]["father"]) > 0)
+

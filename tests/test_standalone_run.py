@@ -72,8 +72,14 @@ class OracleModes(OracleEngine):
     def run_level_survey(self, p, parts, rands, smask):
         return self._res(O.run_level_survey(p, parts, rands, smask))
 
-    def run_level_masclet(self, p, nhy, gas, parts, amr=None):
+    def run_level_masclet(self, p, nhy, gas, parts, amr=None, want_marca=False):
         return self._res(O.run_level_masclet(p, nhy, gas, parts, amr))
+
+    def run_sublevel_masclet(self, p, nhy, gas, marcap, reqp, parts, amr=None, want_marca=False):
+        return self._res(O.run_sublevel_masclet(p, nhy, gas, marcap, reqp, parts, amr))
+
+    def masclet_fields(self, p, nhy, gas, parts, amr=None):
+        return O.masclet_fields(p, nhy, gas, parts, amr)
 
 
 def test_grid_file_level(tmp_path):
@@ -139,3 +145,22 @@ def test_masclet_files_level1(tmp_path):
     o = O.run_level_masclet(p, snap["ng"], mc.gas(snap), None, mc.amr(snap))
     head, levels = _read_voids_file(r["voids"])
     assert len(levels[0]["rows"]) == r["levels"][0]["cat"]["nvoidt"] == o["cat"]["nvoidt"] > 0
+
+
+def test_masclet_two_levels(tmp_path):
+    """Levels 0 and 1 of a MASCLET snapshot through the runner: level 1 inside
+    the level-0 voids, from the level-1 patches; the files hold both levels and
+    the map."""
+    from avism_b200.run import run_masclet_iteration
+    import masclet_case as mc
+    snap = mc.snapshot()
+    grid, gas, dm = mc.write_files(snap, str(tmp_path))
+    p = Params(nx=snap["ng"], periodic=1, lado0=snap["box"], level=0, levmin=0, flag_dens=2, flag_div=2)
+    r = run_masclet_iteration(grid, gas, dm, snap["ng"], p, tmp_path / "out", nlev=2, cubes=True, maps=True,
+                              engine=OracleModes())
+    head, levels = _read_voids_file(r["voids"])
+    assert len(levels) == 2
+    for lv, res in zip(levels, r["levels"]):
+        assert len(lv["rows"]) == res["cat"]["nvoidt"] > 0
+    assert os.path.getsize(r["map"]) > 0
+
