@@ -838,7 +838,8 @@ AmrPatches amr_patches(Ctx &c, const avism_patches *a) {
         AV_CHECK(r.nx[q] >= 1 && r.ny[q] >= 1 && r.nz[q] >= 1 &&
                      r.offset[q + 1] - r.offset[q] == (int64_t)r.nx[q] * r.ny[q] * r.nz[q],
                  AVISM_ERR_ARG, "MASCLET level 1: patch sizes and offsets disagree");
-    const size_t cells = sizeof(float) * (size_t)std::max<int64_t>(r.offset[np], 1);
+    if (r.offset[np] == 0) return r;                    // no patches: no cells to read
+    const size_t cells = sizeof(float) * (size_t)r.offset[np];
     AV_CHECK(a->u11g && a->u12g && a->u13g && a->u14g, AVISM_ERR_ARG, "MASCLET level 1: null patch cells");
     r.u11g = (const float *)to_device(c, B_AMR1, a->u11g, cells);
     r.u12g = (const float *)to_device(c, B_AMR2, a->u12g, cells);

@@ -107,6 +107,19 @@ def test_level1_refuses_patches_outside(gpu, snap, bad):
     assert np.array_equal(u1, u1o) and np.array_equal(dv, dvo)
 
 
+def test_level1_without_patches(gpu, snap):
+    """No level-1 patches: every level-1 cell takes its base cell's U1G and
+    DIVER0, as the oracle gives."""
+    ng = snap["ng"]
+    p = params(snap, 2, 2, 1)
+    none = {k: np.zeros(0, np.int32) for k in ("nx", "ny", "nz", "ix", "iy", "iz")}
+    none.update({k: np.zeros(0, np.float32) for k in ("rx", "ry", "rz", "u11g", "u12g", "u13g", "u14g")})
+    none["offset"] = np.zeros(1, np.int64)
+    u1o, dvo, mdo = O.masclet_fields(p, ng, mc.gas(snap), None, none)
+    u1g, dvg, mdg = gpu.masclet_fields(p, ng, mc.gas(snap), None, none)
+    assert np.array_equal(u1o, u1g) and np.array_equal(dvo, dvg) and mdo == mdg
+
+
 @pytest.mark.parametrize("fd,fv", [(2, 2), (0, -1)])
 def test_level1_inside_level0_voids(gpu, snap, fd, fv):
     """Voids-in-voids on MASCLET input, GPU against the oracle's same sequence:
