@@ -159,8 +159,9 @@ class Voids:
 
 @dataclass
 class Params:
-    """Python view of avism_params; defaults are the README thresholds
-    (README.md:209-224) with h=0.678, Omega_m=0.31 (config/voids.dat:12)."""
+    """Python view of avism_params; defaults are the thresholds the AVISM
+    project's own README recommends (its lines 209-224) with h=0.678,
+    Omega_m=0.31 (config/voids.dat:12)."""
     nx: int = 64
     periodic: int = 1
     lado0: float = 100.0
