@@ -50,6 +50,7 @@ enum BufId : int {
     B_RED0, B_RED1, B_RED2,
     B_QUERY, B_RAD, B_BALL, B_SCAL, B_KNN_R0,
     B_SV, B_PDENS_S, B_HPART_S,                    // per-particle attributes in binned order
+    B_SVW,                                         // (vx, vy, vz, m / PPART_DENS) in binned order
     B_PR_PARAMS, B_PR_PACKED, B_PR_PACKED_TMP,     // learned proposal: parameters, packed weights
     B_PR_TRAIN, B_PR_IDX, B_PR_GRAD, B_PR_ERR,     // training scratch
     B_PR_PYR0, B_PR_PYR1, B_PR_PYR2, B_PR_PYR3,    // feature pyramid

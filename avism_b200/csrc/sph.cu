@@ -122,6 +122,7 @@ struct CellArgs {
     const int8_t *smask;
     const float4 *sv;                 // (vx, vy, vz, m) in binned order
     const float *pd_s;                // particle density in binned order
+    const float4 *svw;                // (vx, vy, vz, m / pd) in binned order (k_cells_knn_w)
     float *hp_s, *u2, *u3, *u4;       // h in binned order
     int do_vel;
     int gauss;                        // KERNEL_MODE = 2
@@ -391,6 +392,16 @@ k_ppart_dens_w(KnnGrid G, int64_t n, int K, const float4 *__restrict__ sv, float
     }
 }
 
+// the records the cell kernel reads per neighbour: velocities and m / PPART_DENS
+// (the quotient of VVEL_INTERP_SPH_VW's weight, once per particle)
+__global__ void k_mass_over_dens(int64_t n, const float4 *__restrict__ sv, const float *__restrict__ pd_s,
+                                 float4 *__restrict__ svw) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = sv[i];
+    svw[i] = make_float4(a.x, a.y, a.z, __fdiv_rn(a.w, pd_s[i]));
+}
+
 // five blocks per SM (48 registers): the cell kernel gains more from the extra
 // warps than it loses to spills (six blocks at 40 registers spill too much)
 template <int KMAX, bool STATS>
@@ -426,20 +437,22 @@ k_cells_knn_w(KnnGrid G, CellArgs A) {
             }
             continue;
         }
-        for (int j = lane; j < cnt; j += 32)
-            atomic_max_pos(&A.hp_s[S.res_pos[j]], sqrtf(__uint_as_float(S.res_d2[j])));
-        if (!A.do_vel) continue;
+        // HPART(j) = MAX(HPART(j), d), then the weight W(d, H) * m / PPART_DENS
+        // (m / PPART_DENS per particle from k_mass_over_dens: the same quotient)
         for (int j = lane; j < cnt; j += 32) {
             const uint32_t pj = S.res_pos[j];
-            const float4 a = A.sv[pj];
-            float w = kernel_w(A.gauss, hk, sqrtf(__uint_as_float(S.res_d2[j])));
-            w = __fmul_rn(w, __fdiv_rn(a.w, A.pd_s[pj]));
+            const float d = sqrtf(__uint_as_float(S.res_d2[j]));
+            atomic_max_pos(&A.hp_s[pj], d);
+            if (!A.do_vel) continue;
+            const float4 a = A.svw[pj];
+            const float w = __fmul_rn(kernel_w(A.gauss, hk, d), a.w);
             const double w8 = (double)w;
             acc[j] = w8;
             acc[SPH_ROW<KMAX> + j] = w8 * (double)a.x;
             acc[2 * SPH_ROW<KMAX> + j] = w8 * (double)a.y;
             acc[3 * SPH_ROW<KMAX> + j] = w8 * (double)a.z;
         }
+        if (!A.do_vel) continue;
         __syncwarp();
         double sum = 0.0;
         if (lane < 4) sum = seq_sum(acc + lane * SPH_ROW<KMAX>, cnt);
@@ -995,11 +1008,16 @@ static void run_sph_kernels_ws(Ctx &c, const KnnGrid &G, const avism_params *p, 
         AV_CUDA(cudaMemsetAsync(cnt_d, 0, sizeof(int32_t), c.stream));
         CellArgs A;
         A.nx = nx; A.rad_lo = L.g.rad_lo; A.K = K; A.dx = L.g.dx; A.rad = rad_d; A.smask = a.smask;
-        A.sv = sv; A.pd_s = pd_s;
+        A.sv = sv; A.pd_s = pd_s; A.svw = nullptr;
         A.hp_s = hp_s; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
         A.gauss = p->kernel_mode == 2;
         A.ball_list = ball_list; A.ball_count = cnt_d;
-        if (vel_sph) sv_velocities(c);
+        if (vel_sph) {
+            sv_velocities(c);
+            float4 *svw = c.get_t<float4>(B_SVW, std::max<int64_t>(a.n, 1));
+            if (a.n > 0) ++c.launches, k_mass_over_dens<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, sv, pd_s, svw);
+            A.svw = svw;
+        }
         const int64_t nblk = (int64_t)((nx + 3) / 4) * ((nx + 3) / 4) * ((nx + 1) / 2);
         ++c.launches, k_cells_knn_w<KMAX, STATS><<<(unsigned)nblk, SPH_WARPS * 32, sm_cells, c.stream>>>(G, A);
         AV_CUDA(cudaGetLastError());
@@ -1055,7 +1073,7 @@ static void run_sph_kernels(Ctx &c, const KnnGrid &G, const avism_params *p, con
         AV_CUDA(cudaMemsetAsync(cnt_d, 0, sizeof(int32_t), c.stream));
         CellArgs A;
         A.nx = nx; A.rad_lo = L.g.rad_lo; A.K = K; A.dx = L.g.dx; A.rad = rad_d; A.smask = a.smask;
-        A.sv = sv; A.pd_s = pd_s;
+        A.sv = sv; A.pd_s = pd_s; A.svw = nullptr;
         A.hp_s = hp_s; A.u2 = a.u2; A.u3 = a.u3; A.u4 = a.u4; A.do_vel = vel_sph ? 1 : 0;
         A.gauss = p->kernel_mode == 2;
         A.ball_list = ball_list; A.ball_count = cnt_d;
