@@ -63,17 +63,17 @@ static __global__ void k_bin_gather(int64_t n, const uint32_t *__restrict__ keys
         for (int64_t b = cur + 1; b <= nbins; b++) start[b] = n;
 }
 
-// (x, y, z, m) and (vx, vy, vz, 0) as float4 records in input order: the
-// binned gather then fetches two 16-byte records per particle instead of seven
-// scattered 4-byte words (one DRAM sector each)
+// (x, y, z, m) and (vx, vy, vz, 0) side by side as one 32-byte record per
+// particle in input order: the binned gather then fetches one DRAM sector per
+// particle instead of seven scattered 4-byte words
 static __global__ void k_pack_particles(int64_t n, const float *__restrict__ x, const float *__restrict__ y,
                                  const float *__restrict__ z, const float *__restrict__ m,
                                  const float *__restrict__ vx, const float *__restrict__ vy,
-                                 const float *__restrict__ vz, float4 *__restrict__ pa, float4 *__restrict__ pb) {
+                                 const float *__restrict__ vz, float4 *__restrict__ pab) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    pa[i] = make_float4(x[i], y[i], z[i], m[i]);
-    pb[i] = make_float4(vx[i], vy[i], vz[i], 0.0f);
+    pab[2 * i] = make_float4(x[i], y[i], z[i], m[i]);
+    pab[2 * i + 1] = make_float4(vx[i], vy[i], vz[i], 0.0f);
 }
 
 // positions and masses only, for the split form (velocities still in flight)
@@ -100,20 +100,22 @@ static __global__ void k_gather_vel(int64_t n, const float4 *__restrict__ sp, co
     sv[i] = make_float4(b.x, b.y, b.z, sv[i].w);
 }
 
-// k_bin_gather with the attributes from the packed records (pa non-null; pb
-// null: masses only, velocities left 0) and, for FINE keys, the quarter-bin
+// k_bin_gather with the attributes from the packed records (pa non-null: with
+// velocities, 32-byte records (pa[2v], pa[2v + 1]); without, 16-byte (x, y, z,
+// m) records and the velocities left 0) and, for FINE keys, the quarter-bin
 // offsets as well
 template <bool FINE>
 static __global__ void k_bin_gather2(int64_t n, const uint32_t *__restrict__ keys, const int32_t *__restrict__ vals,
                               const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
-                              const float4 *__restrict__ pa, const float4 *__restrict__ pb, float4 *__restrict__ sp,
+                              const float4 *__restrict__ pa, bool with_v, float4 *__restrict__ sp,
                               float4 *__restrict__ sv, int64_t *__restrict__ start, int64_t nbins,
                               int32_t *__restrict__ fstart) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int32_t v = vals[i];
     if (pa) {
-        const float4 a = pa[v], b = pb ? pb[v] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float4 a = with_v ? pa[2 * (int64_t)v] : pa[v];
+        const float4 b = with_v ? pa[2 * (int64_t)v + 1] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         sp[i] = make_float4(a.x, a.y, a.z, __int_as_float(v));
         sv[i] = make_float4(b.x, b.y, b.z, a.w);
     } else {

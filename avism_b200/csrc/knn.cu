@@ -60,10 +60,11 @@ BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y,
     AV_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, (int)n, 0, end_bit, c.stream));
     void *t = c.get(B_CUB_TMP, tmp);
     AV_CUDA(cub::DeviceRadixSort::SortPairs(t, tmp, dk, dv, (int)n, 0, end_bit, c.stream));
-    float4 *pa = nullptr, *pb = nullptr;
+    float4 *pa = nullptr;
+    bool with_v = false;
     if (sv) {
-        pa = c.get_t<float4>(B_PX4, n);
         if (c.attr_pending) {
+            pa = c.get_t<float4>(B_PX4, n);
             // split form: the velocities are still being copied from the host;
             // the records take the masses now and the velocities in
             // sv_velocities(), before their first reader
@@ -77,19 +78,20 @@ BinnedParticles bin_particles(Ctx &c, int64_t n, const float *x, const float *y,
             c.svp.vy = vy;
             c.svp.vz = vz;
         } else {
-            pb = c.get_t<float4>(B_PV4, n);
+            pa = c.get_t<float4>(B_PX4, 2 * (size_t)n);
+            with_v = true;
             c.attrs_ready();
-            ++c.launches, k_pack_particles<<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, y, z, m, vx, vy, vz, pa, pb);
+            ++c.launches, k_pack_particles<<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, y, z, m, vx, vy, vz, pa);
         }
     }
     if (fine) {
         int32_t *fstart = c.get_t<int32_t>(B_FSTART, nkeys + 1);
         bp.fstart = fstart;
         ++c.launches, k_bin_gather2<true><<<grid_for(n, 256), 256, 0, c.stream>>>(
-            n, dk.Current(), dv.Current(), x, y, z, pa, pb, sp, sv, start, nbins, fstart);
+            n, dk.Current(), dv.Current(), x, y, z, pa, with_v, sp, sv, start, nbins, fstart);
     } else {
         ++c.launches, k_bin_gather2<false><<<grid_for(n, 256), 256, 0, c.stream>>>(
-            n, dk.Current(), dv.Current(), x, y, z, pa, pb, sp, sv, start, nbins, nullptr);
+            n, dk.Current(), dv.Current(), x, y, z, pa, with_v, sp, sv, start, nbins, nullptr);
     }
     AV_CUDA(cudaGetLastError());
     return bp;
