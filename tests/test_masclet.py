@@ -224,3 +224,35 @@ def test_oracle_level1_inside_level0_voids(snap):
     assert o1["vf"]["nvoid"] > 0 and o1["cat"]["nvoidt"] > 0
     assert np.all(np.asarray(o1["vf"]["cubes"]["father"]) > 0)
 
+
+def test_patch_reader_rejects_short_files_and_small_capacities(tmp_path, snap):
+    """The level-1 patch reader: a gas file cut inside the first patch's
+    records is an I/O error; capacities below the patch or cell counts are
+    refused before anything is written."""
+    import ctypes as C
+    from avism_b200 import _lib
+    from avism_b200.avism import AvismError, read_masclet_patches
+    grid, gas, dm = mc.write_files(snap, str(tmp_path))
+    ng3 = snap["ng"] ** 3
+    base = (8 + 8) + 10 * (8 + 4 * ng3)            # header + the ten level-0 records
+    with open(gas, "rb") as f:
+        b = f.read()
+    short = str(tmp_path / "gas_short")
+    with open(short, "wb") as f:
+        f.write(b[:base + 100])
+    with pytest.raises(AvismError):
+        read_masclet_patches(grid, short, snap["ng"])
+    lib = _lib.load()
+    npatch, ncells = C.c_int32(), C.c_int64()
+    assert lib.avism_io_masclet_patches_size(grid.encode(), C.byref(npatch), C.byref(ncells)) == 0
+    want = mc.amr(snap)
+    assert npatch.value == len(want["nx"]) and ncells.value == len(want["u11g"])
+    arrs = [np.zeros(16, np.int32) for _ in range(6)] + [np.zeros(16, np.float32) for _ in range(3)] + \
+        [np.zeros(17, np.int64)] + [np.zeros(ncells.value, np.float32) for _ in range(4)]
+    ptrs = [a.ctypes.data_as(C.c_void_p) for a in arrs]
+    args = (grid.encode(), gas.encode(), snap["ng"])
+    assert lib.avism_io_read_masclet_patches(*args, npatch.value - 1, ncells.value, *ptrs) != 0
+    assert lib.avism_io_read_masclet_patches(*args, npatch.value, ncells.value - 1, *ptrs) != 0
+    assert lib.avism_io_read_masclet_patches(*args, npatch.value, ncells.value, *ptrs) == 0
+    assert np.array_equal(arrs[-4], want["u11g"])
+
