@@ -8,6 +8,7 @@ as a test failure.  Run from the repository root:
 
     python tests/golden/make_golden.py            # the small fixtures
     python tests/golden/make_golden.py config2    # the 256^3 digests (minutes)
+    python tests/golden/make_golden.py masclet    # the MASCLET snapshot's levels 0 and 1
 """
 import os
 import sys
@@ -102,7 +103,44 @@ def config2_case():
     return out
 
 
+MASCLET_CAT = ("indice", "uvoid", "ncellv", "volnew", "req", "gxc", "gyc", "gzc", "eps", "ip", "umean", "mtot")
+
+
+def masclet_case():
+    """The seeded MASCLET snapshot of tests/masclet_case.py (32^3 gas, DM
+    particles on three levels, four level-1 patches): level 0 with FLAG_DENS =
+    0 (DM + gas) and FLAG_DIV = -1 (linear theory), and level 1 inside the
+    level-0 voids with FLAG_DENS = 0 and FLAG_DIV = 2 (the patches' gas
+    divergence); field digests, cubes and catalogue columns."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    import masclet_case as mc
+    s = mc.snapshot()
+    ng = s["ng"]
+    out = {}
+    p0 = Params(nx=ng, periodic=1, lado0=s["box"], level=0, levmin=0, flag_dens=0, flag_div=-1)
+    r0 = O.run_level_masclet(p0, ng, mc.gas(s), mc.particles(s))
+    mp, rq = O.next_level(p0, r0["vf"]["nvoid"], r0["cat"]["marca"], r0["cat"]["uvoid"], r0["cat"]["req"])
+    p1 = Params(nx=2 * ng, periodic=1, lado0=s["box"], level=1, levmin=0, flag_dens=0, flag_div=2)
+    r1 = O.run_sublevel_masclet(p1, ng, mc.gas(s), mp, rq, mc.particles(s), mc.amr(s))
+    for tag, r in (("l0", r0), ("l1", r1)):
+        out[f"{tag}_u1co"] = np.array(digest(r["u1co"]))
+        out[f"{tag}_diverco"] = np.array(digest(r["diverco"]))
+        out[f"{tag}_meandens"] = np.float32(r["meandens"])
+        out[f"{tag}_nvoid"] = np.int32(r["vf"]["nvoid"])
+        out[f"{tag}_cubes"] = np.array(digest(np.concatenate([np.asarray(r["vf"]["cubes"][k]).view(np.int32)
+                                                              for k in sorted(r["vf"]["cubes"])])))
+        for k in MASCLET_CAT:
+            out[f"{tag}_cat_{k}"] = np.asarray(r["cat"][k])
+        out[f"{tag}_nvoidt"] = np.int32(r["cat"]["nvoidt"])
+        print(tag, r["vf"]["nvoid"], r["cat"]["nvoidt"], flush=True)
+    return out
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "masclet":
+        np.savez_compressed(os.path.join(HERE, "masclet32.npz"), **masclet_case())
+        print("written")
+        sys.exit(0)
     if len(sys.argv) > 1 and sys.argv[1] == "config2":
         np.savez_compressed(os.path.join(HERE, "config2_256.npz"), **config2_case())
         print("written")

@@ -39,6 +39,19 @@ def test_oracle_reproduces_level_fixture():
         assert np.array_equal(r["grid"]["u_mass"], gold[f"p{per}_u_mass"])
 
 
+def test_oracle_reproduces_masclet_fixture():
+    """The MASCLET snapshot's level 0 and its level 1 from the patches inside
+    the level-0 voids (tests/golden/masclet32.npz)."""
+    import sys
+    sys.path.insert(0, GOLD)
+    import make_golden as mg
+    gold = _load("masclet32.npz")
+    got = mg.masclet_case()
+    assert set(got) == set(gold)
+    for k, v in got.items():
+        assert np.array_equal(np.asarray(v), gold[k]), k
+
+
 def test_oracle_reproduces_knn_and_indexx_fixtures():
     g = _load("knn_3000.npz")
     for L, tag in ((50.0, "per"), (0.0, "open")):
