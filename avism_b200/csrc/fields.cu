@@ -572,6 +572,18 @@ static void amr_level1(Ctx &c, const Level &L, const avism_params *p, int nhy, c
     p0.nx = nhy;
     const Level L0 = make_level(&p0);
     const float dx0 = L0.g.dx, dxr_div = dx0 / 2.0f, dxr = L.g.dx, rx1 = L.rad_at(1);
+    // IXR1 = INT(((PATCHRX - 0.5*DXR) - RX1)/DXR + 0.5) (src/amr2uniform.f90:170-172),
+    // every corner checked before the first launch: a value beyond int is refused
+    std::vector<int> r1(3 * (size_t)a.npatch);
+    for (int q = 0; q < a.npatch; q++) {
+        const float rc[3] = {a.rx[q], a.ry[q], a.rz[q]};
+        for (int ax = 0; ax < 3; ax++) {
+            const float f = (((rc[ax] - 0.5f * dxr) - rx1) / dxr) + 0.5f;
+            AV_CHECK(std::isfinite(f) && std::fabs(f) < 1.0e9f, AVISM_ERR_ARG,
+                     "MASCLET level 1: a patch corner lies far outside the level grid");
+            r1[3 * (size_t)q + ax] = (int)f;
+        }
+    }
     float *d0 = c.get_t<float>(B_DIVER2, n0);
     AV_CUDA(cudaMemsetAsync(d0, 0, sizeof(float) * (size_t)n0, c.stream));
     if (nh > 2)
@@ -597,10 +609,7 @@ static void amr_level1(Ctx &c, const Level &L, const avism_params *p, int nhy, c
         if (np <= 0) continue;
         ++c.launches, k_patch_div<<<grid_for(np, 256), 256, 0, c.stream>>>(P, nh, dxr_div, dx0, a.u12g, a.u13g, a.u14g,
                                                                           gas[1], gas[2], gas[3], dv, err);
-        // IXR1 = INT(((PATCHRX - 0.5*DXR) - RX1)/DXR + 0.5) (src/amr2uniform.f90:170-172)
-        const int xr1 = (int)((((a.rx[q] - 0.5f * dxr) - rx1) / dxr) + 0.5f);
-        const int yr1 = (int)((((a.ry[q] - 0.5f * dxr) - rx1) / dxr) + 0.5f);
-        const int zr1 = (int)((((a.rz[q] - 0.5f * dxr) - rx1) / dxr) + 0.5f);
+        const int xr1 = r1[3 * (size_t)q], yr1 = r1[3 * (size_t)q + 1], zr1 = r1[3 * (size_t)q + 2];
         ++c.launches, k_vmesh_add<<<grid_for(np, 256), 256, 0, c.stream>>>(P, nx, nh, xr1, yr1, zr1, a.u11g, dv,
                                                                           flagamr, ugr, divr, flagr, err);
     }

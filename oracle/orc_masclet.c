@@ -86,6 +86,14 @@ static int amr_level1(const avism_params *p, int nhy, const float *u1g, const fl
     uint8_t *flagr = (uint8_t *)calloc((size_t)n0, 1);
     for (int64_t c = 0; c < nc; c++) { flagamr[c] = 1; ugr[c] = 0.0f; divr[c] = 0.0f; }
     int st = AVISM_OK;
+    /* the corners' level-grid offsets must fit an int before the truncation */
+    for (int ip = 0; ip < a->npatch && !st; ip++) {
+        const float rc[3] = {a->rx[ip], a->ry[ip], a->rz[ip]};
+        for (int ax = 0; ax < 3; ax++) {
+            const float f = (((rc[ax] - 0.5f * dxr) - rx1) / dxr) + 0.5f;
+            if (!isfinite(f) || fabsf(f) >= 1.0e9f) st = AVISM_ERR_ARG;
+        }
+    }
     for (int ip = 0; ip < a->npatch && !st; ip++) {
         const int n1 = a->nx[ip], n2 = a->ny[ip], n3 = a->nz[ip];
         const int l1 = a->ix[ip], l2 = a->iy[ip], l3 = a->iz[ip];

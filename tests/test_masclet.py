@@ -183,7 +183,7 @@ def test_oracle_level1_without_patches_is_the_base_grid(snap):
     assert np.array_equal(_inner(p, dve), divr)
 
 
-@pytest.mark.parametrize("bad", ["rim", "vmesh", "offset"])
+@pytest.mark.parametrize("bad", ["rim", "vmesh", "offset", "nan", "huge"])
 def test_oracle_level1_rejects_patches_outside(snap, bad):
     ng = snap["ng"]
     p = Params(nx=2 * ng, periodic=1, lado0=snap["box"], level=1, levmin=1, flag_dens=2, flag_div=2)
@@ -192,8 +192,12 @@ def test_oracle_level1_rejects_patches_outside(snap, bad):
         a["ix"][0] = 1                              # the rim's parent differences need U2G(0)
     elif bad == "vmesh":
         a["rz"][2] = a["rz"][2] + np.float32(40 * 2.0)    # the patch lands beyond the level grid
-    else:
+    elif bad == "offset":
         a["offset"][1] += 1
+    elif bad == "nan":
+        a["rx"][1] = np.float32(np.nan)                 # INT() of it is undefined
+    else:
+        a["ry"][0] = np.float32(1e30)
     with pytest.raises(O.OracleError):
         O.masclet_fields(p, ng, mc.gas(snap), None, a)
 
