@@ -85,7 +85,7 @@ def test_level1_from_files(gpu, snap, tmp_path):
         assert np.array_equal(a["cat"][k], o["cat"][k]), k
 
 
-@pytest.mark.parametrize("bad", ["rim", "vmesh", "missing"])
+@pytest.mark.parametrize("bad", ["rim", "vmesh", "missing", "nan"])
 def test_level1_refuses_patches_outside(gpu, snap, bad):
     """A patch whose rim needs base differences outside 2..NHY-1, or whose cells
     land outside the level grid, is refused (the kernels check every index
@@ -97,6 +97,8 @@ def test_level1_refuses_patches_outside(gpu, snap, bad):
         a["ix"][0] = 1
     elif bad == "vmesh":
         a["rz"][2] = a["rz"][2] + np.float32(80.0)
+    elif bad == "nan":
+        a["rx"][1] = np.float32(np.nan)             # refused on the host, before any launch
     else:
         a = None
     with pytest.raises(AvismError):
