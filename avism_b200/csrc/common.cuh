@@ -185,11 +185,13 @@ struct Ctx {
         attr_pending = false;
         AV_CUDA(cudaStreamWaitEvent(stream, ev_attr, 0));
     }
-    // the caller's host arrays must not be read after a failed call returns
+    // the caller's host arrays must not be read after a failed call returns:
+    // both streams are drained (their copies may still be queued)
     void drop_pending_copies() {
         mass_pending = attr_pending = false;
         svp = SvPending{};
         cudaStreamSynchronize(copy_stream);
+        cudaStreamSynchronize(stream);
     }
 };
 
