@@ -835,8 +835,8 @@ AmrPatches amr_patches(Ctx &c, const avism_patches *a) {
     host_i64(r.offset, a->offset, np + 1);
     AV_CHECK(r.offset[0] >= 0, AVISM_ERR_ARG, "MASCLET level 1: negative patch offset");
     for (size_t q = 0; q < np; q++)
-        AV_CHECK(r.nx[q] >= 1 && r.ny[q] >= 1 && r.nz[q] >= 1 &&
-                     r.offset[q + 1] - r.offset[q] == (int64_t)r.nx[q] * r.ny[q] * r.nz[q],
+        AV_CHECK(r.nx[q] >= 1 && r.ny[q] >= 1 && r.nz[q] >= 1 && r.nx[q] <= (1 << 20) && r.ny[q] <= (1 << 20) &&
+                     r.nz[q] <= (1 << 20) && r.offset[q + 1] - r.offset[q] == (int64_t)r.nx[q] * r.ny[q] * r.nz[q],
                  AVISM_ERR_ARG, "MASCLET level 1: patch sizes and offsets disagree");
     if (r.offset[np] == 0) return r;                    // no patches: no cells to read
     const size_t cells = sizeof(float) * (size_t)r.offset[np];

@@ -292,7 +292,8 @@ int avism_io_masclet_patches_size(const char *grid_path, int32_t *npatch, int64_
     const int64_t np = g.nl >= 1 ? g.npatch[1] : 0;
     int64_t cells = 0;
     for (int64_t i = 0; i < np; i++) {
-        if (g.pn[0][i] < 1 || g.pn[1][i] < 1 || g.pn[2][i] < 1) return AVISM_ERR_IO;
+        for (int a = 0; a < 3; a++)
+            if (g.pn[a][i] < 1 || g.pn[a][i] > (1 << 20)) return AVISM_ERR_IO;   // a patch edge of 2^20 cells at most
         cells += (int64_t)g.pn[0][i] * g.pn[1][i] * g.pn[2][i];
     }
     if (npatch) *npatch = (int32_t)np;

@@ -196,7 +196,8 @@ int orc_masclet_fields(const avism_params *p, int32_t nhy, const float *u1g, con
     if (p->level == 1) {
         if (amr->npatch < 0 || !amr->offset || amr->offset[0] < 0) return AVISM_ERR_ARG;
         for (int q = 0; q < amr->npatch; q++)
-            if (amr->nx[q] < 1 || amr->ny[q] < 1 || amr->nz[q] < 1 ||
+            if (amr->nx[q] < 1 || amr->ny[q] < 1 || amr->nz[q] < 1 || amr->nx[q] > (1 << 20) ||
+                amr->ny[q] > (1 << 20) || amr->nz[q] > (1 << 20) ||
                 amr->offset[q + 1] - amr->offset[q] != (int64_t)amr->nx[q] * amr->ny[q] * amr->nz[q])
                 return AVISM_ERR_ARG;
     }

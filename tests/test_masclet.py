@@ -183,7 +183,7 @@ def test_oracle_level1_without_patches_is_the_base_grid(snap):
     assert np.array_equal(_inner(p, dve), divr)
 
 
-@pytest.mark.parametrize("bad", ["rim", "vmesh", "offset", "nan", "huge"])
+@pytest.mark.parametrize("bad", ["rim", "vmesh", "offset", "nan", "huge", "edge"])
 def test_oracle_level1_rejects_patches_outside(snap, bad):
     ng = snap["ng"]
     p = Params(nx=2 * ng, periodic=1, lado0=snap["box"], level=1, levmin=1, flag_dens=2, flag_div=2)
@@ -196,8 +196,10 @@ def test_oracle_level1_rejects_patches_outside(snap, bad):
         a["offset"][1] += 1
     elif bad == "nan":
         a["rx"][1] = np.float32(np.nan)                 # INT() of it is undefined
-    else:
+    elif bad == "huge":
         a["ry"][0] = np.float32(1e30)
+    else:
+        a["nx"][0] = np.int32(2 ** 21)                  # a size product beyond any grid
     with pytest.raises(O.OracleError):
         O.masclet_fields(p, ng, mc.gas(snap), None, a)
 
